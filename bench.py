@@ -1,0 +1,400 @@
+#!/usr/bin/env python3
+"""Headline benchmark: FCG + BCMG (suitor matching, pairwise aggregation AMG) set-up + solve to
+relative residual 1e-8 on the 27-point 3D Poisson problem on 160^3 (4,096,000 rows,
+109,215,352 non-zeros, FP64 CSR; x* uniform[-1,1] from numpy default_rng(1), b = A x*).
+
+One step = hierarchy set-up + FCG solve with the FP32 V-cycle inside FP64 FCG, inputs resident
+in HBM. The same step with the plain FP64 V-cycle, the fine-level SpMV bandwidth, per-kernel
+roofline figures, the end-to-end time through the C ABI with host buffers, and a CPU baseline
+(the OpenMP restatement of the same method, on this host's cores) are reported beside it.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+Multi-GPU (torchrun, one process per GPU): each rank solves its own copy of the system
+(independent replicas, no collective on the data path); time = max over ranks.
+--impl reference times the reference algorithm's CPU restatement (oracle/, OpenMP) on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FCG+AMG setup+solve s to rel-res 1e-8, FP32-Vcycle vs FP64; SpMV HBM GB/s"
+WORKLOADS = {
+    "poisson27_160": {"stencil": 27, "grid": (160, 160, 160), "seed": 1,
+                      "text": "3D Poisson 27-point 160^3 Dirichlet (diag 26, off -1), FP64 CSR"},
+    "poisson7_50": {"stencil": 7, "grid": (50, 50, 50), "seed": 0,
+                    "text": "3D Poisson 7-point 50^3 Dirichlet (diag 6, off -1), FP64 CSR"},
+    "poisson27_100": {"stencil": 27, "grid": (100, 100, 100), "seed": 1,
+                      "text": "3D Poisson 27-point 100^3 Dirichlet, FP64 CSR"},
+}
+RTOL = 1e-8
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+
+def read_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return PEAKS_FALLBACK["hbm_gbs"], "fallback"
+
+
+def build_problem(wl):
+    import scipy.sparse as sp
+    import bootcmatchgx_b200 as bx
+    st, (nx, ny, nz), seed = wl["stencil"], wl["grid"], wl["seed"]
+    row, col, val = bx.laplacian_3d(st, nx, ny, nz)
+    n = row.size - 1
+    xs = np.random.default_rng(seed).uniform(-1.0, 1.0, n)
+    b = sp.csr_matrix((val, col, row), shape=(n, n)) @ xs
+    return row, col, val, xs, b
+
+
+# ---------------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [l.strip().split(", ") for l in self.f.read().splitlines() if l.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------------
+def cpu_baseline(wl, row, col, val, b, xs, max_seconds=30.0):
+    """The oracle (OpenMP C++ restatement of the same FCG+BCMG method) on this host: full
+    set-up, then FCG iterations until convergence or until the time budget; the solve time is
+    scaled to the iteration count of a converged run when the budget cuts it short."""
+    from oracle import pyoracle as O
+    cores = os.cpu_count() or 1
+    O.num_threads(cores)
+    A = O.Matrix.from_csr(row, col, val)
+    t0 = time.perf_counter()
+    H = O.Hierarchy(A, O.params(rtol=RTOL))
+    t_setup = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    x, info = H.solve(b)
+    t_solve = time.perf_counter() - t0
+    return {"value": t_setup + t_solve, "unit": "s", "cores": cores, "kind": "port",
+            "sample": f"full set-up + full FCG solve ({info['niter']} iterations) of the same "
+                      f"workload with oracle/bcmgx_oracle.cpp, OMP threads={cores}",
+            "setup_s": t_setup, "solve_s": t_solve, "niter": info["niter"],
+            "err_vs_xstar": float(np.linalg.norm(x - xs) / np.linalg.norm(xs))}
+
+
+def reference_arm(a, wl, rank, world):
+    """--impl reference: the reference algorithm on the host cores (the reference itself has no
+    CPU implementation and its CUDA build needs MPI; the oracle port stands in)."""
+    if rank != 0:
+        return None
+    from oracle import pyoracle as O
+    row, col, val, xs, b = build_problem(wl)
+    cores = os.cpu_count() or 1
+    O.num_threads(cores)
+    A = O.Matrix.from_csr(row, col, val)
+    times, niter = [], None
+    budget = 240.0
+    t_start = time.perf_counter()
+    for step in range(a.warmup + a.steps):
+        full = step == 0 or (time.perf_counter() - t_start) < budget / 2
+        t0 = time.perf_counter()
+        H = O.Hierarchy(A, O.params(rtol=RTOL, itnlim=2000 if (full or niter is None) else 3))
+        t1 = time.perf_counter()
+        x, info = H.solve(b)
+        t2 = time.perf_counter()
+        if info["retv"] == 0:
+            niter = info["niter"]
+            total = t2 - t0
+        else:   # bounded sample: set-up + 3 iterations, solve scaled to the converged count
+            total = (t1 - t0) + (t2 - t1) / info["niter"] * niter
+        if step >= a.warmup:
+            times.append(total)
+        del H
+    v = float(np.mean(times))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": a.workload, "problem": wl["text"], "rtol": RTOL,
+                       "rows": int(row.size - 1), "nnz": int(col.size)},
+            "cpu_baseline": {"value": v, "unit": "s", "cores": cores, "kind": "port",
+                             "sample": "oracle/bcmgx_oracle.cpp (OpenMP restatement of FCG+BCMG): "
+                                       "set-up + FCG to 1e-8 per step; when the time budget is "
+                                       "spent a step is set-up + 3 iterations scaled to the "
+                                       f"converged count ({niter})"},
+            "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    return line
+
+
+# ---------------------------------------------------------------------------------------------
+def run_ours(a, wl, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    import bootcmatchgx_b200 as bx
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    row, col, val, xs, b = build_problem(wl)
+    n, nnz = row.size - 1, col.size
+    d_row = torch.from_numpy(row).to(dev)
+    d_col = torch.from_numpy(col).to(dev)
+    d_val = torch.from_numpy(val).to(dev)
+    d_b = torch.from_numpy(b).to(dev)
+    d_x = torch.zeros(n, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    launches0 = bx.lib().bcmgx_launch_count()
+
+    def params(prec, **kw):
+        return bx.params_default(solver="FCG", preconditioner="BCMG", rtol=RTOL, dispnorm=0,
+                                 vcycle_precision=prec, stream=stream.cuda_stream, **kw)
+
+    def step(prec, keep=False):
+        h = bx.Hierarchy(d_row, d_col, d_val, params(prec))
+        d_x.zero_()
+        _, info = h.solve(d_b, d_x)
+        inf = h.info()
+        if keep:
+            return h, info, inf
+        h.free()
+        return None, info, inf
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def timed(prec, steps):
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0 = bx.lib().bcmgx_launch_count()
+        e0.record(stream)
+        infos = []
+        for _ in range(steps):
+            infos.append(step(prec)[1:])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1) / steps
+        launches = (bx.lib().bcmgx_launch_count() - c0) / steps
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, infos, launches
+
+    # ---- headline: FP32 V-cycle inside FP64 FCG
+    for _ in range(a.warmup):
+        step("FP32")
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    ms32, infos32, launches32 = timed("FP32", a.steps)
+    clk = clocks.stop()
+    x32 = d_x.cpu().numpy().copy()
+    # ---- plain FP64 form (same step, FP64 V-cycle)
+    k64 = max(1, min(a.steps, 3))
+    step("FP64")
+    ms64, infos64, _ = timed("FP64", k64)
+    x64 = d_x.cpu().numpy().copy()
+    # ---- tight FP64 oracle solution (rtol 1e-12) for the error statements
+    h_t = bx.Hierarchy(d_row, d_col, d_val, params("FP64", rtol=1e-12))
+    d_x.zero_()
+    h_t.solve(d_b, d_x)
+    xt = d_x.cpu().numpy().copy()
+    h_t.free()
+
+    # ---- kernel figures on kept hierarchies (same stream, CUDA events)
+    h32, _, inf32 = step("FP32", keep=True)
+    k32 = h32.time_kernels(0, reps=20)
+    h64, _, inf64 = step("FP64", keep=True)
+    k64f = h64.time_kernels(0, reps=20)
+    spmv_ms = k64f["spmv"]
+    lvl = [h32.time_kernels(l, reps=10) for l in range(1, inf32["num_levels"])]
+    h32.free()
+    h64.free()
+    peak, peak_kind = read_peaks()
+    bytes_spmv = 12 * nnz + 4 * (n + 1) + 16 * n
+    bytes_jac32 = 8 * nnz + 4 * (n + 1) + 16 * n
+    bytes_jac64 = 12 * nnz + 4 * (n + 1) + 32 * n
+    gbs_spmv = bytes_spmv / (spmv_ms * 1e-3) / 1e9
+    gbs_jac32 = bytes_jac32 / (k32["jacobi"] * 1e-3) / 1e9
+    gbs_jac64 = bytes_jac64 / (k64f["jacobi"] * 1e-3) / 1e9
+
+    # ---- end to end through the C ABI with host buffers (pinned), FP32 V-cycle
+    p_row = torch.from_numpy(row).pin_memory()
+    p_col = torch.from_numpy(col).pin_memory()
+    p_val = torch.from_numpy(val).pin_memory()
+    p_b = torch.from_numpy(b).pin_memory()
+    p_x = torch.zeros(n, dtype=torch.float64).pin_memory()
+    ke = max(1, min(a.steps, 3))
+
+    def e2e_step():
+        h = bx.Hierarchy(p_row.numpy(), p_col.numpy(), p_val.numpy(), params("FP32"))
+        p_x.zero_()
+        xh, info = h.solve(p_b.numpy(), p_x.numpy())
+        h.free()
+        return xh, info
+
+    e2e_step()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(ke):
+        xh, _ = e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - t0) / ke
+    e2e_ms = max(e0.elapsed_time(e1) / ke, wall * 1e3)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+
+    if rank != 0:
+        return None
+    setup32 = float(np.mean([i[1]["setup_ms"] for i in infos32]))
+    solve32 = float(np.mean([i[0]["solve_ms"] for i in infos32]))
+    setup64 = float(np.mean([i[1]["setup_ms"] for i in infos64]))
+    solve64 = float(np.mean([i[0]["solve_ms"] for i in infos64]))
+    nrm = np.linalg.norm
+    line = {
+        "metric": METRIC, "value": ms32 / 1e3, "unit": "s", "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms32, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 outer FCG / f32 V-cycle", "data": "synthetic",
+        "config": {"workload": a.workload, "problem": wl["text"], "rows": int(n), "nnz": int(nnz),
+                   "rhs": f"b = A x*, x* ~ U[-1,1] (numpy default_rng({wl['seed']}))",
+                   "rtol": RTOL, "settings": "FCG_BCMG.properties defaults (aggrsweeps 2, 4+4 l1-Jacobi, "
+                   "20 coarse sweeps, V-cycle)", "vcycle": "fp32",
+                   "l2": "inputs larger than L2 (CSR 1.39 GB)" if nnz > 5e7 else "inputs fit in L2",
+                   "parallelism": f"replicas x{world} (one independent system per GPU)"},
+        "breakdown": {"setup_ms": setup32, "solve_ms": solve32, "niter": infos32[-1][0]["niter"],
+                      "levels": inf32["n"], "level_nnz": inf32["nnz"], "op_cmplx": inf32["op_cmplx"]},
+        "fp64": {"value": ms64 / 1e3, "setup_ms": setup64, "solve_ms": solve64,
+                 "niter": infos64[-1][0]["niter"]},
+        "fp32_speedup_vs_fp64": ms64 / ms32,
+        "errors": {"fp32_vs_xstar": float(nrm(x32 - xs) / nrm(xs)), "fp64_vs_xstar": float(nrm(x64 - xs) / nrm(xs)),
+                   "fp32_vs_fp64_tight": float(nrm(x32 - xt) / nrm(xt)),
+                   "fp64_vs_fp64_tight": float(nrm(x64 - xt) / nrm(xt)),
+                   "fp32_rel_residual": float(nrm(b - _spmv(row, col, val, x32)) / nrm(b))},
+        "spmv": {"gbs": gbs_spmv, "ms": spmv_ms, "bytes": bytes_spmv, "frac_of_peak": gbs_spmv / peak,
+                 "frac_of_8TBs_nominal": gbs_spmv / 8000.0},
+        "kernels_level0": {"fp32_jacobi_ms": k32["jacobi"], "fp32_jacobi_gbs": gbs_jac32,
+                           "fp32_residual_ms": k32["residual"], "fp64_jacobi_ms": k64f["jacobi"],
+                           "fp64_jacobi_gbs": gbs_jac64, "fcg_spmv_dots_ms": k64f["fcg_spmv_dots"]},
+        "kernels_coarse_levels_fp32_jacobi_ms": [round(k["jacobi"], 4) for k in lvl],
+        "roofline": {"kernel": "k_rowop<16,OP_JACOBI,float> (FP32 l1-Jacobi sweep, level 0)",
+                     "bound": "hbm", "achieved": gbs_jac32, "peak": peak, "unit": "GB/s",
+                     "frac": gbs_jac32 / peak, "peak_kind": f"{peak_kind} hbm_gbs (copy)",
+                     "bytes_per_launch": bytes_jac32, "traffic": TRAFFIC.get(a.workload)},
+        "gpu_launches": int(round(launches32)),
+        "e2e": {"value": e2e_ms / 1e3, "unit": "s", "h2d_bytes_per_step": int(row.nbytes + col.nbytes + val.nbytes + b.nbytes),
+                "d2h_bytes_per_step": int(n * 8), "path": "bcmgx_setup(host CSR) + bcmgx_solve(host b, x), pinned"},
+    }
+    if clk:
+        line["clocks"] = clk
+    return line
+
+
+# dram bytes (read + write) of one level-0 FP32 Jacobi launch from the committed ncu capture
+# (profiles/jacobi_fp32_poisson27.md); None until measured.
+TRAFFIC = {}
+
+
+def _spmv(row, col, val, x):
+    import scipy.sparse as sp
+    n = row.size - 1
+    return sp.csr_matrix((val, col, row), shape=(n, n)) @ x
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="poisson27_160", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    a = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    wl = WORKLOADS[a.workload]
+    if a.impl == "reference":
+        line = reference_arm(a, wl, rank, world)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    line = run_ours(a, wl, rank, world, local_rank)
+    if rank == 0 and line is not None:
+        if world == 1 and not a.no_cpu_baseline:
+            row, col, val, xs, b = build_problem(wl)
+            line["cpu_baseline"] = cpu_baseline(wl, row, col, val, b, xs)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,303 @@
+"""Host-side interface of the B200 BCMG/FCG path, mirroring the reference's operator API.
+
+Reference entry points and their counterparts here:
+  Params::initFromPropertiesFile (BCMGX/src/config/Params.cu:330)  -> init_from_properties_file
+  Params::initFromFile (Params.cu:406)                            -> init_from_file
+  prec_setup (BCMGX/src/preconditioner/prec_setup.cu:5)           -> prec_setup -> Hierarchy
+  solve (BCMGX/src/solver/solve.cu:11)                            -> solve / Hierarchy.solve
+  prec_apply (BCMGX/src/preconditioner/prec_apply.cu:6)           -> Hierarchy.prec_apply
+  prec_finalize (BCMGX/src/preconditioner/prec_finalize.cu:8)     -> prec_finalize / Hierarchy.free
+  generate_lap3d_local_matrix / generate_lap_local_matrix
+  (BCMGX/src/utility/input.cu:85-138)                             -> laplacian_3d, laplacian
+  read_matrix_from_file (BCMGX/src/datastruct/CSR.cu:1944)        -> read_matrix_market
+Host arrays are numpy; device arrays are CUDA torch tensors (pointers are passed through).
+All work runs in libbcmgx.so; errors raise BcmgxError with the library's status code.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import BcmgxError, check, lib
+
+SOLVERS = {"CGHS": 0, "FCG": 1, "CGS": 2, "PIPELINED_CGS": 3, "CGS_CUBLAS": 4, "INVALID": 5}
+PRECONDITIONERS = {"NONE": 0, "L1_JACOBI": 1, "BCMG": 2, "AFSAI": 3, "INVALID": 4}
+BOOTSTRAP = {"MULTIPLICATIVE": 0, "SYMMETRIZED_MULTIPLICATIVE": 1, "ADDITIVE": 2, "INVALID": 3}
+CYCLES = {"V_CYCLE": 0, "H_CYCLE": 1, "W_CYCLE": 2, "VARIABLE_V_CYCLE": 3, "INVALID": 4}
+VCYCLE = {"FP64": 0, "FP32": 1}
+_ENUMS = {"solver": SOLVERS, "preconditioner": PRECONDITIONERS, "bootstrap_type": BOOTSTRAP,
+          "cycle_type": CYCLES, "vcycle_precision": VCYCLE}
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return C.c_void_p(a.data_ptr())
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _is_device(a):
+    return hasattr(a, "is_cuda") and a.is_cuda
+
+
+def params_default(**overrides) -> L.Params:
+    """Defaults of struct params (BCMGX/src/config/Params.h:238-291), then overrides."""
+    p = L.Params()
+    check(lib().bcmgx_params_default(C.byref(p)), "bcmgx_params_default")
+    return set_params(p, **overrides)
+
+
+def set_params(p: L.Params, **kw) -> L.Params:
+    for k, v in kw.items():
+        if k in _ENUMS and isinstance(v, str):
+            v = _ENUMS[k][v]
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+def init_from_properties_file(path, **overrides) -> L.Params:
+    p = L.Params()
+    check(lib().bcmgx_params_from_properties(str(path).encode(), C.byref(p)), "reading settings")
+    return set_params(p, **overrides)
+
+
+def init_from_file(path, **overrides) -> L.Params:
+    p = L.Params()
+    check(lib().bcmgx_params_from_legacy_file(str(path).encode(), C.byref(p)), "reading settings")
+    return set_params(p, **overrides)
+
+
+def params_to_dict(p: L.Params) -> dict:
+    return {name: getattr(p, name) for name, _ in L.Params._fields_ if name != "stream"}
+
+
+# ---------------------------------------------------------------------------------------------
+# input generation
+# ---------------------------------------------------------------------------------------------
+def laplacian_3d_size(stencil, nx, ny, nz, P=1, Q=1, R=1):
+    n, z = C.c_int64(), C.c_int64()
+    check(lib().bcmgx_laplacian_3d_size(stencil, nx, ny, nz, P, Q, R, C.byref(n), C.byref(z)),
+          "bcmgx_laplacian_3d_size")
+    return n.value, z.value
+
+
+def laplacian_3d(stencil, nx, ny, nz, P=1, Q=1, R=1):
+    """(row, col, val) of the 7p/27p Laplacian in the reference's global row order."""
+    n, z = laplacian_3d_size(stencil, nx, ny, nz, P, Q, R)
+    row = np.empty(n + 1, np.int32)
+    col = np.empty(z, np.int32)
+    val = np.empty(z, np.float64)
+    check(lib().bcmgx_laplacian_3d(stencil, nx, ny, nz, P, Q, R, _ptr(row), _ptr(col), _ptr(val)),
+          "bcmgx_laplacian_3d")
+    return row, col, val
+
+
+def laplacian(n):
+    """The -a n matrix (generateLocalLaplacian3D): 7-point on n^3, lexicographic."""
+    return laplacian_3d(7, n, n, n)
+
+
+def read_laplacian_cfg(path):
+    out = (C.c_int * 6)()
+    check(lib().bcmgx_read_laplacian_cfg(str(path).encode(), out), "reading the laplacian file")
+    return dict(zip(("nx", "ny", "nz", "P", "Q", "R"), list(out)))
+
+
+def read_matrix_market(path):
+    n, m, z = C.c_int(), C.c_int(), C.c_int64()
+    r, c, v = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    check(lib().bcmgx_read_matrix_market(str(path).encode(), C.byref(n), C.byref(m), C.byref(z),
+                                         C.byref(r), C.byref(c), C.byref(v)), "reading the matrix")
+    try:
+        row = np.ctypeslib.as_array((C.c_int * (n.value + 1)).from_address(r.value)).copy()
+        col = np.ctypeslib.as_array((C.c_int * max(z.value, 1)).from_address(c.value))[: z.value].copy()
+        val = np.ctypeslib.as_array((C.c_double * max(z.value, 1)).from_address(v.value))[: z.value].copy()
+    finally:
+        for p in (r, c, v):
+            lib().bcmgx_host_free(p)
+    return row, col, val
+
+
+def diffusion_7p(nx, ny, nz, kappa):
+    kappa = np.ascontiguousarray(kappa, dtype=np.float64).reshape(-1)
+    n, z = laplacian_3d_size(7, nx, ny, nz)
+    if kappa.size != n:
+        raise ValueError("kappa must have nx*ny*nz entries")
+    row = np.empty(n + 1, np.int32)
+    col = np.empty(z, np.int32)
+    val = np.empty(z, np.float64)
+    check(lib().bcmgx_diffusion_7p(nx, ny, nz, _ptr(kappa), _ptr(row), _ptr(col), _ptr(val)),
+          "bcmgx_diffusion_7p")
+    return row, col, val
+
+
+# ---------------------------------------------------------------------------------------------
+# set-up / solve / finalize
+# ---------------------------------------------------------------------------------------------
+class Hierarchy:
+    """The BCMG hierarchy of one matrix (what prec_setup builds into cgsprec)."""
+
+    def __init__(self, row, col, val, params: L.Params):
+        dev = _is_device(row)
+        if not dev:
+            row = np.ascontiguousarray(row, dtype=np.int32)
+            col = np.ascontiguousarray(col, dtype=np.int32)
+            val = np.ascontiguousarray(val, dtype=np.float64)
+        n = int(row.shape[0]) - 1
+        self._keep = (row, col, val)
+        A = L.Csr(n, n, int(col.shape[0]), _ptr(row), _ptr(col), _ptr(val), 1 if dev else 0)
+        h = C.c_void_p()
+        check(lib().bcmgx_setup(C.byref(A), C.byref(params), C.byref(h)), "prec_setup")
+        self.h = h
+        self.n = n
+        self.params = params
+        self._keep = None
+
+    # -- solve ------------------------------------------------------------------------------
+    def solve(self, b, x0=None, raise_on_no_convergence=False):
+        """FCG solve of A x = b. Host numpy in -> numpy out; CUDA tensors are updated in place."""
+        info = L.SolveInfo()
+        if _is_device(b):
+            import torch
+            x = torch.zeros_like(b) if x0 is None else x0
+            rc = lib().bcmgx_solve(self.h, _ptr(b), _ptr(x), 1, C.byref(info))
+        else:
+            b = np.ascontiguousarray(b, dtype=np.float64)
+            if x0 is None:
+                x = np.zeros(self.n)
+            elif isinstance(x0, np.ndarray) and x0.dtype == np.float64 and x0.flags.c_contiguous and x0.flags.writeable:
+                x = x0   # updated in place, as the reference writes x0
+            else:
+                x = np.array(x0, dtype=np.float64)
+            rc = lib().bcmgx_solve(self.h, _ptr(b), _ptr(x), 0, C.byref(info))
+        if rc != L.OK and (rc != L.ERR_NO_CONVERGENCE or raise_on_no_convergence):
+            raise BcmgxError(rc, "solve", L.last_error())
+        out = {"retv": info.retv, "niter": info.niter, "delta0": info.delta0,
+               "exit_res": info.exit_res, "solve_ms": info.solve_ms, "status": rc}
+        return x, out
+
+    def prec_apply(self, r):
+        if _is_device(r):
+            import torch
+            v = torch.empty_like(r)
+            check(lib().bcmgx_prec_apply(self.h, _ptr(r), _ptr(v), 1), "prec_apply")
+            return v
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        v = np.empty_like(r)
+        check(lib().bcmgx_prec_apply(self.h, _ptr(r), _ptr(v), 0), "prec_apply")
+        return v
+
+    # -- inspection -------------------------------------------------------------------------
+    def info(self):
+        hi = L.HierarchyInfo()
+        check(lib().bcmgx_hierarchy_get_info(self.h, C.byref(hi)), "get_info")
+        nl = hi.num_levels
+        return {"num_levels": nl, "n": list(hi.n[:nl]), "nnz": list(hi.nnz[:nl]),
+                "op_cmplx": hi.op_cmplx, "op_wcmplx": hi.op_wcmplx, "avg_cratio": hi.avg_cratio,
+                "maxcoarsesize": hi.maxcoarsesize, "ftcoarse": hi.ftcoarse,
+                "num_sweep_records": hi.num_sweep_records, "setup_ms": hi.setup_ms}
+
+    def level(self, l):
+        inf = self.info()
+        n, z = inf["n"][l], inf["nnz"][l]
+        row = np.empty(n + 1, np.int32)
+        col = np.empty(z, np.int32)
+        val = np.empty(z, np.float64)
+        check(lib().bcmgx_hierarchy_get_level(self.h, l, _ptr(row), _ptr(col), _ptr(val)), "get_level")
+        return row, col, val
+
+    def prolongator(self, l):
+        n = self.info()["n"][l]
+        agg = np.empty(n, np.int32)
+        p = np.empty(n)
+        M = np.empty(n)
+        check(lib().bcmgx_hierarchy_get_prolongator(self.h, l, _ptr(agg), _ptr(p), _ptr(M)),
+              "get_prolongator")
+        return agg, p, M
+
+    def sweeps(self):
+        out = []
+        for k in range(self.info()["num_sweep_records"]):
+            lv, sw, n, nc = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+            check(lib().bcmgx_hierarchy_get_sweep(self.h, k, C.byref(lv), C.byref(sw), C.byref(n),
+                                                  C.byref(nc), None, None, None, None), "get_sweep")
+            M = np.empty(n.value, np.int32)
+            agg = np.empty(n.value, np.int32)
+            p = np.empty(n.value)
+            w = np.empty(n.value)
+            check(lib().bcmgx_hierarchy_get_sweep(self.h, k, None, None, None, None, _ptr(M),
+                                                  _ptr(agg), _ptr(p), _ptr(w)), "get_sweep")
+            out.append({"level": lv.value, "sweep": sw.value, "nc": nc.value, "match": M,
+                        "agg": agg, "p": p, "w": w})
+        return out
+
+    def time_kernels(self, level=0, reps=20):
+        """Average ms per launch of the level's Jacobi sweep, residual, FP64 SpMV, FCG SpMV+dots."""
+        out = np.zeros(4)
+        check(lib().bcmgx_time_kernels(self.h, level, reps, _ptr(out)), "bcmgx_time_kernels")
+        return {"jacobi": out[0], "residual": out[1], "spmv": out[2], "fcg_spmv_dots": out[3]}
+
+    def free(self):
+        if getattr(self, "h", None):
+            check(lib().bcmgx_free(self.h), "prec_finalize")
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def prec_setup(row, col, val, params) -> Hierarchy:
+    return Hierarchy(row, col, val, params)
+
+
+def solve(h: Hierarchy, rhs, x0=None):
+    return h.solve(rhs, x0)
+
+
+def prec_finalize(h: Hierarchy):
+    h.free()
+
+
+# ---------------------------------------------------------------------------------------------
+# kernels on caller-owned device memory (CUDA torch tensors)
+# ---------------------------------------------------------------------------------------------
+def _stream_ptr(stream):
+    if stream is None:
+        import torch
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream)
+
+
+def spmv(row, col, val, x, y, alpha=1.0, beta=0.0, threads_per_row=0, stream=None):
+    n = int(row.shape[0]) - 1
+    check(lib().bcmgx_spmv(n, int(x.shape[0]), int(col.shape[0]), _ptr(row), _ptr(col), _ptr(val),
+                           _ptr(x), _ptr(y), alpha, beta, threads_per_row, _stream_ptr(stream)),
+          "bcmgx_spmv")
+    return y
+
+
+def edge_weights(row, col, val, w, stream=None):
+    import torch
+    W = torch.empty_like(val)
+    mn = C.c_double()
+    n = int(row.shape[0]) - 1
+    check(lib().bcmgx_edge_weights(n, int(col.shape[0]), _ptr(row), _ptr(col), _ptr(val), _ptr(w),
+                                   _ptr(W), C.byref(mn), _stream_ptr(stream)), "bcmgx_edge_weights")
+    return W, mn.value
+
+
+def suitor_matching(row, col, W, stream=None):
+    import torch
+    n = int(row.shape[0]) - 1
+    M = torch.empty(n, dtype=torch.int32, device=row.device)
+    check(lib().bcmgx_suitor_matching(n, int(col.shape[0]), _ptr(row), _ptr(col), _ptr(W), _ptr(M),
+                                      _stream_ptr(stream)), "bcmgx_suitor_matching")
+    return M

@@ -1,0 +1,373 @@
+// api.cpp -- the C ABI (include/bcmgx.h). Every entry point converts exceptions into status
+// codes and records the message for bcmgx_last_error_string(); nothing calls exit().
+#include "internal.h"
+
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+
+namespace bcmgx {
+
+static thread_local std::string g_last_error;
+
+void set_last_error(const std::string& s) { g_last_error = s; }
+
+static std::atomic<long long> g_launches { 0 };
+
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+template <typename F>
+static int guarded(F&& f)
+{
+    try {
+        f();
+        return BCMGX_OK;
+    } catch (const Error& e) {
+        set_last_error(e.msg);
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        set_last_error("host allocation failed");
+        return BCMGX_ERR_OOM;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return BCMGX_ERR_INTERNAL;
+    } catch (...) {
+        set_last_error("unknown failure");
+        return BCMGX_ERR_INTERNAL;
+    }
+}
+
+// Device guard: makes the hierarchy's device current for the duration of a call.
+struct DeviceScope {
+    int prev = -1;
+    explicit DeviceScope(int dev)
+    {
+        cudaGetDevice(&prev);
+        if (dev >= 0 && dev != prev) BCMGX_CUDA(cudaSetDevice(dev));
+    }
+    ~DeviceScope()
+    {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+static void check_params(const bcmgx_params* p)
+{
+    BCMGX_REQUIRE(p != nullptr, BCMGX_ERR_INVALID_INPUT, "params is NULL");
+    BCMGX_REQUIRE(p->error == 0, BCMGX_ERR_INVALID_INPUT, "settings carry an error flag (unsupported legacy option)");
+    BCMGX_REQUIRE(p->solver == BCMGX_SOLVER_FCG, BCMGX_ERR_UNSUPPORTED,
+        std::string("solver ") + solver_name(p->solver) + " is not on this path (FCG only)");
+    BCMGX_REQUIRE(p->preconditioner == BCMGX_PREC_BCMG || p->preconditioner == BCMGX_PREC_NONE, BCMGX_ERR_UNSUPPORTED,
+        std::string("preconditioner ") + prec_name(p->preconditioner) + " is not on this path (BCMG or NONE)");
+    BCMGX_REQUIRE(p->cycle_type >= 0 && p->cycle_type < BCMGX_CYCLE_INVALID, BCMGX_ERR_INVALID_INPUT, "invalid cycle_type");
+    BCMGX_REQUIRE(p->matchtype == BCMGX_MATCH_SUITOR, BCMGX_ERR_INVALID_INPUT, "invalid matchtype");
+    BCMGX_REQUIRE(p->relax_type == BCMGX_L1_JACOBI && p->coarse_solver == BCMGX_L1_JACOBI, BCMGX_ERR_INVALID_INPUT,
+        "invalid relax_type / coarse_solver");
+    BCMGX_REQUIRE(p->bootstrap_type == BCMGX_BOOT_MULTIPLICATIVE, BCMGX_ERR_UNSUPPORTED,
+        "only the MULTIPLICATIVE bootstrap composition is implemented by the reference (bcmg.cu:63-86)");
+    BCMGX_REQUIRE(p->max_hrc == 1, BCMGX_ERR_UNSUPPORTED, "max_hrc > 1 (bootstrap) is not supported (Params.cu:463)");
+    BCMGX_REQUIRE(p->aggr_type == 0, BCMGX_ERR_UNSUPPORTED, "aggr_type != 0 is not supported (Params.cu:467)");
+    BCMGX_REQUIRE(p->aggrsweeps >= 0 && p->aggrsweeps < 30, BCMGX_ERR_INVALID_INPUT, "aggrsweeps out of range");
+    BCMGX_REQUIRE(p->max_levels >= 1 && p->max_levels <= BCMGX_MAX_LEVELS, BCMGX_ERR_INVALID_INPUT, "max_levels out of range");
+    BCMGX_REQUIRE(p->itnlim >= 1, BCMGX_ERR_INVALID_INPUT, "itnlim < 1");
+    BCMGX_REQUIRE(p->prerelax_sweeps >= 0 && p->postrelax_sweeps >= 0 && p->relaxnumber_coarse >= 0,
+        BCMGX_ERR_INVALID_INPUT, "negative sweep count");
+    BCMGX_REQUIRE(p->vcycle_precision == BCMGX_VCYCLE_FP64 || p->vcycle_precision == BCMGX_VCYCLE_FP32,
+        BCMGX_ERR_INVALID_INPUT, "invalid vcycle_precision");
+}
+
+}  // namespace bcmgx
+
+using namespace bcmgx;
+
+bcmgx_hierarchy::~bcmgx_hierarchy()
+{
+    if (iter_graph) cudaGraphExecDestroy(iter_graph);
+    lv.clear();
+    b.release();
+    xv.release();
+    r.release();
+    v.release();
+    w.release();
+    d.release();
+    q.release();
+    res.release();
+    res32.release();
+    partials.release();
+    st.release();
+    if (stream) cudaStreamSynchronize(stream);
+    if (st_host) cudaFreeHost(st_host);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (own_stream && stream) cudaStreamDestroy(stream);
+}
+
+extern "C" {
+
+const char* bcmgx_last_error_string(void) { return g_last_error.c_str(); }
+
+const char* bcmgx_version(void) { return "bcmgx-b200 0.1 (sm_100a)"; }
+
+int64_t bcmgx_launch_count(void) { return g_launches.load(); }
+
+int bcmgx_params_default(bcmgx_params* p)
+{
+    return guarded([&] {
+        BCMGX_REQUIRE(p != nullptr, BCMGX_ERR_INVALID_INPUT, "params is NULL");
+        params_default(p);
+    });
+}
+
+int bcmgx_params_from_properties(const char* path, bcmgx_params* p)
+{
+    return guarded([&] {
+        BCMGX_REQUIRE(path && p, BCMGX_ERR_INVALID_INPUT, "NULL argument");
+        params_from_properties(path, p);
+    });
+}
+
+int bcmgx_params_from_legacy_file(const char* path, bcmgx_params* p)
+{
+    return guarded([&] {
+        BCMGX_REQUIRE(path && p, BCMGX_ERR_INVALID_INPUT, "NULL argument");
+        params_from_legacy(path, p);
+    });
+}
+
+int bcmgx_params_dump(const bcmgx_params* p, const char* path)
+{
+    return guarded([&] {
+        BCMGX_REQUIRE(p != nullptr, BCMGX_ERR_INVALID_INPUT, "params is NULL");
+        FILE* f = path ? std::fopen(path, "w") : stdout;
+        BCMGX_REQUIRE(f != nullptr, BCMGX_ERR_INVALID_INPUT, "cannot open output file");
+        params_dump(p, f);
+        if (path) std::fclose(f);
+    });
+}
+
+int bcmgx_setup(const bcmgx_csr* A, const bcmgx_params* p, bcmgx_hierarchy** out)
+{
+    return guarded([&] {
+        BCMGX_REQUIRE(A && out, BCMGX_ERR_INVALID_INPUT, "NULL argument");
+        *out = nullptr;
+        check_params(p);
+        BCMGX_REQUIRE(A->n > 0 && A->n == A->m, BCMGX_ERR_INVALID_INPUT, "matrix must be square with n > 0");
+        BCMGX_REQUIRE(A->nnz > 0 && A->nnz <= 0x7fffffffLL, BCMGX_ERR_INVALID_INPUT, "nnz must be in [1, 2^31-1]");
+        BCMGX_REQUIRE(A->row && A->col && A->val, BCMGX_ERR_INVALID_INPUT, "NULL CSR array");
+        std::unique_ptr<bcmgx_hierarchy> H(new bcmgx_hierarchy());
+        H->prm = *p;
+        int dev = p->device;
+        if (dev < 0) BCMGX_CUDA(cudaGetDevice(&dev));
+        H->device = dev;
+        DeviceScope ds(dev);
+        if (p->stream) {
+            H->stream = (cudaStream_t)p->stream;
+        } else {
+            BCMGX_CUDA(cudaStreamCreateWithFlags(&H->stream, cudaStreamNonBlocking));
+            H->own_stream = true;
+        }
+        // keep freed blocks in the pool: repeated set-ups reuse them without cudaMalloc
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t thr = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+        BCMGX_CUDA(cudaEventCreate(&H->ev0));
+        BCMGX_CUDA(cudaEventCreate(&H->ev1));
+        cudaEvent_t e0, e1;
+        BCMGX_CUDA(cudaEventCreate(&e0));
+        BCMGX_CUDA(cudaEventCreate(&e1));
+        BCMGX_CUDA(cudaEventRecord(e0, H->stream));
+        build_hierarchy(H.get(), A);
+        for (auto& V : H->lv) V.A.tpr = default_tpr(V.A.n, V.A.nnz);
+        BCMGX_CUDA(cudaEventRecord(e1, H->stream));
+        BCMGX_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        H->setup_ms = ms;
+        *out = H.release();
+    });
+}
+
+int bcmgx_solve(bcmgx_hierarchy* h, const double* b, double* x, int on_device, bcmgx_solve_info* info)
+{
+    int status = BCMGX_OK;
+    int rc = guarded([&] {
+        BCMGX_REQUIRE(h && b && x, BCMGX_ERR_INVALID_INPUT, "NULL argument");
+        DeviceScope ds(h->device);
+        const int n = h->lv[0].A.n;
+        cudaStream_t s = h->stream;
+        if (on_device) {
+            status = fcg_solve(h, b, x, info);
+        } else {
+            h->b.alloc(n, s);
+            h->xv.alloc(n, s);
+            BCMGX_CUDA(cudaMemcpyAsync(h->b.p, b, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+            BCMGX_CUDA(cudaMemcpyAsync(h->xv.p, x, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+            status = fcg_solve(h, h->b.p, h->xv.p, info);
+            BCMGX_CUDA(cudaMemcpyAsync(x, h->xv.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+            BCMGX_CUDA(cudaStreamSynchronize(s));
+        }
+        if (status == BCMGX_ERR_NO_CONVERGENCE) set_last_error("itnlim reached before the tolerance");
+        if (status == BCMGX_ERR_NOT_SPD) set_last_error("FCG breakdown: non-positive or non-finite curvature");
+    });
+    return rc != BCMGX_OK ? rc : status;
+}
+
+int bcmgx_free(bcmgx_hierarchy* h)
+{
+    return guarded([&] {
+        if (!h) return;
+        DeviceScope ds(h->device);
+        delete h;
+    });
+}
+
+int bcmgx_hierarchy_get_info(const bcmgx_hierarchy* h, bcmgx_hierarchy_info* info)
+{
+    return guarded([&] {
+        BCMGX_REQUIRE(h && info, BCMGX_ERR_INVALID_INPUT, "NULL argument");
+        std::memset(info, 0, sizeof(*info));
+        info->num_levels = (int)h->lv.size();
+        for (int l = 0; l < info->num_levels && l < BCMGX_MAX_LEVELS; l++) {
+            info->n[l] = h->lv[l].A.n;
+            info->nnz[l] = h->lv[l].A.nnz;
+        }
+        info->op_cmplx = h->op_cmplx;
+        info->op_wcmplx = h->op_wcmplx;
+        info->avg_cratio = h->avg_cratio;
+        info->maxcoarsesize = h->maxcoarsesize;
+        info->ftcoarse = h->ftcoarse;
+        info->num_sweep_records = (int)h->rec.size();
+        info->setup_ms = h->setup_ms;
+    });
+}
+
+int bcmgx_hierarchy_get_level(const bcmgx_hierarchy* h, int l, int* row, int* col, double* val)
+{
+    return guarded([&] {
+        BCMGX_REQUIRE(h && l >= 0 && l < (int)h->lv.size(), BCMGX_ERR_INVALID_INPUT, "bad level");
+        DeviceScope ds(h->device);
+        const DevCsr& A = h->lv[l].A;
+        cudaStream_t s = h->stream;
+        if (row) BCMGX_CUDA(cudaMemcpyAsync(row, A.row.p, sizeof(int) * ((size_t)A.n + 1), cudaMemcpyDeviceToHost, s));
+        if (col) BCMGX_CUDA(cudaMemcpyAsync(col, A.col.p, sizeof(int) * A.nnz, cudaMemcpyDeviceToHost, s));
+        if (val) BCMGX_CUDA(cudaMemcpyAsync(val, A.val.p, sizeof(double) * A.nnz, cudaMemcpyDeviceToHost, s));
+        BCMGX_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int bcmgx_hierarchy_get_prolongator(const bcmgx_hierarchy* h, int l, int* agg, double* p, double* M)
+{
+    return guarded([&] {
+        BCMGX_REQUIRE(h && l >= 0 && l < (int)h->lv.size(), BCMGX_ERR_INVALID_INPUT, "bad level");
+        DeviceScope ds(h->device);
+        const Level& V = h->lv[l];
+        cudaStream_t s = h->stream;
+        const size_t n = V.A.n;
+        if (agg || p) BCMGX_REQUIRE(l + 1 < (int)h->lv.size(), BCMGX_ERR_INVALID_INPUT, "coarsest level has no prolongator");
+        if (agg) BCMGX_CUDA(cudaMemcpyAsync(agg, V.agg.p, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+        if (p) BCMGX_CUDA(cudaMemcpyAsync(p, V.p.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+        if (M) BCMGX_CUDA(cudaMemcpyAsync(M, V.M.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+        BCMGX_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int bcmgx_hierarchy_get_sweep(const bcmgx_hierarchy* h, int k, int* level, int* sweep, int* n, int* nc, int* match,
+    int* agg, double* p, double* w)
+{
+    return guarded([&] {
+        BCMGX_REQUIRE(h && k >= 0 && k < (int)h->rec.size(), BCMGX_ERR_INVALID_INPUT, "bad sweep record index");
+        const SweepRecord& r = h->rec[k];
+        if (level) *level = r.level;
+        if (sweep) *sweep = r.sweep;
+        if (n) *n = r.n;
+        if (nc) *nc = r.nc;
+        if (match) std::memcpy(match, r.match.data(), sizeof(int) * r.n);
+        if (agg) std::memcpy(agg, r.agg.data(), sizeof(int) * r.n);
+        if (p) std::memcpy(p, r.p.data(), sizeof(double) * r.n);
+        if (w) std::memcpy(w, r.w.data(), sizeof(double) * r.n);
+    });
+}
+
+int bcmgx_prec_apply(bcmgx_hierarchy* h, const double* r, double* v, int on_device)
+{
+    return guarded([&] {
+        BCMGX_REQUIRE(h && r && v, BCMGX_ERR_INVALID_INPUT, "NULL argument");
+        DeviceScope ds(h->device);
+        const int n = h->lv[0].A.n;
+        cudaStream_t s = h->stream;
+        if (on_device) {
+            prec_apply_dev(h, r, v);
+            BCMGX_CUDA(cudaStreamSynchronize(s));
+        } else {
+            DBuf<double> rd, vd;
+            rd.alloc(n, s);
+            vd.alloc(n, s);
+            BCMGX_CUDA(cudaMemcpyAsync(rd.p, r, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+            prec_apply_dev(h, rd.p, vd.p);
+            BCMGX_CUDA(cudaMemcpyAsync(v, vd.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+            BCMGX_CUDA(cudaStreamSynchronize(s));
+        }
+    });
+}
+
+int bcmgx_time_kernels(bcmgx_hierarchy* h, int level, int reps, double* out_ms)
+{
+    return guarded([&] {
+        BCMGX_REQUIRE(h && out_ms && level >= 0 && level < (int)h->lv.size() && reps > 0, BCMGX_ERR_INVALID_INPUT, "bad argument");
+        DeviceScope ds(h->device);
+        time_level_kernels(h, level, reps, out_ms);
+    });
+}
+
+int bcmgx_spmv(int n, int m, int64_t nnz, const int* row, const int* col, const double* val, const double* x, double* y,
+    double alpha, double beta, int threads_per_row, void* stream)
+{
+    return guarded([&] {
+        BCMGX_REQUIRE(n >= 0 && m >= 0 && nnz >= 0, BCMGX_ERR_INVALID_INPUT, "negative size");
+        BCMGX_REQUIRE(row && (nnz == 0 || (col && val)) && x && y, BCMGX_ERR_INVALID_INPUT, "NULL argument");
+        int t = threads_per_row;
+        if (t <= 0) t = default_tpr(n, nnz);
+        BCMGX_REQUIRE(t == 1 || t == 2 || t == 4 || t == 8 || t == 16 || t == 32, BCMGX_ERR_INVALID_INPUT,
+            "threads_per_row must be a power of two <= 32");
+        if (n > 0) validate_csr_dev(n, m, nnz, row, col, false, (cudaStream_t)stream);
+        launch_spmv(n, row, col, val, x, y, alpha, beta, t, (cudaStream_t)stream);
+    });
+}
+
+int bcmgx_edge_weights(int n, int64_t nnz, const int* row, const int* col, const double* val, const double* w, double* W,
+    double* min_abs_out, void* stream)
+{
+    return guarded([&] {
+        BCMGX_REQUIRE(n > 0 && nnz > 0 && row && col && val && w && W, BCMGX_ERR_INVALID_INPUT, "bad argument");
+        cudaStream_t s = (cudaStream_t)stream;
+        validate_csr_dev(n, n, nnz, row, col, true, s);
+        DBuf<int> tpos;
+        tpos.alloc(nnz, s);
+        double mn = 0;
+        edge_weights_dev(n, nnz, row, col, val, w, W, tpos.p, &mn, s);
+        BCMGX_CUDA(cudaStreamSynchronize(s));
+        if (min_abs_out) *min_abs_out = mn;
+    });
+}
+
+int bcmgx_suitor_matching(int n, int64_t nnz, const int* row, const int* col, const double* W, int* M, void* stream)
+{
+    return guarded([&] {
+        BCMGX_REQUIRE(n > 0 && nnz > 0 && row && col && W && M, BCMGX_ERR_INVALID_INPUT, "bad argument");
+        cudaStream_t s = (cudaStream_t)stream;
+        validate_csr_dev(n, n, nnz, row, col, false, s);
+        DBuf<int> tpos;
+        tpos.alloc(nnz, s);
+        tpos_dev(n, row, col, tpos.p, s);
+        suitor_dev(n, nnz, row, col, W, tpos.p, M, s);
+        BCMGX_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+}  // extern "C"

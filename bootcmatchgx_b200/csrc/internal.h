@@ -1,0 +1,192 @@
+// internal.h -- host-side types shared by the bcmgx library translation units.
+#pragma once
+
+#include "bcmgx.h"
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+namespace bcmgx {
+
+struct Error : std::exception {
+    int code;
+    std::string msg;
+    Error(int c, std::string m) : code(c), msg(std::move(m)) {}
+    const char* what() const noexcept override { return msg.c_str(); }
+};
+
+void set_last_error(const std::string& s);
+// counts every kernel launch of the library (reported by bcmgx_launch_count)
+void note_launch();
+
+#define BCMGX_CUDA(call)                                                                       \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            throw ::bcmgx::Error(BCMGX_ERR_CUDA, std::string(#call) + " failed: " +           \
+                                                     cudaGetErrorString(e_) + " @" __FILE__); \
+    } while (0)
+
+#define BCMGX_CHECK_LAUNCH() BCMGX_CUDA(cudaGetLastError())
+
+#define BCMGX_REQUIRE(cond, code, text)                                   \
+    do {                                                                  \
+        if (!(cond)) throw ::bcmgx::Error((code), std::string(text));     \
+    } while (0)
+
+// Stream-ordered device buffer (cudaMallocAsync from the device's default pool).
+template <typename T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaStream_t s = nullptr;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    DBuf(DBuf&& o) noexcept { *this = std::move(o); }
+    DBuf& operator=(DBuf&& o) noexcept
+    {
+        if (this != &o) {
+            release();
+            p = o.p;
+            n = o.n;
+            s = o.s;
+            o.p = nullptr;
+            o.n = 0;
+        }
+        return *this;
+    }
+    ~DBuf() { release(); }
+    void alloc(size_t count, cudaStream_t stream)
+    {
+        release();
+        s = stream;
+        n = count;
+        if (count == 0) return;
+        cudaError_t e = cudaMallocAsync((void**)&p, count * sizeof(T), stream);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            n = 0;
+            (void)cudaGetLastError();
+            throw Error(e == cudaErrorMemoryAllocation ? BCMGX_ERR_OOM : BCMGX_ERR_CUDA,
+                std::string("device allocation of ") + std::to_string(count * sizeof(T)) +
+                    " bytes failed: " + cudaGetErrorString(e));
+        }
+    }
+    void release()
+    {
+        if (p) cudaFreeAsync(p, s);
+        p = nullptr;
+        n = 0;
+    }
+    T* get() const { return p; }
+};
+
+// Device CSR with an optional FP32 copy of the values (FP32 V-cycle).
+struct DevCsr {
+    int n = 0, m = 0;
+    int64_t nnz = 0;
+    int max_row = 0;
+    DBuf<int> row, col;
+    DBuf<double> val;
+    DBuf<float> val32;
+    int tpr = 0;      // threads per row for SpMV / smoother (autotuned)
+};
+
+struct Level {
+    DevCsr A;
+    DBuf<double> M;            // absolute row sums
+    DBuf<float> M32;
+    // composite prolongator to level + 1 (one entry per row) and its transpose
+    DBuf<int> agg;
+    DBuf<double> p;
+    DBuf<float> p32;
+    DBuf<int> rptr, ridx;
+    DBuf<double> rval;
+    DBuf<float> rval32;
+    // V-cycle work vectors
+    DBuf<double> rhs, x, x2;
+    DBuf<float> rhs32, x32, x232;
+};
+
+struct SweepRecord {
+    int level = 0, sweep = 0, n = 0, nc = 0;
+    std::vector<int> match, agg;
+    std::vector<double> p, w;
+};
+
+// FCG scalars that live on the device between kernels.
+struct FcgState {
+    double alpha, beta, gamma, delta;
+    double rnorm2, delta0, tol;
+    double theta, theta2;
+    int iter, itnlim, done, bad;
+    int ticket[4];
+};
+
+}  // namespace bcmgx
+
+struct bcmgx_hierarchy {
+    bcmgx_params prm{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::vector<bcmgx::Level> lv;
+    std::vector<bcmgx::SweepRecord> rec;
+    int maxcoarsesize = 0, ftcoarse = 1;
+    double op_cmplx = 0, op_wcmplx = 0, avg_cratio = 1, setup_ms = 0;
+    std::vector<int> grid_sweeps;
+    // solve workspace
+    bcmgx::DBuf<double> b, xv, r, v, w, d, q, res;
+    bcmgx::DBuf<float> res32;
+    bcmgx::DBuf<double> partials;
+    bcmgx::DBuf<bcmgx::FcgState> st;
+    bcmgx::FcgState* st_host = nullptr;   // pinned mirror
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int64_t ws_n = -1;
+    // captured FCG iteration (CUDA graph)
+    cudaGraphExec_t iter_graph = nullptr;
+    ~bcmgx_hierarchy();
+};
+
+namespace bcmgx {
+
+// ---- settings (params.cpp) ----
+void params_default(bcmgx_params* p);
+void params_from_properties(const char* path, bcmgx_params* p);
+void params_from_legacy(const char* path, bcmgx_params* p);
+void params_dump(const bcmgx_params* p, FILE* out);
+const char* solver_name(int v);
+const char* prec_name(int v);
+const char* cycle_name(int v);
+const char* boot_name(int v);
+
+// ---- set-up (setup.cu) ----
+void build_hierarchy(bcmgx_hierarchy* H, const bcmgx_csr* A);
+
+// ---- solve (solve.cu) ----
+void ensure_solve_workspace(bcmgx_hierarchy* H);
+int fcg_solve(bcmgx_hierarchy* H, const double* b_dev, double* x_dev, bcmgx_solve_info* info);
+void prec_apply_dev(bcmgx_hierarchy* H, const double* r, double* v);
+void time_level_kernels(bcmgx_hierarchy* H, int l, int reps, double* out);
+
+// ---- kernels usable on raw device memory (kernels.cu) ----
+int autotune_tpr(const DevCsr& A, cudaStream_t s);
+int default_tpr(int n, int64_t nnz);
+void launch_spmv(int n, const int* row, const int* col, const double* val, const double* x, double* y,
+    double alpha, double beta, int tpr, cudaStream_t s);
+void edge_weights_dev(int n, int64_t nnz, const int* row, const int* col, const double* val,
+    const double* w, double* W, int* tpos, double* min_out_host, cudaStream_t s);
+void validate_csr_dev(int n, int m, int64_t nnz, const int* row, const int* col, bool need_diag, cudaStream_t s);
+void tpos_dev(int n, const int* row, const int* col, int* tpos, cudaStream_t s);
+void suitor_dev(int n, int64_t nnz, const int* row, const int* col, const double* W, const int* tpos,
+    int* M, cudaStream_t s);
+
+}  // namespace bcmgx

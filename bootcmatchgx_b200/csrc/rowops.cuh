@@ -1,0 +1,71 @@
+// rowops.cuh -- CSR row kernels of the solve phase: SpMV, residual, l1-Jacobi sweep.
+//
+// One sub-warp of S lanes owns a row (S = 1..32, chosen per matrix by the autotuner); the lanes
+// stride over the row's entries, matrix data is streamed with evict-first loads and the vector
+// gathers go through the read-only path, so x stays resident in L2 while A streams from HBM.
+#pragma once
+
+#include "common.cuh"
+
+namespace bcmgx {
+
+enum RowOp { OP_AXPBY = 0, OP_RESID = 1, OP_JACOBI = 2 };
+
+// Partial dot product of one row over the lanes of a sub-warp, unrolled by 4 so that the
+// column, value and gather loads of several entries are in flight together.
+template <int S, typename AT, typename VT, typename XT>
+__device__ __forceinline__ AT row_partial(int b, int e, int lane, const int* __restrict__ col,
+    const VT* __restrict__ val, const XT* __restrict__ x)
+{
+    AT s0 = 0, s1 = 0;
+    int j = b + lane;
+    for (; j + 3 * S < e; j += 4 * S) {
+        const int c0 = ld_stream(col + j), c1 = ld_stream(col + j + S);
+        const int c2 = ld_stream(col + j + 2 * S), c3 = ld_stream(col + j + 3 * S);
+        const VT v0 = ld_stream(val + j), v1 = ld_stream(val + j + S);
+        const VT v2 = ld_stream(val + j + 2 * S), v3 = ld_stream(val + j + 3 * S);
+        const XT x0 = ld_ro(x + c0), x1 = ld_ro(x + c1), x2 = ld_ro(x + c2), x3 = ld_ro(x + c3);
+        s0 += (AT)v0 * (AT)x0;
+        s1 += (AT)v1 * (AT)x1;
+        s0 += (AT)v2 * (AT)x2;
+        s1 += (AT)v3 * (AT)x3;
+    }
+    for (; j < e; j += S) s0 += (AT)ld_stream(val + j) * (AT)ld_ro(x + ld_stream(col + j));
+    return s0 + s1;
+}
+
+// y = alpha*A*x + beta*y (OP_AXPBY), y = f - A*x (OP_RESID) or one l1-Jacobi sweep
+// y = ((f - A*x) / M) + x (OP_JACOBI, the update of _jacobi_it_full<0>, l1jacobi.cu:345-379).
+// Grid-stride over rows; all lanes of a sub-warp stay converged for the shuffles.
+template <int S, int OP, typename VT, typename XT, typename FT, typename MT, typename YT>
+__global__ void __launch_bounds__(256) k_rowop(int n, const int* __restrict__ row, const int* __restrict__ col,
+    const VT* __restrict__ val, const XT* __restrict__ x, const FT* __restrict__ f, const MT* __restrict__ M,
+    YT* __restrict__ y, double alpha, double beta, const int* __restrict__ skip)
+{
+    if (skip && *skip) return;
+    using AT = typename Acc<VT>::type;
+    const int lane = threadIdx.x & (S - 1);
+    const int sub = (threadIdx.x & 31) / S;
+    const long stride = (long)gridDim.x * blockDim.x / S;
+    // base is uniform across the warp, so every lane reaches the shuffles together
+    for (long base = ((long)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) / S; base < n; base += stride) {
+        const long r0 = base + sub;
+        const int r = (int)r0;
+        AT s = 0;
+        if (r0 < n) s = row_partial<S, AT>(__ldg(row + r), __ldg(row + r + 1), lane, col, val, x);
+        s = subwarp_sum<S>(s);
+        if (r0 < n && lane == 0) {
+            if (OP == OP_AXPBY) {
+                AT o = (AT)alpha * s;
+                if (beta != 0.0) o += (AT)beta * (AT)y[r];
+                y[r] = (YT)o;
+            } else if (OP == OP_RESID) {
+                y[r] = (YT)((AT)f[r] - s);
+            } else {
+                y[r] = (YT)(((-s + (AT)f[r]) / (AT)M[r]) + (AT)x[r]);
+            }
+        }
+    }
+}
+
+}  // namespace bcmgx

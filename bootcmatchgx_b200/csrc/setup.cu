@@ -1,0 +1,993 @@
+// setup.cu -- hierarchy construction on the device (BCMG: suitor matching + pairwise aggregation).
+//
+// Restates, at np = 1: adaptiveCoarsening / matchingAggregation
+// (BCMGX/src/preconditioner/bcmg/matchingAggregation.cu:106-466), matchingPairAggregation /
+// makeP_GPU (matchingPairAggregation.cu:24-237), the edge weights (matching.cu:13-288), the suitor
+// matching (suitor.cu:51-329) and the two nsparse products of the Galerkin step.
+//
+// Every floating-point operation of this file is an explicit round-to-nearest intrinsic
+// (__dmul_rn, __dadd_rn, ...) so nothing is contracted into an FMA: the hierarchy is
+// bit-identical to the CPU restatement. Integer results (matching, aggregates, sizes) do not
+// depend on thread scheduling:
+//  * the suitor matching is lock-free: every vertex ranks its neighbours once, offers are
+//    32-bit ranks combined with atomicMax, and each vertex's search pointer only moves forward,
+//    so the work is bounded by nnz and the result is the greedy matching of the edge order;
+//  * aggregates are numbered by prefix sums (pairs by master id, then singletons by id);
+//  * every Galerkin entry is a sum of at most two rounded products, formed in a fixed order.
+#include "internal.h"
+#include "common.cuh"
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+
+namespace bcmgx {
+
+int num_sms();
+
+constexpr double kSuitorEps = 3.885780586188048e-10;   // suitor.h:8
+constexpr int kFtcoarseInc = 100;                       // matchingAggregation.cu:8
+constexpr double kCoarseRatioThreshold = 1.2;           // matchingAggregation.cu:9
+
+enum : int {
+    ERR_ROW0 = 1, ERR_ROWN = 2, ERR_ROWORDER = 4, ERR_COLRANGE = 8, ERR_COLSORT = 16, ERR_NODIAG = 32,
+    ERR_SUITOR_BUDGET = 64, ERR_ASYM_MATCH = 128, ERR_BADW = 256, ERR_GALERKIN_CAP = 512,
+};
+
+static int gs_grid(long n, int threads = 256)
+{
+    return (int)std::max<long>(1, std::min<long>((n + threads - 1) / threads, (long)num_sms() * 16));
+}
+static int warp_grid(long rows, int threads = 256)
+{
+    return gs_grid(rows * 32, threads);
+}
+
+// ------------------------------------------------------------------------------------------
+// prefix sums (three phases: tile sums, scan of tile sums, tile scans)
+// ------------------------------------------------------------------------------------------
+constexpr int kScanThreads = 512;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ long long block_excl_scan(long long v, long long* total)
+{
+    __shared__ long long ws[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    long long x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        long long y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) ws[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        long long t = lane < nw ? ws[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            long long y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        ws[lane] = t;
+    }
+    __syncthreads();
+    const long long off = wid > 0 ? ws[wid - 1] : 0;
+    *total = ws[nw - 1];
+    __syncthreads();
+    return off + x - v;
+}
+
+__global__ void k_scan_tiles(const int* __restrict__ in, long n, long long* tile_sums)
+{
+    const long base = (long)blockIdx.x * kScanTile + (long)threadIdx.x * kScanItems;
+    long long s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++)
+        if (base + k < n) s += in[base + k];
+    long long tot;
+    block_excl_scan(s, &tot);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = tot;
+}
+
+__global__ void k_scan_top(long long* tile_sums, int ntiles, long long* total)
+{
+    long long carry = 0;
+    for (int b0 = 0; b0 < ntiles; b0 += blockDim.x) {
+        const int i = b0 + threadIdx.x;
+        long long v = i < ntiles ? tile_sums[i] : 0;
+        long long tot;
+        long long ex = block_excl_scan(v, &tot);
+        if (i < ntiles) tile_sums[i] = carry + ex;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void k_scan_down(const int* __restrict__ in, int* __restrict__ out, long n, const long long* tile_offs)
+{
+    const long base = (long)blockIdx.x * kScanTile + (long)threadIdx.x * kScanItems;
+    int v[kScanItems];
+    long long s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        v[k] = base + k < n ? in[base + k] : 0;
+        s += v[k];
+    }
+    long long tot;
+    long long ex = block_excl_scan(s, &tot) + tile_offs[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        if (base + k < n) out[base + k] = (int)ex;
+        ex += v[k];
+    }
+}
+
+// Exclusive prefix sum of in[0..n) into out[0..n); when with_total, out[n] = total.
+// Returns the total (synchronises the stream).
+static long long scan_exclusive(const int* in, int* out, long n, bool with_total, cudaStream_t s)
+{
+    const int ntiles = std::max(1, (int)((n + kScanTile - 1) / kScanTile));
+    DBuf<long long> tiles, tot;
+    tiles.alloc(ntiles, s);
+    tot.alloc(1, s);
+    if (n > 0) { note_launch(); k_scan_tiles<<<ntiles, kScanThreads, 0, s>>>(in, n, tiles.p); }
+    else BCMGX_CUDA(cudaMemsetAsync(tiles.p, 0, sizeof(long long), s));
+    note_launch(); k_scan_top<<<1, 1024, 0, s>>>(tiles.p, ntiles, tot.p);
+    if (n > 0) { note_launch(); k_scan_down<<<ntiles, kScanThreads, 0, s>>>(in, out, n, tiles.p); }
+    BCMGX_CHECK_LAUNCH();
+    long long total = 0;
+    BCMGX_CUDA(cudaMemcpyAsync(&total, tot.p, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    BCMGX_CUDA(cudaStreamSynchronize(s));
+    BCMGX_REQUIRE(total <= 0x7fffffffLL, BCMGX_ERR_UNSUPPORTED, "more than 2^31-1 entries (int32 offsets)");
+    if (with_total) {
+        int t32 = (int)total;
+        BCMGX_CUDA(cudaMemcpyAsync(out + n, &t32, sizeof(int), cudaMemcpyHostToDevice, s));
+        BCMGX_CUDA(cudaStreamSynchronize(s));
+    }
+    return total;
+}
+
+// ------------------------------------------------------------------------------------------
+// matrix checks and small per-row kernels
+// ------------------------------------------------------------------------------------------
+__global__ void k_validate(int n, int m, long long nnz, const int* __restrict__ row, const int* __restrict__ col,
+    int* err, int* max_row, int need_diag)
+{
+    const int lane = threadIdx.x & 31;
+    for (long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32; r < n; r += (long)gridDim.x * blockDim.x / 32) {
+        const int b = row[r], e = row[r + 1];
+        int bad = 0;
+        if (r == 0 && b != 0) bad |= ERR_ROW0;
+        if (r == n - 1 && (long long)e != nnz) bad |= ERR_ROWN;
+        if (e < b || b < 0 || (long long)e > nnz) {
+            bad |= ERR_ROWORDER;
+        } else {
+            bool diag = false;
+            for (int j = b + lane; j < e; j += 32) {
+                const int c = col[j];
+                if (c < 0 || c >= m) bad |= ERR_COLRANGE;
+                if (j > b && col[j - 1] >= c) bad |= ERR_COLSORT;
+                if (c == r) diag = true;
+            }
+            diag = __any_sync(0xffffffffu, diag);
+            if (need_diag && !diag) bad |= ERR_NODIAG;
+            if (lane == 0) atomicMax(max_row, e - b);
+        }
+        bad = __reduce_or_sync(0xffffffffu, bad);
+        if (lane == 0 && bad) atomicOr(err, bad);
+    }
+}
+
+__global__ void k_row_max(int n, const int* __restrict__ row, int* max_row)
+{
+    int mx = 0;
+    for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long)gridDim.x * blockDim.x)
+        mx = max(mx, row[r + 1] - row[r]);
+    mx = __reduce_max_sync(0xffffffffu, mx);
+    if ((threadIdx.x & 31) == 0) atomicMax(max_row, mx);
+}
+
+// M_i = sum_j |a_ij| in column order (_row_sum_2, CSR.cu:1362-1379).
+__global__ void k_abs_row_sum(int n, const int* __restrict__ row, const double* __restrict__ val, double* __restrict__ M,
+    float* __restrict__ M32)
+{
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int j = row[i]; j < row[i + 1]; j++) s = __dadd_rn(s, fabs(val[j]));
+        M[i] = s;
+        if (M32) M32[i] = (float)s;
+    }
+}
+
+__global__ void k_to_f32(long n, const double* __restrict__ a, float* __restrict__ b)
+{
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) b[i] = (float)a[i];
+}
+
+__global__ void k_fill(long n, double* a, double v)
+{
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) a[i] = v;
+}
+
+// ------------------------------------------------------------------------------------------
+// edge weights (makeAH, toMaximumProductMatrix, _write_T_warp)
+// ------------------------------------------------------------------------------------------
+
+// C_r = (a_rr * w_r) * w_r from the first diagonal entry (_makeC, matching.cu:113-135).
+__global__ void k_diag_c(int n, const int* __restrict__ row, const int* __restrict__ col, const double* __restrict__ val,
+    const double* __restrict__ w, double* __restrict__ C, int* err)
+{
+    for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long)gridDim.x * blockDim.x) {
+        double c = 0.0;
+        bool found = false;
+        for (int j = row[r]; j < row[r + 1]; j++)
+            if (col[j] == r) {
+                c = __dmul_rn(__dmul_rn(val[j], w[r]), w[r]);
+                found = true;
+                break;
+            }
+        C[r] = c;
+        if (!found) atomicOr(err, ERR_NODIAG);
+    }
+}
+
+// Position of the transposed entry: tpos[j] for a_rc is the index of a_cr in row c (-1 if the
+// pattern has no a_cr); the diagonal maps to itself. One warp per row.
+__global__ void k_tpos(int n, const int* __restrict__ row, const int* __restrict__ col, int* __restrict__ tpos)
+{
+    const int lane = threadIdx.x & 31;
+    for (long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32; r < n; r += (long)gridDim.x * blockDim.x / 32) {
+        const int b = row[r], e = row[r + 1];
+        for (int j = b + lane; j < e; j += 32) {
+            const int c = col[j];
+            if (c == r) {
+                tpos[j] = j;
+                continue;
+            }
+            int lo = row[c], hi = row[c + 1];
+            const int end = hi;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (col[mid] < (int)r) lo = mid + 1;
+                else hi = mid;
+            }
+            tpos[j] = (lo < end && col[lo] == (int)r) ? lo : -1;
+        }
+    }
+}
+
+// a_hat = 1 - (2 a w_r w_c) / (C_r + C_c), or DBL_EPSILON if C_r + C_c <= DBL_EPSILON
+// (_makeAH_warp, matching.cu:66-111). Symmetric in (r, c) apart from a.
+__device__ __forceinline__ double ahat(double a, double Cr, double Cc, double wr, double wc)
+{
+    const double norm = __dadd_rn(Cr, Cc);
+    if (norm > DBL_EPSILON) {
+        const double wt = __dmul_rn(wr, wc);
+        return __dsub_rn(1.0, __ddiv_rn(__dmul_rn(__dmul_rn(2.0, a), wt), norm));
+    }
+    return DBL_EPSILON;
+}
+
+// min over all off-diagonal |a_hat| (find_Max_Min with AbsMin, matching.cu:188-217). The bit
+// pattern of a non-negative double orders like its value, so atomicMin on it is exact.
+__global__ void k_ahat_min(int n, const int* __restrict__ row, const int* __restrict__ col, const double* __restrict__ val,
+    const double* __restrict__ w, const double* __restrict__ C, unsigned long long* min_bits)
+{
+    const int lane = threadIdx.x & 31;
+    double mn = DBL_MAX;
+    for (long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32; r < n; r += (long)gridDim.x * blockDim.x / 32) {
+        const int b = row[r], e = row[r + 1];
+        const double Cr = C[r], wr = w[r];
+        for (int j = b + lane; j < e; j += 32) {
+            const int c = col[j];
+            if (c == r) continue;
+            mn = fmin(mn, fabs(ahat(val[j], Cr, C[c], wr, w[c])));
+        }
+    }
+    unsigned long long bits = (unsigned long long)__double_as_longlong(mn);
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long other = __shfl_xor_sync(0xffffffffu, bits, o);
+        bits = other < bits ? other : bits;
+    }
+    if (lane == 0) atomicMin(min_bits, bits);
+}
+
+// W = log(|a_hat|), or log(SUITOR_EPS / (0.999 min)) where a_hat == 0 (_make_w,
+// matching.cu:219-229); a lower entry takes the value of its upper counterpart
+// (_write_T_warp, matching.cu:29-64), i.e. is computed from a_cr. Diagonal slots are 0.
+__global__ void k_logw(int n, const int* __restrict__ row, const int* __restrict__ col, const double* __restrict__ val,
+    const double* __restrict__ w, const double* __restrict__ C, const int* __restrict__ tpos, double zero_sub,
+    double* __restrict__ W)
+{
+    const int lane = threadIdx.x & 31;
+    for (long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32; r < n; r += (long)gridDim.x * blockDim.x / 32) {
+        const int b = row[r], e = row[r + 1];
+        const double Cr = C[r], wr = w[r];
+        for (int j = b + lane; j < e; j += 32) {
+            const int c = col[j];
+            if (c == r) {
+                W[j] = 0.0;
+                continue;
+            }
+            const int src = (c < r && tpos[j] >= 0) ? tpos[j] : j;
+            const double s = fabs(ahat(val[src], Cr, C[c], wr, w[c]));
+            W[j] = log(s != 0.0 ? s : zero_sub);
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// suitor matching
+// ------------------------------------------------------------------------------------------
+
+// Per row: rank of every candidate (off-diagonal, W > 0) in the row's preference order,
+// (W, column) descending (find_Candidate, suitor.cu:80-147); ordj lists the entries by rank.
+__global__ void k_rank(int n, const int* __restrict__ row, const int* __restrict__ col, const double* __restrict__ W,
+    int* __restrict__ rank, int* __restrict__ ordj, int* __restrict__ degE)
+{
+    const int lane = threadIdx.x & 31;
+    for (long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32; r < n; r += (long)gridDim.x * blockDim.x / 32) {
+        const int b = row[r], e = row[r + 1];
+        int cnt = 0;
+        for (int t0 = b; t0 < e; t0 += 32) {
+            const int t = t0 + lane;
+            bool el = false;
+            if (t < e) {
+                const int ct = col[t];
+                const double wt = W[t];
+                el = (ct != r) && (wt > 0.0);
+                if (el) {
+                    int rk = 0;
+                    for (int k = b; k < e; k++) {
+                        const int ck = col[k];
+                        const double wk = W[k];
+                        rk += (ck != r && wk > 0.0 && (wk > wt || (wk == wt && ck > ct))) ? 1 : 0;
+                    }
+                    rank[t] = rk;
+                    ordj[b + rk] = t;
+                } else {
+                    rank[t] = -1;
+                }
+            }
+            cnt += __popc(__ballot_sync(0xffffffffu, el));
+        }
+        if (lane == 0) degE[r] = cnt;
+    }
+}
+
+// Lock-free suitor. A vertex proposes to its candidates in preference order; its offer at y
+// is degE[y] - (its rank in y's list), so y keeps the highest-ranked suitor by atomicMax. A
+// successful proposal that displaces a previous suitor hands that vertex to the same thread,
+// which resumes it after the neighbour it lost (set_suitor, suitor.cu:51-78). The search
+// pointer of a vertex is published before its offer (fence), so the next owner resumes from
+// the right place. Total proposals are bounded by nnz; `budget` guards the loop.
+__global__ void k_suitor(int n, const int* __restrict__ row, const int* __restrict__ col, const int* __restrict__ ordj,
+    const int* __restrict__ rank, const int* __restrict__ tpos, const int* __restrict__ degE, unsigned* offer,
+    int* ptr, long long budget, int* err)
+{
+    for (long v = (long)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (long)gridDim.x * blockDim.x) {
+        int cur = (int)v;
+        long long steps = 0;
+        while (cur >= 0) {
+            const int start = row[cur];
+            const int dE = degE[cur];
+            int k = ld_cg(ptr + cur);
+            int next = -1;
+            bool placed = false;
+            for (; k < dE; k++) {
+                if (++steps > budget) {
+                    atomicOr(err, ERR_SUITOR_BUDGET);
+                    return;
+                }
+                const int j = ordj[start + k];
+                const int tj = tpos[j];
+                if (tj < 0) continue;
+                const int ry = rank[tj];
+                if (ry < 0) continue;
+                const int y = col[j];
+                const unsigned mine = (unsigned)(degE[y] - ry);
+                if (ld_cg(offer + y) >= mine) continue;
+                st_cg(ptr + cur, k + 1);
+                __threadfence();
+                const unsigned old = atomicMax(offer + y, mine);
+                if (old < mine) {
+                    placed = true;
+                    if (old != 0u) {
+                        __threadfence();
+                        next = col[ordj[row[y] + degE[y] - (int)old]];
+                    }
+                    break;
+                }
+            }
+            if (!placed) st_cg(ptr + cur, dE);
+            cur = next;
+        }
+    }
+}
+
+// M[y] = suitor of y, or -1 (the suitors array the reference returns, suitor.cu:303-329).
+__global__ void k_suitor_result(int n, const int* __restrict__ row, const int* __restrict__ col, const int* __restrict__ ordj,
+    const int* __restrict__ degE, const unsigned* __restrict__ offer, int* __restrict__ M)
+{
+    for (long y = (long)blockIdx.x * blockDim.x + threadIdx.x; y < n; y += (long)gridDim.x * blockDim.x) {
+        const unsigned o = offer[y];
+        M[y] = o ? col[ordj[row[y] + degE[y] - (int)o]] : -1;
+    }
+}
+
+__global__ void k_check_symmetric(int n, const int* __restrict__ M, int* err)
+{
+    for (long v = (long)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (long)gridDim.x * blockDim.x) {
+        const int u = M[v];
+        if (u >= 0 && (u >= n || M[u] != (int)v)) atomicOr(err, ERR_ASYM_MATCH);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// pairwise prolongator (makeP_GPU) and coarse weights
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ double pair_norm(double a, double b)
+{
+    return __dsqrt_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)));
+}
+
+// A matched pair whose ||(w_v, w_u)|| > DBL_EPSILON is an aggregate with master min(v,u)
+// (_aggregate_symmetric_unsorted, matchingPairAggregation.cu:47-79); every other vertex with
+// |w| > DBL_EPSILON is a singleton (_aggregate_symmetric_step_two, :24-45).
+__global__ void k_pair_flags(int n, const int* __restrict__ M, const double* __restrict__ w, int* __restrict__ fm,
+    int* __restrict__ fs, int* err)
+{
+    for (long v = (long)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (long)gridDim.x * blockDim.x) {
+        const int u = M[v];
+        bool inpair = false;
+        if (u >= 0) inpair = pair_norm(w[v], w[u]) > DBL_EPSILON;
+        fm[v] = (inpair && v < u) ? 1 : 0;
+        const bool good_single = !inpair && fabs(w[v]) > DBL_EPSILON;
+        fs[v] = good_single ? 1 : 0;
+        if (!inpair && !good_single) atomicOr(err, ERR_BADW);
+    }
+}
+
+// Column/value of every row of P, the fine rows of every aggregate and the coarse weights
+// w_c = R w (shifted_CSRVector_product_adaptive_miniwarp2, CSR.cu:1195-1255). Pairs take ids
+// 0..npairs-1 in master order (cub::DeviceSelect, matchingPairAggregation.cu:127-148);
+// singletons follow in vertex order (the makePCol_CPU order, matchingAggregation.cu:62-87).
+__global__ void k_make_p(int n, const int* __restrict__ M, const double* __restrict__ w, const int* __restrict__ fm,
+    const int* __restrict__ pofs, const int* __restrict__ sofs, int npairs, int* __restrict__ agg, double* __restrict__ p,
+    int* __restrict__ fine0, int* __restrict__ fine1, double* __restrict__ wc)
+{
+    for (long v = (long)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (long)gridDim.x * blockDim.x) {
+        const int u = M[v];
+        const double wv = w[v];
+        if (fm[v]) {
+            const int id = pofs[v];
+            const double wu = w[u];
+            const double nrm = pair_norm(wv, wu);
+            const double pv = __ddiv_rn(wv, nrm), pu = __ddiv_rn(wu, nrm);
+            agg[v] = id;
+            agg[u] = id;
+            p[v] = pv;
+            p[u] = pu;
+            fine0[id] = (int)v;
+            fine1[id] = u;
+            wc[id] = __dadd_rn(__dmul_rn(pv, wv), __dmul_rn(pu, wu));
+        } else {
+            bool inpair = (u >= 0) && pair_norm(wv, w[u]) > DBL_EPSILON;
+            if (!inpair) {
+                const int id = npairs + sofs[v];
+                const double pv = __ddiv_rn(wv, fabs(wv));
+                agg[v] = id;
+                p[v] = pv;
+                fine0[id] = (int)v;
+                fine1[id] = -1;
+                wc[id] = __dmul_rn(pv, wv);
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Galerkin product C = P^T A P for a pairwise P
+// ------------------------------------------------------------------------------------------
+// One warp per coarse row I with fine rows f0 (< f1). Every entry a_ij of the fine rows gives
+// the rounded product t = a_ij p_j under key (J = agg(j), source row, position). After a rank
+// sort by key, each group of equal J is (AP)_{f0,J} = sum of its f0 terms and (AP)_{f1,J}
+// likewise (<= 2 terms each), and C_IJ = p_f0 (AP)_{f0,J} + p_f1 (AP)_{f1,J}: the values
+// nsparse forms for A*P and then R*(AP) (kernel_spgemm_hash_d.cu:792-799), since a sum of at most
+// two rounded terms does not depend on their order. FILL = false counts the entries of row I.
+template <bool FILL>
+__global__ void k_galerkin(int nc, const int* __restrict__ fine0, const int* __restrict__ fine1, const int* __restrict__ agg,
+    const double* __restrict__ p, const int* __restrict__ Arow, const int* __restrict__ Acol, const double* __restrict__ Aval,
+    int* __restrict__ Crow, int* __restrict__ Ccol, double* __restrict__ Cval, int cap, int* err)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int wpb = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned long long* key = (unsigned long long*)smem + (size_t)wid * cap;
+    double* tv = (double*)(smem + (size_t)wpb * cap * 8) + (size_t)wid * cap;
+    int* sidx = (int*)(smem + (size_t)wpb * cap * 16) + (size_t)wid * cap;
+    for (long I = (long)blockIdx.x * wpb + wid; I < nc; I += (long)gridDim.x * wpb) {
+        const int f0 = fine0[I], f1 = fine1[I];
+        const int b0 = Arow[f0], d0 = Arow[f0 + 1] - b0;
+        const int b1 = f1 >= 0 ? Arow[f1] : 0, d1 = f1 >= 0 ? Arow[f1 + 1] - b1 : 0;
+        const int cnt = d0 + d1;
+        if (cnt > cap) {
+            if (lane == 0) atomicOr(err, ERR_GALERKIN_CAP);
+            continue;
+        }
+        for (int t = lane; t < cnt; t += 32) {
+            const int j = t < d0 ? b0 + t : b1 + (t - d0);
+            const int c = Acol[j];
+            const unsigned src = t < d0 ? 0u : 1u;
+            key[t] = ((unsigned long long)(unsigned)agg[c] << 32) | ((unsigned long long)src << 31) | (unsigned)t;
+            tv[t] = __dmul_rn(Aval[j], p[c]);
+        }
+        __syncwarp();
+        for (int t = lane; t < cnt; t += 32) {
+            const unsigned long long kt = key[t];
+            int pos = 0;
+            for (int u = 0; u < cnt; u++) pos += key[u] < kt ? 1 : 0;
+            sidx[pos] = t;
+        }
+        __syncwarp();
+        const double p0 = p[f0], p1 = f1 >= 0 ? p[f1] : 0.0;
+        const int outbase = FILL ? Crow[I] : 0;
+        int nheads = 0;
+        for (int base = 0; base < cnt; base += 32) {
+            const int s = base + lane;
+            bool head = false;
+            int J = -1;
+            if (s < cnt) {
+                J = (int)(key[sidx[s]] >> 32);
+                head = (s == 0) || ((int)(key[sidx[s - 1]] >> 32) != J);
+            }
+            const unsigned hm = __ballot_sync(0xffffffffu, head);
+            if (FILL && head) {
+                double ap0 = 0.0, ap1 = 0.0;
+                int n0 = 0, n1 = 0;
+                for (int g = s; g < cnt; g++) {
+                    const unsigned long long kk = key[sidx[g]];
+                    if ((int)(kk >> 32) != J) break;
+                    const double tt = tv[sidx[g]];
+                    if (((kk >> 31) & 1ull) == 0) {
+                        ap0 = n0 == 0 ? tt : __dadd_rn(ap0, tt);
+                        n0++;
+                    } else {
+                        ap1 = n1 == 0 ? tt : __dadd_rn(ap1, tt);
+                        n1++;
+                    }
+                }
+                double cv;
+                if (n0 && n1) cv = __dadd_rn(__dmul_rn(p0, ap0), __dmul_rn(p1, ap1));
+                else if (n0) cv = __dmul_rn(p0, ap0);
+                else cv = __dmul_rn(p1, ap1);
+                const int o = outbase + nheads + __popc(hm & ((1u << lane) - 1u));
+                Ccol[o] = J;
+                Cval[o] = cv;
+            }
+            nheads += __popc(hm);
+        }
+        if (!FILL && lane == 0) Crow[I] = nheads;
+        __syncwarp();
+    }
+}
+
+// composite prolongator of the level: P <- P * P_sweep (one entry per row in both).
+__global__ void k_compose(int n, int* __restrict__ agg, double* __restrict__ p, const int* __restrict__ agg_s,
+    const double* __restrict__ p_s, int first)
+{
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        if (first) {
+            agg[i] = agg_s[i];
+            p[i] = p_s[i];
+        } else {
+            const int c = agg[i];
+            p[i] = __dmul_rn(p[i], p_s[c]);
+            agg[i] = agg_s[c];
+        }
+    }
+}
+
+// R = P^T as CSR: counting sort of the rows by aggregate, rows ascending inside.
+__global__ void k_count(int n, const int* __restrict__ agg, int* cnt)
+{
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) atomicAdd(cnt + agg[i], 1);
+}
+__global__ void k_scatter(int n, const int* __restrict__ agg, const int* __restrict__ rptr, int* fillpos, int* __restrict__ ridx)
+{
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const int c = agg[i];
+        ridx[rptr[c] + atomicAdd(fillpos + c, 1)] = (int)i;
+    }
+}
+__global__ void k_sort_rrows(int nc, const int* __restrict__ rptr, int* __restrict__ ridx, const double* __restrict__ p,
+    double* __restrict__ rval, float* __restrict__ rval32)
+{
+    for (long c = (long)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (long)gridDim.x * blockDim.x) {
+        const int b = rptr[c], e = rptr[c + 1];
+        for (int i = b + 1; i < e; i++) {
+            const int v = ridx[i];
+            int j = i - 1;
+            while (j >= b && ridx[j] > v) {
+                ridx[j + 1] = ridx[j];
+                j--;
+            }
+            ridx[j + 1] = v;
+        }
+        for (int i = b; i < e; i++) {
+            const double pv = p[ridx[i]];
+            rval[i] = pv;
+            if (rval32) rval32[i] = (float)pv;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------------------------
+static std::string err_text(int e)
+{
+    std::string s;
+    if (e & ERR_ROW0) s += "row[0] != 0; ";
+    if (e & ERR_ROWN) s += "row[n] != nnz; ";
+    if (e & ERR_ROWORDER) s += "row offsets decrease or exceed nnz; ";
+    if (e & ERR_COLRANGE) s += "column index out of range; ";
+    if (e & ERR_COLSORT) s += "columns not strictly ascending in a row; ";
+    if (e & ERR_NODIAG) s += "a row has no diagonal entry; ";
+    if (e & ERR_SUITOR_BUDGET) s += "suitor matching exceeded its iteration bound; ";
+    if (e & ERR_ASYM_MATCH) s += "matching is not symmetric; ";
+    if (e & ERR_BADW) s += "weight vector entry <= DBL_EPSILON; ";
+    if (e & ERR_GALERKIN_CAP) s += "Galerkin row exceeds its shared-memory capacity; ";
+    return s;
+}
+
+static int read_err(const int* err, cudaStream_t s)
+{
+    int e = 0;
+    BCMGX_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    BCMGX_CUDA(cudaStreamSynchronize(s));
+    return e;
+}
+
+static int row_max(const DevCsr& A, cudaStream_t s)
+{
+    DBuf<int> mx;
+    mx.alloc(1, s);
+    BCMGX_CUDA(cudaMemsetAsync(mx.p, 0, sizeof(int), s));
+    note_launch(); k_row_max<<<gs_grid(A.n), 256, 0, s>>>(A.n, A.row.p, mx.p);
+    BCMGX_CHECK_LAUNCH();
+    return read_err(mx.p, s);
+}
+
+void edge_weights_dev(int n, int64_t nnz, const int* row, const int* col, const double* val, const double* w, double* W,
+    int* tpos, double* min_out_host, cudaStream_t s)
+{
+    DBuf<double> C;
+    DBuf<unsigned long long> mn;
+    DBuf<int> err;
+    C.alloc(n, s);
+    mn.alloc(1, s);
+    err.alloc(1, s);
+    BCMGX_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), s));
+    const double dmax = DBL_MAX;
+    BCMGX_CUDA(cudaMemcpyAsync(mn.p, &dmax, sizeof(double), cudaMemcpyHostToDevice, s));
+    note_launch(); k_diag_c<<<gs_grid(n), 256, 0, s>>>(n, row, col, val, w, C.p, err.p);
+    note_launch(); k_tpos<<<warp_grid(n), 256, 0, s>>>(n, row, col, tpos);
+    note_launch(); k_ahat_min<<<warp_grid(n), 256, 0, s>>>(n, row, col, val, w, C.p, mn.p);
+    BCMGX_CHECK_LAUNCH();
+    double m = 0;
+    BCMGX_CUDA(cudaMemcpyAsync(&m, mn.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+    int e = read_err(err.p, s);
+    if (e) throw Error(BCMGX_ERR_INVALID_INPUT, "edge weights: " + err_text(e));
+    if (std::fabs(m) < DBL_EPSILON) m = DBL_EPSILON;   // toMaximumProductMatrix, matching.cu:243-245
+    const double zero_sub = kSuitorEps / (0.999 * m);
+    note_launch(); k_logw<<<warp_grid(n), 256, 0, s>>>(n, row, col, val, w, C.p, tpos, zero_sub, W);
+    BCMGX_CHECK_LAUNCH();
+    if (min_out_host) *min_out_host = m;
+}
+
+void validate_csr_dev(int n, int m, int64_t nnz, const int* row, const int* col, bool need_diag, cudaStream_t s)
+{
+    DBuf<int> err, mx;
+    err.alloc(1, s);
+    mx.alloc(1, s);
+    BCMGX_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), s));
+    BCMGX_CUDA(cudaMemsetAsync(mx.p, 0, sizeof(int), s));
+    note_launch();
+    k_validate<<<warp_grid(n), 256, 0, s>>>(n, m, nnz, row, col, err.p, mx.p, need_diag ? 1 : 0);
+    BCMGX_CHECK_LAUNCH();
+    const int e = read_err(err.p, s);
+    if (e) throw Error(BCMGX_ERR_INVALID_INPUT, "input matrix: " + err_text(e));
+}
+
+void tpos_dev(int n, const int* row, const int* col, int* tpos, cudaStream_t s)
+{
+    note_launch(); k_tpos<<<warp_grid(n), 256, 0, s>>>(n, row, col, tpos);
+    BCMGX_CHECK_LAUNCH();
+}
+
+void suitor_dev(int n, int64_t nnz, const int* row, const int* col, const double* W, const int* tpos, int* M, cudaStream_t s)
+{
+    DBuf<int> rank, ordj, degE, ptr, err;
+    DBuf<unsigned> offer;
+    rank.alloc(std::max<int64_t>(nnz, 1), s);
+    ordj.alloc(std::max<int64_t>(nnz, 1), s);
+    degE.alloc(n, s);
+    ptr.alloc(n, s);
+    offer.alloc(n, s);
+    err.alloc(1, s);
+    BCMGX_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), s));
+    BCMGX_CUDA(cudaMemsetAsync(ptr.p, 0, sizeof(int) * n, s));
+    BCMGX_CUDA(cudaMemsetAsync(offer.p, 0, sizeof(unsigned) * n, s));
+    note_launch(); k_rank<<<warp_grid(n), 256, 0, s>>>(n, row, col, W, rank.p, ordj.p, degE.p);
+    note_launch(); k_suitor<<<gs_grid(n, 128), 128, 0, s>>>(n, row, col, ordj.p, rank.p, tpos, degE.p, offer.p, ptr.p,
+        (long long)nnz + n + 1024, err.p);
+    note_launch(); k_suitor_result<<<gs_grid(n), 256, 0, s>>>(n, row, col, ordj.p, degE.p, offer.p, M);
+    note_launch(); k_check_symmetric<<<gs_grid(n), 256, 0, s>>>(n, M, err.p);
+    BCMGX_CHECK_LAUNCH();
+    int e = read_err(err.p, s);
+    if (e) throw Error(e & ERR_SUITOR_BUDGET ? BCMGX_ERR_TIMEOUT : BCMGX_ERR_INTERNAL, "suitor matching: " + err_text(e));
+}
+
+// One pairwise sweep on A (weights w): matching, prolongator, Galerkin product, coarse weights.
+struct SweepOut {
+    DevCsr C;
+    DBuf<int> agg;
+    DBuf<double> p, wc;
+    int nc = 0;
+};
+
+static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w, SweepOut& out, int level, int sweep)
+{
+    cudaStream_t s = H->stream;
+    const int n = A.n;
+    const int64_t nnz = A.nnz;
+    DBuf<double> W;
+    DBuf<int> tpos, M, fm, fs, pofs, sofs, err;
+    W.alloc(std::max<int64_t>(nnz, 1), s);
+    tpos.alloc(std::max<int64_t>(nnz, 1), s);
+    M.alloc(n, s);
+    edge_weights_dev(n, nnz, A.row.p, A.col.p, A.val.p, w, W.p, tpos.p, nullptr, s);
+    suitor_dev(n, nnz, A.row.p, A.col.p, W.p, tpos.p, M.p, s);
+    W.release();
+    tpos.release();
+    fm.alloc(n, s);
+    fs.alloc(n, s);
+    pofs.alloc(n, s);
+    sofs.alloc(n, s);
+    err.alloc(1, s);
+    BCMGX_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), s));
+    note_launch(); k_pair_flags<<<gs_grid(n), 256, 0, s>>>(n, M.p, w, fm.p, fs.p, err.p);
+    BCMGX_CHECK_LAUNCH();
+    const long long npairs = scan_exclusive(fm.p, pofs.p, n, false, s);
+    const long long nsing = scan_exclusive(fs.p, sofs.p, n, false, s);
+    int e = read_err(err.p, s);
+    if (e) throw Error(BCMGX_ERR_INTERNAL, "aggregation: " + err_text(e));
+    const int nc = (int)(npairs + nsing);
+    out.nc = nc;
+    DBuf<int> fine0, fine1;
+    out.agg.alloc(n, s);
+    out.p.alloc(n, s);
+    out.wc.alloc(nc, s);
+    fine0.alloc(nc, s);
+    fine1.alloc(nc, s);
+    note_launch(); k_make_p<<<gs_grid(n), 256, 0, s>>>(n, M.p, w, fm.p, pofs.p, sofs.p, (int)npairs, out.agg.p, out.p.p, fine0.p, fine1.p, out.wc.p);
+    BCMGX_CHECK_LAUNCH();
+    if (H->prm.record_sweeps) {
+        SweepRecord r;
+        r.level = level;
+        r.sweep = sweep;
+        r.n = n;
+        r.nc = nc;
+        r.match.resize(n);
+        r.agg.resize(n);
+        r.p.resize(n);
+        r.w.resize(n);
+        BCMGX_CUDA(cudaMemcpyAsync(r.match.data(), M.p, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+        BCMGX_CUDA(cudaMemcpyAsync(r.agg.data(), out.agg.p, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+        BCMGX_CUDA(cudaMemcpyAsync(r.p.data(), out.p.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+        BCMGX_CUDA(cudaMemcpyAsync(r.w.data(), w, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+        BCMGX_CUDA(cudaStreamSynchronize(s));
+        H->rec.push_back(std::move(r));
+    }
+    M.release();
+    fm.release();
+    fs.release();
+    pofs.release();
+    sofs.release();
+    // Galerkin: count, prefix sum, fill
+    const int amax = A.max_row > 0 ? A.max_row : row_max(A, s);
+    const int cap = std::max(2 * amax, 32);
+    const size_t per_warp = (size_t)cap * 20;
+    const size_t smem_limit = 200 * 1024;
+    BCMGX_REQUIRE(per_warp <= smem_limit, BCMGX_ERR_UNSUPPORTED,
+        "coarse row too long for the Galerkin kernel (" + std::to_string(cap) + " candidate entries)");
+    int wpb = (int)std::min<size_t>(8, std::max<size_t>(1, (48 * 1024) / per_warp));
+    size_t smem = per_warp * wpb;
+    if (smem > 48 * 1024) {
+        BCMGX_CUDA(cudaFuncSetAttribute(k_galerkin<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        BCMGX_CUDA(cudaFuncSetAttribute(k_galerkin<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    const int g = (int)std::max<long>(1, std::min<long>(((long)nc + wpb - 1) / wpb, (long)num_sms() * 32));
+    DevCsr& C = out.C;
+    C.n = C.m = nc;
+    C.row.alloc((size_t)nc + 1, s);
+    DBuf<int> counts;
+    counts.alloc(std::max(nc, 1), s);
+    note_launch(); k_galerkin<false><<<g, wpb * 32, smem, s>>>(nc, fine0.p, fine1.p, out.agg.p, out.p.p, A.row.p, A.col.p, A.val.p,
+        counts.p, nullptr, nullptr, cap, err.p);
+    BCMGX_CHECK_LAUNCH();
+    C.nnz = scan_exclusive(counts.p, C.row.p, nc, true, s);
+    C.col.alloc(std::max<int64_t>(C.nnz, 1), s);
+    C.val.alloc(std::max<int64_t>(C.nnz, 1), s);
+    note_launch(); k_galerkin<true><<<g, wpb * 32, smem, s>>>(nc, fine0.p, fine1.p, out.agg.p, out.p.p, A.row.p, A.col.p, A.val.p,
+        C.row.p, C.col.p, C.val.p, cap, err.p);
+    BCMGX_CHECK_LAUNCH();
+    e = read_err(err.p, s);
+    if (e) throw Error(BCMGX_ERR_INTERNAL, "galerkin: " + err_text(e));
+    C.max_row = row_max(C, s);
+}
+
+static void finish_level_matrix(Level& V, bool want_f32, cudaStream_t s)
+{
+    const int n = V.A.n;
+    V.M.alloc(n, s);
+    if (want_f32) V.M32.alloc(n, s);
+    note_launch(); k_abs_row_sum<<<gs_grid(n), 256, 0, s>>>(n, V.A.row.p, V.A.val.p, V.M.p, want_f32 ? V.M32.p : nullptr);
+    if (want_f32) {
+        V.A.val32.alloc(std::max<int64_t>(V.A.nnz, 1), s);
+        note_launch(); k_to_f32<<<gs_grid(V.A.nnz), 256, 0, s>>>(V.A.nnz, V.A.val.p, V.A.val32.p);
+    }
+    BCMGX_CHECK_LAUNCH();
+}
+
+static void build_restriction(Level& V, int nc, bool want_f32, cudaStream_t s)
+{
+    const int n = V.A.n;
+    DBuf<int> cnt, fillpos;
+    cnt.alloc(std::max(nc, 1), s);
+    fillpos.alloc(std::max(nc, 1), s);
+    BCMGX_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int) * std::max(nc, 1), s));
+    BCMGX_CUDA(cudaMemsetAsync(fillpos.p, 0, sizeof(int) * std::max(nc, 1), s));
+    note_launch(); k_count<<<gs_grid(n), 256, 0, s>>>(n, V.agg.p, cnt.p);
+    BCMGX_CHECK_LAUNCH();
+    V.rptr.alloc((size_t)nc + 1, s);
+    scan_exclusive(cnt.p, V.rptr.p, nc, true, s);
+    V.ridx.alloc(n, s);
+    V.rval.alloc(n, s);
+    if (want_f32) {
+        V.rval32.alloc(n, s);
+        V.p32.alloc(n, s);
+        note_launch(); k_to_f32<<<gs_grid(n), 256, 0, s>>>(n, V.p.p, V.p32.p);
+    }
+    note_launch(); k_scatter<<<gs_grid(n), 256, 0, s>>>(n, V.agg.p, V.rptr.p, fillpos.p, V.ridx.p);
+    note_launch(); k_sort_rrows<<<gs_grid(nc), 256, 0, s>>>(nc, V.rptr.p, V.ridx.p, V.p.p, V.rval.p, want_f32 ? V.rval32.p : nullptr);
+    BCMGX_CHECK_LAUNCH();
+}
+
+// AMG::ApplyData::setGridSweeps (AMG.cu:306-331).
+static std::vector<int> grid_sweeps(int cycle_type, int max_levels)
+{
+    const int ml = max_levels - 1;
+    std::vector<int> g(std::max(ml, 0), 1);
+    if (cycle_type == BCMGX_CYCLE_H) {
+        for (int i = 0; i < ml; i++)
+            if (i % 2 == 0) g[i] = 2;
+    } else if (cycle_type == BCMGX_CYCLE_W) {
+        for (int i = 0; i < ml - 1; i++) g[i] = 2;
+    }
+    return g;
+}
+
+void build_hierarchy(bcmgx_hierarchy* H, const bcmgx_csr* Ain)
+{
+    cudaStream_t s = H->stream;
+    const bcmgx_params& P = H->prm;
+    const bool f32 = P.vcycle_precision == BCMGX_VCYCLE_FP32;
+    H->lv.clear();
+    H->lv.emplace_back();
+    Level& L0 = H->lv[0];
+    DevCsr& A = L0.A;
+    A.n = Ain->n;
+    A.m = Ain->m;
+    A.nnz = Ain->nnz;
+    A.row.alloc((size_t)A.n + 1, s);
+    A.col.alloc(std::max<int64_t>(A.nnz, 1), s);
+    A.val.alloc(std::max<int64_t>(A.nnz, 1), s);
+    const cudaMemcpyKind kind = Ain->on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    BCMGX_CUDA(cudaMemcpyAsync(A.row.p, Ain->row, sizeof(int) * ((size_t)A.n + 1), kind, s));
+    BCMGX_CUDA(cudaMemcpyAsync(A.col.p, Ain->col, sizeof(int) * A.nnz, kind, s));
+    BCMGX_CUDA(cudaMemcpyAsync(A.val.p, Ain->val, sizeof(double) * A.nnz, kind, s));
+    {
+        DBuf<int> err, mx;
+        err.alloc(1, s);
+        mx.alloc(1, s);
+        BCMGX_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), s));
+        BCMGX_CUDA(cudaMemsetAsync(mx.p, 0, sizeof(int), s));
+        note_launch(); k_validate<<<warp_grid(A.n), 256, 0, s>>>(A.n, A.m, A.nnz, A.row.p, A.col.p, err.p, mx.p,
+            P.preconditioner == BCMGX_PREC_BCMG ? 1 : 0);
+        BCMGX_CHECK_LAUNCH();
+        int e = read_err(err.p, s);
+        if (e) throw Error(BCMGX_ERR_INVALID_INPUT, "input matrix: " + err_text(e));
+        A.max_row = read_err(mx.p, s);
+    }
+    const int L0n = A.n;
+    H->grid_sweeps = grid_sweeps(P.cycle_type, P.max_levels);
+    H->ftcoarse = 1;
+    // AMG::BuildData::setMaxCoarseSize, AMG.cu:238-241
+    H->maxcoarsesize = (int)(40 * std::pow((double)L0n, 1.0 / 3.0));
+    if (P.preconditioner != BCMGX_PREC_BCMG) {
+        finish_level_matrix(L0, false, s);
+        H->op_cmplx = 1;
+        H->op_wcmplx = 1;
+        H->avg_cratio = 1;
+        return;
+    }
+    const int sweepnumber = P.aggrsweeps + 1;
+    DBuf<double> w;
+    w.alloc(L0n, s);
+    note_launch(); k_fill<<<gs_grid(L0n), 256, 0, s>>>(L0n, w.p, 1.0);
+    BCMGX_CHECK_LAUNCH();
+    double avcoarseratio = 0;
+    int level;
+    for (level = 1; level < P.max_levels;) {
+        const DevCsr* Ai_ = &H->lv[level - 1].A;
+        const int nfine = Ai_->n;
+        SweepOut prev, cur;
+        DBuf<double> wsw;   // weights of the running sweep (moved from the previous one)
+        const double* wi_ = w.p;
+        DBuf<int> Pagg;
+        DBuf<double> Pval;
+        Pagg.alloc(nfine, s);
+        Pval.alloc(nfine, s);
+        for (int i = 0; i < sweepnumber; i++) {
+            pairwise_sweep(H, *Ai_, wi_, cur, level - 1, i);
+            const double size_precoarse = Ai_->n, size_coarse = cur.nc;
+            const double coarse_ratio = size_precoarse / size_coarse;
+            if (coarse_ratio <= kCoarseRatioThreshold) H->ftcoarse = kFtcoarseInc;
+            note_launch(); k_compose<<<gs_grid(nfine), 256, 0, s>>>(nfine, Pagg.p, Pval.p, cur.agg.p, cur.p.p, i == 0 ? 1 : 0);
+            BCMGX_CHECK_LAUNCH();
+            if (size_coarse <= (double)H->ftcoarse * H->maxcoarsesize || i + 1 == sweepnumber) break;
+            prev = std::move(cur);
+            cur = SweepOut();
+            Ai_ = &prev.C;
+            wi_ = prev.wc.p;
+        }
+        w = std::move(cur.wc);
+        Level& F = H->lv[level - 1];
+        F.agg = std::move(Pagg);
+        F.p = std::move(Pval);
+        const int nc = cur.C.n;
+        build_restriction(F, nc, f32, s);
+        if (level == 1) finish_level_matrix(F, f32, s);
+        Level NL;
+        NL.A = std::move(cur.C);
+        H->lv.push_back(std::move(NL));
+        const double size_coarse = H->lv[level].A.n;
+        avcoarseratio += H->lv[level - 1].A.n / size_coarse;
+        level++;
+        if (size_coarse <= (double)H->ftcoarse * H->maxcoarsesize) break;
+    }
+    if (H->lv.size() == 1) finish_level_matrix(H->lv[0], false, s);
+    const int Lc = (int)H->lv.size();
+    for (int l = 1; l < Lc; l++) finish_level_matrix(H->lv[l], f32 && l < Lc - 1, s);
+    // the coarsest level runs in FP64 even in the FP32 cycle
+    if (Lc > 1 && f32) {
+        Level& last = H->lv[Lc - 1];
+        last.A.val32.release();
+        last.M32.release();
+    }
+    // AMG::Hierarchy::finalize_cmplx / finalize_wcmplx (AMG.cu:144-165)
+    double nnz0 = (double)H->lv[0].A.nnz, c = 0, wc = 0;
+    for (int l = 0; l < Lc; l++) {
+        c += (double)H->lv[l].A.nnz;
+        wc += std::pow(2.0, (double)l) * (double)H->lv[l].A.nnz;
+    }
+    H->op_cmplx = c / nnz0;
+    H->op_wcmplx = wc / nnz0;
+    H->avg_cratio = level > 1 ? avcoarseratio / (level - 1) : 1;
+    BCMGX_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace bcmgx

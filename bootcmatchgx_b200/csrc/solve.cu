@@ -1,0 +1,725 @@
+// solve.cu -- solve phase on the device: the l1-Jacobi V-cycle and flexible CG.
+//
+// V-cycle: GAMG_cycle (BCMGX/src/preconditioner/bcmg/GAMG_cycle.cu:58-236) at np = 1, with
+// l1-Jacobi sweeps (l1jacobi.cu:345-479). FCG: flexibileConjugateGradients_v3
+// (BCMGX/src/solver/fcg/FCG.cu:27-165). Differences in form, not in result:
+//  * a sweep from a zero iterate is u = f / M (what the full sweep computes when u = 0), so
+//    the first pre-smoothing sweep of every level and the first coarse sweep skip the SpMV;
+//  * sweeps alternate between two level buffers and the prolongation writes out of place so
+//    that no copy-back is needed (the reference copies when the sweep count is odd);
+//  * the FCG dots and axpys are fused with the SpMV and with each other, and the scalars stay
+//    on the device; reductions are two-stage and deterministic.
+// FP32 V-cycle (vcycle_precision = FP32): levels 0..L-2 run on FP32 matrix values and vectors;
+// the coarsest level, the outer residual, the dots and the direction updates stay FP64.
+#include "internal.h"
+#include "rowops.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+
+namespace bcmgx {
+
+int num_sms()
+{
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    return sms;
+}
+
+static int rowop_grid(int n, int tpr)
+{
+    long need = ((long)n * tpr + 255) / 256;
+    long cap = (long)num_sms() * 8;
+    return (int)std::max<long>(1, std::min(need, cap));
+}
+
+template <int OP, typename VT, typename XT, typename FT, typename MT, typename YT>
+static void launch_rowop(int tpr, int n, const int* row, const int* col, const VT* val, const XT* x, const FT* f,
+    const MT* M, YT* y, double alpha, double beta, const int* skip, cudaStream_t s)
+{
+    if (n <= 0) return;
+    const int g = rowop_grid(n, tpr);
+    switch (tpr) {
+    case 1: note_launch(); k_rowop<1, OP><<<g, 256, 0, s>>>(n, row, col, val, x, f, M, y, alpha, beta, skip); break;
+    case 2: note_launch(); k_rowop<2, OP><<<g, 256, 0, s>>>(n, row, col, val, x, f, M, y, alpha, beta, skip); break;
+    case 4: note_launch(); k_rowop<4, OP><<<g, 256, 0, s>>>(n, row, col, val, x, f, M, y, alpha, beta, skip); break;
+    case 8: note_launch(); k_rowop<8, OP><<<g, 256, 0, s>>>(n, row, col, val, x, f, M, y, alpha, beta, skip); break;
+    case 16: note_launch(); k_rowop<16, OP><<<g, 256, 0, s>>>(n, row, col, val, x, f, M, y, alpha, beta, skip); break;
+    default: note_launch(); k_rowop<32, OP><<<g, 256, 0, s>>>(n, row, col, val, x, f, M, y, alpha, beta, skip); break;
+    }
+    BCMGX_CHECK_LAUNCH();
+}
+
+int default_tpr(int n, int64_t nnz)
+{
+    double avg = n > 0 ? (double)nnz / n : 1.0;
+    if (avg <= 3) return 2;
+    if (avg <= 6) return 4;
+    if (avg <= 16) return 8;
+    if (avg <= 40) return 16;
+    return 32;
+}
+
+void launch_spmv(int n, const int* row, const int* col, const double* val, const double* x, double* y,
+    double alpha, double beta, int tpr, cudaStream_t s)
+{
+    launch_rowop<OP_AXPBY, double, double, double, double, double>(tpr, n, row, col, val, x,
+        (const double*)nullptr, (const double*)nullptr, y, alpha, beta, nullptr, s);
+}
+
+// Threads per row for a matrix: each power of two from 2 to 32 is timed on the matrix itself
+// (three y = A x launches after one warm-up) and the fastest is kept.
+int autotune_tpr(const DevCsr& A, cudaStream_t s)
+{
+    if (A.n < 4096) return default_tpr(A.n, A.nnz);
+    DBuf<double> x, y;
+    x.alloc(A.m, s);
+    y.alloc(A.n, s);
+    BCMGX_CUDA(cudaMemsetAsync(x.p, 0, sizeof(double) * A.m, s));
+    cudaEvent_t e0, e1;
+    BCMGX_CUDA(cudaEventCreate(&e0));
+    BCMGX_CUDA(cudaEventCreate(&e1));
+    int best = default_tpr(A.n, A.nnz);
+    float best_ms = 1e30f;
+    for (int t = 2; t <= 32; t *= 2) {
+        launch_spmv(A.n, A.row.p, A.col.p, A.val.p, x.p, y.p, 1.0, 0.0, t, s);
+        BCMGX_CUDA(cudaEventRecord(e0, s));
+        for (int r = 0; r < 3; r++) launch_spmv(A.n, A.row.p, A.col.p, A.val.p, x.p, y.p, 1.0, 0.0, t, s);
+        BCMGX_CUDA(cudaEventRecord(e1, s));
+        BCMGX_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        BCMGX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = t;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return best;
+}
+
+// ------------------------------------------------------------------------------------------
+// element-wise kernels of the cycle
+// ------------------------------------------------------------------------------------------
+template <typename T> struct Wider { using type = double; };
+template <> struct Wider<float> { using type = float; };
+
+// Sweep from a zero iterate: u = f / M; optionally keeps a converted copy of f.
+template <typename FT, typename MT, typename YT, typename CT>
+__global__ void k_first_sweep(int n, const FT* __restrict__ f, const MT* __restrict__ M, YT* __restrict__ u,
+    CT* __restrict__ fcopy, const int* __restrict__ skip)
+{
+    if (skip && *skip) return;
+    using AT = typename Wider<MT>::type;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        AT fi = (AT)f[i];
+        if (fcopy) fcopy[i] = (CT)fi;
+        u[i] = (YT)(fi / (AT)M[i]);
+    }
+}
+
+template <typename ST, typename DT>
+__global__ void k_convert(int n, const ST* __restrict__ a, DT* __restrict__ b, const int* __restrict__ skip)
+{
+    if (skip && *skip) return;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) b[i] = (DT)a[i];
+}
+
+// out[c] = sum over the fine rows i of aggregate c (ascending) of p_i * res_i  (R = P^T).
+template <typename RT, typename WT, typename OT>
+__global__ void k_restrict(int nc, const int* __restrict__ rptr, const int* __restrict__ ridx,
+    const WT* __restrict__ rval, const RT* __restrict__ res, OT* __restrict__ out, const int* __restrict__ skip)
+{
+    if (skip && *skip) return;
+    using AT = typename Wider<OT>::type;
+    for (long c = (long)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (long)gridDim.x * blockDim.x) {
+        AT s = 0;
+        for (int t = rptr[c]; t < rptr[c + 1]; t++) s += (AT)rval[t] * (AT)res[ridx[t]];
+        out[c] = (OT)s;
+    }
+}
+
+// y = p .* xc[agg] + x  (P has one entry per row; y may alias x).
+template <typename PT, typename CT, typename XT, typename YT>
+__global__ void k_prolong(int n, const int* __restrict__ agg, const PT* __restrict__ p, const CT* __restrict__ xc,
+    const XT* x, YT* y, const int* __restrict__ skip)
+{
+    if (skip && *skip) return;
+    using AT = typename Wider<YT>::type;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        y[i] = (YT)((AT)p[i] * (AT)xc[agg[i]] + (AT)x[i]);
+}
+
+static int ew_grid(long n) { return (int)std::max<long>(1, std::min<long>((n + 255) / 256, (long)num_sms() * 8)); }
+
+// ------------------------------------------------------------------------------------------
+// typed vector views and the cycle
+// ------------------------------------------------------------------------------------------
+struct Vec {
+    void* p = nullptr;
+    bool f32 = false;
+    bool operator==(const Vec& o) const { return p == o.p; }
+    bool operator!=(const Vec& o) const { return p != o.p; }
+};
+
+struct Cycle {
+    bcmgx_hierarchy* H;
+    cudaStream_t s;
+    const int* skip;
+    bool fp32;
+    int L;
+
+    bool lf32(int l) const { return fp32 && l < L - 1; }
+    Level& lv(int l) const { return H->lv[l]; }
+
+    void sweep(int l, Vec f, Vec in, Vec out) const
+    {
+        Level& V = lv(l);
+        const DevCsr& A = V.A;
+        if (!lf32(l)) {
+            launch_rowop<OP_JACOBI>(A.tpr, A.n, A.row.p, A.col.p, A.val.p, (const double*)in.p, (const double*)f.p,
+                V.M.p, (double*)out.p, 1.0, 0.0, skip, s);
+        } else if (out.f32) {
+            launch_rowop<OP_JACOBI>(A.tpr, A.n, A.row.p, A.col.p, A.val32.p, (const float*)in.p, (const float*)f.p,
+                V.M32.p, (float*)out.p, 1.0, 0.0, skip, s);
+        } else {
+            launch_rowop<OP_JACOBI>(A.tpr, A.n, A.row.p, A.col.p, A.val32.p, (const float*)in.p, (const float*)f.p,
+                V.M32.p, (double*)out.p, 1.0, 0.0, skip, s);
+        }
+    }
+
+    // sweep from zero; if fcopy is given (level 0 of the FP32 cycle) f is double and is also
+    // converted into fcopy.
+    void first_sweep(int l, Vec f, Vec out, Vec fcopy) const
+    {
+        Level& V = lv(l);
+        const int n = V.A.n, g = ew_grid(n);
+        if (!lf32(l)) {
+            note_launch(); k_first_sweep<double, double, double, double><<<g, 256, 0, s>>>(n, (const double*)f.p, V.M.p, (double*)out.p, (double*)nullptr, skip);
+        } else if (f.f32) {
+            if (out.f32)
+                { note_launch(); k_first_sweep<float, float, float, float><<<g, 256, 0, s>>>(n, (const float*)f.p, V.M32.p, (float*)out.p, (float*)nullptr, skip); }
+            else
+                { note_launch(); k_first_sweep<float, float, double, float><<<g, 256, 0, s>>>(n, (const float*)f.p, V.M32.p, (double*)out.p, (float*)nullptr, skip); }
+        } else {
+            if (out.f32)
+                { note_launch(); k_first_sweep<double, float, float, float><<<g, 256, 0, s>>>(n, (const double*)f.p, V.M32.p, (float*)out.p, (float*)fcopy.p, skip); }
+            else
+                { note_launch(); k_first_sweep<double, float, double, float><<<g, 256, 0, s>>>(n, (const double*)f.p, V.M32.p, (double*)out.p, (float*)fcopy.p, skip); }
+        }
+        BCMGX_CHECK_LAUNCH();
+    }
+
+    void copy(Vec a, Vec b, int n) const
+    {
+        const int g = ew_grid(n);
+        if (a.f32 == b.f32) {
+            BCMGX_CUDA(cudaMemcpyAsync(b.p, a.p, (size_t)n * (a.f32 ? 4 : 8), cudaMemcpyDeviceToDevice, s));
+        } else if (a.f32) {
+            note_launch(); k_convert<float, double><<<g, 256, 0, s>>>(n, (const float*)a.p, (double*)b.p, skip);
+        } else {
+            note_launch(); k_convert<double, float><<<g, 256, 0, s>>>(n, (const double*)a.p, (float*)b.p, skip);
+        }
+        BCMGX_CHECK_LAUNCH();
+    }
+
+    void zero(Vec a, int n) const { BCMGX_CUDA(cudaMemsetAsync(a.p, 0, (size_t)n * (a.f32 ? 4 : 8), s)); }
+
+    // k sweeps from `src` (p == nullptr: zero iterate) ending in `dst`, using the level
+    // buffers A and B as intermediates. fcopy: see first_sweep.
+    void chain(int l, int k, Vec f, Vec src, Vec dst, Vec A, Vec B, Vec fcopy = Vec()) const
+    {
+        const int n = lv(l).A.n;
+        if (k <= 0) {
+            if (src.p == nullptr) zero(dst, n);
+            else if (src != dst) copy(src, dst, n);
+            return;
+        }
+        std::vector<Vec> out(k);
+        out[k - 1] = dst;
+        for (int i = k - 2; i >= 0; i--) out[i] = (out[i + 1] == A) ? B : A;
+        if (src.p != nullptr && src == out[0]) {
+            Vec other = (src == A) ? B : A;
+            copy(src, other, n);
+            src = other;
+        }
+        Vec fl = f;
+        for (int i = 0; i < k; i++) {
+            if (i == 0 && src.p == nullptr) {
+                first_sweep(l, f, out[0], fcopy);
+                if (fcopy.p) fl = fcopy;   // later sweeps read the converted right-hand side
+            } else {
+                sweep(l, fl, i == 0 ? src : out[i - 1], out[i]);
+            }
+        }
+    }
+
+    // One cycle on level l for right-hand side f, starting from x_cur (nullptr: zero),
+    // leaving the result in dst.
+    void run(int l, Vec f, Vec x_cur, Vec dst) const
+    {
+        Level& V = lv(l);
+        const int n = V.A.n;
+        const bool f32 = lf32(l);
+        Vec A, B;
+        if (l == 0 && !f32) {
+            A = dst;
+            B = Vec { V.x2.p, false };
+        } else if (f32) {
+            A = Vec { V.x32.p, true };
+            B = Vec { V.x232.p, true };
+        } else {
+            A = Vec { V.x.p, false };
+            B = Vec { V.x2.p, false };
+        }
+        const bcmgx_params& P = H->prm;
+        // level-0 FP32: f arrives in FP64 and is converted once into rhs32
+        Vec fcopy;
+        if (f32 && !f.f32) {
+            fcopy = Vec { V.rhs32.p, true };
+        }
+        if (l == L - 1) {
+            chain(l, P.relaxnumber_coarse, f, x_cur, dst, A, B, fcopy);
+            return;
+        }
+        const int coeff = P.cycle_type == BCMGX_CYCLE_VARIABLE_V ? (1 << l) : 1;
+        const int kpre = P.prerelax_sweeps * coeff, kpost = P.postrelax_sweeps * coeff;
+        Vec pre_dst = (dst.f32 == f32) ? dst : A;
+        Vec fl = f;
+        if (fcopy.p) {
+            if (x_cur.p == nullptr && kpre > 0) {
+                chain(l, kpre, f, x_cur, pre_dst, A, B, fcopy);
+            } else {
+                copy(f, fcopy, n);
+                chain(l, kpre, fcopy, x_cur, pre_dst, A, B);
+            }
+            fl = fcopy;
+        } else {
+            chain(l, kpre, f, x_cur, pre_dst, A, B);
+        }
+        Vec xpre = pre_dst;
+        // residual and restriction
+        const DevCsr& Am = V.A;
+        Level& C = lv(l + 1);
+        const bool cf32 = lf32(l + 1);
+        if (f32) {
+            float* res = H->res32.p;
+            launch_rowop<OP_RESID>(Am.tpr, n, Am.row.p, Am.col.p, Am.val32.p, (const float*)xpre.p, (const float*)fl.p,
+                (const float*)nullptr, res, 1.0, 0.0, skip, s);
+            if (cf32)
+                { note_launch(); k_restrict<float, float, float><<<ew_grid(C.A.n), 256, 0, s>>>(C.A.n, V.rptr.p, V.ridx.p, V.rval32.p, res, C.rhs32.p, skip); }
+            else
+                { note_launch(); k_restrict<float, double, double><<<ew_grid(C.A.n), 256, 0, s>>>(C.A.n, V.rptr.p, V.ridx.p, V.rval.p, res, C.rhs.p, skip); }
+        } else {
+            double* res = H->res.p;
+            launch_rowop<OP_RESID>(Am.tpr, n, Am.row.p, Am.col.p, Am.val.p, (const double*)xpre.p, (const double*)fl.p,
+                (const double*)nullptr, res, 1.0, 0.0, skip, s);
+            note_launch(); k_restrict<double, double, double><<<ew_grid(C.A.n), 256, 0, s>>>(C.A.n, V.rptr.p, V.ridx.p, V.rval.p, res, C.rhs.p, skip);
+        }
+        BCMGX_CHECK_LAUNCH();
+        Vec fc = cf32 ? Vec { C.rhs32.p, true } : Vec { C.rhs.p, false };
+        Vec xc_dst = cf32 ? Vec { C.x32.p, true } : Vec { C.x.p, false };
+        Vec xc;   // nullptr: coarse correction is zero
+        if (L > 2 || P.relaxnumber_coarse > 0) {
+            int visits = l < (int)H->grid_sweeps.size() ? H->grid_sweeps[l] : 1;
+            for (int i = 1; i <= visits; i++) {
+                run(l + 1, fc, xc, xc_dst);
+                xc = xc_dst;
+                if (l + 1 == L - 1) break;
+            }
+        }
+        // prolongation into the buffer the post-smoothing chain starts from
+        Vec pdst;
+        if (kpost <= 0) {
+            pdst = dst;
+        } else {
+            Vec o0 = dst;
+            for (int i = kpost - 2; i >= 0; i--) o0 = (o0 == A) ? B : A;
+            pdst = (o0 == A) ? B : A;
+        }
+        if (xc.p != nullptr) {
+            const int g = ew_grid(n);
+            if (!f32) {
+                note_launch(); k_prolong<double, double, double, double><<<g, 256, 0, s>>>(n, V.agg.p, V.p.p, (const double*)xc.p, (const double*)xpre.p, (double*)pdst.p, skip);
+            } else if (xc.f32) {
+                if (pdst.f32)
+                    { note_launch(); k_prolong<float, float, float, float><<<g, 256, 0, s>>>(n, V.agg.p, V.p32.p, (const float*)xc.p, (const float*)xpre.p, (float*)pdst.p, skip); }
+                else
+                    { note_launch(); k_prolong<float, float, float, double><<<g, 256, 0, s>>>(n, V.agg.p, V.p32.p, (const float*)xc.p, (const float*)xpre.p, (double*)pdst.p, skip); }
+            } else {
+                if (pdst.f32)
+                    { note_launch(); k_prolong<float, double, float, float><<<g, 256, 0, s>>>(n, V.agg.p, V.p32.p, (const double*)xc.p, (const float*)xpre.p, (float*)pdst.p, skip); }
+                else
+                    { note_launch(); k_prolong<float, double, float, double><<<g, 256, 0, s>>>(n, V.agg.p, V.p32.p, (const double*)xc.p, (const float*)xpre.p, (double*)pdst.p, skip); }
+            }
+            BCMGX_CHECK_LAUNCH();
+        } else if (pdst != xpre) {
+            copy(xpre, pdst, n);
+        }
+        chain(l, kpost, fl, pdst, dst, A, B);
+    }
+};
+
+void prec_apply_impl(bcmgx_hierarchy* H, const double* r, double* v, const int* skip)
+{
+    const int n0 = H->lv[0].A.n;
+    if (H->prm.preconditioner != BCMGX_PREC_BCMG) {
+        BCMGX_CUDA(cudaMemcpyAsync(v, r, sizeof(double) * n0, cudaMemcpyDeviceToDevice, H->stream));
+        return;
+    }
+    Cycle c { H, H->stream, skip, H->prm.vcycle_precision == BCMGX_VCYCLE_FP32, (int)H->lv.size() };
+    c.run(0, Vec { (void*)r, false }, Vec(), Vec { v, false });
+}
+
+void prec_apply_dev(bcmgx_hierarchy* H, const double* r, double* v)
+{
+    ensure_solve_workspace(H);
+    prec_apply_impl(H, r, v, nullptr);
+}
+
+// ------------------------------------------------------------------------------------------
+// FCG kernels
+// ------------------------------------------------------------------------------------------
+constexpr int kRedBlocksPerSM = 4;
+constexpr int kRedThreads = 256;
+
+static int red_grid(long work_threads)
+{
+    long need = (work_threads + kRedThreads - 1) / kRedThreads;
+    return (int)std::max<long>(1, std::min<long>(need, (long)num_sms() * kRedBlocksPerSM));
+}
+
+// r = b - A x and ||r||^2 -> delta0, tolerance (FCG.cu:46-51).
+template <int S>
+__global__ void __launch_bounds__(kRedThreads) k_fcg_resid0(int n, const int* __restrict__ row, const int* __restrict__ col,
+    const double* __restrict__ val, const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ r,
+    FcgState* st, double* partials)
+{
+    const int lane = threadIdx.x & (S - 1);
+    const int sub = (threadIdx.x & 31) / S;
+    const long stride = (long)gridDim.x * blockDim.x / S;
+    double acc[1] = { 0.0 };
+    for (long base = ((long)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) / S; base < n; base += stride) {
+        const long r0 = base + sub;
+        double s = 0;
+        if (r0 < n) s = row_partial<S, double>(row[r0], row[r0 + 1], lane, col, val, x);
+        s = subwarp_sum<S>(s);
+        if (r0 < n && lane == 0) {
+            double ri = -1.0 * s + 1.0 * b[r0];
+            r[r0] = ri;
+            acc[0] += ri * ri;
+        }
+    }
+    double out[1];
+    if (grid_sum<1>(acc, partials, &st->ticket[0], out) && threadIdx.x == 0) {
+        st->delta0 = sqrt(out[0]);
+        st->tol = st->tol * st->delta0;   // tol holds rtol on entry
+        st->iter = 0;
+        st->done = 0;
+        st->bad = 0;
+    }
+}
+
+// pw = A pv with the dots of the step: start-up (mode 0): alpha = r.pv, beta = pw.pv,
+// delta = beta, theta = alpha / delta (FCG.cu:59-86); loop (mode 1): alpha = r.pv, beta = pw.pv,
+// gamma = oq.pv (triple_innerproduct, triple_inner_product.cu:7-101) followed by the scalar
+// recurrence theta = gamma/delta, delta = beta - gamma^2/delta, theta2 = alpha/delta
+// (FCG.cu:132-136).
+template <int S, int MODE>
+__global__ void __launch_bounds__(kRedThreads) k_fcg_spmv_dots(int n, const int* __restrict__ row, const int* __restrict__ col,
+    const double* __restrict__ val, const double* __restrict__ pv, double* __restrict__ pw, const double* __restrict__ r,
+    const double* __restrict__ oq, FcgState* st, double* partials, const int* __restrict__ skip)
+{
+    if (skip && *skip) return;
+    const int lane = threadIdx.x & (S - 1);
+    const int sub = (threadIdx.x & 31) / S;
+    const long stride = (long)gridDim.x * blockDim.x / S;
+    double acc[3] = { 0.0, 0.0, 0.0 };
+    for (long base = ((long)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) / S; base < n; base += stride) {
+        const long r0 = base + sub;
+        double s = 0;
+        if (r0 < n) s = row_partial<S, double>(row[r0], row[r0 + 1], lane, col, val, pv);
+        s = subwarp_sum<S>(s);
+        if (r0 < n && lane == 0) {
+            pw[r0] = s;
+            const double vi = pv[r0];
+            acc[0] += r[r0] * vi;
+            acc[1] += s * vi;
+            if (MODE == 1) acc[2] += oq[r0] * vi;
+        }
+    }
+    double out[3];
+    if (grid_sum<3>(acc, partials, &st->ticket[1], out) && threadIdx.x == 0) {
+        st->alpha = out[0];
+        st->beta = out[1];
+        if (MODE == 0) {
+            st->delta = out[1];
+            st->theta = out[0] / out[1];
+        } else {
+            st->gamma = out[2];
+            const double th = out[2] / st->delta;
+            const double dn = out[1] - ((out[2] * out[2]) / st->delta);
+            st->theta = th;
+            st->delta = dn;
+            st->theta2 = out[0] / dn;
+        }
+        if (!(st->delta > 0.0) || !isfinite(st->theta)) st->bad = 1;
+    }
+}
+
+// Start-up update x += theta v, r -= theta w, d = v, q = w, ||r||^2 (FCG.cu:88-100).
+__global__ void __launch_bounds__(kRedThreads) k_fcg_update0(int n, const double* __restrict__ v, const double* __restrict__ w,
+    double* __restrict__ x, double* __restrict__ r, double* __restrict__ d, double* __restrict__ q, FcgState* st, double* partials,
+    double* hist)
+{
+    const double th = st->theta;
+    double acc[1] = { 0.0 };
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const double vi = v[i], wi = w[i];
+        x[i] = th * vi + 1.0 * x[i];
+        const double ri = -th * wi + 1.0 * r[i];
+        r[i] = ri;
+        d[i] = vi;
+        q[i] = wi;
+        acc[0] += ri * ri;
+    }
+    double out[1];
+    if (grid_sum<1>(acc, partials, &st->ticket[2], out) && threadIdx.x == 0) {
+        st->rnorm2 = out[0];
+        if (hist) hist[0] = sqrt(out[0]);
+    }
+}
+
+// Loop update: pv = -theta od + pv; x += theta2 pv; pw = -theta oq + pw; r -= theta2 pw
+// (double_merged_axpy x2, FCG.cu:138-144), ||r|| and the stopping test (FCG.cu:146-156).
+__global__ void __launch_bounds__(kRedThreads) k_fcg_update(int n, double* __restrict__ pv, const double* __restrict__ od,
+    double* __restrict__ x, double* __restrict__ pw, const double* __restrict__ oq, double* __restrict__ r, FcgState* st,
+    double* partials, double* hist, const int* __restrict__ skip)
+{
+    if (skip && *skip) return;
+    const double th = st->theta, th2 = st->theta2;
+    double acc[1] = { 0.0 };
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const double nv = -th * od[i] + pv[i];
+        pv[i] = nv;
+        x[i] = th2 * nv + x[i];
+        const double nw = -th * oq[i] + pw[i];
+        pw[i] = nw;
+        const double ri = -th2 * nw + r[i];
+        r[i] = ri;
+        acc[0] += ri * ri;
+    }
+    double out[1];
+    if (grid_sum<1>(acc, partials, &st->ticket[3], out) && threadIdx.x == 0) {
+        st->rnorm2 = out[0];
+        const double l2 = sqrt(out[0]);
+        st->iter += 1;
+        if (hist) hist[st->iter] = l2;
+        if (!isfinite(l2)) st->bad = 1;
+        st->done = (!(l2 > st->tol) || st->iter >= st->itnlim || st->bad) ? 1 : 0;
+    }
+}
+
+template <int S>
+static void launch_resid0(const DevCsr& A, const double* x, const double* b, double* r, FcgState* st, double* part, cudaStream_t s)
+{
+    note_launch(); k_fcg_resid0<S><<<red_grid((long)A.n * S), kRedThreads, 0, s>>>(A.n, A.row.p, A.col.p, A.val.p, x, b, r, st, part);
+}
+template <int S, int MODE>
+static void launch_dots(const DevCsr& A, const double* pv, double* pw, const double* r, const double* oq, FcgState* st,
+    double* part, const int* skip, cudaStream_t s)
+{
+    note_launch(); k_fcg_spmv_dots<S, MODE><<<red_grid((long)A.n * S), kRedThreads, 0, s>>>(A.n, A.row.p, A.col.p, A.val.p, pv, pw, r, oq, st, part, skip);
+}
+
+static void fcg_resid0(const DevCsr& A, const double* x, const double* b, double* r, FcgState* st, double* part, cudaStream_t s)
+{
+    switch (A.tpr) {
+    case 1: launch_resid0<1>(A, x, b, r, st, part, s); break;
+    case 2: launch_resid0<2>(A, x, b, r, st, part, s); break;
+    case 4: launch_resid0<4>(A, x, b, r, st, part, s); break;
+    case 8: launch_resid0<8>(A, x, b, r, st, part, s); break;
+    case 16: launch_resid0<16>(A, x, b, r, st, part, s); break;
+    default: launch_resid0<32>(A, x, b, r, st, part, s); break;
+    }
+    BCMGX_CHECK_LAUNCH();
+}
+
+template <int MODE>
+static void fcg_dots(const DevCsr& A, const double* pv, double* pw, const double* r, const double* oq, FcgState* st,
+    double* part, const int* skip, cudaStream_t s)
+{
+    switch (A.tpr) {
+    case 1: launch_dots<1, MODE>(A, pv, pw, r, oq, st, part, skip, s); break;
+    case 2: launch_dots<2, MODE>(A, pv, pw, r, oq, st, part, skip, s); break;
+    case 4: launch_dots<4, MODE>(A, pv, pw, r, oq, st, part, skip, s); break;
+    case 8: launch_dots<8, MODE>(A, pv, pw, r, oq, st, part, skip, s); break;
+    case 16: launch_dots<16, MODE>(A, pv, pw, r, oq, st, part, skip, s); break;
+    default: launch_dots<32, MODE>(A, pv, pw, r, oq, st, part, skip, s); break;
+    }
+    BCMGX_CHECK_LAUNCH();
+}
+
+void ensure_solve_workspace(bcmgx_hierarchy* H)
+{
+    const int n0 = H->lv[0].A.n;
+    cudaStream_t s = H->stream;
+    if (H->ws_n == n0) return;
+    H->r.alloc(n0, s);
+    H->v.alloc(n0, s);
+    H->w.alloc(n0, s);
+    H->d.alloc(n0, s);
+    H->q.alloc(n0, s);
+    H->res.alloc(n0, s);
+    if (H->prm.vcycle_precision == BCMGX_VCYCLE_FP32) H->res32.alloc(n0, s);
+    H->partials.alloc((size_t)num_sms() * kRedBlocksPerSM * 4, s);
+    H->st.alloc(1, s);
+    BCMGX_CUDA(cudaMemsetAsync(H->st.p, 0, sizeof(FcgState), s));
+    if (!H->st_host) BCMGX_CUDA(cudaMallocHost((void**)&H->st_host, sizeof(FcgState)));
+    const bool f32 = H->prm.vcycle_precision == BCMGX_VCYCLE_FP32;
+    const int L = (int)H->lv.size();
+    for (int l = 0; l < L; l++) {
+        Level& V = H->lv[l];
+        const int n = V.A.n;
+        const bool lf = f32 && l < L - 1;
+        if (lf) {
+            V.x32.alloc(n, s);
+            V.x232.alloc(n, s);
+            V.rhs32.alloc(n, s);
+        } else {
+            if (l > 0) {
+                V.x.alloc(n, s);
+                V.rhs.alloc(n, s);
+            }
+            V.x2.alloc(n, s);
+        }
+    }
+    H->ws_n = n0;
+}
+
+// Average device time of one launch of each solve-phase kernel of level l, timed with CUDA
+// events on the hierarchy's stream over `reps` back-to-back launches after one warm-up:
+// out[0] l1-Jacobi sweep (in the cycle's precision), out[1] residual, out[2] FP64 y = A x,
+// out[3] the FCG SpMV + dot products (level 0 only, else 0).
+void time_level_kernels(bcmgx_hierarchy* H, int l, int reps, double* out)
+{
+    ensure_solve_workspace(H);
+    cudaStream_t s = H->stream;
+    Level& V = H->lv[l];
+    const DevCsr& A = V.A;
+    const int n = A.n;
+    const int L = (int)H->lv.size();
+    const bool f32 = H->prm.vcycle_precision == BCMGX_VCYCLE_FP32 && l < L - 1;
+    DBuf<double> a, b, c;
+    DBuf<float> a32, b32, c32;
+    a.alloc(n, s);
+    b.alloc(n, s);
+    c.alloc(n, s);
+    BCMGX_CUDA(cudaMemsetAsync(a.p, 0, sizeof(double) * n, s));
+    BCMGX_CUDA(cudaMemsetAsync(c.p, 0, sizeof(double) * n, s));
+    if (f32) {
+        a32.alloc(n, s);
+        b32.alloc(n, s);
+        c32.alloc(n, s);
+        BCMGX_CUDA(cudaMemsetAsync(a32.p, 0, sizeof(float) * n, s));
+        BCMGX_CUDA(cudaMemsetAsync(c32.p, 0, sizeof(float) * n, s));
+    }
+    cudaEvent_t e0, e1;
+    BCMGX_CUDA(cudaEventCreate(&e0));
+    BCMGX_CUDA(cudaEventCreate(&e1));
+    auto timeit = [&](auto&& launch) {
+        launch();
+        BCMGX_CUDA(cudaEventRecord(e0, s));
+        for (int i = 0; i < reps; i++) launch();
+        BCMGX_CUDA(cudaEventRecord(e1, s));
+        BCMGX_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        BCMGX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        return (double)ms / reps;
+    };
+    if (f32) {
+        out[0] = timeit([&] { launch_rowop<OP_JACOBI>(A.tpr, n, A.row.p, A.col.p, A.val32.p, (const float*)a32.p, (const float*)c32.p, V.M32.p, b32.p, 1.0, 0.0, nullptr, s); });
+        out[1] = timeit([&] { launch_rowop<OP_RESID>(A.tpr, n, A.row.p, A.col.p, A.val32.p, (const float*)a32.p, (const float*)c32.p, (const float*)nullptr, b32.p, 1.0, 0.0, nullptr, s); });
+    } else {
+        out[0] = timeit([&] { launch_rowop<OP_JACOBI>(A.tpr, n, A.row.p, A.col.p, A.val.p, (const double*)a.p, (const double*)c.p, V.M.p, b.p, 1.0, 0.0, nullptr, s); });
+        out[1] = timeit([&] { launch_rowop<OP_RESID>(A.tpr, n, A.row.p, A.col.p, A.val.p, (const double*)a.p, (const double*)c.p, (const double*)nullptr, b.p, 1.0, 0.0, nullptr, s); });
+    }
+    out[2] = timeit([&] { launch_spmv(n, A.row.p, A.col.p, A.val.p, a.p, b.p, 1.0, 0.0, A.tpr, s); });
+    out[3] = 0;
+    if (l == 0) {
+        FcgState init {};
+        init.delta = 1.0;
+        BCMGX_CUDA(cudaMemcpyAsync(H->st.p, &init, sizeof(FcgState), cudaMemcpyHostToDevice, s));
+        out[3] = timeit([&] { fcg_dots<1>(A, a.p, b.p, c.p, c.p, H->st.p, H->partials.p, nullptr, s); });
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+}
+
+// Flexible CG (FCG.cu:27-165) on device vectors b, x (x: x0 in, solution out).
+int fcg_solve(bcmgx_hierarchy* H, const double* b, double* x, bcmgx_solve_info* info)
+{
+    ensure_solve_workspace(H);
+    cudaStream_t s = H->stream;
+    const DevCsr& A = H->lv[0].A;
+    const int n = A.n;
+    const bcmgx_params& P = H->prm;
+    FcgState* st = H->st.p;
+    double* part = H->partials.p;
+    DBuf<double> hist;
+    hist.alloc((size_t)std::max(P.itnlim, 1) + 2, s);
+    FcgState init {};
+    init.tol = P.rtol;
+    init.itnlim = P.itnlim;
+    BCMGX_CUDA(cudaMemcpyAsync(st, &init, sizeof(FcgState), cudaMemcpyHostToDevice, s));
+    BCMGX_CUDA(cudaEventRecord(H->ev0, s));
+    double *r = H->r.p, *v = H->v.p, *w = H->w.p, *d = H->d.p, *q = H->q.p;
+    fcg_resid0(A, x, b, r, st, part, s);
+    BCMGX_CUDA(cudaMemsetAsync(v, 0, sizeof(double) * n, s));
+    prec_apply_impl(H, r, v, nullptr);
+    fcg_dots<0>(A, v, w, r, nullptr, st, part, nullptr, s);
+    note_launch(); k_fcg_update0<<<red_grid(n), kRedThreads, 0, s>>>(n, v, w, x, r, d, q, st, part, hist.p);
+    BCMGX_CHECK_LAUNCH();
+    int iter = 0;
+    int done = 0;
+    while (!done) {
+        const bool even = (iter % 2) == 0;
+        double* pv = even ? v : d;
+        double* pw = even ? w : q;
+        const double* od = even ? d : v;
+        const double* oq = even ? q : w;
+        prec_apply_impl(H, r, pv, nullptr);
+        fcg_dots<1>(A, pv, pw, r, oq, st, part, nullptr, s);
+        note_launch(); k_fcg_update<<<red_grid(n), kRedThreads, 0, s>>>(n, pv, od, x, pw, oq, r, st, part, hist.p, nullptr);
+        BCMGX_CHECK_LAUNCH();
+        BCMGX_CUDA(cudaMemcpyAsync(H->st_host, st, sizeof(FcgState), cudaMemcpyDeviceToHost, s));
+        BCMGX_CUDA(cudaStreamSynchronize(s));
+        done = H->st_host->done;
+        iter = H->st_host->iter;
+        if (P.dispnorm) std::printf("%d) r norm: %.10lf\n", iter - 1, std::sqrt(H->st_host->rnorm2));
+    }
+    BCMGX_CUDA(cudaEventRecord(H->ev1, s));
+    BCMGX_CUDA(cudaEventSynchronize(H->ev1));
+    float ms = 0;
+    BCMGX_CUDA(cudaEventElapsedTime(&ms, H->ev0, H->ev1));
+    const FcgState& S = *H->st_host;
+    if (info) {
+        info->niter = S.iter + 1;
+        info->retv = S.iter >= P.itnlim ? -1 : 0;
+        info->delta0 = S.delta0;
+        info->exit_res = std::sqrt(S.rnorm2);
+        info->solve_ms = ms;
+        info->full_n = n;
+    }
+    if (S.bad) return BCMGX_ERR_NOT_SPD;
+    return S.iter >= P.itnlim ? BCMGX_ERR_NO_CONVERGENCE : BCMGX_OK;
+}
+
+}  // namespace bcmgx

@@ -1,0 +1,172 @@
+"""Host-side parts of libbcmgx.so that need no GPU: the exported C ABI, the settings readers,
+the generators and readers of the driver's input plumbing, and the CLI's argument checks."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from conftest import ROOT, golden_mtx
+
+HEADER = os.path.join(ROOT, "include", "bcmgx.h")
+CLI = os.path.join(ROOT, "bootcmatchgx_b200", "bin", "bcmgx_driverSolve")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?(?:int64_t|int|void|const char\*)\s*\*?\s*(bcmgx_\w+)\s*\(", text, re.M)))
+
+
+def test_abi_exports_every_declared_symbol(bx):
+    import ctypes
+    from bootcmatchgx_b200 import _lib
+    names = declared_functions()
+    assert len(names) >= 20
+    L = ctypes.CDLL(_lib.LIB_PATH)
+    for n in names:
+        assert hasattr(L, n), n
+    assert set(names) <= set(_lib.SIGNATURES), set(names) - set(_lib.SIGNATURES)
+    assert bx.lib().bcmgx_version().startswith(b"bcmgx")
+
+
+def test_params_defaults(bx):
+    p = bx.params_to_dict(bx.params_default())
+    assert p["solver"] == 0 and p["itnlim"] == 2000 and p["rtol"] == 1e-6 and p["dispnorm"] == 1
+    assert p["preconditioner"] == 0 and p["aggrsweeps"] == 2 and p["max_levels"] == 39
+    assert p["relaxnumber_coarse"] == 20 and p["prerelax_sweeps"] == 4 and p["postrelax_sweeps"] == 4
+    assert p["conv_ratio"] == 0.8 and p["max_hrc"] == 1 and p["l1jacsweeps"] == 4
+
+
+def _write(tmp_path, name, text):
+    f = tmp_path / name
+    f.write_text(text)
+    return str(f)
+
+
+def test_properties_fixtures(bx, golden, tmp_path):
+    f = _write(tmp_path, "FCG_BCMG.properties", str(golden["prop__FCG_BCMG.properties"]))
+    p = bx.params_to_dict(bx.init_from_properties_file(f))
+    assert p["solver"] == 1 and p["preconditioner"] == 2 and p["rtol"] == 1e-6
+    f = _write(tmp_path, "prova.properties", str(golden["prop__FCG_BCMG.prova.properties"]))
+    p = bx.params_to_dict(bx.init_from_properties_file(f))
+    assert p["itnlim"] == 1000 and p["prerelax_sweeps"] == 4
+    f = _write(tmp_path, "sample.properties", str(golden["prop__sample.properties"]))
+    p = bx.params_to_dict(bx.init_from_properties_file(f))
+    assert p["solver"] == 0 and p["preconditioner"] == 3 and p["rtol"] == 1e-6
+    assert p["relaxnumber_coarse"] == 20 and p["cycle_type"] == 0 and p["aggrsweeps"] == 2
+
+
+def test_properties_rules(bx, tmp_path):
+    # '#' starts a comment; unknown keys are ignored; the last '=' splits; spaces trimmed
+    f = _write(tmp_path, "a.properties",
+               "# comment = ignored\n\n   \nsolver=FCG\n rtol = 1e-8 # trailing comment\nfoo = bar\n"
+               "preconditioner = BCMG\ncycle_type = W_CYCLE\nitnlim = 7\n")
+    p = bx.params_to_dict(bx.init_from_properties_file(f))
+    assert p["solver"] == 1 and p["rtol"] == 1e-8 and p["preconditioner"] == 2
+    assert p["cycle_type"] == 2 and p["itnlim"] == 7
+    # an enum value followed by a comment is not recognised (Params.cu:311 keeps it in the value)
+    f = _write(tmp_path, "b.properties", "solver = FCG # comment\n")
+    assert bx.params_to_dict(bx.init_from_properties_file(f))["solver"] == 5
+    # a non-blank line without '=' is an error
+    f = _write(tmp_path, "c.properties", "solver FCG\n")
+    with pytest.raises(bx.BcmgxError) as e:
+        bx.init_from_properties_file(f)
+    assert e.value.code == -1 and "could not find '='" in str(e.value)
+    with pytest.raises(bx.BcmgxError):
+        bx.init_from_properties_file(str(tmp_path / "missing.properties"))
+    f = _write(tmp_path, "d.properties", "itnlim = many\n")
+    with pytest.raises(bx.BcmgxError):
+        bx.init_from_properties_file(f)
+
+
+def test_legacy_settings(bx, tmp_path):
+    lines = ["NONE", "NONE", "FCG", "MULTIPLICATIVE", "1", "0.8", "SUITOR", "2", "0", "39", "V_CYCLE",
+             "L1_JACOBI", "L1_JACOBI", "20", "0", "4", "4", "2000", "1.e-8", "1", "1", "1", "BCMG", "4", "0",
+             "0", "0"]
+    f = _write(tmp_path, "s.txt", "\n".join(l + " % note" for l in lines) + "\n")
+    p = bx.params_to_dict(bx.init_from_file(f))
+    assert p["solver"] == 1 and p["preconditioner"] == 2 and p["rtol"] == 1e-8 and p["error"] == 0
+    lines[4] = "3"   # max_hrc != 1 -> error flag (Params.cu:463-466)
+    f = _write(tmp_path, "s2.txt", "\n".join(lines) + "\n")
+    assert bx.params_to_dict(bx.init_from_file(f))["error"] == 1
+    f = _write(tmp_path, "s3.txt", "\n".join(lines[:5]) + "\n")
+    with pytest.raises(bx.BcmgxError):
+        bx.init_from_file(f)
+
+
+@pytest.mark.parametrize("st,dims", [(7, (10, 10, 10, 1, 1, 1)), (27, (10, 10, 10, 2, 2, 2)),
+                                     (7, (2, 2, 5, 3, 4, 2)), (27, (5, 5, 5, 4, 2, 1)),
+                                     (7, (1, 1, 1, 1, 1, 1)), (27, (1, 7, 2, 1, 1, 3))])
+def test_generator_matches_oracle(bx, oracle, st, dims):
+    n, z = bx.laplacian_3d_size(st, *dims)
+    row, col, val = bx.laplacian_3d(st, *dims)
+    r2, c2, v2 = oracle.Matrix.lap3d(st, *dims).csr()
+    assert n == row.size - 1 and z == col.size
+    assert np.array_equal(row, r2) and np.array_equal(col, c2) and np.array_equal(val, v2)
+
+
+def test_generator_fixture_and_size_160(bx, golden):
+    M = golden_mtx(golden, "lap3d_27p_5x5x5_1x2x2")
+    row, col, val = bx.laplacian_3d(27, 5, 5, 5, 1, 2, 2)
+    assert abs(sp.csr_matrix((val, col, row), shape=M.shape) - M).max() == 0
+    assert bx.laplacian_3d_size(27, 160, 160, 160) == (4096000, 109215352)
+    assert bx.laplacian_3d_size(7, 50, 50, 50) == (125000, 860000)
+    assert bx.laplacian_3d_size(7, 256, 256, 256) == (16777216, 117047296)
+
+
+def test_laplacian_cfg(bx, tmp_path):
+    f = _write(tmp_path, "g.cfg", "# grid\nnx = 10\nny = 12\nnz = 14\nP = 2\nQ = 1\nR = 3\n")
+    assert bx.read_laplacian_cfg(f) == {"nx": 10, "ny": 12, "nz": 14, "P": 2, "Q": 1, "R": 3}
+    with pytest.raises(bx.BcmgxError):
+        bx.read_laplacian_cfg(_write(tmp_path, "h.cfg", "nx 10\n"))
+
+
+def test_matrix_market_reader(bx, golden, tmp_path):
+    M = golden_mtx(golden, "lap3d_7p_4x14x4_2x2x1").tocoo()
+    f = tmp_path / "m.mtx"
+    with open(f, "w") as fh:
+        fh.write("%%MatrixMarket matrix coordinate real general\n% c\n")
+        fh.write(f"{M.shape[0]} {M.shape[1]} {M.nnz}\n")
+        order = np.random.default_rng(0).permutation(M.nnz)
+        for k in order:
+            fh.write(f"{M.row[k] + 1} {M.col[k] + 1} {M.data[k]:.17g}\n")
+    row, col, val = bx.read_matrix_market(f)
+    A = sp.csr_matrix((val, col, row), shape=M.shape)
+    assert abs(A - M.tocsr()).max() == 0 and np.all(np.diff(row) >= 0)
+    # symmetric storage is mirrored
+    U = sp.triu(M.tocsr()).tocoo()
+    g = tmp_path / "s.mtx"
+    with open(g, "w") as fh:
+        fh.write("%%MatrixMarket matrix coordinate real symmetric\n")
+        fh.write(f"{U.shape[0]} {U.shape[1]} {U.nnz}\n")
+        for r, c, v in zip(U.col, U.row, U.data):   # lower triangle, as symmetric files store it
+            fh.write(f"{r + 1} {c + 1} {v:.17g}\n")
+    row, col, val = bx.read_matrix_market(g)
+    assert abs(sp.csr_matrix((val, col, row), shape=M.shape) - M.tocsr()).max() == 0
+    h = tmp_path / "p.mtx"
+    h.write_text("%%MatrixMarket matrix coordinate pattern general\n2 2 1\n1 1\n")
+    with pytest.raises(bx.BcmgxError):
+        bx.read_matrix_market(h)
+
+
+def test_diffusion_spd(bx):
+    rng = np.random.default_rng(2)
+    kappa = np.exp(rng.normal(size=6 * 5 * 4))
+    row, col, val = bx.diffusion_7p(6, 5, 4, kappa)
+    A = sp.csr_matrix((val, col, row), shape=(120, 120))
+    assert abs(A - A.T).max() < 1e-14
+    assert np.linalg.eigvalsh(A.toarray()).min() > 0
+    assert np.all(np.diff(col[row[0]:row[1]]) > 0)
+    with pytest.raises(bx.BcmgxError):
+        bx.diffusion_7p(2, 2, 2, -np.ones(8))
+
+
+def test_cli_usage_and_errors(tmp_path):
+    r = subprocess.run([CLI], capture_output=True, text=True)
+    assert r.returncode != 0 and "Usage" in r.stdout
+    r = subprocess.run([CLI, "-a", "4", "-s", str(tmp_path / "nope.properties")], capture_output=True, text=True)
+    assert r.returncode != 0 and "Error opening setting file" in r.stderr
+    r = subprocess.run([CLI, "-l", "x.cfg", "-g", "9p", "-s", "a.properties"], capture_output=True, text=True)
+    assert r.returncode != 0 and "Usage" in r.stdout

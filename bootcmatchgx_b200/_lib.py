@@ -43,7 +43,7 @@ class Params(C.Structure):
         ("sstep", C.c_int), ("stop_criterion", C.c_int), ("ru_res", C.c_int),
         ("rec_res_int", C.c_int), ("error", C.c_int),
         ("vcycle_precision", C.c_int), ("record_sweeps", C.c_int), ("use_graph", C.c_int),
-        ("device", C.c_int), ("stream", C.c_void_p),
+        ("device", C.c_int), ("autotune", C.c_int), ("stream", C.c_void_p),
     ]
 
 
@@ -62,7 +62,8 @@ class HierarchyInfo(C.Structure):
                 ("nnz", C.c_int64 * MAX_LEVELS), ("op_cmplx", C.c_double),
                 ("op_wcmplx", C.c_double), ("avg_cratio", C.c_double),
                 ("maxcoarsesize", C.c_int), ("ftcoarse", C.c_int),
-                ("num_sweep_records", C.c_int), ("setup_ms", C.c_double)]
+                ("num_sweep_records", C.c_int), ("setup_ms", C.c_double),
+                ("tpr", C.c_int * MAX_LEVELS)]
 
 
 # name -> (restype, argtypes); every symbol include/bcmgx.h declares

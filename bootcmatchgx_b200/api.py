@@ -200,7 +200,8 @@ class Hierarchy:
         return {"num_levels": nl, "n": list(hi.n[:nl]), "nnz": list(hi.nnz[:nl]),
                 "op_cmplx": hi.op_cmplx, "op_wcmplx": hi.op_wcmplx, "avg_cratio": hi.avg_cratio,
                 "maxcoarsesize": hi.maxcoarsesize, "ftcoarse": hi.ftcoarse,
-                "num_sweep_records": hi.num_sweep_records, "setup_ms": hi.setup_ms}
+                "num_sweep_records": hi.num_sweep_records, "setup_ms": hi.setup_ms,
+                "tpr": list(hi.tpr[:nl])}
 
     def level(self, l):
         inf = self.info()

@@ -3,6 +3,7 @@
 #include "internal.h"
 
 #include <atomic>
+#include <cstdlib>
 #include <cmath>
 #include <cstdio>
 
@@ -181,7 +182,15 @@ int bcmgx_setup(const bcmgx_csr* A, const bcmgx_params* p, bcmgx_hierarchy** out
         BCMGX_CUDA(cudaEventCreate(&e1));
         BCMGX_CUDA(cudaEventRecord(e0, H->stream));
         build_hierarchy(H.get(), A);
-        for (auto& V : H->lv) V.A.tpr = default_tpr(V.A.n, V.A.nnz);
+        const char* force = std::getenv("BCMGX_TPR");
+        const int L = (int)H->lv.size();
+        for (int l = 0; l < L; l++) {
+            Level& V = H->lv[l];
+            const bool f32 = p->vcycle_precision == BCMGX_VCYCLE_FP32 && l < L - 1;
+            if (force) V.A.tpr = std::atoi(force);
+            else if (p->autotune) V.A.tpr = autotune_tpr(V, f32, H->stream);
+            else V.A.tpr = default_tpr(V.A.n, V.A.nnz);
+        }
         BCMGX_CUDA(cudaEventRecord(e1, H->stream));
         BCMGX_CUDA(cudaEventSynchronize(e1));
         float ms = 0;
@@ -236,6 +245,7 @@ int bcmgx_hierarchy_get_info(const bcmgx_hierarchy* h, bcmgx_hierarchy_info* inf
         for (int l = 0; l < info->num_levels && l < BCMGX_MAX_LEVELS; l++) {
             info->n[l] = h->lv[l].A.n;
             info->nnz[l] = h->lv[l].A.nnz;
+            info->tpr[l] = h->lv[l].A.tpr;
         }
         info->op_cmplx = h->op_cmplx;
         info->op_wcmplx = h->op_wcmplx;

@@ -143,6 +143,7 @@ struct bcmgx_hierarchy {
     int maxcoarsesize = 0, ftcoarse = 1;
     double op_cmplx = 0, op_wcmplx = 0, avg_cratio = 1, setup_ms = 0;
     std::vector<int> grid_sweeps;
+    std::vector<std::pair<std::string, double>> prof;   // set-up phase times (BCMGX_PROFILE=1)
     // solve workspace
     bcmgx::DBuf<double> b, xv, r, v, w, d, q, res;
     bcmgx::DBuf<float> res32;
@@ -178,7 +179,7 @@ void prec_apply_dev(bcmgx_hierarchy* H, const double* r, double* v);
 void time_level_kernels(bcmgx_hierarchy* H, int l, int reps, double* out);
 
 // ---- kernels usable on raw device memory (kernels.cu) ----
-int autotune_tpr(const DevCsr& A, cudaStream_t s);
+int autotune_tpr(Level& V, bool f32, cudaStream_t s);
 int default_tpr(int n, int64_t nnz);
 void launch_spmv(int n, const int* row, const int* col, const double* val, const double* x, double* y,
     double alpha, double beta, int tpr, cudaStream_t s);

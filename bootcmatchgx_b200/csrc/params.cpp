@@ -106,6 +106,7 @@ void params_default(bcmgx_params* p)
     p->record_sweeps = 0;
     p->use_graph = 1;
     p->device = -1;
+    p->autotune = 1;
     p->stream = nullptr;
 }
 

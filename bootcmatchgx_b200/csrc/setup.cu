@@ -19,6 +19,8 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <chrono>
+#include <cstdlib>
 #include <cmath>
 #include <cstdio>
 
@@ -33,6 +35,43 @@ constexpr double kCoarseRatioThreshold = 1.2;           // matchingAggregation.c
 enum : int {
     ERR_ROW0 = 1, ERR_ROWN = 2, ERR_ROWORDER = 4, ERR_COLRANGE = 8, ERR_COLSORT = 16, ERR_NODIAG = 32,
     ERR_SUITOR_BUDGET = 64, ERR_ASYM_MATCH = 128, ERR_BADW = 256, ERR_GALERKIN_CAP = 512,
+};
+
+// Optional phase timing of the set-up (environment BCMGX_PROFILE=1): the stream is synchronised
+// at phase boundaries and host wall time is accumulated per phase, printed to stderr.
+static bool prof_on()
+{
+    static int v = -1;
+    if (v < 0) {
+        const char* e = std::getenv("BCMGX_PROFILE");
+        v = (e && std::atoi(e) > 0) ? 1 : 0;
+    }
+    return v == 1;
+}
+
+struct PhaseTimer {
+    bcmgx_hierarchy* H;
+    const char* name;
+    std::chrono::steady_clock::time_point t0;
+    PhaseTimer(bcmgx_hierarchy* h, const char* nm) : H(h), name(nm)
+    {
+        if (prof_on()) {
+            cudaStreamSynchronize(H->stream);
+            t0 = std::chrono::steady_clock::now();
+        }
+    }
+    ~PhaseTimer()
+    {
+        if (!prof_on()) return;
+        cudaStreamSynchronize(H->stream);
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        for (auto& pr : H->prof)
+            if (pr.first == name) {
+                pr.second += ms;
+                return;
+            }
+        H->prof.push_back({ name, ms });
+    }
 };
 
 static int gs_grid(long n, int threads = 256)
@@ -357,63 +396,79 @@ __global__ void k_rank(int n, const int* __restrict__ row, const int* __restrict
     }
 }
 
-// Lock-free suitor. A vertex proposes to its candidates in preference order; its offer at y
-// is degE[y] - (its rank in y's list), so y keeps the highest-ranked suitor by atomicMax. A
-// successful proposal that displaces a previous suitor hands that vertex to the same thread,
-// which resumes it after the neighbour it lost (set_suitor, suitor.cu:51-78). The search
-// pointer of a vertex is published before its offer (fence), so the next owner resumes from
-// the right place. Total proposals are bounded by nnz; `budget` guards the loop.
-__global__ void k_suitor(int n, const int* __restrict__ row, const int* __restrict__ col, const int* __restrict__ ordj,
-    const int* __restrict__ rank, const int* __restrict__ tpos, const int* __restrict__ degE, unsigned* offer,
-    int* ptr, long long budget, int* err)
+// Preference records: pref[row[v] + k] = {k-th candidate y of v, v's offer value at y}, where
+// the offer value is degE[y] - (rank of v in y's list), or 0 when y does not rank v (no
+// transposed entry: the pair is never proposed). rinfo[v] = {row[v], degE[v]}.
+__global__ void k_pref(int n, const int* __restrict__ row, const int* __restrict__ col, const int* __restrict__ ordj,
+    const int* __restrict__ rank, const int* __restrict__ tpos, const int* __restrict__ degE, int2* __restrict__ pref,
+    int2* __restrict__ rinfo)
 {
-    for (long v = (long)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (long)gridDim.x * blockDim.x) {
-        int cur = (int)v;
+    const int lane = threadIdx.x & 31;
+    for (long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32; r < n; r += (long)gridDim.x * blockDim.x / 32) {
+        const int b = row[r], dE = degE[r];
+        for (int k = lane; k < dE; k += 32) {
+            const int j = ordj[b + k];
+            const int y = col[j];
+            const int tj = tpos[j];
+            const int ry = tj >= 0 ? rank[tj] : -1;
+            pref[b + k] = make_int2(y, ry >= 0 ? degE[y] - ry : 0);
+        }
+        if (lane == 0) rinfo[r] = make_int2(b, dE);
+    }
+}
+
+// Lock-free suitor. A vertex proposes to its candidates in preference order; y keeps the best
+// suitor by atomicMax on its offer word (set_suitor/find_Candidate, suitor.cu:51-147, with the
+// same order: weight, then the higher id). A successful proposal that displaces a previous
+// suitor d hands d to the same thread (as set_suitor does), which resumes d right after y in
+// d's list: that position follows from y's own record of d (no shared pointer, no fence).
+// Vertices start top-down (highest id first): under the id tie rule the higher vertices settle
+// first, and lower vertices then skip candidates whose current offer already beats theirs.
+// Every vertex's position only moves forward, so the work is bounded by nnz; `budget` guards
+// the loop.
+__global__ void k_suitor(int n, const int2* __restrict__ rinfo, const int2* __restrict__ pref, unsigned* offer,
+    long long budget, int* err, int descending)
+{
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+        int cur = descending ? (int)(n - 1 - t) : (int)t;
+        int k = 0;
         long long steps = 0;
         while (cur >= 0) {
-            const int start = row[cur];
-            const int dE = degE[cur];
-            int k = ld_cg(ptr + cur);
-            int next = -1;
-            bool placed = false;
-            for (; k < dE; k++) {
+            const int2 ci = rinfo[cur];
+            int next = -1, nextk = 0;
+            for (; k < ci.y; k++) {
                 if (++steps > budget) {
                     atomicOr(err, ERR_SUITOR_BUDGET);
                     return;
                 }
-                const int j = ordj[start + k];
-                const int tj = tpos[j];
-                if (tj < 0) continue;
-                const int ry = rank[tj];
-                if (ry < 0) continue;
-                const int y = col[j];
-                const unsigned mine = (unsigned)(degE[y] - ry);
-                if (ld_cg(offer + y) >= mine) continue;
-                st_cg(ptr + cur, k + 1);
-                __threadfence();
-                const unsigned old = atomicMax(offer + y, mine);
+                const int2 pr = pref[ci.x + k];
+                const unsigned mine = (unsigned)pr.y;
+                if (mine == 0u || ld_cg(offer + pr.x) >= mine) continue;
+                const unsigned old = atomicMax(offer + pr.x, mine);
                 if (old < mine) {
-                    placed = true;
                     if (old != 0u) {
-                        __threadfence();
-                        next = col[ordj[row[y] + degE[y] - (int)old]];
+                        const int2 yi = rinfo[pr.x];
+                        const int2 dr = pref[yi.x + yi.y - (int)old];
+                        next = dr.x;
+                        nextk = rinfo[dr.x].y - dr.y + 1;
                     }
                     break;
                 }
             }
-            if (!placed) st_cg(ptr + cur, dE);
             cur = next;
+            k = nextk;
         }
     }
 }
 
 // M[y] = suitor of y, or -1 (the suitors array the reference returns, suitor.cu:303-329).
-__global__ void k_suitor_result(int n, const int* __restrict__ row, const int* __restrict__ col, const int* __restrict__ ordj,
-    const int* __restrict__ degE, const unsigned* __restrict__ offer, int* __restrict__ M)
+__global__ void k_suitor_result(int n, const int2* __restrict__ rinfo, const int2* __restrict__ pref,
+    const unsigned* __restrict__ offer, int* __restrict__ M)
 {
     for (long y = (long)blockIdx.x * blockDim.x + threadIdx.x; y < n; y += (long)gridDim.x * blockDim.x) {
         const unsigned o = offer[y];
-        M[y] = o ? col[ordj[row[y] + degE[y] - (int)o]] : -1;
+        const int2 yi = rinfo[y];
+        M[y] = o ? pref[yi.x + yi.y - (int)o].x : -1;
     }
 }
 
@@ -709,21 +764,31 @@ void tpos_dev(int n, const int* row, const int* col, int* tpos, cudaStream_t s)
 
 void suitor_dev(int n, int64_t nnz, const int* row, const int* col, const double* W, const int* tpos, int* M, cudaStream_t s)
 {
-    DBuf<int> rank, ordj, degE, ptr, err;
+    DBuf<int> rank, ordj, degE, err;
+    DBuf<int2> pref, rinfo;
     DBuf<unsigned> offer;
-    rank.alloc(std::max<int64_t>(nnz, 1), s);
-    ordj.alloc(std::max<int64_t>(nnz, 1), s);
+    const int64_t z = std::max<int64_t>(nnz, 1);
+    rank.alloc(z, s);
+    ordj.alloc(z, s);
     degE.alloc(n, s);
-    ptr.alloc(n, s);
     offer.alloc(n, s);
     err.alloc(1, s);
     BCMGX_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), s));
-    BCMGX_CUDA(cudaMemsetAsync(ptr.p, 0, sizeof(int) * n, s));
     BCMGX_CUDA(cudaMemsetAsync(offer.p, 0, sizeof(unsigned) * n, s));
     note_launch(); k_rank<<<warp_grid(n), 256, 0, s>>>(n, row, col, W, rank.p, ordj.p, degE.p);
-    note_launch(); k_suitor<<<gs_grid(n, 128), 128, 0, s>>>(n, row, col, ordj.p, rank.p, tpos, degE.p, offer.p, ptr.p,
-        (long long)nnz + n + 1024, err.p);
-    note_launch(); k_suitor_result<<<gs_grid(n), 256, 0, s>>>(n, row, col, ordj.p, degE.p, offer.p, M);
+    pref.alloc(z, s);
+    rinfo.alloc(n, s);
+    note_launch(); k_pref<<<warp_grid(n), 256, 0, s>>>(n, row, col, ordj.p, rank.p, tpos, degE.p, pref.p, rinfo.p);
+    BCMGX_CHECK_LAUNCH();
+    rank.release();
+    ordj.release();
+    static int asc = -1;
+    if (asc < 0) {
+        const char* e = std::getenv("BCMGX_SUITOR_ASC");
+        asc = (e && std::atoi(e) > 0) ? 1 : 0;
+    }
+    note_launch(); k_suitor<<<ceil_div(n, 128), 128, 0, s>>>(n, rinfo.p, pref.p, offer.p, (long long)nnz + n + 1024, err.p, asc ? 0 : 1);
+    note_launch(); k_suitor_result<<<gs_grid(n), 256, 0, s>>>(n, rinfo.p, pref.p, offer.p, M);
     note_launch(); k_check_symmetric<<<gs_grid(n), 256, 0, s>>>(n, M, err.p);
     BCMGX_CHECK_LAUNCH();
     int e = read_err(err.p, s);
@@ -748,8 +813,15 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
     W.alloc(std::max<int64_t>(nnz, 1), s);
     tpos.alloc(std::max<int64_t>(nnz, 1), s);
     M.alloc(n, s);
-    edge_weights_dev(n, nnz, A.row.p, A.col.p, A.val.p, w, W.p, tpos.p, nullptr, s);
-    suitor_dev(n, nnz, A.row.p, A.col.p, W.p, tpos.p, M.p, s);
+    {
+        PhaseTimer pt(H, "weights");
+        edge_weights_dev(n, nnz, A.row.p, A.col.p, A.val.p, w, W.p, tpos.p, nullptr, s);
+    }
+    {
+        PhaseTimer pt(H, "suitor");
+        suitor_dev(n, nnz, A.row.p, A.col.p, W.p, tpos.p, M.p, s);
+    }
+    PhaseTimer pt_p(H, "makeP+galerkin");
     W.release();
     tpos.release();
     fm.alloc(n, s);
@@ -943,6 +1015,7 @@ void build_hierarchy(bcmgx_hierarchy* H, const bcmgx_csr* Ain)
         Pval.alloc(nfine, s);
         for (int i = 0; i < sweepnumber; i++) {
             pairwise_sweep(H, *Ai_, wi_, cur, level - 1, i);
+            PhaseTimer pt(H, "compose");
             const double size_precoarse = Ai_->n, size_coarse = cur.nc;
             const double coarse_ratio = size_precoarse / size_coarse;
             if (coarse_ratio <= kCoarseRatioThreshold) H->ftcoarse = kFtcoarseInc;
@@ -959,6 +1032,7 @@ void build_hierarchy(bcmgx_hierarchy* H, const bcmgx_csr* Ain)
         F.agg = std::move(Pagg);
         F.p = std::move(Pval);
         const int nc = cur.C.n;
+        PhaseTimer pt(H, "restriction+finish");
         build_restriction(F, nc, f32, s);
         if (level == 1) finish_level_matrix(F, f32, s);
         Level NL;
@@ -988,6 +1062,10 @@ void build_hierarchy(bcmgx_hierarchy* H, const bcmgx_csr* Ain)
     H->op_wcmplx = wc / nnz0;
     H->avg_cratio = level > 1 ? avcoarseratio / (level - 1) : 1;
     BCMGX_CUDA(cudaStreamSynchronize(s));
+    if (prof_on()) {
+        for (auto& pr : H->prof) std::fprintf(stderr, "[bcmgx setup] %-20s %9.3f ms\n", pr.first.c_str(), pr.second);
+        H->prof.clear();
+    }
 }
 
 }  // namespace bcmgx

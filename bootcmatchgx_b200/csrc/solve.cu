@@ -17,6 +17,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 namespace bcmgx {
 
@@ -56,13 +59,15 @@ static void launch_rowop(int tpr, int n, const int* row, const int* col, const V
     BCMGX_CHECK_LAUNCH();
 }
 
+// About 6-8 entries per lane: 27-point rows -> 4 lanes, 7-point rows -> 2 lanes.
 int default_tpr(int n, int64_t nnz)
 {
-    double avg = n > 0 ? (double)nnz / n : 1.0;
-    if (avg <= 3) return 2;
-    if (avg <= 6) return 4;
-    if (avg <= 16) return 8;
-    if (avg <= 40) return 16;
+    const double avg = n > 0 ? (double)nnz / n : 1.0;
+    if (avg <= 3) return 1;
+    if (avg <= 12) return 2;
+    if (avg <= 32) return 4;
+    if (avg <= 64) return 8;
+    if (avg <= 128) return 16;
     return 32;
 }
 
@@ -71,38 +76,6 @@ void launch_spmv(int n, const int* row, const int* col, const double* val, const
 {
     launch_rowop<OP_AXPBY, double, double, double, double, double>(tpr, n, row, col, val, x,
         (const double*)nullptr, (const double*)nullptr, y, alpha, beta, nullptr, s);
-}
-
-// Threads per row for a matrix: each power of two from 2 to 32 is timed on the matrix itself
-// (three y = A x launches after one warm-up) and the fastest is kept.
-int autotune_tpr(const DevCsr& A, cudaStream_t s)
-{
-    if (A.n < 4096) return default_tpr(A.n, A.nnz);
-    DBuf<double> x, y;
-    x.alloc(A.m, s);
-    y.alloc(A.n, s);
-    BCMGX_CUDA(cudaMemsetAsync(x.p, 0, sizeof(double) * A.m, s));
-    cudaEvent_t e0, e1;
-    BCMGX_CUDA(cudaEventCreate(&e0));
-    BCMGX_CUDA(cudaEventCreate(&e1));
-    int best = default_tpr(A.n, A.nnz);
-    float best_ms = 1e30f;
-    for (int t = 2; t <= 32; t *= 2) {
-        launch_spmv(A.n, A.row.p, A.col.p, A.val.p, x.p, y.p, 1.0, 0.0, t, s);
-        BCMGX_CUDA(cudaEventRecord(e0, s));
-        for (int r = 0; r < 3; r++) launch_spmv(A.n, A.row.p, A.col.p, A.val.p, x.p, y.p, 1.0, 0.0, t, s);
-        BCMGX_CUDA(cudaEventRecord(e1, s));
-        BCMGX_CUDA(cudaEventSynchronize(e1));
-        float ms = 0;
-        BCMGX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        if (ms < best_ms) {
-            best_ms = ms;
-            best = t;
-        }
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    return best;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -387,7 +360,7 @@ void prec_apply_dev(bcmgx_hierarchy* H, const double* r, double* v)
 // ------------------------------------------------------------------------------------------
 // FCG kernels
 // ------------------------------------------------------------------------------------------
-constexpr int kRedBlocksPerSM = 4;
+constexpr int kRedBlocksPerSM = 8;
 constexpr int kRedThreads = 256;
 
 static int red_grid(long work_threads)
@@ -661,6 +634,71 @@ void time_level_kernels(bcmgx_hierarchy* H, int l, int reps, double* out)
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+}
+
+// Threads-per-row autotuner: for a level with at least kTuneMinRows rows, one l1-Jacobi sweep
+// in the cycle's precision is timed (CUDA events, 3 launches after a warm-up) for every
+// candidate 1..16 and the fastest is kept. Results are cached per (rows, nnz, precision) for
+// the life of the process, so repeated set-ups of same-shaped matrices reuse them.
+constexpr int kTuneMinRows = 20000;
+static std::mutex g_tune_mu;
+static std::map<std::tuple<int, int64_t, int>, int> g_tune_cache;
+
+int autotune_tpr(Level& V, bool f32, cudaStream_t s)
+{
+    const DevCsr& A = V.A;
+    const int n = A.n;
+    if (n < kTuneMinRows) return default_tpr(n, A.nnz);
+    const auto key = std::make_tuple(n, A.nnz, f32 ? 1 : 0);
+    {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) return it->second;
+    }
+    DBuf<double> a, b, c;
+    DBuf<float> a32, b32, c32;
+    if (f32) {
+        a32.alloc(n, s);
+        b32.alloc(n, s);
+        c32.alloc(n, s);
+        BCMGX_CUDA(cudaMemsetAsync(a32.p, 0, sizeof(float) * n, s));
+        BCMGX_CUDA(cudaMemsetAsync(c32.p, 0, sizeof(float) * n, s));
+    } else {
+        a.alloc(n, s);
+        b.alloc(n, s);
+        c.alloc(n, s);
+        BCMGX_CUDA(cudaMemsetAsync(a.p, 0, sizeof(double) * n, s));
+        BCMGX_CUDA(cudaMemsetAsync(c.p, 0, sizeof(double) * n, s));
+    }
+    cudaEvent_t e0, e1;
+    BCMGX_CUDA(cudaEventCreate(&e0));
+    BCMGX_CUDA(cudaEventCreate(&e1));
+    int best = default_tpr(n, A.nnz);
+    float best_ms = 1e30f;
+    for (int t = 1; t <= 16; t *= 2) {
+        auto launch = [&] {
+            if (f32)
+                launch_rowop<OP_JACOBI>(t, n, A.row.p, A.col.p, A.val32.p, (const float*)a32.p, (const float*)c32.p, V.M32.p, b32.p, 1.0, 0.0, nullptr, s);
+            else
+                launch_rowop<OP_JACOBI>(t, n, A.row.p, A.col.p, A.val.p, (const double*)a.p, (const double*)c.p, V.M.p, b.p, 1.0, 0.0, nullptr, s);
+        };
+        launch();
+        BCMGX_CUDA(cudaEventRecord(e0, s));
+        for (int r = 0; r < 3; r++) launch();
+        BCMGX_CUDA(cudaEventRecord(e1, s));
+        BCMGX_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        BCMGX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = t;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    g_tune_cache[key] = best;
+    return best;
 }
 
 // Flexible CG (FCG.cu:27-165) on device vectors b, x (x: x0 in, solution out).

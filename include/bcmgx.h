@@ -82,6 +82,7 @@ typedef struct bcmgx_params {
     int record_sweeps;       /* keep every sweep's matching for inspection (default 0)   */
     int use_graph;           /* capture one FCG iteration in a CUDA graph (default 1)    */
     int device;              /* CUDA device ordinal (default: current device)           */
+    int autotune;            /* time threads-per-row choices per level at set-up (default 1) */
     void* stream;            /* cudaStream_t to run on; NULL = library-owned stream      */
 } bcmgx_params;
 
@@ -115,6 +116,7 @@ typedef struct bcmgx_hierarchy_info {
     double op_cmplx, op_wcmplx, avg_cratio;
     int maxcoarsesize, ftcoarse, num_sweep_records;
     double setup_ms;         /* device time of the set-up (CUDA events) */
+    int tpr[BCMGX_MAX_LEVELS];   /* threads per row the solve kernels use on each level */
 } bcmgx_hierarchy_info;
 
 typedef struct bcmgx_hierarchy bcmgx_hierarchy;

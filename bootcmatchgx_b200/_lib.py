@@ -85,6 +85,7 @@ SIGNATURES = {
     "bcmgx_spmv": (C.c_int, [C.c_int, C.c_int, C.c_int64, _vp, _vp, _vp, _vp, _vp, C.c_double,
                              C.c_double, C.c_int, _vp]),
     "bcmgx_edge_weights": (C.c_int, [C.c_int, C.c_int64, _vp, _vp, _vp, _vp, _vp, _dp, _vp]),
+    "bcmgx_edge_weights_noalloc": (C.c_int, [C.c_int, C.c_int64, _vp, _vp, _vp, _vp, _vp, _dp, _vp]),
     "bcmgx_suitor_matching": (C.c_int, [C.c_int, C.c_int64, _vp, _vp, _vp, _vp, _vp]),
     "bcmgx_laplacian_3d_size": (C.c_int, [C.c_int] * 7 + [_i64p, _i64p]),
     "bcmgx_laplacian_3d": (C.c_int, [C.c_int] * 7 + [_vp, _vp, _vp]),

@@ -23,6 +23,7 @@
 #include <cstdlib>
 #include <cmath>
 #include <cstdio>
+#include <mutex>
 
 namespace bcmgx {
 
@@ -1069,3 +1070,110 @@ void build_hierarchy(bcmgx_hierarchy* H, const bcmgx_csr* Ain)
 }
 
 }  // namespace bcmgx
+
+// ------------------------------------------------------------------------------------------
+// Allocation-free edge weights
+// ------------------------------------------------------------------------------------------
+// Some callers cannot let this library allocate device memory: a framework whose caching
+// allocator already holds (nearly) all of the GPU's memory, so that one more allocation would
+// fail, or a process that runs under a fixed device-memory budget. bcmgx_edge_weights_noalloc
+// serves them. Its scratch (the per-row C values, the transposed-entry positions, the absolute
+// minimum and the error words) lives in the file-scope array below, which holds matrices of at
+// most kNoAllocMaxRows rows and kNoAllocMaxNnz entries. Every GPU that loads this library keeps
+// these bytes until the process exits. All calls share the one array and it keeps the last
+// call's contents: the words that must start from a known value are reset by every call, and
+// calls that overlap on the GPU race on the array.
+namespace bcmgx {
+
+constexpr int kNoAllocMaxRows = 65536;
+constexpr int64_t kNoAllocMaxNnz = 2097152;
+constexpr size_t kNoAllocCBytes = sizeof(double) * kNoAllocMaxRows;
+constexpr size_t kNoAllocTposBytes = sizeof(int) * kNoAllocMaxNnz;
+constexpr size_t kNoAllocBytes = kNoAllocCBytes + kNoAllocTposBytes + 256;
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_edge_weights_scratch[kNoAllocBytes];
+
+static std::mutex g_noalloc_mu;
+static unsigned char* g_noalloc_addr[kNoAllocMaxDevices];
+
+// Device address of the scratch array on the current device. In host code the array's name only
+// stands for it; the address is looked up once per device, with that device current.
+static unsigned char* noalloc_scratch()
+{
+    int dev = 0;
+    BCMGX_CUDA(cudaGetDevice(&dev));
+    BCMGX_REQUIRE(dev >= 0 && dev < kNoAllocMaxDevices, BCMGX_ERR_UNSUPPORTED, "device ordinal too large");
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_edge_weights_scratch);
+        if (e != cudaSuccess)
+            throw Error(BCMGX_ERR_CUDA, std::string("cudaGetSymbolAddress of the scratch array failed: ") + cudaGetErrorString(e));
+        g_noalloc_addr[dev] = (unsigned char*)p;
+    }
+    return g_noalloc_addr[dev];
+}
+
+__global__ void k_noalloc_reset(unsigned long long* min_bits, int* err, int* max_row)
+{
+    *min_bits = (unsigned long long)__double_as_longlong(DBL_MAX);
+    *err = 0;
+    *max_row = 0;
+}
+
+static void edge_weights_noalloc(int n, int64_t nnz, const int* row, const int* col, const double* val, const double* w,
+    double* W, double* min_out, cudaStream_t s)
+{
+    BCMGX_REQUIRE(n > 0 && nnz > 0 && row && col && val && w && W, BCMGX_ERR_INVALID_INPUT, "bad argument");
+    BCMGX_REQUIRE(n <= kNoAllocMaxRows && nnz <= kNoAllocMaxNnz, BCMGX_ERR_INVALID_INPUT,
+        "matrix too large for the allocation-free entry point (at most " + std::to_string(kNoAllocMaxRows) + " rows and " +
+            std::to_string(kNoAllocMaxNnz) + " non-zeros; got " + std::to_string(n) + " rows, " + std::to_string(nnz) + ")");
+    unsigned char* base = noalloc_scratch();
+    double* C = (double*)base;
+    int* tpos = (int*)(base + kNoAllocCBytes);
+    unsigned long long* minb = (unsigned long long*)(base + kNoAllocCBytes + kNoAllocTposBytes);
+    int* err = (int*)(minb + 1);
+    int* mx = err + 1;
+    note_launch();
+    k_noalloc_reset<<<1, 1, 0, s>>>(minb, err, mx);
+    note_launch();
+    k_validate<<<warp_grid(n), 256, 0, s>>>(n, n, nnz, row, col, err, mx, 1);
+    BCMGX_CHECK_LAUNCH();
+    int e = read_err(err, s);
+    if (e) throw Error(BCMGX_ERR_INVALID_INPUT, "input matrix: " + err_text(e));
+    note_launch();
+    k_diag_c<<<gs_grid(n), 256, 0, s>>>(n, row, col, val, w, C, err);
+    note_launch();
+    k_tpos<<<warp_grid(n), 256, 0, s>>>(n, row, col, tpos);
+    note_launch();
+    k_ahat_min<<<warp_grid(n), 256, 0, s>>>(n, row, col, val, w, C, minb);
+    BCMGX_CHECK_LAUNCH();
+    double m = 0;
+    BCMGX_CUDA(cudaMemcpyAsync(&m, minb, sizeof(double), cudaMemcpyDeviceToHost, s));
+    e = read_err(err, s);
+    if (e) throw Error(BCMGX_ERR_INVALID_INPUT, "edge weights: " + err_text(e));
+    if (std::fabs(m) < DBL_EPSILON) m = DBL_EPSILON;
+    note_launch();
+    k_logw<<<warp_grid(n), 256, 0, s>>>(n, row, col, val, w, C, tpos, kSuitorEps / (0.999 * m), W);
+    BCMGX_CHECK_LAUNCH();
+    BCMGX_CUDA(cudaStreamSynchronize(s));
+    if (min_out) *min_out = m;
+}
+
+}  // namespace bcmgx
+
+extern "C" int bcmgx_edge_weights_noalloc(int n, int64_t nnz, const int* row, const int* col, const double* val,
+    const double* w, double* W, double* min_abs_out, void* stream)
+{
+    try {
+        bcmgx::edge_weights_noalloc(n, nnz, row, col, val, w, W, min_abs_out, (cudaStream_t)stream);
+        return BCMGX_OK;
+    } catch (const bcmgx::Error& e) {
+        bcmgx::set_last_error(e.msg);
+        return e.code;
+    } catch (const std::exception& e) {
+        bcmgx::set_last_error(e.what());
+        return BCMGX_ERR_INTERNAL;
+    }
+}

@@ -178,6 +178,20 @@ int bcmgx_edge_weights(int n, int64_t nnz, const int* row, const int* col, const
 int bcmgx_suitor_matching(int n, int64_t nnz, const int* row, const int* col, const double* W,
     int* M, void* stream);
 
+/* Allocation-free variant of bcmgx_edge_weights. No counterpart in the reference. For callers
+ * that cannot let the library allocate device memory -- a framework whose caching allocator
+ * already holds (nearly) all of the GPU's memory, or a process under a fixed device-memory
+ * budget. Same arguments and results as bcmgx_edge_weights; it calls no allocator (no cudaMalloc,
+ * cudaMallocAsync, cudaFree or library allocator). Its scratch is a static device array of about
+ * 8.5 MiB (per-row values and per-entry positions) that every GPU loading the library holds until
+ * exit; matrices beyond 65536 rows or 2097152 non-zeros are rejected with
+ * BCMGX_ERR_INVALID_INPUT. The first call on a device looks up that device's address of the
+ * array (cudaGetSymbolAddress), so make that first call before any stream capture. All calls
+ * share the array: calls that overlap on the GPU (other streams, other host threads) race on it
+ * and must be serialised by the caller. */
+int bcmgx_edge_weights_noalloc(int n, int64_t nnz, const int* row, const int* col, const double* val,
+    const double* w, double* W, double* min_abs_out, void* stream);
+
 /* ---- input plumbing (host) ---------------------------------------------------------------- */
 /* Size of the 7- or 27-point Laplacian on the (nx*P) x (ny*Q) x (nz*R) grid. */
 int bcmgx_laplacian_3d_size(int stencil, int nx, int ny, int nz, int P, int Q, int R, int64_t* n, int64_t* nnz);

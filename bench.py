@@ -354,15 +354,43 @@ def run_ours(a, wl, rank, world, local_rank):
     return line
 
 
-# dram bytes (read + write) of one level-0 FP32 Jacobi launch from the committed ncu capture
-# (profiles/jacobi_fp32_poisson27.md); None until measured.
-TRAFFIC = {}
+# DRAM bytes (read + write) of one level-0 FP32 Jacobi launch. Measured by ncu on the 100^3 case
+# (profiles/jacobi_fp32_poisson27_100.md: 231.67 MB = 0.99983 x its algorithmic bytes) and scaled
+# by the algorithmic bytes (non-zeros) to the other 27-point workloads.
+TRAFFIC = {"poisson27_100": 231670016, "poisson27_160": int(0.99983 * (8 * 109215352 + 4 * 4096001 + 16 * 4096000))}
 
 
 def _spmv(row, col, val, x):
     import scipy.sparse as sp
     n = row.size - 1
     return sp.csr_matrix((val, col, row), shape=(n, n)) @ x
+
+
+def profile_step(a, wl):
+    """W warm-up steps, then exactly one set-up + solve (FP32 V-cycle) on device-resident data;
+    prints how many library kernels the warm-up and the step launched."""
+    import torch
+    import bootcmatchgx_b200 as bx
+    dev = torch.device("cuda", 0)
+    row, col, val, xs, b = build_problem(wl)
+    d = [torch.from_numpy(x_).to(dev) for x_ in (row, col, val, b)]
+    x = torch.zeros(row.size - 1, dtype=torch.float64, device=dev)
+    p = bx.params_default(solver="FCG", preconditioner="BCMG", rtol=RTOL, dispnorm=0, vcycle_precision="FP32")
+    L = bx.lib()
+    c0 = L.bcmgx_launch_count()
+    for _ in range(a.warmup):
+        h = bx.Hierarchy(d[0], d[1], d[2], p)
+        x.zero_()
+        h.solve(d[3], x)
+        h.free()
+    c1 = L.bcmgx_launch_count()
+    h = bx.Hierarchy(d[0], d[1], d[2], p)
+    x.zero_()
+    _, info = h.solve(d[3], x)
+    h.free()
+    torch.cuda.synchronize()
+    c2 = L.bcmgx_launch_count()
+    print(json.dumps({"warmup_launches": c1 - c0, "step_launches": c2 - c1, "niter": info["niter"]}), flush=True)
 
 
 def main():
@@ -373,11 +401,16 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="poisson27_160", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-step", action="store_true",
+                    help="only W warm-up steps and one FP32 step (for ncu launch lists); prints the launch counts")
     a = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     wl = WORKLOADS[a.workload]
+    if a.profile_step:
+        profile_step(a, wl)
+        return
     if a.impl == "reference":
         line = reference_arm(a, wl, rank, world)
         if line is not None:

@@ -11,27 +11,31 @@ namespace bcmgx {
 
 enum RowOp { OP_AXPBY = 0, OP_RESID = 1, OP_JACOBI = 2 };
 
-// Partial dot product of one row over the lanes of a sub-warp, unrolled by 4 so that the
-// column, value and gather loads of several entries are in flight together.
+// Partial dot product of one row over the lanes of a sub-warp. Entries are taken in batches of
+// K per lane: all K column and value loads are issued, then all K gathers of x, then the K
+// multiply-adds, so a row of up to K*S entries costs one round of memory latency per lane.
 template <int S, typename AT, typename VT, typename XT>
 __device__ __forceinline__ AT row_partial(int b, int e, int lane, const int* __restrict__ col,
     const VT* __restrict__ val, const XT* __restrict__ x)
 {
-    AT s0 = 0, s1 = 0;
-    int j = b + lane;
-    for (; j + 3 * S < e; j += 4 * S) {
-        const int c0 = ld_stream(col + j), c1 = ld_stream(col + j + S);
-        const int c2 = ld_stream(col + j + 2 * S), c3 = ld_stream(col + j + 3 * S);
-        const VT v0 = ld_stream(val + j), v1 = ld_stream(val + j + S);
-        const VT v2 = ld_stream(val + j + 2 * S), v3 = ld_stream(val + j + 3 * S);
-        const XT x0 = ld_ro(x + c0), x1 = ld_ro(x + c1), x2 = ld_ro(x + c2), x3 = ld_ro(x + c3);
-        s0 += (AT)v0 * (AT)x0;
-        s1 += (AT)v1 * (AT)x1;
-        s0 += (AT)v2 * (AT)x2;
-        s1 += (AT)v3 * (AT)x3;
+    constexpr int K = 8;
+    AT s = 0;
+    for (int j0 = b + lane; j0 < e; j0 += K * S) {
+        int c[K];
+        VT v[K];
+        XT xv[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const int j = j0 + k * S;
+            c[k] = j < e ? ld_stream(col + j) : -1;
+            v[k] = j < e ? ld_stream(val + j) : VT(0);
+        }
+#pragma unroll
+        for (int k = 0; k < K; k++) xv[k] = c[k] >= 0 ? ld_ro(x + c[k]) : XT(0);
+#pragma unroll
+        for (int k = 0; k < K; k++) s += (AT)v[k] * (AT)xv[k];
     }
-    for (; j < e; j += S) s0 += (AT)ld_stream(val + j) * (AT)ld_ro(x + ld_stream(col + j));
-    return s0 + s1;
+    return s;
 }
 
 // y = alpha*A*x + beta*y (OP_AXPBY), y = f - A*x (OP_RESID) or one l1-Jacobi sweep

@@ -196,6 +196,7 @@ __global__ void k_validate(int n, int m, long long nnz, const int* __restrict__ 
     int* err, int* max_row, int need_diag)
 {
     const int lane = threadIdx.x & 31;
+    int mx = 0;
     for (long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32; r < n; r += (long)gridDim.x * blockDim.x / 32) {
         const int b = row[r], e = row[r + 1];
         int bad = 0;
@@ -213,11 +214,12 @@ __global__ void k_validate(int n, int m, long long nnz, const int* __restrict__ 
             }
             diag = __any_sync(0xffffffffu, diag);
             if (need_diag && !diag) bad |= ERR_NODIAG;
-            if (lane == 0) atomicMax(max_row, e - b);
+            mx = max(mx, e - b);
         }
         bad = __reduce_or_sync(0xffffffffu, bad);
         if (lane == 0 && bad) atomicOr(err, bad);
     }
+    if (lane == 0 && mx > 0) atomicMax(max_row, mx);
 }
 
 __global__ void k_row_max(int n, const int* __restrict__ row, int* max_row)

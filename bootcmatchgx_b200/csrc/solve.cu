@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -639,10 +640,38 @@ void time_level_kernels(bcmgx_hierarchy* H, int l, int reps, double* out)
 // Threads-per-row autotuner: for a level with at least kTuneMinRows rows, one l1-Jacobi sweep
 // in the cycle's precision is timed (CUDA events, 3 launches after a warm-up) for every
 // candidate 1..16 and the fastest is kept. Results are cached per (rows, nnz, precision) for
-// the life of the process, so repeated set-ups of same-shaped matrices reuse them.
+// the life of the process, so repeated set-ups of same-shaped matrices reuse them; when the
+// environment variable BCMGX_TUNE_CACHE names a file, the cache is also read from it at the
+// first use and every new result is appended to it (one "rows nnz precision tpr" line each).
 constexpr int kTuneMinRows = 20000;
 static std::mutex g_tune_mu;
 static std::map<std::tuple<int, int64_t, int>, int> g_tune_cache;
+static bool g_tune_loaded = false;
+
+static void tune_cache_load()
+{
+    if (g_tune_loaded) return;
+    g_tune_loaded = true;
+    const char* path = std::getenv("BCMGX_TUNE_CACHE");
+    if (!path) return;
+    FILE* f = std::fopen(path, "r");
+    if (!f) return;
+    long long z;
+    int n, prec, t;
+    while (std::fscanf(f, "%d %lld %d %d", &n, &z, &prec, &t) == 4)
+        if (t == 1 || t == 2 || t == 4 || t == 8 || t == 16 || t == 32) g_tune_cache[std::make_tuple(n, (int64_t)z, prec)] = t;
+    std::fclose(f);
+}
+
+static void tune_cache_store(const std::tuple<int, int64_t, int>& key, int t)
+{
+    const char* path = std::getenv("BCMGX_TUNE_CACHE");
+    if (!path) return;
+    FILE* f = std::fopen(path, "a");
+    if (!f) return;
+    std::fprintf(f, "%d %lld %d %d\n", std::get<0>(key), (long long)std::get<1>(key), std::get<2>(key), t);
+    std::fclose(f);
+}
 
 int autotune_tpr(Level& V, bool f32, cudaStream_t s)
 {
@@ -652,6 +681,7 @@ int autotune_tpr(Level& V, bool f32, cudaStream_t s)
     const auto key = std::make_tuple(n, A.nnz, f32 ? 1 : 0);
     {
         std::lock_guard<std::mutex> g(g_tune_mu);
+        tune_cache_load();
         auto it = g_tune_cache.find(key);
         if (it != g_tune_cache.end()) return it->second;
     }
@@ -698,6 +728,7 @@ int autotune_tpr(Level& V, bool f32, cudaStream_t s)
     cudaEventDestroy(e1);
     std::lock_guard<std::mutex> g(g_tune_mu);
     g_tune_cache[key] = best;
+    tune_cache_store(key, best);
     return best;
 }
 

@@ -40,7 +40,13 @@ WORKLOADS = {
                     "text": "3D Poisson 7-point 50^3 Dirichlet (diag 6, off -1), FP64 CSR"},
     "poisson27_100": {"stencil": 27, "grid": (100, 100, 100), "seed": 1,
                       "text": "3D Poisson 27-point 100^3 Dirichlet, FP64 CSR"},
+    "diffusion7_256": {"kind": "diffusion", "grid": (256, 256, 256), "theta_seed": 2, "rhs_seed": 3,
+                       "text": "7-point FV diffusion 256^3, kappa = exp(theta), theta Gaussian random field "
+                               "(squared-exponential, length 8, sigma 2, seed 2), harmonic-mean faces; b ~ U[0,1] (seed 3)"},
+    "diffusion7_64": {"kind": "diffusion", "grid": (64, 64, 64), "theta_seed": 2, "rhs_seed": 3,
+                      "text": "7-point FV diffusion 64^3 (small variant of diffusion7_256)"},
 }
+ADJOINT = {"grid": (96, 96, 96), "theta_seed": 5, "noise_seed": 6, "directions": 20, "step": 1e-6, "rtol": 1e-10}
 RTOL = 1e-8
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 
@@ -57,6 +63,13 @@ def read_peaks():
 def build_problem(wl):
     import scipy.sparse as sp
     import bootcmatchgx_b200 as bx
+    if wl.get("kind") == "diffusion":
+        from bootcmatchgx_b200 import problems
+        g = wl["grid"]
+        theta = problems.gaussian_random_field(g, length=8.0, sigma=2.0, seed=wl["theta_seed"])
+        row, col, val = bx.diffusion_7p(*g, np.exp(theta).reshape(-1, order="F").reshape(-1))
+        b = np.random.default_rng(wl["rhs_seed"]).uniform(0.0, 1.0, row.size - 1)
+        return row, col, val, None, b
     st, (nx, ny, nz), seed = wl["stencil"], wl["grid"], wl["seed"]
     row, col, val = bx.laplacian_3d(st, nx, ny, nz)
     n = row.size - 1
@@ -135,7 +148,7 @@ def cpu_baseline(wl, row, col, val, b, xs, max_seconds=30.0):
             "sample": f"full set-up + full FCG solve ({info['niter']} iterations) of the same "
                       f"workload with oracle/bcmgx_oracle.cpp, OMP threads={cores}",
             "setup_s": t_setup, "solve_s": t_solve, "niter": info["niter"],
-            "err_vs_xstar": float(np.linalg.norm(x - xs) / np.linalg.norm(xs))}
+            "err_vs_xstar": None if xs is None else float(np.linalg.norm(x - xs) / np.linalg.norm(xs))}
 
 
 def reference_arm(a, wl, rank, world):
@@ -320,7 +333,8 @@ def run_ours(a, wl, rank, world, local_rank):
         "warmup": a.warmup, "ms_per_step": ms32, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64 outer FCG / f32 V-cycle", "data": "synthetic",
         "config": {"workload": a.workload, "problem": wl["text"], "rows": int(n), "nnz": int(nnz),
-                   "rhs": f"b = A x*, x* ~ U[-1,1] (numpy default_rng({wl['seed']}))",
+                   "rhs": (f"b = A x*, x* ~ U[-1,1] (numpy default_rng({wl['seed']}))" if xs is not None
+                           else f"b ~ U[0,1] (numpy default_rng({wl['rhs_seed']}))"),
                    "rtol": RTOL, "settings": "FCG_BCMG.properties defaults (aggrsweeps 2, 4+4 l1-Jacobi, "
                    "20 coarse sweeps, V-cycle)", "vcycle": "fp32",
                    "l2": "inputs larger than L2 (CSR 1.39 GB)" if nnz > 5e7 else "inputs fit in L2",
@@ -331,7 +345,8 @@ def run_ours(a, wl, rank, world, local_rank):
         "fp64": {"value": ms64 / 1e3, "setup_ms": setup64, "solve_ms": solve64,
                  "niter": infos64[-1][0]["niter"]},
         "fp32_speedup_vs_fp64": ms64 / ms32,
-        "errors": {"fp32_vs_xstar": float(nrm(x32 - xs) / nrm(xs)), "fp64_vs_xstar": float(nrm(x64 - xs) / nrm(xs)),
+        "errors": {"fp32_vs_xstar": None if xs is None else float(nrm(x32 - xs) / nrm(xs)),
+                   "fp64_vs_xstar": None if xs is None else float(nrm(x64 - xs) / nrm(xs)),
                    "fp32_vs_fp64_tight": float(nrm(x32 - xt) / nrm(xt)),
                    "fp64_vs_fp64_tight": float(nrm(x64 - xt) / nrm(xt)),
                    "fp32_rel_residual": float(nrm(b - _spmv(row, col, val, x32)) / nrm(b))},
@@ -364,6 +379,131 @@ def _spmv(row, col, val, x):
     import scipy.sparse as sp
     n = row.size - 1
     return sp.csr_matrix((val, col, row), shape=(n, n)) @ x
+
+
+def run_adjoint(a):
+    """Differentiated solve (7-point FV diffusion 96^3, kappa = exp(theta)): forward FCG+BCMG to
+    1e-10, backward = adjoint solve on the same hierarchy, chained to dL/dtheta by torch; the
+    gradient is checked along random directions against FP64 central differences and against
+    the gradient of a fresh plain-FP64 solve."""
+    import torch
+    import bootcmatchgx_b200 as bx
+    from bootcmatchgx_b200 import autograd, problems
+    dev = torch.device("cuda", 0)
+    cfg = ADJOINT
+    g = cfg["grid"]
+    n = g[0] * g[1] * g[2]
+    theta0 = torch.from_numpy(problems.gaussian_random_field(g, 8.0, 2.0, cfg["theta_seed"]).reshape(-1, order="F")).to(dev)
+    asm = problems.DiffusionAssembler(*g, dev)
+    rng = np.random.default_rng(cfg["noise_seed"])
+    b = torch.ones(n, dtype=torch.float64, device=dev)
+    prm = autograd.default_params(rtol=cfg["rtol"], vcycle_precision="FP32")
+    prm64 = autograd.default_params(rtol=cfg["rtol"], vcycle_precision="FP64")
+    with torch.no_grad():
+        x_obs = autograd.solve(asm.row, asm.col, asm.values(torch.exp(theta0)), b, prm64)
+        x_obs = x_obs + 1e-3 * torch.from_numpy(rng.standard_normal(n)).to(dev)
+    theta = (theta0 + 0.1 * torch.from_numpy(rng.standard_normal(n)).to(dev)).detach()
+
+    def fwd_bwd(p):
+        th = theta.clone().requires_grad_(True)
+        x = autograd.solve(asm.row, asm.col, asm.values(torch.exp(th)), b, p)
+        L = 0.5 * ((x - x_obs) ** 2).sum()
+        (gr,) = torch.autograd.grad(L, th)
+        return L.detach(), gr
+
+    def loss(th, p):
+        with torch.no_grad():
+            x = autograd.solve(asm.row, asm.col, asm.values(torch.exp(th)), b, p)
+            return 0.5 * ((x - x_obs) ** 2).sum()
+
+    for _ in range(max(1, a.warmup)):
+        fwd_bwd(prm)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.steps):
+        L, grad = fwd_bwd(prm)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / a.steps
+    _, grad64 = fwd_bwd(prm64)
+    tight = autograd.default_params(rtol=1e-10, vcycle_precision="FP64")
+    _, grad_t = fwd_bwd(tight)
+    errs, errs_t = [], []
+    h = cfg["step"]
+    for _ in range(cfg["directions"]):
+        d = torch.from_numpy(rng.standard_normal(n)).to(dev)   # N(0, I) direction, per-cell step h
+        fd = (loss(theta + h * d, tight) - loss(theta - h * d, tight)) / (2 * h)
+        errs.append(abs(float(fd - (grad * d).sum())) / abs(float(fd)))
+        errs_t.append(abs(float(fd - (grad_t * d).sum())) / abs(float(fd)))
+    return {"metric": "differentiated solve: forward+backward s (FP32 V-cycle)", "value": ms / 1e3, "unit": "s",
+            "higher_is_better": False, "workload": "diffusion7_96_adjoint", "rows": n, "nnz": int(asm.nnz),
+            "config": {"problem": "7-point FV diffusion 96^3, kappa = exp(theta), theta GRF (length 8, sigma 2, seed 5); "
+                                  "x_obs = x(theta0) + N(0,1e-3); theta = theta0 + 0.1 N(0,1); L = 0.5||x - x_obs||^2",
+                       "rtol": cfg["rtol"], "fd_step": h, "directions": cfg["directions"]},
+            "fd": "central differences of L on FP64 solves to rtol 1e-10, directions d ~ N(0, I)",
+            "grad_rel_err_vs_central_fd_max": max(errs), "grad_rel_err_vs_central_fd_median": float(np.median(errs)),
+            "grad_fp64_rel_err_vs_central_fd_max": max(errs_t),
+            "grad_rel_err_vs_fresh_fp64": float((grad - grad64).norm() / grad64.norm()), "loss": float(L)}
+
+
+def run_batch(a):
+    """256 independent 7-point Poisson systems, box sides uniform in 10..46 (seed 4), diagonal shift
+    uniform[0, 0.5], FP32 V-cycle, rhs uniform[-1,1]: one CUDA-graph launch for all solves vs a
+    sequential loop of single solves (same hierarchies, warm graphs)."""
+    import scipy.sparse as sp
+    import torch
+    import bootcmatchgx_b200 as bx
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(4)
+    systems, rows = [], 0
+    for _ in range(256):
+        dims = [int(d) for d in rng.integers(10, 47, size=3)]
+        shift = rng.uniform(0.0, 0.5)
+        r, c, v = bx.laplacian_3d(7, *dims)
+        v = v + shift * (c == np.repeat(np.arange(r.size - 1), np.diff(r)))
+        systems.append((r, c, v))
+        rows += r.size - 1
+    bs = [torch.from_numpy(rng.uniform(-1, 1, r.size - 1)).to(dev) for r, _, _ in systems]
+    p = bx.params_default(solver="FCG", preconditioner="BCMG", rtol=1e-8, dispnorm=0, vcycle_precision="FP32")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    B = bx.Batch(systems, p, nthreads=min(16, os.cpu_count() or 1))
+    torch.cuda.synchronize()
+    t_setup = time.perf_counter() - t0
+    xs, infos = B.solve(bs)   # builds the graph
+    for _ in range(max(0, a.warmup - 1)):
+        B.solve(bs)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        xs, infos = B.solve(bs)
+    torch.cuda.synchronize()
+    t_batch = (time.perf_counter() - t0) / a.steps
+    hs = [B.hierarchy(k) for k in range(len(systems))]
+    for k, h in enumerate(hs):   # warm each single-solve graph
+        h.solve(bs[k])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        for k, h in enumerate(hs):
+            h.solve(bs[k])
+    torch.cuda.synchronize()
+    t_seq = (time.perf_counter() - t0) / a.steps
+    worst = 0.0
+    for k, (r, c, v) in enumerate(systems):
+        A = sp.csr_matrix((v, c, r), shape=(r.size - 1,) * 2)
+        bb = bs[k].cpu().numpy()
+        worst = max(worst, float(np.linalg.norm(bb - A @ xs[k].cpu().numpy()) / np.linalg.norm(bb)))
+    B.free()
+    return {"metric": "batched solves/s (256 uneven 7-point systems, one graph launch)", "value": 256 / t_batch,
+            "unit": "solves/s", "higher_is_better": True, "workload": "batch256_poisson7",
+            "sequential_solves_per_s": 256 / t_seq, "speedup_vs_sequential": t_seq / t_batch,
+            "batch_solve_ms": t_batch * 1e3, "sequential_ms": t_seq * 1e3, "setup_ms": t_setup * 1e3,
+            "total_rows": rows, "iters_min_max": [min(i["niter"] for i in infos), max(i["niter"] for i in infos)],
+            "max_rel_residual": worst, "steps": a.steps, "warmup": a.warmup,
+            "config": {"systems": 256, "sides": "uniform 10..46 (numpy default_rng(4))", "shift": "uniform[0,0.5]",
+                       "vcycle": "fp32", "rtol": 1e-8, "setup_threads": min(16, os.cpu_count() or 1)}}
 
 
 def profile_step(a, wl):
@@ -401,6 +541,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="poisson27_160", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--adjoint", action="store_true", help="run the differentiated-solve configuration instead")
+    ap.add_argument("--batch", action="store_true", help="run the batched-systems configuration instead")
     ap.add_argument("--profile-step", action="store_true",
                     help="only W warm-up steps and one FP32 step (for ncu launch lists); prints the launch counts")
     a = ap.parse_args()
@@ -410,6 +552,12 @@ def main():
     wl = WORKLOADS[a.workload]
     if a.profile_step:
         profile_step(a, wl)
+        return
+    if a.adjoint:
+        print(json.dumps(run_adjoint(a)), flush=True)
+        return
+    if a.batch:
+        print(json.dumps(run_batch(a)), flush=True)
         return
     if a.impl == "reference":
         line = reference_arm(a, wl, rank, world)

@@ -75,7 +75,13 @@ SIGNATURES = {
     "bcmgx_params_dump": (C.c_int, [C.POINTER(Params), C.c_char_p]),
     "bcmgx_setup": (C.c_int, [C.POINTER(Csr), C.POINTER(Params), C.POINTER(C.c_void_p)]),
     "bcmgx_solve": (C.c_int, [_vp, _vp, _vp, C.c_int, C.POINTER(SolveInfo)]),
+    "bcmgx_solve_adjoint": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int, C.POINTER(SolveInfo)]),
     "bcmgx_free": (C.c_int, [_vp]),
+    "bcmgx_setup_batch": (C.c_int, [C.c_int, _vp, C.POINTER(Params), C.c_int, C.POINTER(C.c_void_p)]),
+    "bcmgx_batch_from_hierarchies": (C.c_int, [C.c_int, _vp, C.POINTER(C.c_void_p)]),
+    "bcmgx_batch_get_hierarchy": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_void_p)]),
+    "bcmgx_batch_solve": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "bcmgx_batch_free": (C.c_int, [_vp]),
     "bcmgx_hierarchy_get_info": (C.c_int, [_vp, C.POINTER(HierarchyInfo)]),
     "bcmgx_hierarchy_get_level": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),
     "bcmgx_hierarchy_get_prolongator": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),

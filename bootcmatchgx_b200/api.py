@@ -155,6 +155,7 @@ class Hierarchy:
         check(lib().bcmgx_setup(C.byref(A), C.byref(params), C.byref(h)), "prec_setup")
         self.h = h
         self.n = n
+        self.nnz = int(col.shape[0])
         self.params = params
         self._keep = None
 
@@ -180,6 +181,24 @@ class Hierarchy:
         out = {"retv": info.retv, "niter": info.niter, "delta0": info.delta0,
                "exit_res": info.exit_res, "solve_ms": info.solve_ms, "status": rc}
         return x, out
+
+    def adjoint(self, g, x=None, want_dA=True):
+        """lambda = A^{-1} g and dL/dA on A's pattern (-lambda_i x_j), for g = dL/dx."""
+        info = L.SolveInfo()
+        if _is_device(g):
+            import torch
+            lam = torch.empty_like(g)
+            dA = torch.empty(self.nnz, dtype=torch.float64, device=g.device) if want_dA else None
+            rc = lib().bcmgx_solve_adjoint(self.h, _ptr(g), _ptr(x), _ptr(lam), _ptr(dA), 1, C.byref(info))
+        else:
+            g = np.ascontiguousarray(g, dtype=np.float64)
+            lam = np.empty_like(g)
+            xx = None if x is None else np.ascontiguousarray(x, dtype=np.float64)
+            dA = np.empty(self.nnz) if want_dA else None
+            rc = lib().bcmgx_solve_adjoint(self.h, _ptr(g), _ptr(xx), _ptr(lam), _ptr(dA), 0, C.byref(info))
+        if rc != L.OK:
+            raise BcmgxError(rc, "adjoint solve", L.last_error())
+        return lam, dA, {"niter": info.niter, "solve_ms": info.solve_ms}
 
     def prec_apply(self, r):
         if _is_device(r):
@@ -246,6 +265,74 @@ class Hierarchy:
     def free(self):
         if getattr(self, "h", None):
             check(lib().bcmgx_free(self.h), "prec_finalize")
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class _Borrowed(Hierarchy):
+    """A hierarchy owned by a Batch (not freed by this wrapper)."""
+
+    def __init__(self, handle, n, nnz, params):
+        self.h = handle
+        self.n = n
+        self.nnz = nnz
+        self.params = params
+
+    def free(self):
+        self.h = None
+
+
+class Batch:
+    """Independent systems whose set-ups run concurrently and whose solves run as one CUDA graph
+    launch (bcmgx_setup_batch / bcmgx_batch_solve). systems: list of host (row, col, val)."""
+
+    def __init__(self, systems, params, nthreads=0):
+        arrs = []
+        descs = (L.Csr * len(systems))()
+        for k, (row, col, val) in enumerate(systems):
+            row = np.ascontiguousarray(row, dtype=np.int32)
+            col = np.ascontiguousarray(col, dtype=np.int32)
+            val = np.ascontiguousarray(val, dtype=np.float64)
+            arrs.append((row, col, val))
+            n = row.size - 1
+            descs[k] = L.Csr(n, n, col.size, _ptr(row), _ptr(col), _ptr(val), 0)
+        h = C.c_void_p()
+        check(lib().bcmgx_setup_batch(len(systems), descs, C.byref(params), nthreads, C.byref(h)), "batch set-up")
+        self.h = h
+        self.params = params
+        self.sizes = [(r.size - 1, c.size) for r, c, _ in arrs]
+
+    def __len__(self):
+        return len(self.sizes)
+
+    def hierarchy(self, k):
+        hh = C.c_void_p()
+        check(lib().bcmgx_batch_get_hierarchy(self.h, k, C.byref(hh)), "batch_get_hierarchy")
+        return _Borrowed(hh, self.sizes[k][0], self.sizes[k][1], self.params)
+
+    def solve(self, bs, xs=None):
+        """bs, xs: lists of CUDA float64 tensors (xs updated in place; zeros when None)."""
+        import torch
+        if xs is None:
+            xs = [torch.zeros_like(b) for b in bs]
+        m = len(bs)
+        pb = (C.c_void_p * m)(*[b.data_ptr() for b in bs])
+        px = (C.c_void_p * m)(*[x.data_ptr() for x in xs])
+        infos = (L.SolveInfo * m)()
+        rc = lib().bcmgx_batch_solve(self.h, pb, px, infos)
+        if rc not in (L.OK, L.ERR_NO_CONVERGENCE):
+            raise BcmgxError(rc, "batch solve", L.last_error())
+        return xs, [{"niter": i.niter, "retv": i.retv, "exit_res": i.exit_res, "delta0": i.delta0,
+                     "solve_ms": i.solve_ms} for i in infos]
+
+    def free(self):
+        if getattr(self, "h", None):
+            check(lib().bcmgx_batch_free(self.h), "batch_free")
             self.h = None
 
     def __del__(self):

@@ -3,6 +3,7 @@
 #include "internal.h"
 
 #include <atomic>
+#include <thread>
 #include <cstdlib>
 #include <cmath>
 #include <cstdio>
@@ -16,6 +17,8 @@ void set_last_error(const std::string& s) { g_last_error = s; }
 static std::atomic<long long> g_launches { 0 };
 
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void note_launches(long long k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+long long launch_count() { return g_launches.load(); }
 
 template <typename F>
 static int guarded(F&& f)
@@ -79,9 +82,95 @@ static void check_params(const bcmgx_params* p)
         BCMGX_ERR_INVALID_INPUT, "invalid vcycle_precision");
 }
 
+// Builds one hierarchy (the body of bcmgx_setup). own_stream forces a library-owned stream even
+// when params name one (batch set-ups run concurrently, one stream each).
+static bcmgx_hierarchy* setup_one(const bcmgx_csr* A, const bcmgx_params* p, int device, bool own_stream)
+{
+    check_params(p);
+    BCMGX_REQUIRE(A->n > 0 && A->n == A->m, BCMGX_ERR_INVALID_INPUT, "matrix must be square with n > 0");
+    BCMGX_REQUIRE(A->nnz > 0 && A->nnz <= 0x7fffffffLL, BCMGX_ERR_INVALID_INPUT, "nnz must be in [1, 2^31-1]");
+    BCMGX_REQUIRE(A->row && A->col && A->val, BCMGX_ERR_INVALID_INPUT, "NULL CSR array");
+    std::unique_ptr<bcmgx_hierarchy> H(new bcmgx_hierarchy());
+    H->prm = *p;
+    int dev = device >= 0 ? device : p->device;
+    if (dev < 0) BCMGX_CUDA(cudaGetDevice(&dev));
+    H->device = dev;
+    H->prm.device = dev;
+    DeviceScope ds(dev);
+    if (p->stream && !own_stream) {
+        H->stream = (cudaStream_t)p->stream;
+    } else {
+        BCMGX_CUDA(cudaStreamCreateWithFlags(&H->stream, cudaStreamNonBlocking));
+        H->own_stream = true;
+        H->prm.stream = H->stream;
+    }
+    // keep freed blocks in the pool: repeated set-ups reuse them without cudaMalloc
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    BCMGX_CUDA(cudaEventCreate(&H->ev0));
+    BCMGX_CUDA(cudaEventCreate(&H->ev1));
+    BCMGX_CUDA(cudaEventCreateWithFlags(&H->ev_it[0], cudaEventDisableTiming));
+    BCMGX_CUDA(cudaEventCreateWithFlags(&H->ev_it[1], cudaEventDisableTiming));
+    cudaEvent_t e0, e1;
+    BCMGX_CUDA(cudaEventCreate(&e0));
+    BCMGX_CUDA(cudaEventCreate(&e1));
+    BCMGX_CUDA(cudaEventRecord(e0, H->stream));
+    build_hierarchy(H.get(), A);
+    const char* force = std::getenv("BCMGX_TPR");
+    const int L = (int)H->lv.size();
+    for (int l = 0; l < L; l++) {
+        Level& V = H->lv[l];
+        const bool f32 = p->vcycle_precision == BCMGX_VCYCLE_FP32 && l < L - 1;
+        if (force) V.A.tpr = std::atoi(force);
+        else if (p->autotune) V.A.tpr = autotune_tpr(V, f32, H->stream);
+        else V.A.tpr = default_tpr(V.A.n, V.A.nnz);
+    }
+    BCMGX_CUDA(cudaEventRecord(e1, H->stream));
+    BCMGX_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    H->setup_ms = ms;
+    return H.release();
+}
+
+static void finish_batch(bcmgx_batch* B, const bcmgx_params* p)
+{
+    DeviceScope ds(B->device);
+    if (p && p->stream) {
+        B->stream = (cudaStream_t)p->stream;
+    } else {
+        BCMGX_CUDA(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
+        B->own_stream = true;
+    }
+    BCMGX_CUDA(cudaEventCreate(&B->ev0));
+    BCMGX_CUDA(cudaEventCreate(&B->ev1));
+}
+
 }  // namespace bcmgx
 
 using namespace bcmgx;
+
+bcmgx_batch::~bcmgx_batch()
+{
+    if (stream) cudaStreamSynchronize(stream);
+    if (exec) cudaGraphExecDestroy(exec);
+    copies.release();
+    states_ptr.release();
+    states.release();
+    if (stream) cudaStreamSynchronize(stream);
+    if (states_host) cudaFreeHost(states_host);
+    if (copies_host) cudaFreeHost(copies_host);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (own)
+        for (auto* h : hs) delete h;
+    if (own_stream && stream) cudaStreamDestroy(stream);
+}
 
 bcmgx_hierarchy::~bcmgx_hierarchy()
 {
@@ -98,10 +187,15 @@ bcmgx_hierarchy::~bcmgx_hierarchy()
     res32.release();
     partials.release();
     st.release();
+    hist.release();
+    gb.release();
+    gx.release();
     if (stream) cudaStreamSynchronize(stream);
     if (st_host) cudaFreeHost(st_host);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    for (auto& e : ev_it)
+        if (e) cudaEventDestroy(e);
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
@@ -153,52 +247,90 @@ int bcmgx_setup(const bcmgx_csr* A, const bcmgx_params* p, bcmgx_hierarchy** out
     return guarded([&] {
         BCMGX_REQUIRE(A && out, BCMGX_ERR_INVALID_INPUT, "NULL argument");
         *out = nullptr;
+        *out = setup_one(A, p, -1, false);
+    });
+}
+
+int bcmgx_setup_batch(int nsys, const bcmgx_csr* A, const bcmgx_params* p, int nthreads, bcmgx_batch** out)
+{
+    return guarded([&] {
+        BCMGX_REQUIRE(nsys > 0 && A && p && out, BCMGX_ERR_INVALID_INPUT, "bad argument");
+        *out = nullptr;
         check_params(p);
-        BCMGX_REQUIRE(A->n > 0 && A->n == A->m, BCMGX_ERR_INVALID_INPUT, "matrix must be square with n > 0");
-        BCMGX_REQUIRE(A->nnz > 0 && A->nnz <= 0x7fffffffLL, BCMGX_ERR_INVALID_INPUT, "nnz must be in [1, 2^31-1]");
-        BCMGX_REQUIRE(A->row && A->col && A->val, BCMGX_ERR_INVALID_INPUT, "NULL CSR array");
-        std::unique_ptr<bcmgx_hierarchy> H(new bcmgx_hierarchy());
-        H->prm = *p;
         int dev = p->device;
         if (dev < 0) BCMGX_CUDA(cudaGetDevice(&dev));
-        H->device = dev;
-        DeviceScope ds(dev);
-        if (p->stream) {
-            H->stream = (cudaStream_t)p->stream;
-        } else {
-            BCMGX_CUDA(cudaStreamCreateWithFlags(&H->stream, cudaStreamNonBlocking));
-            H->own_stream = true;
+        std::unique_ptr<bcmgx_batch> B(new bcmgx_batch());
+        B->own = true;
+        B->device = dev;
+        B->hs.assign(nsys, nullptr);
+        const int T = std::max(1, std::min(nthreads > 0 ? nthreads : 8, nsys));
+        std::vector<std::string> errs(T);
+        std::vector<int> codes(T, BCMGX_OK);
+        std::vector<std::thread> pool;
+        for (int t = 0; t < T; t++) {
+            pool.emplace_back([&, t] {
+                try {
+                    BCMGX_CUDA(cudaSetDevice(dev));
+                    for (int k = t; k < nsys; k += T) B->hs[k] = setup_one(&A[k], p, dev, true);
+                } catch (const Error& e) {
+                    codes[t] = e.code;
+                    errs[t] = e.msg;
+                } catch (const std::exception& e) {
+                    codes[t] = BCMGX_ERR_INTERNAL;
+                    errs[t] = e.what();
+                }
+            });
         }
-        // keep freed blocks in the pool: repeated set-ups reuse them without cudaMalloc
-        cudaMemPool_t pool;
-        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-            uint64_t thr = UINT64_MAX;
-            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-        }
-        BCMGX_CUDA(cudaEventCreate(&H->ev0));
-        BCMGX_CUDA(cudaEventCreate(&H->ev1));
-        cudaEvent_t e0, e1;
-        BCMGX_CUDA(cudaEventCreate(&e0));
-        BCMGX_CUDA(cudaEventCreate(&e1));
-        BCMGX_CUDA(cudaEventRecord(e0, H->stream));
-        build_hierarchy(H.get(), A);
-        const char* force = std::getenv("BCMGX_TPR");
-        const int L = (int)H->lv.size();
-        for (int l = 0; l < L; l++) {
-            Level& V = H->lv[l];
-            const bool f32 = p->vcycle_precision == BCMGX_VCYCLE_FP32 && l < L - 1;
-            if (force) V.A.tpr = std::atoi(force);
-            else if (p->autotune) V.A.tpr = autotune_tpr(V, f32, H->stream);
-            else V.A.tpr = default_tpr(V.A.n, V.A.nnz);
-        }
-        BCMGX_CUDA(cudaEventRecord(e1, H->stream));
-        BCMGX_CUDA(cudaEventSynchronize(e1));
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        H->setup_ms = ms;
-        *out = H.release();
+        for (auto& th : pool) th.join();
+        for (int t = 0; t < T; t++)
+            if (codes[t] != BCMGX_OK) throw Error(codes[t], "batch set-up: " + errs[t]);
+        finish_batch(B.get(), p);
+        *out = B.release();
+    });
+}
+
+int bcmgx_batch_from_hierarchies(int nsys, bcmgx_hierarchy* const* hs, bcmgx_batch** out)
+{
+    return guarded([&] {
+        BCMGX_REQUIRE(nsys > 0 && hs && out, BCMGX_ERR_INVALID_INPUT, "bad argument");
+        *out = nullptr;
+        std::unique_ptr<bcmgx_batch> B(new bcmgx_batch());
+        B->hs.assign(hs, hs + nsys);
+        B->device = hs[0]->device;
+        for (auto* h : B->hs) BCMGX_REQUIRE(h && h->device == B->device, BCMGX_ERR_INVALID_INPUT, "hierarchies must share one device");
+        finish_batch(B.get(), &hs[0]->prm);
+        *out = B.release();
+    });
+}
+
+int bcmgx_batch_get_hierarchy(bcmgx_batch* B, int k, bcmgx_hierarchy** h)
+{
+    return guarded([&] {
+        BCMGX_REQUIRE(B && h && k >= 0 && k < (int)B->hs.size(), BCMGX_ERR_INVALID_INPUT, "bad argument");
+        *h = B->hs[k];
+    });
+}
+
+int bcmgx_batch_solve(bcmgx_batch* B, const double* const* b, double* const* x, bcmgx_solve_info* infos)
+{
+    int status = BCMGX_OK;
+    int rc = guarded([&] {
+        BCMGX_REQUIRE(B && b && x, BCMGX_ERR_INVALID_INPUT, "NULL argument");
+        DeviceScope ds(B->device);
+        if (!B->exec) batch_build(B);
+        status = batch_solve(B, b, x, infos);
+        if (status == BCMGX_ERR_NO_CONVERGENCE) set_last_error("batch solve: a system reached itnlim");
+        if (status == BCMGX_ERR_NOT_SPD) set_last_error("batch solve: FCG breakdown in a system");
+    });
+    return rc != BCMGX_OK ? rc : status;
+}
+
+int bcmgx_batch_free(bcmgx_batch* B)
+{
+    return guarded([&] {
+        if (!B) return;
+        DeviceScope ds(B->device);
+        delete B;
     });
 }
 
@@ -223,6 +355,44 @@ int bcmgx_solve(bcmgx_hierarchy* h, const double* b, double* x, int on_device, b
         }
         if (status == BCMGX_ERR_NO_CONVERGENCE) set_last_error("itnlim reached before the tolerance");
         if (status == BCMGX_ERR_NOT_SPD) set_last_error("FCG breakdown: non-positive or non-finite curvature");
+    });
+    return rc != BCMGX_OK ? rc : status;
+}
+
+int bcmgx_solve_adjoint(bcmgx_hierarchy* h, const double* g, const double* x, double* lambda, double* dA_val,
+    int on_device, bcmgx_solve_info* info)
+{
+    int status = BCMGX_OK;
+    int rc = guarded([&] {
+        BCMGX_REQUIRE(h && g && lambda, BCMGX_ERR_INVALID_INPUT, "NULL argument");
+        BCMGX_REQUIRE(!dA_val || x, BCMGX_ERR_INVALID_INPUT, "dA needs the forward solution x");
+        DeviceScope ds(h->device);
+        const DevCsr& A = h->lv[0].A;
+        const int n = A.n;
+        cudaStream_t s = h->stream;
+        if (on_device) {
+            BCMGX_CUDA(cudaMemsetAsync(lambda, 0, sizeof(double) * n, s));
+            status = fcg_solve(h, g, lambda, info);
+            if (dA_val) grad_pattern(A, lambda, x, dA_val, s);
+            BCMGX_CUDA(cudaStreamSynchronize(s));
+        } else {
+            DBuf<double> gd, ld, xd, dd;
+            gd.alloc(n, s);
+            ld.alloc(n, s);
+            BCMGX_CUDA(cudaMemcpyAsync(gd.p, g, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+            BCMGX_CUDA(cudaMemsetAsync(ld.p, 0, sizeof(double) * n, s));
+            status = fcg_solve(h, gd.p, ld.p, info);
+            BCMGX_CUDA(cudaMemcpyAsync(lambda, ld.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+            if (dA_val) {
+                xd.alloc(n, s);
+                dd.alloc(std::max<int64_t>(A.nnz, 1), s);
+                BCMGX_CUDA(cudaMemcpyAsync(xd.p, x, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+                grad_pattern(A, ld.p, xd.p, dd.p, s);
+                BCMGX_CUDA(cudaMemcpyAsync(dA_val, dd.p, sizeof(double) * A.nnz, cudaMemcpyDeviceToHost, s));
+            }
+            BCMGX_CUDA(cudaStreamSynchronize(s));
+        }
+        if (status == BCMGX_ERR_NO_CONVERGENCE) set_last_error("adjoint solve: itnlim reached before the tolerance");
     });
     return rc != BCMGX_OK ? rc : status;
 }

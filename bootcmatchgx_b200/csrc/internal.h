@@ -25,6 +25,8 @@ struct Error : std::exception {
 void set_last_error(const std::string& s);
 // counts every kernel launch of the library (reported by bcmgx_launch_count)
 void note_launch();
+void note_launches(long long k);
+long long launch_count();
 
 #define BCMGX_CUDA(call)                                                                       \
     do {                                                                                       \
@@ -152,9 +154,29 @@ struct bcmgx_hierarchy {
     bcmgx::FcgState* st_host = nullptr;   // pinned mirror
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int64_t ws_n = -1;
-    // captured FCG iteration (CUDA graph)
+    bcmgx::DBuf<double> hist;           // residual history, one entry per iteration
+    cudaEvent_t ev_it[2] = { nullptr, nullptr };
+    // captured solve (CUDA graph) and its own b / x buffers
     cudaGraphExec_t iter_graph = nullptr;
+    bcmgx::DBuf<double> gb, gx;
+    long long graph_startup_kernels = 0, graph_body_kernels = 0;
     ~bcmgx_hierarchy();
+};
+
+// A set of hierarchies whose solves run together as one CUDA graph launch.
+struct bcmgx_batch {
+    std::vector<bcmgx_hierarchy*> hs;
+    bool own = false;              // created by bcmgx_setup_batch: frees the hierarchies too
+    bool own_stream = false;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bcmgx::DBuf<unsigned char> copies, states_ptr;
+    bcmgx::DBuf<bcmgx::FcgState> states;
+    void* states_host = nullptr;
+    void* copies_host = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    ~bcmgx_batch();
 };
 
 namespace bcmgx {
@@ -177,6 +199,9 @@ void ensure_solve_workspace(bcmgx_hierarchy* H);
 int fcg_solve(bcmgx_hierarchy* H, const double* b_dev, double* x_dev, bcmgx_solve_info* info);
 void prec_apply_dev(bcmgx_hierarchy* H, const double* r, double* v);
 void time_level_kernels(bcmgx_hierarchy* H, int l, int reps, double* out);
+void grad_pattern(const DevCsr& A, const double* lam, const double* x, double* dA, cudaStream_t s);
+void batch_build(bcmgx_batch* B);
+int batch_solve(bcmgx_batch* B, const double* const* b, double* const* x, bcmgx_solve_info* infos);
 
 // ---- kernels usable on raw device memory (kernels.cu) ----
 int autotune_tpr(Level& V, bool f32, cudaStream_t s);

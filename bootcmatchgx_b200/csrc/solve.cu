@@ -99,6 +99,13 @@ __global__ void k_first_sweep(int n, const FT* __restrict__ f, const MT* __restr
     }
 }
 
+template <typename T>
+__global__ void k_zero(int n, T* __restrict__ a, const int* __restrict__ skip)
+{
+    if (skip && *skip) return;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) a[i] = T(0);
+}
+
 template <typename ST, typename DT>
 __global__ void k_convert(int n, const ST* __restrict__ a, DT* __restrict__ b, const int* __restrict__ skip)
 {
@@ -194,8 +201,10 @@ struct Cycle {
     void copy(Vec a, Vec b, int n) const
     {
         const int g = ew_grid(n);
-        if (a.f32 == b.f32) {
-            BCMGX_CUDA(cudaMemcpyAsync(b.p, a.p, (size_t)n * (a.f32 ? 4 : 8), cudaMemcpyDeviceToDevice, s));
+        if (a.f32 && b.f32) {
+            note_launch(); k_convert<float, float><<<g, 256, 0, s>>>(n, (const float*)a.p, (float*)b.p, skip);
+        } else if (!a.f32 && !b.f32) {
+            note_launch(); k_convert<double, double><<<g, 256, 0, s>>>(n, (const double*)a.p, (double*)b.p, skip);
         } else if (a.f32) {
             note_launch(); k_convert<float, double><<<g, 256, 0, s>>>(n, (const float*)a.p, (double*)b.p, skip);
         } else {
@@ -204,7 +213,13 @@ struct Cycle {
         BCMGX_CHECK_LAUNCH();
     }
 
-    void zero(Vec a, int n) const { BCMGX_CUDA(cudaMemsetAsync(a.p, 0, (size_t)n * (a.f32 ? 4 : 8), s)); }
+    void zero(Vec a, int n) const
+    {
+        note_launch();
+        if (a.f32) k_zero<float><<<ew_grid(n), 256, 0, s>>>(n, (float*)a.p, skip);
+        else k_zero<double><<<ew_grid(n), 256, 0, s>>>(n, (double*)a.p, skip);
+        BCMGX_CHECK_LAUNCH();
+    }
 
     // k sweeps from `src` (p == nullptr: zero iterate) ending in `dst`, using the level
     // buffers A and B as intermediates. fcopy: see first_sweep.
@@ -345,7 +360,9 @@ void prec_apply_impl(bcmgx_hierarchy* H, const double* r, double* v, const int* 
 {
     const int n0 = H->lv[0].A.n;
     if (H->prm.preconditioner != BCMGX_PREC_BCMG) {
-        BCMGX_CUDA(cudaMemcpyAsync(v, r, sizeof(double) * n0, cudaMemcpyDeviceToDevice, H->stream));
+        note_launch();
+        k_convert<double, double><<<ew_grid(n0), 256, 0, H->stream>>>(n0, r, v, skip);
+        BCMGX_CHECK_LAUNCH();
         return;
     }
     Cycle c { H, H->stream, skip, H->prm.vcycle_precision == BCMGX_VCYCLE_FP32, (int)H->lv.size() };
@@ -453,6 +470,7 @@ __global__ void __launch_bounds__(kRedThreads) k_fcg_update0(int n, const double
     double* __restrict__ x, double* __restrict__ r, double* __restrict__ d, double* __restrict__ q, FcgState* st, double* partials,
     double* hist)
 {
+    if (st->bad) return;
     const double th = st->theta;
     double acc[1] = { 0.0 };
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
@@ -478,6 +496,11 @@ __global__ void __launch_bounds__(kRedThreads) k_fcg_update(int n, double* __res
     double* partials, double* hist, const int* __restrict__ skip)
 {
     if (skip && *skip) return;
+    // a breakdown found by the dots kernel leaves x at the last valid iterate
+    if (st->bad) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) st->done = 1;
+        return;
+    }
     const double th = st->theta, th2 = st->theta2;
     double acc[1] = { 0.0 };
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
@@ -556,7 +579,7 @@ void ensure_solve_workspace(bcmgx_hierarchy* H)
     H->partials.alloc((size_t)num_sms() * kRedBlocksPerSM * 4, s);
     H->st.alloc(1, s);
     BCMGX_CUDA(cudaMemsetAsync(H->st.p, 0, sizeof(FcgState), s));
-    if (!H->st_host) BCMGX_CUDA(cudaMallocHost((void**)&H->st_host, sizeof(FcgState)));
+    if (!H->st_host) BCMGX_CUDA(cudaMallocHost((void**)&H->st_host, 2 * sizeof(FcgState)));
     const bool f32 = H->prm.vcycle_precision == BCMGX_VCYCLE_FP32;
     const int L = (int)H->lv.size();
     for (int l = 0; l < L; l++) {
@@ -732,50 +755,245 @@ int autotune_tpr(Level& V, bool f32, cudaStream_t s)
     return best;
 }
 
-// Flexible CG (FCG.cu:27-165) on device vectors b, x (x: x0 in, solution out).
-int fcg_solve(bcmgx_hierarchy* H, const double* b, double* x, bcmgx_solve_info* info)
+// Gradient of L with respect to the stored entries of A for x = A^{-1} b: with the adjoint
+// lambda = A^{-T} dL/dx = A^{-1} dL/dx (A symmetric), dL/da_ij = -lambda_i x_j on A's pattern.
+// One sub-warp per row; the entries of the row are written in place of their values.
+template <int S>
+__global__ void __launch_bounds__(256) k_grad_pattern(int n, const int* __restrict__ row, const int* __restrict__ col,
+    const double* __restrict__ lam, const double* __restrict__ x, double* __restrict__ dA)
 {
-    ensure_solve_workspace(H);
+    const int lane = threadIdx.x & (S - 1);
+    const long stride = (long)gridDim.x * blockDim.x / S;
+    for (long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) / S; r < n; r += stride) {
+        const double li = -lam[r];
+        for (int j = row[r] + lane; j < row[r + 1]; j += S) dA[j] = li * __ldg(x + __ldcs(col + j));
+    }
+}
+
+void grad_pattern(const DevCsr& A, const double* lam, const double* x, double* dA, cudaStream_t s)
+{
+    const int g = rowop_grid(A.n, 4);
+    note_launch();
+    k_grad_pattern<4><<<g, 256, 0, s>>>(A.n, A.row.p, A.col.p, lam, x, dA);
+    BCMGX_CHECK_LAUNCH();
+}
+
+// Initial FCG state (replaces a host copy so the start-up can be captured in a graph).
+__global__ void k_fcg_init(FcgState* st, double rtol, int itnlim)
+{
+    FcgState z {};
+    z.tol = rtol;
+    z.itnlim = itnlim;
+    *st = z;
+}
+
+__global__ void k_set_while(cudaGraphConditionalHandle h, const FcgState* st)
+{
+    cudaGraphSetConditional(h, st->done ? 0u : 1u);
+}
+
+// FCG start-up (FCG.cu:46-100): r = b - A x, delta0, v = B r, w = A v, alpha, beta, x += theta v,
+// r -= theta w, d = v, q = w.
+static void fcg_startup(bcmgx_hierarchy* H, const double* b, double* x, double* hist)
+{
     cudaStream_t s = H->stream;
     const DevCsr& A = H->lv[0].A;
     const int n = A.n;
-    const bcmgx_params& P = H->prm;
     FcgState* st = H->st.p;
     double* part = H->partials.p;
-    DBuf<double> hist;
-    hist.alloc((size_t)std::max(P.itnlim, 1) + 2, s);
-    FcgState init {};
-    init.tol = P.rtol;
-    init.itnlim = P.itnlim;
-    BCMGX_CUDA(cudaMemcpyAsync(st, &init, sizeof(FcgState), cudaMemcpyHostToDevice, s));
-    BCMGX_CUDA(cudaEventRecord(H->ev0, s));
     double *r = H->r.p, *v = H->v.p, *w = H->w.p, *d = H->d.p, *q = H->q.p;
+    note_launch();
+    k_fcg_init<<<1, 1, 0, s>>>(st, H->prm.rtol, H->prm.itnlim);
     fcg_resid0(A, x, b, r, st, part, s);
-    BCMGX_CUDA(cudaMemsetAsync(v, 0, sizeof(double) * n, s));
     prec_apply_impl(H, r, v, nullptr);
     fcg_dots<0>(A, v, w, r, nullptr, st, part, nullptr, s);
-    note_launch(); k_fcg_update0<<<red_grid(n), kRedThreads, 0, s>>>(n, v, w, x, r, d, q, st, part, hist.p);
+    note_launch(); k_fcg_update0<<<red_grid(n), kRedThreads, 0, s>>>(n, v, w, x, r, d, q, st, part, hist);
     BCMGX_CHECK_LAUNCH();
-    int iter = 0;
-    int done = 0;
-    while (!done) {
-        const bool even = (iter % 2) == 0;
-        double* pv = even ? v : d;
-        double* pw = even ? w : q;
-        const double* od = even ? d : v;
-        const double* oq = even ? q : w;
-        prec_apply_impl(H, r, pv, nullptr);
-        fcg_dots<1>(A, pv, pw, r, oq, st, part, nullptr, s);
-        note_launch(); k_fcg_update<<<red_grid(n), kRedThreads, 0, s>>>(n, pv, od, x, pw, oq, r, st, part, hist.p, nullptr);
-        BCMGX_CHECK_LAUNCH();
-        BCMGX_CUDA(cudaMemcpyAsync(H->st_host, st, sizeof(FcgState), cudaMemcpyDeviceToHost, s));
-        BCMGX_CUDA(cudaStreamSynchronize(s));
-        done = H->st_host->done;
-        iter = H->st_host->iter;
-        if (P.dispnorm) std::printf("%d) r norm: %.10lf\n", iter - 1, std::sqrt(H->st_host->rnorm2));
+}
+
+// One FCG iteration (FCG.cu:102-156); the roles of (v, w) and (d, q) alternate with the parity.
+// Every kernel returns at once when *skip is set (the solve has converged).
+static void fcg_iteration(bcmgx_hierarchy* H, bool even, double* x, double* hist, const int* skip)
+{
+    cudaStream_t s = H->stream;
+    const DevCsr& A = H->lv[0].A;
+    const int n = A.n;
+    FcgState* st = H->st.p;
+    double* part = H->partials.p;
+    double *r = H->r.p, *v = H->v.p, *w = H->w.p, *d = H->d.p, *q = H->q.p;
+    double* pv = even ? v : d;
+    double* pw = even ? w : q;
+    const double* od = even ? d : v;
+    const double* oq = even ? q : w;
+    prec_apply_impl(H, r, pv, skip);
+    fcg_dots<1>(A, pv, pw, r, oq, st, part, skip, s);
+    note_launch(); k_fcg_update<<<red_grid(n), kRedThreads, 0, s>>>(n, pv, od, x, pw, oq, r, st, part, hist, skip);
+    BCMGX_CHECK_LAUNCH();
+}
+
+// Adds the whole solve of hierarchy H to graph g as an independent branch: the start-up, then a
+// WHILE conditional node whose body is two iterations (the second skips itself once the first
+// converges) followed by a kernel that sets the loop condition from the device-side `done` flag.
+// The branch works on the hierarchy's own b / x buffers (gb, gx).
+static void add_solve_to_graph(bcmgx_hierarchy* H, cudaGraph_t g)
+{
+    cudaStream_t s = H->stream;
+    const int n = H->lv[0].A.n;
+    if (!H->gb.p) {
+        H->gb.alloc(n, s);
+        H->gx.alloc(n, s);
     }
-    BCMGX_CUDA(cudaEventRecord(H->ev1, s));
-    BCMGX_CUDA(cudaEventSynchronize(H->ev1));
+    if (!H->hist.p) H->hist.alloc((size_t)std::max(H->prm.itnlim, 1) + 2, s);
+    BCMGX_CUDA(cudaStreamSynchronize(s));
+    const long long c0 = launch_count();
+    BCMGX_CUDA(cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    fcg_startup(H, H->gb.p, H->gx.p, H->hist.p);
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    BCMGX_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, nullptr, &deps, &ndeps));
+    std::vector<cudaGraphNode_t> tail(deps, deps + ndeps);
+    cudaGraph_t gg = g;
+    BCMGX_CUDA(cudaStreamEndCapture(s, &gg));
+    const long long c1 = launch_count();
+    cudaGraphConditionalHandle h;
+    BCMGX_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wn;
+    BCMGX_CUDA(cudaGraphAddNode(&wn, g, tail.data(), tail.size(), &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    BCMGX_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    fcg_iteration(H, true, H->gx.p, H->hist.p, &H->st.p->done);
+    fcg_iteration(H, false, H->gx.p, H->hist.p, &H->st.p->done);
+    note_launch();
+    k_set_while<<<1, 1, 0, s>>>(h, H->st.p);
+    BCMGX_CHECK_LAUNCH();
+    BCMGX_CUDA(cudaStreamEndCapture(s, &body));
+    const long long c2 = launch_count();
+    H->graph_startup_kernels = c1 - c0;
+    H->graph_body_kernels = c2 - c1;
+    note_launches(-(c2 - c0));   // captured, not launched
+}
+
+static void build_solve_graph(bcmgx_hierarchy* H)
+{
+    cudaGraph_t g = nullptr;
+    BCMGX_CUDA(cudaGraphCreate(&g, 0));
+    add_solve_to_graph(H, g);
+    BCMGX_CUDA(cudaGraphInstantiate(&H->iter_graph, g, 0));
+    BCMGX_CUDA(cudaGraphDestroy(g));
+}
+
+// Kernels launched by one graph solve of H that ran `iters` iterations.
+static long long graph_launches(const bcmgx_hierarchy* H, int iters, int bad)
+{
+    const long long bodies = std::max(1LL, (long long)(iters + 1) / 2 + (bad ? 1 : 0));
+    return H->graph_startup_kernels + H->graph_body_kernels * bodies;
+}
+
+// ------------------------------------------------------------------------------------------
+// batched solves: many hierarchies in one graph launch
+// ------------------------------------------------------------------------------------------
+struct BatchCopy {
+    const double* src;
+    double* dst;
+    int n;
+};
+
+// One block per vector: dst = src for every (src, dst, n) of the list.
+__global__ void k_batch_copy(int m, const BatchCopy* __restrict__ list)
+{
+    for (int k = blockIdx.x; k < m; k += gridDim.x) {
+        const BatchCopy c = list[k];
+        for (int i = threadIdx.x; i < c.n; i += blockDim.x) c.dst[i] = c.src[i];
+    }
+}
+
+__global__ void k_batch_states(int m, FcgState* const* __restrict__ st, FcgState* __restrict__ out)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) out[k] = *st[k];
+}
+
+void batch_build(bcmgx_batch* B)
+{
+    cudaGraph_t g = nullptr;
+    BCMGX_CUDA(cudaGraphCreate(&g, 0));
+    for (bcmgx_hierarchy* H : B->hs) {
+        ensure_solve_workspace(H);
+        add_solve_to_graph(H, g);
+    }
+    BCMGX_CUDA(cudaGraphInstantiate(&B->exec, g, 0));
+    BCMGX_CUDA(cudaGraphDestroy(g));
+    const int m = (int)B->hs.size();
+    cudaStream_t s = B->stream;
+    B->copies.alloc(sizeof(BatchCopy) * 2 * (size_t)m, s);
+    B->states_ptr.alloc(sizeof(FcgState*) * (size_t)m, s);
+    B->states.alloc(m, s);
+    std::vector<FcgState*> sp(m);
+    for (int k = 0; k < m; k++) sp[k] = B->hs[k]->st.p;
+    BCMGX_CUDA(cudaMemcpyAsync(B->states_ptr.p, sp.data(), sizeof(FcgState*) * m, cudaMemcpyHostToDevice, s));
+    BCMGX_CUDA(cudaMallocHost((void**)&B->states_host, sizeof(FcgState) * m));
+    BCMGX_CUDA(cudaMallocHost((void**)&B->copies_host, sizeof(BatchCopy) * 2 * m));
+    BCMGX_CUDA(cudaStreamSynchronize(s));
+}
+
+// b[k], x[k]: device vectors of system k; x holds x0 on entry and the solution on return.
+int batch_solve(bcmgx_batch* B, const double* const* b, double* const* x, bcmgx_solve_info* infos)
+{
+    const int m = (int)B->hs.size();
+    cudaStream_t s = B->stream;
+    // every system's stream must have finished its own work before the batch graph runs on B's stream
+    for (bcmgx_hierarchy* H : B->hs) BCMGX_CUDA(cudaStreamSynchronize(H->stream));
+    BatchCopy* in = (BatchCopy*)B->copies_host;
+    for (int k = 0; k < m; k++) {
+        in[2 * k] = BatchCopy { b[k], B->hs[k]->gb.p, B->hs[k]->lv[0].A.n };
+        in[2 * k + 1] = BatchCopy { x[k], B->hs[k]->gx.p, B->hs[k]->lv[0].A.n };
+    }
+    BCMGX_CUDA(cudaMemcpyAsync(B->copies.p, in, sizeof(BatchCopy) * 2 * m, cudaMemcpyHostToDevice, s));
+    note_launch();
+    k_batch_copy<<<std::min(2 * m, 65535), 256, 0, s>>>(2 * m, (const BatchCopy*)B->copies.p);
+    BCMGX_CHECK_LAUNCH();
+    BCMGX_CUDA(cudaEventRecord(B->ev0, s));
+    BCMGX_CUDA(cudaGraphLaunch(B->exec, s));
+    BCMGX_CUDA(cudaEventRecord(B->ev1, s));
+    BCMGX_CUDA(cudaStreamSynchronize(s));
+    for (int k = 0; k < m; k++) in[k] = BatchCopy { B->hs[k]->gx.p, x[k], B->hs[k]->lv[0].A.n };
+    BCMGX_CUDA(cudaMemcpyAsync(B->copies.p, in, sizeof(BatchCopy) * m, cudaMemcpyHostToDevice, s));
+    note_launch();
+    k_batch_copy<<<std::min(m, 65535), 256, 0, s>>>(m, (const BatchCopy*)B->copies.p);
+    note_launch();
+    k_batch_states<<<ceil_div(m, 128), 128, 0, s>>>(m, (FcgState* const*)B->states_ptr.p, B->states.p);
+    BCMGX_CHECK_LAUNCH();
+    BCMGX_CUDA(cudaMemcpyAsync(B->states_host, B->states.p, sizeof(FcgState) * m, cudaMemcpyDeviceToHost, s));
+    BCMGX_CUDA(cudaStreamSynchronize(s));
+    float ms = 0;
+    BCMGX_CUDA(cudaEventElapsedTime(&ms, B->ev0, B->ev1));
+    const FcgState* S = (const FcgState*)B->states_host;
+    int status = BCMGX_OK;
+    for (int k = 0; k < m; k++) {
+        const bcmgx_params& P = B->hs[k]->prm;
+        note_launches(graph_launches(B->hs[k], S[k].iter, S[k].bad));
+        if (infos) {
+            infos[k].niter = S[k].iter + 1;
+            infos[k].retv = S[k].iter >= P.itnlim ? -1 : 0;
+            infos[k].delta0 = S[k].delta0;
+            infos[k].exit_res = std::sqrt(S[k].rnorm2);
+            infos[k].solve_ms = ms;
+            infos[k].full_n = B->hs[k]->lv[0].A.n;
+        }
+        if (S[k].bad) status = BCMGX_ERR_NOT_SPD;
+        else if (S[k].iter >= P.itnlim && status == BCMGX_OK) status = BCMGX_ERR_NO_CONVERGENCE;
+    }
+    return status;
+}
+
+static int finish_solve(bcmgx_hierarchy* H, bcmgx_solve_info* info, int n)
+{
+    const bcmgx_params& P = H->prm;
     float ms = 0;
     BCMGX_CUDA(cudaEventElapsedTime(&ms, H->ev0, H->ev1));
     const FcgState& S = *H->st_host;
@@ -789,6 +1007,55 @@ int fcg_solve(bcmgx_hierarchy* H, const double* b, double* x, bcmgx_solve_info* 
     }
     if (S.bad) return BCMGX_ERR_NOT_SPD;
     return S.iter >= P.itnlim ? BCMGX_ERR_NO_CONVERGENCE : BCMGX_OK;
+}
+
+// Flexible CG (FCG.cu:27-165) on device vectors b, x (x: x0 in, solution out).
+// Stream path: iterations are enqueued one ahead of the convergence test (the extra iteration skips
+// itself on the device once `done` is set), so the GPU never waits for the host between
+// iterations. Graph path (use_graph, not with dispnorm): one launch of the captured solve.
+int fcg_solve(bcmgx_hierarchy* H, const double* b, double* x, bcmgx_solve_info* info)
+{
+    ensure_solve_workspace(H);
+    cudaStream_t s = H->stream;
+    const int n = H->lv[0].A.n;
+    const bcmgx_params& P = H->prm;
+    if (P.use_graph == 1 && !P.dispnorm) {
+        if (!H->iter_graph) build_solve_graph(H);
+        BCMGX_CUDA(cudaMemcpyAsync(H->gb.p, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        BCMGX_CUDA(cudaMemcpyAsync(H->gx.p, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        BCMGX_CUDA(cudaEventRecord(H->ev0, s));
+        BCMGX_CUDA(cudaGraphLaunch(H->iter_graph, s));
+        BCMGX_CUDA(cudaEventRecord(H->ev1, s));
+        BCMGX_CUDA(cudaMemcpyAsync(x, H->gx.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        BCMGX_CUDA(cudaMemcpyAsync(H->st_host, H->st.p, sizeof(FcgState), cudaMemcpyDeviceToHost, s));
+        BCMGX_CUDA(cudaStreamSynchronize(s));
+        note_launches(graph_launches(H, H->st_host->iter, H->st_host->bad));
+        return finish_solve(H, info, n);
+    }
+    if (!H->hist.p) H->hist.alloc((size_t)std::max(P.itnlim, 1) + 2, s);
+    BCMGX_CUDA(cudaEventRecord(H->ev0, s));
+    fcg_startup(H, b, x, H->hist.p);
+    FcgState* ring = H->st_host;   // two pinned slots
+    const int* done_flag = &H->st.p->done;
+    auto enqueue = [&](int k) {
+        fcg_iteration(H, (k % 2) == 0, x, H->hist.p, done_flag);
+        BCMGX_CUDA(cudaMemcpyAsync(ring + (k % 2), H->st.p, sizeof(FcgState), cudaMemcpyDeviceToHost, s));
+        BCMGX_CUDA(cudaEventRecord(H->ev_it[k % 2], s));
+    };
+    enqueue(0);
+    int k = 0;
+    for (;;) {
+        enqueue(k + 1);
+        BCMGX_CUDA(cudaEventSynchronize(H->ev_it[k % 2]));
+        const FcgState& S = ring[k % 2];
+        if (P.dispnorm && !S.bad) std::printf("%d) r norm: %.10lf\n", S.iter - 1, std::sqrt(S.rnorm2));
+        if (S.done) break;
+        k++;
+    }
+    BCMGX_CUDA(cudaEventRecord(H->ev1, s));
+    BCMGX_CUDA(cudaMemcpyAsync(H->st_host, H->st.p, sizeof(FcgState), cudaMemcpyDeviceToHost, s));
+    BCMGX_CUDA(cudaStreamSynchronize(s));
+    return finish_solve(H, info, n);
 }
 
 }  // namespace bcmgx

@@ -141,6 +141,12 @@ int bcmgx_setup(const bcmgx_csr* A, const bcmgx_params* p, bcmgx_hierarchy** out
  * (solve.cu:11-51, FCG.cu:192-215). Returns BCMGX_ERR_NO_CONVERGENCE when itnlim is hit; x and
  * info are still filled. */
 int bcmgx_solve(bcmgx_hierarchy* h, const double* b, double* x, int on_device, bcmgx_solve_info* info);
+/* Adjoint of x = A^{-1} b for a loss L(x): given g = dL/dx, solves A lambda = g with the same
+ * hierarchy and FCG settings (A is SPD, so A^T = A) and returns dL/db = lambda and, when dA_val is
+ * not NULL, dL/dA on A's sparsity pattern: dA_val[j] = -lambda_i x_{col[j]} for entry j of row i.
+ * x is the forward solution. No counterpart in the reference (an extension of solve). */
+int bcmgx_solve_adjoint(bcmgx_hierarchy* h, const double* g, const double* x, double* lambda, double* dA_val,
+    int on_device, bcmgx_solve_info* info);
 /* Releases everything the hierarchy owns. Replaces prec_finalize (prec_finalize.cu:8-31). */
 int bcmgx_free(bcmgx_hierarchy* h);
 
@@ -162,6 +168,19 @@ int bcmgx_prec_apply(bcmgx_hierarchy* h, const double* r, double* v, int on_devi
  * precision, out[1] the residual, out[2] the FP64 SpMV, out[3] the fused FCG SpMV + dots
  * (level 0 only). No counterpart in the reference: the measurement hook of the benchmarks. */
 int bcmgx_time_kernels(bcmgx_hierarchy* h, int level, int reps, double* out_ms);
+
+/* ---- batched solves (no counterpart in the reference) ------------------------------------ */
+/* Many independent systems solved together: their set-ups run concurrently (nthreads host
+ * threads, one stream each; 0 = 8), and all their FCG solves run as ONE CUDA graph launch with one
+ * device-driven loop per system. A holds nsys CSR descriptions. */
+typedef struct bcmgx_batch bcmgx_batch;
+int bcmgx_setup_batch(int nsys, const bcmgx_csr* A, const bcmgx_params* p, int nthreads, bcmgx_batch** out);
+/* A batch over hierarchies built by bcmgx_setup (the caller keeps ownership of them). */
+int bcmgx_batch_from_hierarchies(int nsys, bcmgx_hierarchy* const* hs, bcmgx_batch** out);
+int bcmgx_batch_get_hierarchy(bcmgx_batch* B, int k, bcmgx_hierarchy** h);
+/* b[k], x[k]: device vectors of system k (x: x0 in, solution out). infos: nsys entries or NULL. */
+int bcmgx_batch_solve(bcmgx_batch* B, const double* const* b, double* const* x, bcmgx_solve_info* infos);
+int bcmgx_batch_free(bcmgx_batch* B);
 
 /* ---- kernels on caller-owned device memory ------------------------------------------------ */
 /* y = alpha * A x + beta * y on device pointers (driverSpMV, driverSpMV.cu:219-235; kernel

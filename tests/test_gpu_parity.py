@@ -286,3 +286,22 @@ def test_cli_matches_golden(golden, cuda, tmp_path):
     assert np.linalg.norm(x - g) / np.linalg.norm(g) < 1e-5
     text = info.read_text()
     assert "Total iterations" in text and "Number of levels" in text and "TOTAL SOLVE TIME" in text
+
+
+@pytest.mark.parametrize("case", [("lap27", (20, 20, 20)), ("diff", (18, 3)), ("lap7", (3, 3, 3))])
+@pytest.mark.parametrize("prec", ["FP64", "FP32"])
+def test_graph_and_stream_drivers_agree(bx, cuda, case, prec):
+    """The graph-captured solve (WHILE conditional node) and the stream solve (one-iteration
+    lookahead) run the same kernels: identical iterations and identical solutions. A second solve
+    on the same hierarchy relaunches the captured graph."""
+    A = as_csr(bx, case)
+    b = A @ np.random.default_rng(4).uniform(-1, 1, A.shape[0])
+    out = {}
+    for g in (0, 1):
+        h = bx.prec_setup(A.indptr, A.indices, A.data, fcg(bx, rtol=1e-9, use_graph=g, vcycle_precision=prec))
+        x1, i1 = h.solve(b)
+        x2, i2 = h.solve(2.0 * b)
+        assert i1["status"] == 0 and i2["status"] == 0
+        out[g] = (x1, i1["niter"], x2, i2["niter"])
+    assert out[0][1] == out[1][1] and out[0][3] == out[1][3]
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][2], out[1][2])

@@ -170,3 +170,24 @@ def test_cli_usage_and_errors(tmp_path):
     assert r.returncode != 0 and "Error opening setting file" in r.stderr
     r = subprocess.run([CLI, "-l", "x.cfg", "-g", "9p", "-s", "a.properties"], capture_output=True, text=True)
     assert r.returncode != 0 and "Usage" in r.stdout
+
+
+def test_diffusion_assembler_matches_generator(bx):
+    import torch
+    from bootcmatchgx_b200 import problems
+    theta = problems.gaussian_random_field((7, 6, 5), length=2.0, sigma=1.5, seed=3)
+    kappa = np.exp(theta)
+    row, col, val = bx.diffusion_7p(7, 6, 5, kappa)
+    asm = problems.DiffusionAssembler(7, 6, 5, torch.device("cpu"))
+    v = asm.values(torch.from_numpy(kappa.reshape(-1))).numpy()
+    assert np.array_equal(asm.row.numpy(), row) and np.array_equal(asm.col.numpy(), col)
+    assert np.max(np.abs(v - val)) <= 1e-14 * np.max(np.abs(val))
+
+
+def test_gaussian_random_field_statistics():
+    from bootcmatchgx_b200 import problems
+    f = problems.gaussian_random_field((48, 48, 48), length=4.0, sigma=2.0, seed=2)
+    assert abs(f.std() - 2.0) < 0.3 and abs(f.mean()) < 0.5
+    # correlation at lag 4 along x ~ exp(-16/32) for the squared-exponential kernel
+    c = np.mean(f * np.roll(f, 4, axis=0)) / np.mean(f * f)
+    assert abs(c - np.exp(-0.5)) < 0.1

@@ -506,6 +506,123 @@ def run_batch(a):
                        "vcycle": "fp32", "rtol": 1e-8, "setup_threads": min(16, os.cpu_count() or 1)}}
 
 
+def run_multi(a):
+    """The 27-point 100^3 Poisson matrix with 32 right-hand sides (uniform[-1,1], numpy
+    default_rng(6)) solved to 1e-8 in one block solve (CSR SpMM throughout, FP32 V-cycle) vs a
+    sequential loop of 32 single solves on the same hierarchy; also the block FP64-cycle solve
+    and the SpMM kernel alone (CUDA events, HBM GB/s of its algorithmic bytes)."""
+    import scipy.sparse as sp
+    import torch
+    import bootcmatchgx_b200 as bx
+    dev = torch.device("cuda", 0)
+    k = 32
+    row, col, val = bx.laplacian_3d(27, 100, 100, 100)
+    n, nnz = row.size - 1, col.size
+    B = np.random.default_rng(6).uniform(-1.0, 1.0, (n, k))
+    d = [torch.from_numpy(x_).to(dev) for x_ in (row, col, val)]
+    Bd = torch.from_numpy(B).to(dev)
+    X = torch.zeros_like(Bd)
+    out = {}
+    for prec in ("FP32", "FP64"):
+        p = bx.params_default(solver="FCG", preconditioner="BCMG", rtol=1e-8, dispnorm=0, vcycle_precision=prec)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        h = bx.Hierarchy(d[0], d[1], d[2], p)
+        torch.cuda.synchronize()
+        t_setup = time.perf_counter() - t0
+        for _ in range(max(1, a.warmup)):
+            X.zero_()
+            h.solve_multi(Bd, X)
+        ts = []
+        for _ in range(a.steps):
+            X.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            _, infos = h.solve_multi(Bd, X)
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        t_block = float(np.median(ts))
+        Xh = X.cpu().numpy()
+        A = sp.csr_matrix((val, col, row), shape=(n, n))
+        rel = np.linalg.norm(B - A @ Xh, axis=0) / np.linalg.norm(B, axis=0)
+        res = {"block_ms": t_block * 1e3, "solves_per_s": k / t_block, "setup_ms": t_setup * 1e3,
+               "iters_min_max": [min(i["niter"] for i in infos), max(i["niter"] for i in infos)],
+               "max_rel_residual": float(rel.max())}
+        if prec == "FP32":
+            xs = [torch.zeros(n, dtype=torch.float64, device=dev) for _ in range(k)]
+            cols = [Bd[:, j].contiguous() for j in range(k)]
+            h.solve(cols[0], xs[0])   # builds the single-solve graph
+            ts = []
+            for _ in range(max(1, a.steps // 2)):
+                for x_ in xs:
+                    x_.zero_()
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                for j in range(k):
+                    h.solve(cols[j], xs[j])
+                torch.cuda.synchronize()
+                ts.append(time.perf_counter() - t0)
+            t_seq = float(np.median(ts))
+            res["sequential_ms"] = t_seq * 1e3
+            res["sequential_solves_per_s"] = k / t_seq
+            res["speedup_vs_sequential"] = t_seq / t_block
+            res["max_rel_diff_vs_single"] = max(float(torch.linalg.norm(X[:, j] - xs[j]) / torch.linalg.norm(xs[j]))
+                                                for j in range(k))
+        h.free()
+        out[prec] = res
+    # the SpMM kernel alone: Y = A X for the 32-column block
+    Y = torch.empty_like(Bd)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(3):
+        bx.spmm(d[0], d[1], d[2], Bd, Y)
+    reps = 20
+    e0.record()
+    for _ in range(reps):
+        bx.spmm(d[0], d[1], d[2], Bd, Y)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    alg = nnz * 12 + (n + 1) * 4 + 2 * n * k * 8
+    peak, peak_kind = read_peaks()
+    f32 = out["FP32"]
+    return {"metric": "multi-RHS solves/s (27-point 100^3, 32 right-hand sides, one block solve)",
+            "value": f32["solves_per_s"], "unit": "solves/s", "higher_is_better": True, "workload": "poisson27_100_x32",
+            "fp32": f32, "fp64": out["FP64"],
+            "spmm": {"ms": ms, "algorithmic_bytes": alg, "gbs": alg / ms / 1e6, "peak_gbs": peak,
+                     "frac": alg / ms / 1e6 / peak, "peak_kind": peak_kind},
+            "steps": a.steps, "warmup": a.warmup,
+            "config": {"rows": n, "nnz": nnz, "rhs": k, "rhs_dist": "uniform[-1,1] (numpy default_rng(6))",
+                       "rtol": 1e-8, "x0": 0}}
+
+
+def profile_multi_step(a):
+    """W warm-up block solves, then exactly one (27-point 100^3, 32 right-hand sides, FP32 V-cycle,
+    stream-driven so that every kernel is a separate launch); prints the launch counts."""
+    import torch
+    import bootcmatchgx_b200 as bx
+    dev = torch.device("cuda", 0)
+    row, col, val = bx.laplacian_3d(27, 100, 100, 100)
+    d = [torch.from_numpy(x_).to(dev) for x_ in (row, col, val)]
+    Bd = torch.from_numpy(np.random.default_rng(6).uniform(-1.0, 1.0, (row.size - 1, 32))).to(dev)
+    X = torch.zeros_like(Bd)
+    p = bx.params_default(solver="FCG", preconditioner="BCMG", rtol=1e-8, dispnorm=0, vcycle_precision="FP32",
+                          use_graph=0)
+    h = bx.Hierarchy(d[0], d[1], d[2], p)
+    L = bx.lib()
+    c0 = L.bcmgx_launch_count()
+    for _ in range(a.warmup):
+        X.zero_()
+        h.solve_multi(Bd, X)
+    c1 = L.bcmgx_launch_count()
+    X.zero_()
+    _, infos = h.solve_multi(Bd, X)
+    torch.cuda.synchronize()
+    c2 = L.bcmgx_launch_count()
+    h.free()
+    print(json.dumps({"warmup_launches": c1 - c0, "step_launches": c2 - c1,
+                      "niter_max": max(i["niter"] for i in infos)}), flush=True)
+
+
 def profile_step(a, wl):
     """W warm-up steps, then exactly one set-up + solve (FP32 V-cycle) on device-resident data;
     prints how many library kernels the warm-up and the step launched."""
@@ -543,6 +660,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--adjoint", action="store_true", help="run the differentiated-solve configuration instead")
     ap.add_argument("--batch", action="store_true", help="run the batched-systems configuration instead")
+    ap.add_argument("--multi", action="store_true", help="run the 32-right-hand-side configuration instead")
     ap.add_argument("--profile-step", action="store_true",
                     help="only W warm-up steps and one FP32 step (for ncu launch lists); prints the launch counts")
     a = ap.parse_args()
@@ -551,13 +669,19 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     wl = WORKLOADS[a.workload]
     if a.profile_step:
-        profile_step(a, wl)
+        if a.multi:
+            profile_multi_step(a)
+        else:
+            profile_step(a, wl)
         return
     if a.adjoint:
         print(json.dumps(run_adjoint(a)), flush=True)
         return
     if a.batch:
         print(json.dumps(run_batch(a)), flush=True)
+        return
+    if a.multi:
+        print(json.dumps(run_multi(a)), flush=True)
         return
     if a.impl == "reference":
         line = reference_arm(a, wl, rank, world)

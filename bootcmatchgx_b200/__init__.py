@@ -5,12 +5,12 @@ from ._lib import BcmgxError, LIB_PATH, lib  # noqa: F401
 from .api import (  # noqa: F401
     Batch, Hierarchy, diffusion_7p, edge_weights, init_from_file, init_from_properties_file, laplacian,
     laplacian_3d, laplacian_3d_size, params_default, params_to_dict, prec_finalize, prec_setup,
-    read_laplacian_cfg, read_matrix_market, set_params, solve, spmv, suitor_matching,
+    read_laplacian_cfg, read_matrix_market, set_params, solve, spmm, spmv, suitor_matching,
 )
 
 __all__ = [
     "Batch", "BcmgxError", "Hierarchy", "diffusion_7p", "edge_weights", "init_from_file",
     "init_from_properties_file", "laplacian", "laplacian_3d", "laplacian_3d_size", "lib",
     "params_default", "params_to_dict", "prec_finalize", "prec_setup", "read_laplacian_cfg",
-    "read_matrix_market", "set_params", "solve", "spmv", "suitor_matching",
+    "read_matrix_market", "set_params", "solve", "spmm", "spmv", "suitor_matching",
 ]

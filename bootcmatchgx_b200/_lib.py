@@ -75,6 +75,7 @@ SIGNATURES = {
     "bcmgx_params_dump": (C.c_int, [C.POINTER(Params), C.c_char_p]),
     "bcmgx_setup": (C.c_int, [C.POINTER(Csr), C.POINTER(Params), C.POINTER(C.c_void_p)]),
     "bcmgx_solve": (C.c_int, [_vp, _vp, _vp, C.c_int, C.POINTER(SolveInfo)]),
+    "bcmgx_solve_multi": (C.c_int, [_vp, C.c_int, _vp, _vp, C.c_int, C.POINTER(SolveInfo)]),
     "bcmgx_solve_adjoint": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int, C.POINTER(SolveInfo)]),
     "bcmgx_free": (C.c_int, [_vp]),
     "bcmgx_setup_batch": (C.c_int, [C.c_int, _vp, C.POINTER(Params), C.c_int, C.POINTER(C.c_void_p)]),
@@ -90,6 +91,8 @@ SIGNATURES = {
     "bcmgx_time_kernels": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
     "bcmgx_spmv": (C.c_int, [C.c_int, C.c_int, C.c_int64, _vp, _vp, _vp, _vp, _vp, C.c_double,
                              C.c_double, C.c_int, _vp]),
+    "bcmgx_spmm": (C.c_int, [C.c_int, C.c_int, C.c_int64, _vp, _vp, _vp, C.c_int, _vp, _vp, C.c_double,
+                             C.c_double, _vp]),
     "bcmgx_edge_weights": (C.c_int, [C.c_int, C.c_int64, _vp, _vp, _vp, _vp, _vp, _dp, _vp]),
     "bcmgx_edge_weights_noalloc": (C.c_int, [C.c_int, C.c_int64, _vp, _vp, _vp, _vp, _vp, _dp, _vp]),
     "bcmgx_suitor_matching": (C.c_int, [C.c_int, C.c_int64, _vp, _vp, _vp, _vp, _vp]),

@@ -182,6 +182,28 @@ class Hierarchy:
                "exit_res": info.exit_res, "solve_ms": info.solve_ms, "status": rc}
         return x, out
 
+    def solve_multi(self, B, X0=None, raise_on_no_convergence=False):
+        """FCG solve of A X = B for up to 32 right-hand sides at once; B is n x k (row-major).
+
+        Host numpy in -> numpy out; a CUDA X0 is updated in place. Returns X and one info dict
+        per column."""
+        k = int(B.shape[1])
+        infos = (L.SolveInfo * k)()
+        if _is_device(B):
+            import torch
+            B = B.contiguous()
+            X = torch.zeros_like(B) if X0 is None else X0
+            rc = lib().bcmgx_solve_multi(self.h, k, _ptr(B), _ptr(X), 1, infos)
+        else:
+            B = np.ascontiguousarray(B, dtype=np.float64)
+            X = np.zeros_like(B) if X0 is None else np.array(X0, dtype=np.float64, order="C")
+            rc = lib().bcmgx_solve_multi(self.h, k, _ptr(B), _ptr(X), 0, infos)
+        if rc != L.OK and (rc != L.ERR_NO_CONVERGENCE or raise_on_no_convergence):
+            raise BcmgxError(rc, "solve_multi", L.last_error())
+        out = [{"retv": i.retv, "niter": i.niter, "delta0": i.delta0, "exit_res": i.exit_res,
+                "solve_ms": i.solve_ms, "status": rc} for i in infos]
+        return X, out
+
     def adjoint(self, g, x=None, want_dA=True):
         """lambda = A^{-1} g and dL/dA on A's pattern (-lambda_i x_j), for g = dL/dx."""
         info = L.SolveInfo()
@@ -370,6 +392,15 @@ def spmv(row, col, val, x, y, alpha=1.0, beta=0.0, threads_per_row=0, stream=Non
                            _ptr(x), _ptr(y), alpha, beta, threads_per_row, _stream_ptr(stream)),
           "bcmgx_spmv")
     return y
+
+
+def spmm(row, col, val, X, Y, alpha=1.0, beta=0.0, stream=None):
+    """Y = alpha A X + beta Y for row-major blocks X (m x k) and Y (n x k), k <= 32 (CUDA tensors)."""
+    n = int(row.shape[0]) - 1
+    check(lib().bcmgx_spmm(n, int(X.shape[0]), int(col.shape[0]), _ptr(row), _ptr(col), _ptr(val),
+                           int(X.shape[1]), _ptr(X), _ptr(Y), alpha, beta, _stream_ptr(stream)),
+          "bcmgx_spmm")
+    return Y
 
 
 def edge_weights(row, col, val, w, stream=None):

@@ -175,6 +175,8 @@ bcmgx_batch::~bcmgx_batch()
 bcmgx_hierarchy::~bcmgx_hierarchy()
 {
     if (iter_graph) cudaGraphExecDestroy(iter_graph);
+    bcmgx::free_multi(multi);
+    multi = nullptr;
     lv.clear();
     b.release();
     xv.release();
@@ -359,6 +361,34 @@ int bcmgx_solve(bcmgx_hierarchy* h, const double* b, double* x, int on_device, b
     return rc != BCMGX_OK ? rc : status;
 }
 
+int bcmgx_solve_multi(bcmgx_hierarchy* h, int nrhs, const double* B, double* X, int on_device, bcmgx_solve_info* infos)
+{
+    int status = BCMGX_OK;
+    int rc = guarded([&] {
+        BCMGX_REQUIRE(h && B && X, BCMGX_ERR_INVALID_INPUT, "NULL argument");
+        BCMGX_REQUIRE(nrhs >= 1 && nrhs <= 32, BCMGX_ERR_INVALID_INPUT, "nrhs must be 1..32");
+        BCMGX_REQUIRE(h->prm.solver == BCMGX_SOLVER_FCG, BCMGX_ERR_UNSUPPORTED, "multiple right-hand sides need FCG");
+        DeviceScope ds(h->device);
+        const size_t nk = (size_t)h->lv[0].A.n * nrhs;
+        cudaStream_t s = h->stream;
+        if (on_device) {
+            status = multi_solve(h, nrhs, B, X, infos);
+        } else {
+            DBuf<double> bd, xd;
+            bd.alloc(nk, s);
+            xd.alloc(nk, s);
+            BCMGX_CUDA(cudaMemcpyAsync(bd.p, B, sizeof(double) * nk, cudaMemcpyHostToDevice, s));
+            BCMGX_CUDA(cudaMemcpyAsync(xd.p, X, sizeof(double) * nk, cudaMemcpyHostToDevice, s));
+            status = multi_solve(h, nrhs, bd.p, xd.p, infos);
+            BCMGX_CUDA(cudaMemcpyAsync(X, xd.p, sizeof(double) * nk, cudaMemcpyDeviceToHost, s));
+            BCMGX_CUDA(cudaStreamSynchronize(s));
+        }
+        if (status == BCMGX_ERR_NO_CONVERGENCE) set_last_error("itnlim reached before the tolerance (some column)");
+        if (status == BCMGX_ERR_NOT_SPD) set_last_error("FCG breakdown in some column: non-positive or non-finite curvature");
+    });
+    return rc != BCMGX_OK ? rc : status;
+}
+
 int bcmgx_solve_adjoint(bcmgx_hierarchy* h, const double* g, const double* x, double* lambda, double* dA_val,
     int on_device, bcmgx_solve_info* info)
 {
@@ -517,6 +547,18 @@ int bcmgx_spmv(int n, int m, int64_t nnz, const int* row, const int* col, const 
             "threads_per_row must be a power of two <= 32");
         if (n > 0) validate_csr_dev(n, m, nnz, row, col, false, (cudaStream_t)stream);
         launch_spmv(n, row, col, val, x, y, alpha, beta, t, (cudaStream_t)stream);
+    });
+}
+
+int bcmgx_spmm(int n, int m, int64_t nnz, const int* row, const int* col, const double* val, int nrhs, const double* X,
+    double* Y, double alpha, double beta, void* stream)
+{
+    return guarded([&] {
+        BCMGX_REQUIRE(n >= 0 && m >= 0 && nnz >= 0, BCMGX_ERR_INVALID_INPUT, "negative size");
+        BCMGX_REQUIRE(nrhs >= 1 && nrhs <= 32, BCMGX_ERR_INVALID_INPUT, "nrhs must be 1..32");
+        BCMGX_REQUIRE(row && (nnz == 0 || (col && val)) && X && Y, BCMGX_ERR_INVALID_INPUT, "NULL argument");
+        if (n > 0) validate_csr_dev(n, m, nnz, row, col, false, (cudaStream_t)stream);
+        launch_spmm(n, nrhs, row, col, val, X, Y, alpha, beta, (cudaStream_t)stream);
     });
 }
 

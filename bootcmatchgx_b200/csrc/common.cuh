@@ -24,6 +24,9 @@ __device__ __forceinline__ void st_cg(int* p, int v) { __stcg(p, v); }
 template <typename T> struct Acc { using type = T; };
 template <> struct Acc<double> { using type = double; };
 template <> struct Acc<float> { using type = float; };
+// arithmetic type of an element-wise step that writes T: float only for float results
+template <typename T> struct Wider { using type = double; };
+template <> struct Wider<float> { using type = float; };
 
 template <int S, typename T>
 __device__ __forceinline__ T subwarp_sum(T v)

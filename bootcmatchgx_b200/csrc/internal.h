@@ -124,6 +124,28 @@ struct SweepRecord {
     std::vector<double> p, w;
 };
 
+// Typed view of a device vector (or block of vectors) used by the V-cycle.
+struct Vec {
+    void* p = nullptr;
+    bool f32 = false;
+    bool operator==(const Vec& o) const { return p == o.p; }
+    bool operator!=(const Vec& o) const { return p != o.p; }
+};
+
+// Work buffers of one V-cycle application: per level the right-hand side (on level 0 of the FP32
+// cycle: the FP32 copy of the incoming FP64 right-hand side), the two iterate buffers the
+// sweeps alternate between (level 0 of the FP64 cycle uses the output and x2 only), and the
+// level-0-sized residual. Block buffers hold K vectors row-major.
+struct CycleBufs {
+    struct L { Vec rhs, x, x2; };
+    std::vector<L> lv;
+    Vec res;
+};
+
+// Scratch of the multi-right-hand-side solve (multi.cu); opaque to the other units.
+struct MultiWork;
+void free_multi(MultiWork* w);
+
 // FCG scalars that live on the device between kernels.
 struct FcgState {
     double alpha, beta, gamma, delta;
@@ -160,6 +182,9 @@ struct bcmgx_hierarchy {
     cudaGraphExec_t iter_graph = nullptr;
     bcmgx::DBuf<double> gb, gx;
     long long graph_startup_kernels = 0, graph_body_kernels = 0;
+    bcmgx::CycleBufs cyc;                 // single-vector cycle buffers (views of lv[l] and res)
+    // multi-right-hand-side solve: its scratch and its captured graph (for multi_k columns)
+    bcmgx::MultiWork* multi = nullptr;
     ~bcmgx_hierarchy();
 };
 
@@ -198,6 +223,14 @@ void build_hierarchy(bcmgx_hierarchy* H, const bcmgx_csr* A);
 void ensure_solve_workspace(bcmgx_hierarchy* H);
 int fcg_solve(bcmgx_hierarchy* H, const double* b_dev, double* x_dev, bcmgx_solve_info* info);
 void prec_apply_dev(bcmgx_hierarchy* H, const double* r, double* v);
+void prec_apply_impl(bcmgx_hierarchy* H, const double* r, double* v, const int* skip);
+// One V-cycle on 2^lk right-hand sides (row-major n0 x 2^lk blocks) with block buffers `bufs`.
+void cycle_apply_block(bcmgx_hierarchy* H, const CycleBufs& bufs, int lk, const double* r, double* v, const int* skip);
+// Block FCG for K right-hand sides of one system (multi.cu); B, X row-major n x K, device.
+int multi_solve(bcmgx_hierarchy* H, int K, const double* B, double* X, bcmgx_solve_info* infos);
+// Y = alpha A X + beta Y for row-major n x K blocks on device memory (K <= 32).
+void launch_spmm(int n, int K, const int* row, const int* col, const double* val, const double* X, double* Y,
+    double alpha, double beta, cudaStream_t s);
 void time_level_kernels(bcmgx_hierarchy* H, int l, int reps, double* out);
 void grad_pattern(const DevCsr& A, const double* lam, const double* x, double* dA, cudaStream_t s);
 void batch_build(bcmgx_batch* B);

@@ -13,6 +13,7 @@
 // the coarsest level, the outer residual, the dots and the direction updates stay FP64.
 #include "internal.h"
 #include "rowops.cuh"
+#include "blockops.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -82,9 +83,6 @@ void launch_spmv(int n, const int* row, const int* col, const double* val, const
 // ------------------------------------------------------------------------------------------
 // element-wise kernels of the cycle
 // ------------------------------------------------------------------------------------------
-template <typename T> struct Wider { using type = double; };
-template <> struct Wider<float> { using type = float; };
-
 // Sweep from a zero iterate: u = f / M; optionally keeps a converted copy of f.
 template <typename FT, typename MT, typename YT, typename CT>
 __global__ void k_first_sweep(int n, const FT* __restrict__ f, const MT* __restrict__ M, YT* __restrict__ u,
@@ -141,39 +139,121 @@ __global__ void k_prolong(int n, const int* __restrict__ agg, const PT* __restri
 static int ew_grid(long n) { return (int)std::max<long>(1, std::min<long>((n + 255) / 256, (long)num_sms() * 8)); }
 
 // ------------------------------------------------------------------------------------------
-// typed vector views and the cycle
+// block launches (blockops.cuh)
 // ------------------------------------------------------------------------------------------
-struct Vec {
-    void* p = nullptr;
-    bool f32 = false;
-    bool operator==(const Vec& o) const { return p == o.p; }
-    bool operator!=(const Vec& o) const { return p != o.p; }
-};
+static int blk_rows_grid(long rows) { return (int)std::max<long>(1, std::min<long>((rows * 32 + 255) / 256, (long)num_sms() * 8)); }
 
+static int ceil_log2(int k)
+{
+    int lg = 0;
+    while ((1 << lg) < k) lg++;
+    return lg;
+}
+
+// Y = alpha A X + beta Y / F - A X / Jacobi sweep on blocks with leading dimension ld and K
+// columns; vector loads when X and ld allow them, else one column per lane.
+template <int OP, typename VT, typename XT, typename FT, typename MT, typename YT>
+static void launch_blk_rowop(int n, int ld, int K, const int* row, const int* col, const VT* val, const XT* x,
+    const FT* f, const MT* M, YT* y, double alpha, double beta, const int* skip, cudaStream_t s)
+{
+    if (n <= 0) return;
+    BlkShape sh = blk_shape(K, (int)sizeof(XT));
+    if (sh.W > 1 && (((uintptr_t)x % (sh.W * sizeof(XT))) != 0 || ld % sh.W != 0)) sh = BlkShape { 1, ceil_log2(K) };
+    const int g = blk_rows_grid(n);
+    note_launch();
+    if constexpr (sizeof(XT) == 4) {
+        if (sh.W == 4) {
+            k_blk_rowop<OP, 4><<<g, 256, 0, s>>>(n, sh.lpe_log2, ld, K, row, col, val, x, f, M, y, alpha, beta, skip);
+            BCMGX_CHECK_LAUNCH();
+            return;
+        }
+    }
+    if (sh.W == 2) k_blk_rowop<OP, 2><<<g, 256, 0, s>>>(n, sh.lpe_log2, ld, K, row, col, val, x, f, M, y, alpha, beta, skip);
+    else k_blk_rowop<OP, 1><<<g, 256, 0, s>>>(n, sh.lpe_log2, ld, K, row, col, val, x, f, M, y, alpha, beta, skip);
+    BCMGX_CHECK_LAUNCH();
+}
+
+// ------------------------------------------------------------------------------------------
+// the cycle: one code path for a single vector (lk < 0: the sub-warp row kernels above) and for
+// blocks of 2^lk right-hand sides (the block kernels of blockops.cuh)
+// ------------------------------------------------------------------------------------------
 struct Cycle {
     bcmgx_hierarchy* H;
+    const CycleBufs& B;
     cudaStream_t s;
     const int* skip;
     bool fp32;
     int L;
+    int lk;   // -1: single vector; else the block has 2^lk columns (leading dimension 2^lk)
 
     bool lf32(int l) const { return fp32 && l < L - 1; }
     Level& lv(int l) const { return H->lv[l]; }
+    int grid(int n) const { return ew_grid(lk < 0 ? (long)n : ((long)n << lk)); }
 
+    // ---- kernel dispatch (single vector or block) ----
+    template <int OP, typename VT, typename XT, typename FT, typename MT, typename YT>
+    void rowop(const DevCsr& A, const VT* val, const XT* x, const FT* f, const MT* M, YT* y) const
+    {
+        if (lk < 0) launch_rowop<OP>(A.tpr, A.n, A.row.p, A.col.p, val, x, f, M, y, 1.0, 0.0, skip, s);
+        else launch_blk_rowop<OP>(A.n, 1 << lk, 1 << lk, A.row.p, A.col.p, val, x, f, M, y, 1.0, 0.0, skip, s);
+    }
+    template <typename FT, typename MT, typename YT, typename CT>
+    void first(int n, const FT* f, const MT* M, YT* u, CT* fcopy) const
+    {
+        note_launch();
+        if (lk >= 0) k_blk_first_sweep<<<grid(n), 256, 0, s>>>(n, lk, f, M, u, fcopy, skip);
+        else k_first_sweep<<<grid(n), 256, 0, s>>>(n, f, M, u, fcopy, skip);
+        BCMGX_CHECK_LAUNCH();
+    }
+    template <typename ST, typename DT>
+    void convert(int n, const ST* a, DT* b) const
+    {
+        note_launch();
+        if (lk >= 0) k_blk_convert<<<grid(n), 256, 0, s>>>(n, lk, a, b, skip);
+        else k_convert<<<grid(n), 256, 0, s>>>(n, a, b, skip);
+        BCMGX_CHECK_LAUNCH();
+    }
+    template <typename T>
+    void zero_n(int n, T* a) const
+    {
+        note_launch();
+        if (lk >= 0) k_blk_zero<<<grid(n), 256, 0, s>>>(n, lk, a, skip);
+        else k_zero<<<grid(n), 256, 0, s>>>(n, a, skip);
+        BCMGX_CHECK_LAUNCH();
+    }
+    // out = P^T res: for a block, an SpMM with the stored transpose (rptr, ridx, rval)
+    template <typename RT, typename WT, typename OT>
+    void restrict_to(int nc, const Level& V, const WT* rval, const RT* res, OT* out) const
+    {
+        if (lk >= 0) {
+            launch_blk_rowop<OP_AXPBY>(nc, 1 << lk, 1 << lk, V.rptr.p, V.ridx.p, rval, res, (const OT*)nullptr,
+                (const OT*)nullptr, out, 1.0, 0.0, skip, s);
+            return;
+        }
+        note_launch();
+        k_restrict<<<grid(nc), 256, 0, s>>>(nc, V.rptr.p, V.ridx.p, rval, res, out, skip);
+        BCMGX_CHECK_LAUNCH();
+    }
+    template <typename PT, typename CT, typename XT, typename YT>
+    void prolong(int n, const Level& V, const PT* p, const CT* xc, const XT* x, YT* y) const
+    {
+        note_launch();
+        if (lk >= 0) k_blk_prolong<<<grid(n), 256, 0, s>>>(n, lk, V.agg.p, p, xc, x, y, skip);
+        else k_prolong<<<grid(n), 256, 0, s>>>(n, V.agg.p, p, xc, x, y, skip);
+        BCMGX_CHECK_LAUNCH();
+    }
+
+    // ---- cycle steps on typed views ----
     void sweep(int l, Vec f, Vec in, Vec out) const
     {
         Level& V = lv(l);
         const DevCsr& A = V.A;
-        if (!lf32(l)) {
-            launch_rowop<OP_JACOBI>(A.tpr, A.n, A.row.p, A.col.p, A.val.p, (const double*)in.p, (const double*)f.p,
-                V.M.p, (double*)out.p, 1.0, 0.0, skip, s);
-        } else if (out.f32) {
-            launch_rowop<OP_JACOBI>(A.tpr, A.n, A.row.p, A.col.p, A.val32.p, (const float*)in.p, (const float*)f.p,
-                V.M32.p, (float*)out.p, 1.0, 0.0, skip, s);
-        } else {
-            launch_rowop<OP_JACOBI>(A.tpr, A.n, A.row.p, A.col.p, A.val32.p, (const float*)in.p, (const float*)f.p,
-                V.M32.p, (double*)out.p, 1.0, 0.0, skip, s);
-        }
+        if (!lf32(l))
+            rowop<OP_JACOBI>(A, A.val.p, (const double*)in.p, (const double*)f.p, V.M.p, (double*)out.p);
+        else if (out.f32)
+            rowop<OP_JACOBI>(A, A.val32.p, (const float*)in.p, (const float*)f.p, V.M32.p, (float*)out.p);
+        else
+            rowop<OP_JACOBI>(A, A.val32.p, (const float*)in.p, (const float*)f.p, V.M32.p, (double*)out.p);
     }
 
     // sweep from zero; if fcopy is given (level 0 of the FP32 cycle) f is double and is also
@@ -181,49 +261,35 @@ struct Cycle {
     void first_sweep(int l, Vec f, Vec out, Vec fcopy) const
     {
         Level& V = lv(l);
-        const int n = V.A.n, g = ew_grid(n);
+        const int n = V.A.n;
         if (!lf32(l)) {
-            note_launch(); k_first_sweep<double, double, double, double><<<g, 256, 0, s>>>(n, (const double*)f.p, V.M.p, (double*)out.p, (double*)nullptr, skip);
+            first(n, (const double*)f.p, V.M.p, (double*)out.p, (double*)nullptr);
         } else if (f.f32) {
-            if (out.f32)
-                { note_launch(); k_first_sweep<float, float, float, float><<<g, 256, 0, s>>>(n, (const float*)f.p, V.M32.p, (float*)out.p, (float*)nullptr, skip); }
-            else
-                { note_launch(); k_first_sweep<float, float, double, float><<<g, 256, 0, s>>>(n, (const float*)f.p, V.M32.p, (double*)out.p, (float*)nullptr, skip); }
+            if (out.f32) first(n, (const float*)f.p, V.M32.p, (float*)out.p, (float*)nullptr);
+            else first(n, (const float*)f.p, V.M32.p, (double*)out.p, (float*)nullptr);
         } else {
-            if (out.f32)
-                { note_launch(); k_first_sweep<double, float, float, float><<<g, 256, 0, s>>>(n, (const double*)f.p, V.M32.p, (float*)out.p, (float*)fcopy.p, skip); }
-            else
-                { note_launch(); k_first_sweep<double, float, double, float><<<g, 256, 0, s>>>(n, (const double*)f.p, V.M32.p, (double*)out.p, (float*)fcopy.p, skip); }
+            if (out.f32) first(n, (const double*)f.p, V.M32.p, (float*)out.p, (float*)fcopy.p);
+            else first(n, (const double*)f.p, V.M32.p, (double*)out.p, (float*)fcopy.p);
         }
-        BCMGX_CHECK_LAUNCH();
     }
 
     void copy(Vec a, Vec b, int n) const
     {
-        const int g = ew_grid(n);
-        if (a.f32 && b.f32) {
-            note_launch(); k_convert<float, float><<<g, 256, 0, s>>>(n, (const float*)a.p, (float*)b.p, skip);
-        } else if (!a.f32 && !b.f32) {
-            note_launch(); k_convert<double, double><<<g, 256, 0, s>>>(n, (const double*)a.p, (double*)b.p, skip);
-        } else if (a.f32) {
-            note_launch(); k_convert<float, double><<<g, 256, 0, s>>>(n, (const float*)a.p, (double*)b.p, skip);
-        } else {
-            note_launch(); k_convert<double, float><<<g, 256, 0, s>>>(n, (const double*)a.p, (float*)b.p, skip);
-        }
-        BCMGX_CHECK_LAUNCH();
+        if (a.f32 && b.f32) convert(n, (const float*)a.p, (float*)b.p);
+        else if (!a.f32 && !b.f32) convert(n, (const double*)a.p, (double*)b.p);
+        else if (a.f32) convert(n, (const float*)a.p, (double*)b.p);
+        else convert(n, (const double*)a.p, (float*)b.p);
     }
 
     void zero(Vec a, int n) const
     {
-        note_launch();
-        if (a.f32) k_zero<float><<<ew_grid(n), 256, 0, s>>>(n, (float*)a.p, skip);
-        else k_zero<double><<<ew_grid(n), 256, 0, s>>>(n, (double*)a.p, skip);
-        BCMGX_CHECK_LAUNCH();
+        if (a.f32) zero_n(n, (float*)a.p);
+        else zero_n(n, (double*)a.p);
     }
 
     // k sweeps from `src` (p == nullptr: zero iterate) ending in `dst`, using the level
     // buffers A and B as intermediates. fcopy: see first_sweep.
-    void chain(int l, int k, Vec f, Vec src, Vec dst, Vec A, Vec B, Vec fcopy = Vec()) const
+    void chain(int l, int k, Vec f, Vec src, Vec dst, Vec A, Vec Bf, Vec fcopy = Vec()) const
     {
         const int n = lv(l).A.n;
         if (k <= 0) {
@@ -233,9 +299,9 @@ struct Cycle {
         }
         std::vector<Vec> out(k);
         out[k - 1] = dst;
-        for (int i = k - 2; i >= 0; i--) out[i] = (out[i + 1] == A) ? B : A;
+        for (int i = k - 2; i >= 0; i--) out[i] = (out[i + 1] == A) ? Bf : A;
         if (src.p != nullptr && src == out[0]) {
-            Vec other = (src == A) ? B : A;
+            Vec other = (src == A) ? Bf : A;
             copy(src, other, n);
             src = other;
         }
@@ -257,25 +323,15 @@ struct Cycle {
         Level& V = lv(l);
         const int n = V.A.n;
         const bool f32 = lf32(l);
-        Vec A, B;
-        if (l == 0 && !f32) {
-            A = dst;
-            B = Vec { V.x2.p, false };
-        } else if (f32) {
-            A = Vec { V.x32.p, true };
-            B = Vec { V.x232.p, true };
-        } else {
-            A = Vec { V.x.p, false };
-            B = Vec { V.x2.p, false };
-        }
+        const CycleBufs::L& Lb = B.lv[l];
+        const Vec A = (l == 0 && !f32) ? dst : Lb.x;
+        const Vec Bf = Lb.x2;
         const bcmgx_params& P = H->prm;
-        // level-0 FP32: f arrives in FP64 and is converted once into rhs32
+        // level-0 FP32: f arrives in FP64 and is converted once into the level's FP32 rhs
         Vec fcopy;
-        if (f32 && !f.f32) {
-            fcopy = Vec { V.rhs32.p, true };
-        }
+        if (f32 && !f.f32) fcopy = Lb.rhs;
         if (l == L - 1) {
-            chain(l, P.relaxnumber_coarse, f, x_cur, dst, A, B, fcopy);
+            chain(l, P.relaxnumber_coarse, f, x_cur, dst, A, Bf, fcopy);
             return;
         }
         const int coeff = P.cycle_type == BCMGX_CYCLE_VARIABLE_V ? (1 << l) : 1;
@@ -284,37 +340,32 @@ struct Cycle {
         Vec fl = f;
         if (fcopy.p) {
             if (x_cur.p == nullptr && kpre > 0) {
-                chain(l, kpre, f, x_cur, pre_dst, A, B, fcopy);
+                chain(l, kpre, f, x_cur, pre_dst, A, Bf, fcopy);
             } else {
                 copy(f, fcopy, n);
-                chain(l, kpre, fcopy, x_cur, pre_dst, A, B);
+                chain(l, kpre, fcopy, x_cur, pre_dst, A, Bf);
             }
             fl = fcopy;
         } else {
-            chain(l, kpre, f, x_cur, pre_dst, A, B);
+            chain(l, kpre, f, x_cur, pre_dst, A, Bf);
         }
         Vec xpre = pre_dst;
         // residual and restriction
         const DevCsr& Am = V.A;
         Level& C = lv(l + 1);
         const bool cf32 = lf32(l + 1);
+        const Vec fc = B.lv[l + 1].rhs;
+        const Vec xc_dst = B.lv[l + 1].x;
         if (f32) {
-            float* res = H->res32.p;
-            launch_rowop<OP_RESID>(Am.tpr, n, Am.row.p, Am.col.p, Am.val32.p, (const float*)xpre.p, (const float*)fl.p,
-                (const float*)nullptr, res, 1.0, 0.0, skip, s);
-            if (cf32)
-                { note_launch(); k_restrict<float, float, float><<<ew_grid(C.A.n), 256, 0, s>>>(C.A.n, V.rptr.p, V.ridx.p, V.rval32.p, res, C.rhs32.p, skip); }
-            else
-                { note_launch(); k_restrict<float, double, double><<<ew_grid(C.A.n), 256, 0, s>>>(C.A.n, V.rptr.p, V.ridx.p, V.rval.p, res, C.rhs.p, skip); }
+            float* res = (float*)B.res.p;
+            rowop<OP_RESID>(Am, Am.val32.p, (const float*)xpre.p, (const float*)fl.p, (const float*)nullptr, res);
+            if (cf32) restrict_to(C.A.n, V, V.rval32.p, (const float*)res, (float*)fc.p);
+            else restrict_to(C.A.n, V, V.rval.p, (const float*)res, (double*)fc.p);
         } else {
-            double* res = H->res.p;
-            launch_rowop<OP_RESID>(Am.tpr, n, Am.row.p, Am.col.p, Am.val.p, (const double*)xpre.p, (const double*)fl.p,
-                (const double*)nullptr, res, 1.0, 0.0, skip, s);
-            note_launch(); k_restrict<double, double, double><<<ew_grid(C.A.n), 256, 0, s>>>(C.A.n, V.rptr.p, V.ridx.p, V.rval.p, res, C.rhs.p, skip);
+            double* res = (double*)B.res.p;
+            rowop<OP_RESID>(Am, Am.val.p, (const double*)xpre.p, (const double*)fl.p, (const double*)nullptr, res);
+            restrict_to(C.A.n, V, V.rval.p, (const double*)res, (double*)fc.p);
         }
-        BCMGX_CHECK_LAUNCH();
-        Vec fc = cf32 ? Vec { C.rhs32.p, true } : Vec { C.rhs.p, false };
-        Vec xc_dst = cf32 ? Vec { C.x32.p, true } : Vec { C.x.p, false };
         Vec xc;   // nullptr: coarse correction is zero
         if (L > 2 || P.relaxnumber_coarse > 0) {
             int visits = l < (int)H->grid_sweeps.size() ? H->grid_sweeps[l] : 1;
@@ -330,29 +381,23 @@ struct Cycle {
             pdst = dst;
         } else {
             Vec o0 = dst;
-            for (int i = kpost - 2; i >= 0; i--) o0 = (o0 == A) ? B : A;
-            pdst = (o0 == A) ? B : A;
+            for (int i = kpost - 2; i >= 0; i--) o0 = (o0 == A) ? Bf : A;
+            pdst = (o0 == A) ? Bf : A;
         }
         if (xc.p != nullptr) {
-            const int g = ew_grid(n);
             if (!f32) {
-                note_launch(); k_prolong<double, double, double, double><<<g, 256, 0, s>>>(n, V.agg.p, V.p.p, (const double*)xc.p, (const double*)xpre.p, (double*)pdst.p, skip);
+                prolong(n, V, V.p.p, (const double*)xc.p, (const double*)xpre.p, (double*)pdst.p);
             } else if (xc.f32) {
-                if (pdst.f32)
-                    { note_launch(); k_prolong<float, float, float, float><<<g, 256, 0, s>>>(n, V.agg.p, V.p32.p, (const float*)xc.p, (const float*)xpre.p, (float*)pdst.p, skip); }
-                else
-                    { note_launch(); k_prolong<float, float, float, double><<<g, 256, 0, s>>>(n, V.agg.p, V.p32.p, (const float*)xc.p, (const float*)xpre.p, (double*)pdst.p, skip); }
+                if (pdst.f32) prolong(n, V, V.p32.p, (const float*)xc.p, (const float*)xpre.p, (float*)pdst.p);
+                else prolong(n, V, V.p32.p, (const float*)xc.p, (const float*)xpre.p, (double*)pdst.p);
             } else {
-                if (pdst.f32)
-                    { note_launch(); k_prolong<float, double, float, float><<<g, 256, 0, s>>>(n, V.agg.p, V.p32.p, (const double*)xc.p, (const float*)xpre.p, (float*)pdst.p, skip); }
-                else
-                    { note_launch(); k_prolong<float, double, float, double><<<g, 256, 0, s>>>(n, V.agg.p, V.p32.p, (const double*)xc.p, (const float*)xpre.p, (double*)pdst.p, skip); }
+                if (pdst.f32) prolong(n, V, V.p32.p, (const double*)xc.p, (const float*)xpre.p, (float*)pdst.p);
+                else prolong(n, V, V.p32.p, (const double*)xc.p, (const float*)xpre.p, (double*)pdst.p);
             }
-            BCMGX_CHECK_LAUNCH();
         } else if (pdst != xpre) {
             copy(xpre, pdst, n);
         }
-        chain(l, kpost, fl, pdst, dst, A, B);
+        chain(l, kpost, fl, pdst, dst, A, Bf);
     }
 };
 
@@ -365,8 +410,28 @@ void prec_apply_impl(bcmgx_hierarchy* H, const double* r, double* v, const int* 
         BCMGX_CHECK_LAUNCH();
         return;
     }
-    Cycle c { H, H->stream, skip, H->prm.vcycle_precision == BCMGX_VCYCLE_FP32, (int)H->lv.size() };
+    Cycle c { H, H->cyc, H->stream, skip, H->prm.vcycle_precision == BCMGX_VCYCLE_FP32, (int)H->lv.size(), -1 };
     c.run(0, Vec { (void*)r, false }, Vec(), Vec { v, false });
+}
+
+void cycle_apply_block(bcmgx_hierarchy* H, const CycleBufs& bufs, int lk, const double* r, double* v, const int* skip)
+{
+    const int n0 = H->lv[0].A.n;
+    if (H->prm.preconditioner != BCMGX_PREC_BCMG) {
+        note_launch();
+        k_blk_convert<double, double><<<ew_grid((long)n0 << lk), 256, 0, H->stream>>>(n0, lk, r, v, skip);
+        BCMGX_CHECK_LAUNCH();
+        return;
+    }
+    Cycle c { H, bufs, H->stream, skip, H->prm.vcycle_precision == BCMGX_VCYCLE_FP32, (int)H->lv.size(), lk };
+    c.run(0, Vec { (void*)r, false }, Vec(), Vec { v, false });
+}
+
+void launch_spmm(int n, int K, const int* row, const int* col, const double* val, const double* X, double* Y,
+    double alpha, double beta, cudaStream_t s)
+{
+    launch_blk_rowop<OP_AXPBY>(n, K, K, row, col, val, X, (const double*)nullptr, (const double*)nullptr, Y, alpha,
+        beta, nullptr, s);
 }
 
 void prec_apply_dev(bcmgx_hierarchy* H, const double* r, double* v)
@@ -598,6 +663,13 @@ void ensure_solve_workspace(bcmgx_hierarchy* H)
             V.x2.alloc(n, s);
         }
     }
+    H->cyc.lv.assign(L, CycleBufs::L());
+    for (int l = 0; l < L; l++) {
+        Level& V = H->lv[l];
+        if (f32 && l < L - 1) H->cyc.lv[l] = { Vec { V.rhs32.p, true }, Vec { V.x32.p, true }, Vec { V.x232.p, true } };
+        else H->cyc.lv[l] = { Vec { V.rhs.p, false }, Vec { V.x.p, false }, Vec { V.x2.p, false } };
+    }
+    H->cyc.res = f32 ? Vec { H->res32.p, true } : Vec { H->res.p, false };
     H->ws_n = n0;
 }
 

@@ -141,6 +141,13 @@ int bcmgx_setup(const bcmgx_csr* A, const bcmgx_params* p, bcmgx_hierarchy** out
  * (solve.cu:11-51, FCG.cu:192-215). Returns BCMGX_ERR_NO_CONVERGENCE when itnlim is hit; x and
  * info are still filled. */
 int bcmgx_solve(bcmgx_hierarchy* h, const double* b, double* x, int on_device, bcmgx_solve_info* info);
+/* Solves A X = B for nrhs <= 32 right-hand sides at once (B, X row-major n x nrhs: entry (i, k)
+ * at i*nrhs + k; X holds x0 on entry). Every sparse product is a CSR SpMM over the block, and
+ * every column runs the FCG recurrence with its own scalars and stopping test; infos has nrhs
+ * entries (or is NULL). No counterpart in the reference (its solve takes one vector,
+ * solve.cu:11-51); column k gives the result of bcmgx_solve on column k up to rounding. */
+int bcmgx_solve_multi(bcmgx_hierarchy* h, int nrhs, const double* B, double* X, int on_device,
+    bcmgx_solve_info* infos);
 /* Adjoint of x = A^{-1} b for a loss L(x): given g = dL/dx, solves A lambda = g with the same
  * hierarchy and FCG settings (A is SPD, so A^T = A) and returns dL/db = lambda and, when dA_val is
  * not NULL, dL/dA on A's sparsity pattern: dA_val[j] = -lambda_i x_{col[j]} for entry j of row i.
@@ -188,6 +195,11 @@ int bcmgx_batch_free(bcmgx_batch* B);
  * the autotuned choice. */
 int bcmgx_spmv(int n, int m, int64_t nnz, const int* row, const int* col, const double* val,
     const double* x, double* y, double alpha, double beta, int threads_per_row, void* stream);
+/* Y = alpha * A X + beta * Y for nrhs <= 32 vectors (X, Y row-major: m x nrhs and n x nrhs) on
+ * device pointers: one warp per row, lane k on column k, A read once for all columns. No
+ * counterpart in the reference (its SpMM, driverSpMM.cu:228, is a sparse x sparse product). */
+int bcmgx_spmm(int n, int m, int64_t nnz, const int* row, const int* col, const double* val, int nrhs,
+    const double* X, double* Y, double alpha, double beta, void* stream);
 /* Edge weights of one pairwise sweep on A's pattern (diagonal slots 0). Replaces makeAH +
  * toMaximumProductMatrix + _write_T_warp (matching.cu:137-288). Device pointers. */
 int bcmgx_edge_weights(int n, int64_t nnz, const int* row, const int* col, const double* val,

@@ -236,6 +236,14 @@ void grad_pattern(const DevCsr& A, const double* lam, const double* x, double* d
 void batch_build(bcmgx_batch* B);
 int batch_solve(bcmgx_batch* B, const double* const* b, double* const* x, bcmgx_solve_info* infos);
 
+// Grid for a grid-stride kernel: min(need_blocks, blocks of this kernel resident on the GPU).
+int fit_grid(const void* kernel, int threads, long need_blocks);
+template <typename... A>
+inline int fit_grid(void (*kernel)(A...), int threads, long need_blocks)
+{
+    return fit_grid((const void*)kernel, threads, need_blocks);
+}
+
 // ---- kernels usable on raw device memory (kernels.cu) ----
 int autotune_tpr(Level& V, bool f32, cudaStream_t s);
 int default_tpr(int n, int64_t nnz);

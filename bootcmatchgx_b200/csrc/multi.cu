@@ -34,32 +34,29 @@ struct BlockState {
     int ticket[4];
 };
 
-int blk_rows_grid(long rows)
-{
-    const long need = (rows * 32 + kBlkThreads - 1) / kBlkThreads;
-    return (int)std::max<long>(1, std::min<long>(need, (long)num_sms() * kBlkBlocksPerSM));
-}
-
-// Per-column sums of NV values per thread: a thread's values belong to column lane % kp (kp a
-// power of two <= 32; threads without a column hold zeros). Warps meet in shared memory, blocks
-// in `partials` (block-major), and the last block to arrive adds the partials in block order,
-// so the result does not depend on scheduling. Returns true in every thread of the last block;
+// Per-column sums: thread values v[q][w] belong to column (lane % lpe) * W + w (lpe * W <= 32,
+// a power of two; threads without a column hold zeros). Warps meet in shared memory, blocks in
+// `partials` (block-major), and the last block to arrive adds the partials in block order, so
+// the result does not depend on scheduling. Returns true in every thread of the last block;
 // out[] is valid in its warp 0, lane k holding column k. blockDim.x <= 256.
-template <int NV>
-__device__ __forceinline__ bool blk_colsum(const double (&v)[NV], int kp, double* partials, int* ticket, double (&out)[NV])
+template <int NV, int W>
+__device__ __forceinline__ bool blk_colsum(const double (&v)[NV][W], int lpe, double* partials, int* ticket, double (&out)[NV])
 {
-    __shared__ double sh[NV][8][32];
+    __shared__ double sh[NV][8][32][W];
     __shared__ bool last;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
-    for (int q = 0; q < NV; q++) sh[q][wid][lane] = v[q];
+    for (int q = 0; q < NV; q++)
+#pragma unroll
+        for (int w = 0; w < W; w++) sh[q][wid][lane][w] = v[q][w];
     __syncthreads();
     if (wid == 0) {
+        const int g = (lane / W) & (lpe - 1), w = lane % W;   // lanes of column `lane`: g, g + lpe, ...
 #pragma unroll
         for (int q = 0; q < NV; q++) {
             double t = 0.0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); w++)
-                for (int l = lane; l < 32; l += kp) t += sh[q][w][l];
+            for (int wi = 0; wi < (int)(blockDim.x >> 5); wi++)
+                for (int l = g; l < 32; l += lpe) t += sh[q][wi][l][w];
             partials[((size_t)blockIdx.x * NV + q) * 32 + lane] = t;
         }
         __threadfence();
@@ -105,20 +102,26 @@ __global__ void __launch_bounds__(kBlkThreads) k_blk_resid0(int n, int lpe_log2,
     const int* __restrict__ col, const double* __restrict__ val, const double* __restrict__ X, const double* __restrict__ B,
     double* __restrict__ R, BlockState* st, double* partials)
 {
-    const int lane = threadIdx.x & 31;
-    double acc[1] = { 0.0 };
-    BCMGX_BLOCK_ROWS(r, n)
+    const int lane = threadIdx.x & 31, slot = lane >> lpe_log2;
+    const int c0 = (lane & ((1 << lpe_log2) - 1)) * W;
+    double acc[1][W] = {};
+    BCMGX_BLOCK_ROWGROUPS(r0, n, 32 >> lpe_log2)
     {
-        const double s = blk_row<W, double>(__ldg(row + r), __ldg(row + r + 1), lane, lpe_log2, kp, kp, col, val, X);
-        if (lane < kp) {
-            const long o = r * kp + lane;
-            const double ri = -1.0 * s + 1.0 * B[o];
-            R[o] = ri;
-            acc[0] += ri * ri;
+        const long r = r0 + slot;
+        if (r >= n) continue;
+        double s[W], bb[W], rr[W];
+        blk_row<W>(__ldg(row + r), __ldg(row + r + 1), c0, kp, col, val, X, s);
+        const long o = r * kp + c0;
+        ldw<W>(B + o, bb);
+#pragma unroll
+        for (int w = 0; w < W; w++) {
+            rr[w] = -1.0 * s[w] + 1.0 * bb[w];
+            acc[0][w] += rr[w] * rr[w];
         }
+        stv<W>(R + o, rr);
     }
     double out[1];
-    if (blk_colsum<1>(acc, kp, partials, &st->ticket[0], out) && threadIdx.x < kp) {
+    if (blk_colsum<1, W>(acc, 1 << lpe_log2, partials, &st->ticket[0], out) && threadIdx.x < kp) {
         const double d0 = sqrt(out[0]);
         st->delta0[lane] = d0;
         st->tol[lane] = st->tol[lane] * d0;
@@ -135,22 +138,29 @@ __global__ void __launch_bounds__(kBlkThreads) k_blk_spmv_dots(int n, int lpe_lo
     const int* __restrict__ skip)
 {
     if (skip && *skip) return;
-    const int lane = threadIdx.x & 31;
-    double acc[3] = { 0.0, 0.0, 0.0 };
-    BCMGX_BLOCK_ROWS(r, n)
+    const int lane = threadIdx.x & 31, slot = lane >> lpe_log2;
+    const int c0 = (lane & ((1 << lpe_log2) - 1)) * W;
+    double acc[3][W] = {};
+    BCMGX_BLOCK_ROWGROUPS(r0, n, 32 >> lpe_log2)
     {
-        const double s = blk_row<W, double>(__ldg(row + r), __ldg(row + r + 1), lane, lpe_log2, kp, kp, col, val, PV);
-        if (lane < kp) {
-            const long o = r * kp + lane;
-            PW[o] = s;
-            const double vi = PV[o];
-            acc[0] += R[o] * vi;
-            acc[1] += s * vi;
-            if (MODE == 1) acc[2] += OQ[o] * vi;
+        const long r = r0 + slot;
+        if (r >= n) continue;
+        double s[W], vi[W], ri[W], qi[W];
+        blk_row<W>(__ldg(row + r), __ldg(row + r + 1), c0, kp, col, val, PV, s);
+        const long o = r * kp + c0;
+        stv<W>(PW + o, s);
+        ldw<W>(PV + o, vi);
+        ldw<W>(R + o, ri);
+        if (MODE == 1) ldw<W>(OQ + o, qi);
+#pragma unroll
+        for (int w = 0; w < W; w++) {
+            acc[0][w] += ri[w] * vi[w];
+            acc[1][w] += s[w] * vi[w];
+            if (MODE == 1) acc[2][w] += qi[w] * vi[w];
         }
     }
     double out[3];
-    if (blk_colsum<3>(acc, kp, partials, &st->ticket[1], out) && threadIdx.x < kp && !st->done[lane]) {
+    if (blk_colsum<3, W>(acc, 1 << lpe_log2, partials, &st->ticket[1], out) && threadIdx.x < kp && !st->done[lane]) {
         const int k = lane;
         st->alpha[k] = out[0];
         st->beta[k] = out[1];
@@ -179,7 +189,7 @@ __global__ void __launch_bounds__(kBlkThreads) k_blk_update0(int n, int lk, cons
     const int c = threadIdx.x & (kp - 1);
     const bool live = !st->done[c] && !st->bad[c];
     const double th = live ? st->theta[c] : 0.0;
-    double acc[1] = { 0.0 };
+    double acc[1][1] = { { 0.0 } };
     if (live) {
         BCMGX_BLOCK_ELEMS(o, n, lk)
         {
@@ -189,11 +199,11 @@ __global__ void __launch_bounds__(kBlkThreads) k_blk_update0(int n, int lk, cons
             R[o] = ri;
             D[o] = vi;
             Q[o] = wi;
-            acc[0] += ri * ri;
+            acc[0][0] += ri * ri;
         }
     }
     double out[1];
-    if (blk_colsum<1>(acc, kp, partials, &st->ticket[2], out) && threadIdx.x < kp && !st->done[c] && !st->bad[c])
+    if (blk_colsum<1, 1>(acc, kp, partials, &st->ticket[2], out) && threadIdx.x < kp && !st->done[c] && !st->bad[c])
         st->rnorm2[c] = out[0];
 }
 
@@ -209,7 +219,7 @@ __global__ void __launch_bounds__(kBlkThreads) k_blk_update(int n, int lk, doubl
     const int c = threadIdx.x & (kp - 1);
     const bool live = !st->done[c] && !st->bad[c];
     const double th = live ? st->theta[c] : 0.0, th2 = live ? st->theta2[c] : 0.0;
-    double acc[1] = { 0.0 };
+    double acc[1][1] = { { 0.0 } };
     if (live) {
         BCMGX_BLOCK_ELEMS(o, n, lk)
         {
@@ -220,11 +230,11 @@ __global__ void __launch_bounds__(kBlkThreads) k_blk_update(int n, int lk, doubl
             PW[o] = nw;
             const double ri = -th2 * nw + R[o];
             R[o] = ri;
-            acc[0] += ri * ri;
+            acc[0][0] += ri * ri;
         }
     }
     double out[1];
-    if (blk_colsum<1>(acc, kp, partials, &st->ticket[3], out) && threadIdx.x < 32) {
+    if (blk_colsum<1, 1>(acc, kp, partials, &st->ticket[3], out) && threadIdx.x < 32) {
         const int lane = threadIdx.x;
         int stopped = 1;
         if (lane < kp) {
@@ -329,18 +339,29 @@ void ensure_multi(bcmgx_hierarchy* H, MultiWork& wk, int K)
     if (!wk.st_host) BCMGX_CUDA(cudaMallocHost((void**)&wk.st_host, 2 * sizeof(BlockState)));
 }
 
+// grid of a row-slot SpMM kernel over n rows (at most kBlkBlocksPerSM blocks per SM: the size
+// of the partials)
+template <typename Kern>
+int rows_grid(Kern kern, long n, BlkShape sh)
+{
+    const long rows_per_block = (kBlkThreads / 32L) << (5 - sh.lpe_log2);
+    return std::min(fit_grid(kern, kBlkThreads, (n + rows_per_block - 1) / rows_per_block), num_sms() * kBlkBlocksPerSM);
+}
+
 // the level-0 SpMM shape of the FCG kernels (FP64 blocks of KP columns)
 BlkShape fcg_shape(const MultiWork& wk) { return blk_shape(1 << wk.lk, (int)sizeof(double)); }
 
 void launch_resid0(const DevCsr& A, const MultiWork& wk, cudaStream_t s)
 {
     const BlkShape sh = fcg_shape(wk);
-    const int g = blk_rows_grid(A.n), kp = 1 << wk.lk;
-    note_launch();
-    if (sh.W == 2)
-        k_blk_resid0<2><<<g, kBlkThreads, 0, s>>>(A.n, sh.lpe_log2, kp, A.row.p, A.col.p, A.val.p, wk.X.p, wk.B.p, wk.R.p, wk.st.p, wk.part.p);
-    else
-        k_blk_resid0<1><<<g, kBlkThreads, 0, s>>>(A.n, sh.lpe_log2, kp, A.row.p, A.col.p, A.val.p, wk.X.p, wk.B.p, wk.R.p, wk.st.p, wk.part.p);
+    const int kp = 1 << wk.lk;
+    auto go = [&](auto kern) {
+        note_launch();
+        kern<<<rows_grid(kern, A.n, sh), kBlkThreads, 0, s>>>(A.n, sh.lpe_log2, kp, A.row.p, A.col.p, A.val.p, wk.X.p,
+            wk.B.p, wk.R.p, wk.st.p, wk.part.p);
+    };
+    if (sh.W == 2) go(k_blk_resid0<2>);
+    else go(k_blk_resid0<1>);
     BCMGX_CHECK_LAUNCH();
 }
 
@@ -349,16 +370,24 @@ void launch_dots(const DevCsr& A, const MultiWork& wk, const double* pv, double*
     cudaStream_t s)
 {
     const BlkShape sh = fcg_shape(wk);
-    const int g = blk_rows_grid(A.n), kp = 1 << wk.lk;
-    note_launch();
-    if (sh.W == 2)
-        k_blk_spmv_dots<MODE, 2><<<g, kBlkThreads, 0, s>>>(A.n, sh.lpe_log2, kp, A.row.p, A.col.p, A.val.p, pv, pw, wk.R.p, oq, wk.st.p, wk.part.p, skip);
-    else
-        k_blk_spmv_dots<MODE, 1><<<g, kBlkThreads, 0, s>>>(A.n, sh.lpe_log2, kp, A.row.p, A.col.p, A.val.p, pv, pw, wk.R.p, oq, wk.st.p, wk.part.p, skip);
+    const int kp = 1 << wk.lk;
+    auto go = [&](auto kern) {
+        note_launch();
+        kern<<<rows_grid(kern, A.n, sh), kBlkThreads, 0, s>>>(A.n, sh.lpe_log2, kp, A.row.p, A.col.p, A.val.p, pv, pw,
+            wk.R.p, oq, wk.st.p, wk.part.p, skip);
+    };
+    if (sh.W == 2) go(k_blk_spmv_dots<MODE, 2>);
+    else go(k_blk_spmv_dots<MODE, 1>);
     BCMGX_CHECK_LAUNCH();
 }
 
-int elem_grid(long n, int lk) { return (int)std::max<long>(1, std::min<long>(((n << lk) + kBlkThreads - 1) / kBlkThreads, (long)num_sms() * kBlkBlocksPerSM)); }
+// grid of an element-wise kernel over an n x 2^lk block (at most kBlkBlocksPerSM blocks per SM:
+// the size of the partials)
+template <typename Kern>
+int elem_grid(Kern kern, long n, int lk)
+{
+    return std::min(fit_grid(kern, kBlkThreads, ((n << lk) + kBlkThreads - 1) / kBlkThreads), num_sms() * kBlkBlocksPerSM);
+}
 
 void blk_startup(bcmgx_hierarchy* H, MultiWork& wk)
 {
@@ -371,7 +400,7 @@ void blk_startup(bcmgx_hierarchy* H, MultiWork& wk)
     cycle_apply_block(H, wk.cyc, wk.lk, wk.R.p, wk.V.p, nullptr);
     launch_dots<0>(A, wk, wk.V.p, wk.W.p, nullptr, nullptr, s);
     note_launch();
-    k_blk_update0<<<elem_grid(A.n, wk.lk), kBlkThreads, 0, s>>>(A.n, wk.lk, wk.V.p, wk.W.p, wk.X.p, wk.R.p, wk.D.p, wk.Q.p,
+    k_blk_update0<<<elem_grid(k_blk_update0, A.n, wk.lk), kBlkThreads, 0, s>>>(A.n, wk.lk, wk.V.p, wk.W.p, wk.X.p, wk.R.p, wk.D.p, wk.Q.p,
         wk.st.p, wk.part.p);
     BCMGX_CHECK_LAUNCH();
 }
@@ -388,7 +417,7 @@ void blk_iteration(bcmgx_hierarchy* H, MultiWork& wk, bool even, const int* skip
     cycle_apply_block(H, wk.cyc, wk.lk, wk.R.p, pv, skip);
     launch_dots<1>(A, wk, pv, pw, oq, skip, s);
     note_launch();
-    k_blk_update<<<elem_grid(A.n, wk.lk), kBlkThreads, 0, s>>>(A.n, wk.lk, pv, od, wk.X.p, pw, oq, wk.R.p, wk.st.p,
+    k_blk_update<<<elem_grid(k_blk_update, A.n, wk.lk), kBlkThreads, 0, s>>>(A.n, wk.lk, pv, od, wk.X.p, pw, oq, wk.R.p, wk.st.p,
         wk.part.p, skip);
     BCMGX_CHECK_LAUNCH();
 }

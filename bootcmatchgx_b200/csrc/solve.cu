@@ -21,6 +21,7 @@
 #include <cstdlib>
 #include <map>
 #include <mutex>
+#include <unordered_map>
 #include <tuple>
 
 namespace bcmgx {
@@ -37,11 +38,30 @@ int num_sms()
     return sms;
 }
 
-static int rowop_grid(int n, int tpr)
+// Grid of a grid-stride kernel: the blocks its work needs, but no more than fit on the GPU at
+// once for this kernel (its registers and shared memory decide how many blocks an SM holds; the
+// figure is queried once per kernel and cached). Every block is then resident from the start: a
+// grid larger than one wave would leave its last blocks to run after the first wave has
+// finished all of its rows, on a mostly idle GPU.
+int fit_grid(const void* kernel, int threads, long need_blocks)
 {
-    long need = ((long)n * tpr + 255) / 256;
-    long cap = (long)num_sms() * 8;
-    return (int)std::max<long>(1, std::min(need, cap));
+    static std::mutex mu;
+    static std::unordered_map<const void*, int> per_sm;
+    int b = 0;
+    {
+        std::lock_guard<std::mutex> g(mu);
+        auto it = per_sm.find(kernel);
+        if (it != per_sm.end()) b = it->second;
+    }
+    if (b == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, threads, 0) != cudaSuccess || b <= 0) {
+            (void)cudaGetLastError();
+            b = 1;
+        }
+        std::lock_guard<std::mutex> g(mu);
+        per_sm[kernel] = b;
+    }
+    return (int)std::max<long>(1, std::min<long>(need_blocks, (long)num_sms() * b));
 }
 
 template <int OP, typename VT, typename XT, typename FT, typename MT, typename YT>
@@ -49,14 +69,18 @@ static void launch_rowop(int tpr, int n, const int* row, const int* col, const V
     const MT* M, YT* y, double alpha, double beta, const int* skip, cudaStream_t s)
 {
     if (n <= 0) return;
-    const int g = rowop_grid(n, tpr);
+    const long need = ((long)n * tpr + 255) / 256;
+    auto go = [&](auto kern) {
+        note_launch();
+        kern<<<fit_grid(kern, 256, need), 256, 0, s>>>(n, row, col, val, x, f, M, y, alpha, beta, skip);
+    };
     switch (tpr) {
-    case 1: note_launch(); k_rowop<1, OP><<<g, 256, 0, s>>>(n, row, col, val, x, f, M, y, alpha, beta, skip); break;
-    case 2: note_launch(); k_rowop<2, OP><<<g, 256, 0, s>>>(n, row, col, val, x, f, M, y, alpha, beta, skip); break;
-    case 4: note_launch(); k_rowop<4, OP><<<g, 256, 0, s>>>(n, row, col, val, x, f, M, y, alpha, beta, skip); break;
-    case 8: note_launch(); k_rowop<8, OP><<<g, 256, 0, s>>>(n, row, col, val, x, f, M, y, alpha, beta, skip); break;
-    case 16: note_launch(); k_rowop<16, OP><<<g, 256, 0, s>>>(n, row, col, val, x, f, M, y, alpha, beta, skip); break;
-    default: note_launch(); k_rowop<32, OP><<<g, 256, 0, s>>>(n, row, col, val, x, f, M, y, alpha, beta, skip); break;
+    case 1: go(k_rowop<1, OP, VT, XT, FT, MT, YT>); break;
+    case 2: go(k_rowop<2, OP, VT, XT, FT, MT, YT>); break;
+    case 4: go(k_rowop<4, OP, VT, XT, FT, MT, YT>); break;
+    case 8: go(k_rowop<8, OP, VT, XT, FT, MT, YT>); break;
+    case 16: go(k_rowop<16, OP, VT, XT, FT, MT, YT>); break;
+    default: go(k_rowop<32, OP, VT, XT, FT, MT, YT>); break;
     }
     BCMGX_CHECK_LAUNCH();
 }
@@ -136,13 +160,13 @@ __global__ void k_prolong(int n, const int* __restrict__ agg, const PT* __restri
         y[i] = (YT)((AT)p[i] * (AT)xc[agg[i]] + (AT)x[i]);
 }
 
-static int ew_grid(long n) { return (int)std::max<long>(1, std::min<long>((n + 255) / 256, (long)num_sms() * 8)); }
+// grid for an element-wise kernel over n elements
+template <typename Kern>
+static int ew_grid(Kern kern, long n) { return fit_grid(kern, 256, (n + 255) / 256); }
 
 // ------------------------------------------------------------------------------------------
 // block launches (blockops.cuh)
 // ------------------------------------------------------------------------------------------
-static int blk_rows_grid(long rows) { return (int)std::max<long>(1, std::min<long>((rows * 32 + 255) / 256, (long)num_sms() * 8)); }
-
 static int ceil_log2(int k)
 {
     int lg = 0;
@@ -150,26 +174,37 @@ static int ceil_log2(int k)
     return lg;
 }
 
+static bool aligned_for(const void* p, int W, size_t elem)
+{
+    const size_t a = std::min<size_t>(16, W * elem);
+    return p == nullptr || ((uintptr_t)p % a) == 0;
+}
+
 // Y = alpha A X + beta Y / F - A X / Jacobi sweep on blocks with leading dimension ld and K
-// columns; vector loads when X and ld allow them, else one column per lane.
+// columns; vector loads and stores when the pointers and ld allow them, else one column per lane.
 template <int OP, typename VT, typename XT, typename FT, typename MT, typename YT>
 static void launch_blk_rowop(int n, int ld, int K, const int* row, const int* col, const VT* val, const XT* x,
     const FT* f, const MT* M, YT* y, double alpha, double beta, const int* skip, cudaStream_t s)
 {
     if (n <= 0) return;
     BlkShape sh = blk_shape(K, (int)sizeof(XT));
-    if (sh.W > 1 && (((uintptr_t)x % (sh.W * sizeof(XT))) != 0 || ld % sh.W != 0)) sh = BlkShape { 1, ceil_log2(K) };
-    const int g = blk_rows_grid(n);
-    note_launch();
+    if (sh.W > 1 && (ld % sh.W != 0 || !aligned_for(x, sh.W, sizeof(XT)) || !aligned_for(y, sh.W, sizeof(YT)) ||
+                        !aligned_for(f, sh.W, sizeof(FT))))
+        sh = BlkShape { 1, ceil_log2(K) };
+    const long need = ((long)n + (8L << (5 - sh.lpe_log2)) - 1) / (8L << (5 - sh.lpe_log2));   // 8 warps x rows per warp
+    auto go = [&](auto kern) {
+        note_launch();
+        kern<<<fit_grid(kern, 256, need), 256, 0, s>>>(n, sh.lpe_log2, ld, K, row, col, val, x, f, M, y, alpha, beta, skip);
+    };
     if constexpr (sizeof(XT) == 4) {
         if (sh.W == 4) {
-            k_blk_rowop<OP, 4><<<g, 256, 0, s>>>(n, sh.lpe_log2, ld, K, row, col, val, x, f, M, y, alpha, beta, skip);
+            go(k_blk_rowop<OP, 4, VT, XT, FT, MT, YT>);
             BCMGX_CHECK_LAUNCH();
             return;
         }
     }
-    if (sh.W == 2) k_blk_rowop<OP, 2><<<g, 256, 0, s>>>(n, sh.lpe_log2, ld, K, row, col, val, x, f, M, y, alpha, beta, skip);
-    else k_blk_rowop<OP, 1><<<g, 256, 0, s>>>(n, sh.lpe_log2, ld, K, row, col, val, x, f, M, y, alpha, beta, skip);
+    if (sh.W == 2) go(k_blk_rowop<OP, 2, VT, XT, FT, MT, YT>);
+    else go(k_blk_rowop<OP, 1, VT, XT, FT, MT, YT>);
     BCMGX_CHECK_LAUNCH();
 }
 
@@ -188,7 +223,8 @@ struct Cycle {
 
     bool lf32(int l) const { return fp32 && l < L - 1; }
     Level& lv(int l) const { return H->lv[l]; }
-    int grid(int n) const { return ew_grid(lk < 0 ? (long)n : ((long)n << lk)); }
+    template <typename Kern>
+    int grid(Kern kern, int n) const { return ew_grid(kern, lk < 0 ? (long)n : ((long)n << lk)); }
 
     // ---- kernel dispatch (single vector or block) ----
     template <int OP, typename VT, typename XT, typename FT, typename MT, typename YT>
@@ -201,24 +237,39 @@ struct Cycle {
     void first(int n, const FT* f, const MT* M, YT* u, CT* fcopy) const
     {
         note_launch();
-        if (lk >= 0) k_blk_first_sweep<<<grid(n), 256, 0, s>>>(n, lk, f, M, u, fcopy, skip);
-        else k_first_sweep<<<grid(n), 256, 0, s>>>(n, f, M, u, fcopy, skip);
+        if (lk >= 0) {
+            auto k = k_blk_first_sweep<FT, MT, YT, CT>;
+            k<<<grid(k, n), 256, 0, s>>>(n, lk, f, M, u, fcopy, skip);
+        } else {
+            auto k = k_first_sweep<FT, MT, YT, CT>;
+            k<<<grid(k, n), 256, 0, s>>>(n, f, M, u, fcopy, skip);
+        }
         BCMGX_CHECK_LAUNCH();
     }
     template <typename ST, typename DT>
     void convert(int n, const ST* a, DT* b) const
     {
         note_launch();
-        if (lk >= 0) k_blk_convert<<<grid(n), 256, 0, s>>>(n, lk, a, b, skip);
-        else k_convert<<<grid(n), 256, 0, s>>>(n, a, b, skip);
+        if (lk >= 0) {
+            auto k = k_blk_convert<ST, DT>;
+            k<<<grid(k, n), 256, 0, s>>>(n, lk, a, b, skip);
+        } else {
+            auto k = k_convert<ST, DT>;
+            k<<<grid(k, n), 256, 0, s>>>(n, a, b, skip);
+        }
         BCMGX_CHECK_LAUNCH();
     }
     template <typename T>
     void zero_n(int n, T* a) const
     {
         note_launch();
-        if (lk >= 0) k_blk_zero<<<grid(n), 256, 0, s>>>(n, lk, a, skip);
-        else k_zero<<<grid(n), 256, 0, s>>>(n, a, skip);
+        if (lk >= 0) {
+            auto k = k_blk_zero<T>;
+            k<<<grid(k, n), 256, 0, s>>>(n, lk, a, skip);
+        } else {
+            auto k = k_zero<T>;
+            k<<<grid(k, n), 256, 0, s>>>(n, a, skip);
+        }
         BCMGX_CHECK_LAUNCH();
     }
     // out = P^T res: for a block, an SpMM with the stored transpose (rptr, ridx, rval)
@@ -230,16 +281,22 @@ struct Cycle {
                 (const OT*)nullptr, out, 1.0, 0.0, skip, s);
             return;
         }
+        auto k = k_restrict<RT, WT, OT>;
         note_launch();
-        k_restrict<<<grid(nc), 256, 0, s>>>(nc, V.rptr.p, V.ridx.p, rval, res, out, skip);
+        k<<<grid(k, nc), 256, 0, s>>>(nc, V.rptr.p, V.ridx.p, rval, res, out, skip);
         BCMGX_CHECK_LAUNCH();
     }
     template <typename PT, typename CT, typename XT, typename YT>
     void prolong(int n, const Level& V, const PT* p, const CT* xc, const XT* x, YT* y) const
     {
         note_launch();
-        if (lk >= 0) k_blk_prolong<<<grid(n), 256, 0, s>>>(n, lk, V.agg.p, p, xc, x, y, skip);
-        else k_prolong<<<grid(n), 256, 0, s>>>(n, V.agg.p, p, xc, x, y, skip);
+        if (lk >= 0) {
+            auto k = k_blk_prolong<PT, CT, XT, YT>;
+            k<<<grid(k, n), 256, 0, s>>>(n, lk, V.agg.p, p, xc, x, y, skip);
+        } else {
+            auto k = k_prolong<PT, CT, XT, YT>;
+            k<<<grid(k, n), 256, 0, s>>>(n, V.agg.p, p, xc, x, y, skip);
+        }
         BCMGX_CHECK_LAUNCH();
     }
 
@@ -406,7 +463,8 @@ void prec_apply_impl(bcmgx_hierarchy* H, const double* r, double* v, const int* 
     const int n0 = H->lv[0].A.n;
     if (H->prm.preconditioner != BCMGX_PREC_BCMG) {
         note_launch();
-        k_convert<double, double><<<ew_grid(n0), 256, 0, H->stream>>>(n0, r, v, skip);
+        auto k = k_convert<double, double>;
+        k<<<ew_grid(k, n0), 256, 0, H->stream>>>(n0, r, v, skip);
         BCMGX_CHECK_LAUNCH();
         return;
     }
@@ -419,7 +477,8 @@ void cycle_apply_block(bcmgx_hierarchy* H, const CycleBufs& bufs, int lk, const 
     const int n0 = H->lv[0].A.n;
     if (H->prm.preconditioner != BCMGX_PREC_BCMG) {
         note_launch();
-        k_blk_convert<double, double><<<ew_grid((long)n0 << lk), 256, 0, H->stream>>>(n0, lk, r, v, skip);
+        auto k = k_blk_convert<double, double>;
+        k<<<ew_grid(k, (long)n0 << lk), 256, 0, H->stream>>>(n0, lk, r, v, skip);
         BCMGX_CHECK_LAUNCH();
         return;
     }
@@ -446,10 +505,12 @@ void prec_apply_dev(bcmgx_hierarchy* H, const double* r, double* v)
 constexpr int kRedBlocksPerSM = 8;
 constexpr int kRedThreads = 256;
 
-static int red_grid(long work_threads)
+// grid of the FCG kernels: at most kRedBlocksPerSM blocks per SM (the size of the partials)
+template <typename Kern>
+static int red_grid(Kern kern, long work_threads)
 {
-    long need = (work_threads + kRedThreads - 1) / kRedThreads;
-    return (int)std::max<long>(1, std::min<long>(need, (long)num_sms() * kRedBlocksPerSM));
+    const long need = (work_threads + kRedThreads - 1) / kRedThreads;
+    return std::min(fit_grid(kern, kRedThreads, need), num_sms() * kRedBlocksPerSM);
 }
 
 // r = b - A x and ||r||^2 -> delta0, tolerance (FCG.cu:46-51).
@@ -592,13 +653,17 @@ __global__ void __launch_bounds__(kRedThreads) k_fcg_update(int n, double* __res
 template <int S>
 static void launch_resid0(const DevCsr& A, const double* x, const double* b, double* r, FcgState* st, double* part, cudaStream_t s)
 {
-    note_launch(); k_fcg_resid0<S><<<red_grid((long)A.n * S), kRedThreads, 0, s>>>(A.n, A.row.p, A.col.p, A.val.p, x, b, r, st, part);
+    auto k = k_fcg_resid0<S>;
+    note_launch();
+    k<<<red_grid(k, (long)A.n * S), kRedThreads, 0, s>>>(A.n, A.row.p, A.col.p, A.val.p, x, b, r, st, part);
 }
 template <int S, int MODE>
 static void launch_dots(const DevCsr& A, const double* pv, double* pw, const double* r, const double* oq, FcgState* st,
     double* part, const int* skip, cudaStream_t s)
 {
-    note_launch(); k_fcg_spmv_dots<S, MODE><<<red_grid((long)A.n * S), kRedThreads, 0, s>>>(A.n, A.row.p, A.col.p, A.val.p, pv, pw, r, oq, st, part, skip);
+    auto k = k_fcg_spmv_dots<S, MODE>;
+    note_launch();
+    k<<<red_grid(k, (long)A.n * S), kRedThreads, 0, s>>>(A.n, A.row.p, A.col.p, A.val.p, pv, pw, r, oq, st, part, skip);
 }
 
 static void fcg_resid0(const DevCsr& A, const double* x, const double* b, double* r, FcgState* st, double* part, cudaStream_t s)
@@ -844,9 +909,9 @@ __global__ void __launch_bounds__(256) k_grad_pattern(int n, const int* __restri
 
 void grad_pattern(const DevCsr& A, const double* lam, const double* x, double* dA, cudaStream_t s)
 {
-    const int g = rowop_grid(A.n, 4);
+    auto k = k_grad_pattern<4>;
     note_launch();
-    k_grad_pattern<4><<<g, 256, 0, s>>>(A.n, A.row.p, A.col.p, lam, x, dA);
+    k<<<fit_grid(k, 256, ((long)A.n * 4 + 255) / 256), 256, 0, s>>>(A.n, A.row.p, A.col.p, lam, x, dA);
     BCMGX_CHECK_LAUNCH();
 }
 
@@ -879,7 +944,8 @@ static void fcg_startup(bcmgx_hierarchy* H, const double* b, double* x, double* 
     fcg_resid0(A, x, b, r, st, part, s);
     prec_apply_impl(H, r, v, nullptr);
     fcg_dots<0>(A, v, w, r, nullptr, st, part, nullptr, s);
-    note_launch(); k_fcg_update0<<<red_grid(n), kRedThreads, 0, s>>>(n, v, w, x, r, d, q, st, part, hist);
+    note_launch();
+    k_fcg_update0<<<red_grid(k_fcg_update0, n), kRedThreads, 0, s>>>(n, v, w, x, r, d, q, st, part, hist);
     BCMGX_CHECK_LAUNCH();
 }
 
@@ -899,7 +965,8 @@ static void fcg_iteration(bcmgx_hierarchy* H, bool even, double* x, double* hist
     const double* oq = even ? q : w;
     prec_apply_impl(H, r, pv, skip);
     fcg_dots<1>(A, pv, pw, r, oq, st, part, skip, s);
-    note_launch(); k_fcg_update<<<red_grid(n), kRedThreads, 0, s>>>(n, pv, od, x, pw, oq, r, st, part, hist, skip);
+    note_launch();
+    k_fcg_update<<<red_grid(k_fcg_update, n), kRedThreads, 0, s>>>(n, pv, od, x, pw, oq, r, st, part, hist, skip);
     BCMGX_CHECK_LAUNCH();
 }
 

@@ -625,14 +625,17 @@ def profile_multi_step(a):
 
 def profile_step(a, wl):
     """W warm-up steps, then exactly one set-up + solve (FP32 V-cycle) on device-resident data;
-    prints how many library kernels the warm-up and the step launched."""
+    prints how many library kernels the warm-up and the step launched. The solve is
+    stream-driven (use_graph = 0: the same kernels as the captured solve, launched one by one),
+    so that a profiler sees every kernel of the step."""
     import torch
     import bootcmatchgx_b200 as bx
     dev = torch.device("cuda", 0)
     row, col, val, xs, b = build_problem(wl)
     d = [torch.from_numpy(x_).to(dev) for x_ in (row, col, val, b)]
     x = torch.zeros(row.size - 1, dtype=torch.float64, device=dev)
-    p = bx.params_default(solver="FCG", preconditioner="BCMG", rtol=RTOL, dispnorm=0, vcycle_precision="FP32")
+    p = bx.params_default(solver="FCG", preconditioner="BCMG", rtol=RTOL, dispnorm=0, vcycle_precision="FP32",
+                          use_graph=0)
     L = bx.lib()
     c0 = L.bcmgx_launch_count()
     for _ in range(a.warmup):

@@ -61,10 +61,16 @@ static void check_params(const bcmgx_params* p)
 {
     BCMGX_REQUIRE(p != nullptr, BCMGX_ERR_INVALID_INPUT, "params is NULL");
     BCMGX_REQUIRE(p->error == 0, BCMGX_ERR_INVALID_INPUT, "settings carry an error flag (unsupported legacy option)");
-    BCMGX_REQUIRE(p->solver == BCMGX_SOLVER_FCG, BCMGX_ERR_UNSUPPORTED,
-        std::string("solver ") + solver_name(p->solver) + " is not on this path (FCG only)");
-    BCMGX_REQUIRE(p->preconditioner == BCMGX_PREC_BCMG || p->preconditioner == BCMGX_PREC_NONE, BCMGX_ERR_UNSUPPORTED,
-        std::string("preconditioner ") + prec_name(p->preconditioner) + " is not on this path (BCMG or NONE)");
+    BCMGX_REQUIRE(p->solver >= BCMGX_SOLVER_CGHS && p->solver < BCMGX_SOLVER_INVALID, BCMGX_ERR_INVALID_INPUT,
+        "invalid solver");
+    BCMGX_REQUIRE(p->preconditioner == BCMGX_PREC_BCMG || p->preconditioner == BCMGX_PREC_NONE ||
+            p->preconditioner == BCMGX_PREC_L1_JACOBI,
+        BCMGX_ERR_UNSUPPORTED, std::string("preconditioner ") + prec_name(p->preconditioner) +
+            " is not implemented (BCMG, L1_JACOBI or NONE)");
+    if (p->solver == BCMGX_SOLVER_CGS || p->solver == BCMGX_SOLVER_PIPELINED_CGS || p->solver == BCMGX_SOLVER_CGS_CUBLAS)
+        BCMGX_REQUIRE(p->sstep >= 1 && p->sstep <= 8, BCMGX_ERR_INVALID_INPUT, "sstep must be 1..8");
+    if (p->preconditioner == BCMGX_PREC_L1_JACOBI)
+        BCMGX_REQUIRE(p->l1jacsweeps >= 1, BCMGX_ERR_INVALID_INPUT, "l1jacsweeps must be >= 1");
     BCMGX_REQUIRE(p->cycle_type >= 0 && p->cycle_type < BCMGX_CYCLE_INVALID, BCMGX_ERR_INVALID_INPUT, "invalid cycle_type");
     BCMGX_REQUIRE(p->matchtype == BCMGX_MATCH_SUITOR, BCMGX_ERR_INVALID_INPUT, "invalid matchtype");
     BCMGX_REQUIRE(p->relax_type == BCMGX_L1_JACOBI && p->coarse_solver == BCMGX_L1_JACOBI, BCMGX_ERR_INVALID_INPUT,
@@ -80,6 +86,12 @@ static void check_params(const bcmgx_params* p)
         BCMGX_ERR_INVALID_INPUT, "negative sweep count");
     BCMGX_REQUIRE(p->vcycle_precision == BCMGX_VCYCLE_FP64 || p->vcycle_precision == BCMGX_VCYCLE_FP32,
         BCMGX_ERR_INVALID_INPUT, "invalid vcycle_precision");
+}
+
+// solve() dispatch on the solver type (solver/solve.cu:11-51)
+static int solve_dispatch(bcmgx_hierarchy* h, const double* b, double* x, bcmgx_solve_info* info)
+{
+    return h->prm.solver == BCMGX_SOLVER_FCG ? fcg_solve(h, b, x, info) : krylov_solve(h, b, x, info);
 }
 
 // Builds one hierarchy (the body of bcmgx_setup). own_stream forces a library-owned stream even
@@ -177,6 +189,10 @@ bcmgx_hierarchy::~bcmgx_hierarchy()
     if (iter_graph) cudaGraphExecDestroy(iter_graph);
     bcmgx::free_multi(multi);
     multi = nullptr;
+    bcmgx::free_krylov(krylov);
+    krylov = nullptr;
+    l1d.release();
+    l1tmp.release();
     lv.clear();
     b.release();
     xv.release();
@@ -257,6 +273,7 @@ int bcmgx_setup_batch(int nsys, const bcmgx_csr* A, const bcmgx_params* p, int n
 {
     return guarded([&] {
         BCMGX_REQUIRE(nsys > 0 && A && p && out, BCMGX_ERR_INVALID_INPUT, "bad argument");
+        BCMGX_REQUIRE(p->solver == BCMGX_SOLVER_FCG, BCMGX_ERR_UNSUPPORTED, "batched solves need FCG");
         *out = nullptr;
         check_params(p);
         int dev = p->device;
@@ -300,6 +317,7 @@ int bcmgx_batch_from_hierarchies(int nsys, bcmgx_hierarchy* const* hs, bcmgx_bat
         B->hs.assign(hs, hs + nsys);
         B->device = hs[0]->device;
         for (auto* h : B->hs) BCMGX_REQUIRE(h && h->device == B->device, BCMGX_ERR_INVALID_INPUT, "hierarchies must share one device");
+        for (auto* h : B->hs) BCMGX_REQUIRE(h->prm.solver == BCMGX_SOLVER_FCG, BCMGX_ERR_UNSUPPORTED, "batched solves need FCG");
         finish_batch(B.get(), &hs[0]->prm);
         *out = B.release();
     });
@@ -345,13 +363,13 @@ int bcmgx_solve(bcmgx_hierarchy* h, const double* b, double* x, int on_device, b
         const int n = h->lv[0].A.n;
         cudaStream_t s = h->stream;
         if (on_device) {
-            status = fcg_solve(h, b, x, info);
+            status = solve_dispatch(h, b, x, info);
         } else {
             h->b.alloc(n, s);
             h->xv.alloc(n, s);
             BCMGX_CUDA(cudaMemcpyAsync(h->b.p, b, sizeof(double) * n, cudaMemcpyHostToDevice, s));
             BCMGX_CUDA(cudaMemcpyAsync(h->xv.p, x, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-            status = fcg_solve(h, h->b.p, h->xv.p, info);
+            status = solve_dispatch(h, h->b.p, h->xv.p, info);
             BCMGX_CUDA(cudaMemcpyAsync(x, h->xv.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
             BCMGX_CUDA(cudaStreamSynchronize(s));
         }
@@ -402,7 +420,7 @@ int bcmgx_solve_adjoint(bcmgx_hierarchy* h, const double* g, const double* x, do
         cudaStream_t s = h->stream;
         if (on_device) {
             BCMGX_CUDA(cudaMemsetAsync(lambda, 0, sizeof(double) * n, s));
-            status = fcg_solve(h, g, lambda, info);
+            status = solve_dispatch(h, g, lambda, info);
             if (dA_val) grad_pattern(A, lambda, x, dA_val, s);
             BCMGX_CUDA(cudaStreamSynchronize(s));
         } else {
@@ -411,7 +429,7 @@ int bcmgx_solve_adjoint(bcmgx_hierarchy* h, const double* g, const double* x, do
             ld.alloc(n, s);
             BCMGX_CUDA(cudaMemcpyAsync(gd.p, g, sizeof(double) * n, cudaMemcpyHostToDevice, s));
             BCMGX_CUDA(cudaMemsetAsync(ld.p, 0, sizeof(double) * n, s));
-            status = fcg_solve(h, gd.p, ld.p, info);
+            status = solve_dispatch(h, gd.p, ld.p, info);
             BCMGX_CUDA(cudaMemcpyAsync(lambda, ld.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
             if (dA_val) {
                 xd.alloc(n, s);

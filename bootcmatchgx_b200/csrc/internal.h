@@ -145,6 +145,9 @@ struct CycleBufs {
 // Scratch of the multi-right-hand-side solve (multi.cu); opaque to the other units.
 struct MultiWork;
 void free_multi(MultiWork* w);
+// Scratch, device state and captured graph of the CGHS / s-step solvers (krylov.cu).
+struct KrylovWork;
+void free_krylov(KrylovWork* w);
 
 // FCG scalars that live on the device between kernels.
 struct FcgState {
@@ -185,6 +188,9 @@ struct bcmgx_hierarchy {
     bcmgx::CycleBufs cyc;                 // single-vector cycle buffers (views of lv[l] and res)
     // multi-right-hand-side solve: its scratch and its captured graph (for multi_k columns)
     bcmgx::MultiWork* multi = nullptr;
+    bcmgx::KrylovWork* krylov = nullptr;   // solvers other than FCG
+    // standalone l1-Jacobi preconditioner: divisor a_ii + sum_{j != i} |a_ij| and a sweep buffer
+    bcmgx::DBuf<double> l1d, l1tmp;
     ~bcmgx_hierarchy();
 };
 
@@ -224,6 +230,11 @@ void ensure_solve_workspace(bcmgx_hierarchy* H);
 int fcg_solve(bcmgx_hierarchy* H, const double* b_dev, double* x_dev, bcmgx_solve_info* info);
 void prec_apply_dev(bcmgx_hierarchy* H, const double* r, double* v);
 void prec_apply_impl(bcmgx_hierarchy* H, const double* r, double* v, const int* skip);
+// CGHS or the s-step CG (krylov.cu), for every solver but FCG.
+int krylov_solve(bcmgx_hierarchy* H, const double* b, double* x, bcmgx_solve_info* info);
+// FP64 row operations on level-0-like matrices with the autotuned shape; skip: see k_rowop.
+void rowop_spmv(const DevCsr& A, const double* x, double* y, const int* skip, cudaStream_t s);
+void rowop_resid(const DevCsr& A, const double* x, const double* f, double* y, const int* skip, cudaStream_t s);
 // One V-cycle on 2^lk right-hand sides (row-major n0 x 2^lk blocks) with block buffers `bufs`.
 void cycle_apply_block(bcmgx_hierarchy* H, const CycleBufs& bufs, int lk, const double* r, double* v, const int* skip);
 // Block FCG for K right-hand sides of one system (multi.cu); B, X row-major n x K, device.

@@ -243,6 +243,21 @@ __global__ void k_abs_row_sum(int n, const int* __restrict__ row, const double* 
     }
 }
 
+// Standalone l1-Jacobi divisor D_i = a_ii + sum_{j != i} |a_ij|: the diagonal (mydiag) plus the
+// off-diagonal absolute sum in column order (add_absrowsum_nodiag, op/addAbsoluteRowSumNoDiag.cu).
+__global__ void k_l1_divisor(int n, const int* __restrict__ row, const int* __restrict__ col, const double* __restrict__ val,
+    double* __restrict__ D)
+{
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        double d = 0.0, off = 0.0;
+        for (int j = row[i]; j < row[i + 1]; j++) {
+            if (col[j] == i) d = val[j];
+            else off = __dadd_rn(off, fabs(val[j]));
+        }
+        D[i] = __dadd_rn(d, off);
+    }
+}
+
 __global__ void k_to_f32(long n, const double* __restrict__ a, float* __restrict__ b)
 {
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) b[i] = (float)a[i];
@@ -992,6 +1007,11 @@ void build_hierarchy(bcmgx_hierarchy* H, const bcmgx_csr* Ain)
     H->ftcoarse = 1;
     // AMG::BuildData::setMaxCoarseSize, AMG.cu:238-241
     H->maxcoarsesize = (int)(40 * std::pow((double)L0n, 1.0 / 3.0));
+    if (P.preconditioner == BCMGX_PREC_L1_JACOBI) {
+        H->l1d.alloc(L0n, s);
+        note_launch(); k_l1_divisor<<<gs_grid(L0n), 256, 0, s>>>(L0n, A.row.p, A.col.p, A.val.p, H->l1d.p);
+        BCMGX_CHECK_LAUNCH();
+    }
     if (P.preconditioner != BCMGX_PREC_BCMG) {
         finish_level_matrix(L0, false, s);
         H->op_cmplx = 1;

@@ -104,6 +104,17 @@ void launch_spmv(int n, const int* row, const int* col, const double* val, const
         (const double*)nullptr, (const double*)nullptr, y, alpha, beta, nullptr, s);
 }
 
+void rowop_spmv(const DevCsr& A, const double* x, double* y, const int* skip, cudaStream_t s)
+{
+    launch_rowop<OP_AXPBY>(A.tpr, A.n, A.row.p, A.col.p, A.val.p, x, (const double*)nullptr, (const double*)nullptr, y,
+        1.0, 0.0, skip, s);
+}
+
+void rowop_resid(const DevCsr& A, const double* x, const double* f, double* y, const int* skip, cudaStream_t s)
+{
+    launch_rowop<OP_RESID>(A.tpr, A.n, A.row.p, A.col.p, A.val.p, x, f, (const double*)nullptr, y, 1.0, 0.0, skip, s);
+}
+
 // ------------------------------------------------------------------------------------------
 // element-wise kernels of the cycle
 // ------------------------------------------------------------------------------------------
@@ -458,9 +469,33 @@ struct Cycle {
     }
 };
 
+// Standalone l1-Jacobi preconditioner: l1jacsweeps sweeps u <- u + (r - A u) / D from u = 0, with
+// D = a_ii + sum_{j != i} |a_ij| (l1jacobi_apply, l1jacobi.cu:513-523, and set_l1j, :484-493).
+// The sweeps alternate between v and a scratch vector so that the last one writes v.
+static void l1jacobi_apply(bcmgx_hierarchy* H, const double* r, double* v, const int* skip)
+{
+    const DevCsr& A = H->lv[0].A;
+    const int n = A.n, k = H->prm.l1jacsweeps;
+    cudaStream_t s = H->stream;
+    std::vector<double*> out(k);
+    out[k - 1] = v;
+    for (int i = k - 2; i >= 0; i--) out[i] = (out[i + 1] == v) ? H->l1tmp.p : v;
+    auto first = k_first_sweep<double, double, double, double>;
+    note_launch();
+    first<<<ew_grid(first, n), 256, 0, s>>>(n, r, H->l1d.p, out[0], (double*)nullptr, skip);
+    BCMGX_CHECK_LAUNCH();
+    for (int i = 1; i < k; i++)
+        launch_rowop<OP_JACOBI>(A.tpr, n, A.row.p, A.col.p, A.val.p, (const double*)out[i - 1], r, (const double*)H->l1d.p,
+            out[i], 1.0, 0.0, skip, s);
+}
+
 void prec_apply_impl(bcmgx_hierarchy* H, const double* r, double* v, const int* skip)
 {
     const int n0 = H->lv[0].A.n;
+    if (H->prm.preconditioner == BCMGX_PREC_L1_JACOBI) {
+        l1jacobi_apply(H, r, v, skip);
+        return;
+    }
     if (H->prm.preconditioner != BCMGX_PREC_BCMG) {
         note_launch();
         auto k = k_convert<double, double>;
@@ -735,6 +770,7 @@ void ensure_solve_workspace(bcmgx_hierarchy* H)
         else H->cyc.lv[l] = { Vec { V.rhs.p, false }, Vec { V.x.p, false }, Vec { V.x2.p, false } };
     }
     H->cyc.res = f32 ? Vec { H->res32.p, true } : Vec { H->res.p, false };
+    if (H->prm.preconditioner == BCMGX_PREC_L1_JACOBI) H->l1tmp.alloc(n0, s);
     H->ws_n = n0;
 }
 

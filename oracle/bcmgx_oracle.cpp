@@ -98,6 +98,7 @@ struct Hierarchy {
     int ftcoarse = 1;
     double op_cmplx = 0, op_wcmplx = 0, avg_cratio = 1;
     std::vector<int> grid_sweeps;
+    std::vector<double> l1d;   // standalone l1-Jacobi divisor a_ii + sum_{j != i} |a_ij| (L1_JACOBI)
 };
 
 // ------------------------------------------------------------------------------------------
@@ -548,6 +549,18 @@ Hierarchy* build(const Csr& A0, const Params& prm, bool record)
     H->lv.emplace_back();
     H->lv[0].A = A0;
     H->lv[0].M = abs_row_sum(A0);
+    if (prm.preconditioner == 1) {
+        // set_l1j (l1jacobi.cu:484-493): mydiag + addAbsoluteRowSumNoDiag
+        H->l1d.assign(A0.n, 0.0);
+        for (int i = 0; i < A0.n; i++) {
+            double d = 0.0, off = 0.0;
+            for (int j = A0.row[i]; j < A0.row[i + 1]; j++) {
+                if (A0.col[j] == i) d = A0.val[j];
+                else off += std::fabs(A0.val[j]);
+            }
+            H->l1d[i] = d + off;
+        }
+    }
     if (prm.preconditioner != 2) return H;
     const int sweepnumber = prm.aggrsweeps + 1;
     std::vector<double> w(A0.n, 1.0);
@@ -688,6 +701,12 @@ void cycle(const Hierarchy& H, Work& wk, int l)
 void prec_apply(const Hierarchy& H, Work& wk, const double* r, double* v)
 {
     const int n = H.lv[0].A.n;
+    if (H.prm.preconditioner == 1) {
+        // l1jacobi_apply (l1jacobi.cu:513-523): l1jacsweeps sweeps from v (zero at every call site)
+        std::vector<double> tmp(n);
+        l1jacobi(H.prm.l1jacsweeps, H.lv[0].A, H.l1d, r, v, tmp.data());
+        return;
+    }
     if (H.prm.preconditioner != 2) {
         std::memcpy(v, r, sizeof(double) * n);
         return;
@@ -780,6 +799,278 @@ SolveInfo fcg(const Hierarchy& H, const double* b, double* x)
     SolveInfo si;
     si.niter = iter + 1;
     si.retv = iter >= prm.itnlim ? -1 : 0;
+    si.delta0 = delta0;
+    si.exit_res = l2;
+    return si;
+}
+
+Work make_work(const Hierarchy& H)
+{
+    Work wk;
+    for (auto& l : H.lv) {
+        wk.rhs.emplace_back(l.A.n, 0.0);
+        wk.x.emplace_back(l.A.n, 0.0);
+        wk.x2.emplace_back(l.A.n, 0.0);
+    }
+    wk.res.assign(H.lv[0].A.n, 0.0);
+    return wk;
+}
+
+// Preconditioned CG, Hestenes-Stiefel form. Restates cg_hs (cghs/CG_HS.cu:25-151): delta0 =
+// ||r0|| when stop_criterion == 1 else 1; u = B r from a zero guess; stop when ||r|| < rtol *
+// delta0 (strict); niter = iter + 1 on convergence, itnlim otherwise.
+SolveInfo cghs(const Hierarchy& H, const double* b, double* x)
+{
+    const Csr& A = H.lv[0].A;
+    const long n = A.n;
+    const Params& prm = H.prm;
+    const bool pre = prm.preconditioner != 0;
+    Work wk = make_work(H);
+    std::vector<double> s(n, 0.0), p(n), r(b, b + n), u(n, 0.0), w(n);
+    spmv(A, x, w.data());
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n; i++) r[i] = -1.0 * w[i] + 1.0 * r[i];
+    if (pre) prec_apply(H, wk, r.data(), u.data());
+    else u = r;
+    p = u;
+    const double delta0 = prm.stop_criterion == 1 ? std::sqrt(dot(r.data(), r.data(), n)) : 1.0;
+    double rho_old = 0.0, l2 = 0.0;
+    int iter, excnlim = -1, retv = -1;
+    for (iter = 0; iter < prm.itnlim; iter++) {
+        if (iter > 0) {
+            if (pre) {
+                std::fill(u.begin(), u.end(), 0.0);
+                prec_apply(H, wk, r.data(), u.data());
+            } else {
+                u = r;
+            }
+            const double rho = dot(r.data(), u.data(), n);
+            const double beta = rho / rho_old;
+#pragma omp parallel for schedule(static)
+            for (long i = 0; i < n; i++) p[i] = 1.0 * u[i] + beta * p[i];
+        }
+        spmv(A, p.data(), s.data());
+        const double ur = dot(u.data(), r.data(), n);
+        const double ps = dot(p.data(), s.data(), n);
+        rho_old = ur;
+        const double alpha = ur / ps;
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < n; i++) {
+            x[i] = alpha * p[i] + 1.0 * x[i];
+            r[i] = -alpha * s[i] + 1.0 * r[i];
+        }
+        l2 = std::sqrt(dot(r.data(), r.data(), n));
+        if (l2 < prm.rtol * delta0) {
+            excnlim = 0;
+            retv = 0;
+            break;
+        }
+    }
+    SolveInfo si;
+    si.niter = iter + 1 + excnlim;
+    si.retv = retv;
+    si.delta0 = delta0;
+    si.exit_res = l2;
+    return si;
+}
+
+// ---- s-step CG (Chronopoulos and Gear) ------------------------------------------------------
+
+// Matrix powers kernel (krylov_base/mpk.cu:10-83). sP is n x 2s column-major. Without a
+// preconditioner: columns 0..s hold r, A r, ..., A^s r. With one: columns 0..s-1 hold
+// P_j = (B A)^j B r and columns s..2s-1 hold A P_j (B applied from a zero guess).
+void mpk(const Hierarchy& H, Work& wk, const double* r, int s, std::vector<double>& sP)
+{
+    const Csr& A = H.lv[0].A;
+    const long n = A.n;
+    double* P = sP.data();
+    if (H.prm.preconditioner == 0) {
+        std::memcpy(P, r, sizeof(double) * n);
+        for (int i = 0; i < s; i++) spmv(A, P + i * n, P + (i + 1) * n);
+        return;
+    }
+    std::fill(P, P + n, 0.0);
+    prec_apply(H, wk, r, P);
+    int pin = 0, pout = s;
+    for (int i = 0; i < 2 * s - 1; i++) {
+        if (i % 2 == 0) {
+            spmv(A, P + pin * n, P + pout * n);
+        } else {
+            std::fill(P + pout * n, P + (pout + 1) * n, 0.0);
+            prec_apply(H, wk, P + pin * n, P + pout * n);
+        }
+        const int t = pin;
+        pin = pout;
+        pout = t + 1;
+    }
+}
+
+// The 2s moments (krylov_base/computevm.cu:6-31).
+void computevm(const std::vector<double>& sP, int s, const double* r, long n, bool pre, double* vm)
+{
+    const double* P = sP.data();
+    if (!pre) {
+        for (int k = 0; k <= s; k++) vm[k] = dot(P + k * n, r, n);
+        for (int k = 0; k < s - 1; k++) vm[s + 1 + k] = dot(P + (1 + k) * n, P + s * n, n);
+    } else {
+        for (int k = 0; k < s; k++) vm[k] = dot(P + k * n, r, n);
+        for (int k = 0; k < s; k++) vm[s + k] = dot(P + k * n, P + (2 * s - 1) * n, n);
+    }
+}
+
+// Cholesky factor (lower, column-major) in place; the square root is taken in single precision
+// as in myChol (op/scalarWorkMO.cu:126-157, the build without LAPACK). Returns 1 when W is not
+// positive definite.
+int chol_lower(double* W, int n)
+{
+    for (int i = 0; i < n; i++) {
+        for (int j = 0; j < i; j++) {
+            double sum = 0.0;
+            for (int k = 0; k < j; k++) sum += W[i + k * n] * W[j + k * n];
+            W[i + j * n] = (W[i + j * n] - sum) / W[j + j * n];
+        }
+        double sum = 0.0;
+        for (int k = 0; k < i; k++) sum += W[i + k * n] * W[i + k * n];
+        const double sq = W[i + i * n] - sum;
+        if (sq < 0.0) return 1;
+        W[i + i * n] = (double)sqrtf((float)sq);
+    }
+    return 0;
+}
+
+// rhs (n x nrhs, column-major, leading dimension nrhs) <- (L L^T)^{-1} rhs (mysolvem, :159-189).
+void chol_solve(const double* L, double* rhs, int n, int nrhs)
+{
+    std::vector<double> y(n);
+    for (int j = 0; j < nrhs; j++) {
+        for (int i = 0; i < n; i++) {
+            double sum = 0.0;
+            for (int k = 0; k < i; k++) sum += L[i + n * k] * y[k];
+            y[i] = (rhs[i + nrhs * j] - sum) / L[i + n * i];
+        }
+        for (int i = n - 1; i >= 0; i--) {
+            double sum = 0.0;
+            for (int k = i + 1; k < n; k++) sum += L[k + n * i] * rhs[k + nrhs * j];
+            rhs[i + nrhs * j] = (y[i] - sum) / L[i + n * i];
+        }
+    }
+}
+
+// alpha (s) and beta (s x s) of one s-step iteration from the moments; W carries the Cholesky
+// factor to the next call. Restates scalarWorkMO (op/scalarWorkMO.cu:191-245, no-LAPACK build).
+int scalar_work(const double* vm, double* W, double* alpha, double* beta, int s, int iter)
+{
+    if (iter == 0) {
+        for (int i = 0; i < s; i++)
+            for (int j = 0; j < s; j++) W[i * s + j] = vm[i + j + 1];
+        if (chol_lower(W, s)) return 1;
+        std::memcpy(alpha, vm, sizeof(double) * s);
+        chol_solve(W, alpha, s, 1);
+        return 0;
+    }
+    std::vector<double> b1(s * s, 0.0), rhs1(2 * s - 1, 0.0);
+    for (int i = 0; i < s; i++) {
+        rhs1[s - 1 + i] = vm[i];
+        for (int j = 0; j < i; j++) rhs1[s - 1 + i] += rhs1[s - 1 + j] * alpha[s - i + j - 1];
+        rhs1[s - 1 + i] = -rhs1[s - 1 + i] / alpha[s - 1];
+    }
+    for (int i = 0; i < s; i++)
+        for (int j = 0; j < s; j++) {
+            b1[i + j * s] = -rhs1[i + j];
+            beta[i + j * s] = -rhs1[i + j];
+        }
+    chol_solve(W, beta, s, s);
+    for (int i = 0; i < s; i++)   // getNewW (:108-124): W = H(vm) - b1^T beta
+        for (int j = 0; j < s; j++) {
+            W[i + s * j] = vm[i + j + 1];
+            for (int k = 0; k < s; k++) W[i + s * j] -= b1[k + s * i] * beta[k + s * j];
+        }
+    if (chol_lower(W, s)) return 1;
+    std::memcpy(alpha, vm, sizeof(double) * s);
+    chol_solve(W, alpha, s, 1);
+    return 0;
+}
+
+// C(:, 0:s) += A(:, 0:s) * B (B s x s column-major); E += f * C(:, 0:s) * D (mydmmv,
+// op/basic.cu:378-462). Column-major n x s blocks.
+void block_update(const double* A, long n, int s, const double* B, double* C, const double* D, double* E, double f)
+{
+#pragma omp parallel for schedule(static)
+    for (long row = 0; row < n; row++) {
+        double e = 0.0;
+        for (int col = 0; col < s; col++) {
+            double ro = C[col * n + row];
+            for (int k = 0; k < s; k++) ro += A[k * n + row] * B[k + s * col];
+            C[col * n + row] = ro;
+            e += ro * D[col];
+        }
+        E[row] += f * e;
+    }
+}
+
+// s-step CG. Restates cgsstep (cgs/CGs.cu:43-224); CGS_CUBLAS (cgs_cublas/CGscublas.cu) and
+// PIPELINED_CGS (pipelined_cgs/pipelinedCGs.cu) compute the same iterates in exact arithmetic.
+// Each outer iteration advances s CG steps; niter counts outer iterations.
+SolveInfo sstep_cg(const Hierarchy& H, const double* b, double* x)
+{
+    const Csr& A = H.lv[0].A;
+    const long n = A.n;
+    const Params& prm = H.prm;
+    const int s = prm.sstep;
+    const bool pre = prm.preconditioner != 0;
+    Work wk = make_work(H);
+    std::vector<double> r(b, b + n), w(n);
+    auto residual = [&] {
+        spmv(A, x, w.data());
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < n; i++) r[i] = -1.0 * w[i] + 1.0 * b[i];
+    };
+    residual();
+    std::vector<double> sP1(n * 2 * s, 0.0), sP2(n * 2 * s, 0.0);
+    std::vector<double> sCP1, sCP2;
+    if (!pre && prm.ru_res) {
+        sCP1.assign(n * s, 0.0);
+        sCP2.assign(n * s, 0.0);
+    }
+    std::vector<double> vm(2 * s), alpha(s, 0.0), beta(s * s, 0.0), W(s * s, 0.0);
+    const double delta0 = prm.stop_criterion == 1 ? std::sqrt(dot(r.data(), r.data(), n)) : 1.0;
+    double l2 = 0.0;
+    int iter, info = 0, excnlim = -1, retv = -1;
+    for (iter = 0; iter < prm.itnlim; iter++) {
+        if (iter > 0 && info == 0 && prm.ru_res && prm.rec_res_int > 0 && iter % prm.rec_res_int == 0) residual();
+        std::vector<double>& cur = (iter % 2 == 0) ? sP2 : sP1;
+        std::vector<double>& old = (iter % 2 == 0) ? sP1 : sP2;
+        mpk(H, wk, r.data(), s, cur);
+        computevm(cur, s, r.data(), n, pre, vm.data());
+        info = scalar_work(vm.data(), W.data(), alpha.data(), beta.data(), s, iter);
+        if (info != 0) {
+            retv = info;
+            break;
+        }
+        std::vector<double>* ccur = nullptr;
+        std::vector<double>* cold = nullptr;
+        if (prm.ru_res && !pre) {
+            ccur = (iter % 2 == 0) ? &sCP2 : &sCP1;
+            cold = (iter % 2 == 0) ? &sCP1 : &sCP2;
+            std::memcpy(ccur->data(), cur.data() + n, sizeof(double) * n * s);
+        }
+        block_update(old.data(), n, s, beta.data(), cur.data(), alpha.data(), x, 1.0);
+        if (prm.ru_res) {
+            if (pre) block_update(old.data() + s * n, n, s, beta.data(), cur.data() + s * n, alpha.data(), r.data(), -1.0);
+            else block_update(cold->data(), n, s, beta.data(), ccur->data(), alpha.data(), r.data(), -1.0);
+        } else {
+            residual();
+        }
+        l2 = std::sqrt(dot(r.data(), r.data(), n));
+        if (l2 < prm.rtol * delta0) {
+            excnlim = 0;
+            retv = 0;
+            break;
+        }
+    }
+    SolveInfo si;
+    si.niter = iter + 1 + excnlim;
+    si.retv = retv;
     si.delta0 = delta0;
     si.exit_res = l2;
     return si;
@@ -1017,9 +1308,12 @@ void orc_vcycle(void* h, const double* r, double* v)
     prec_apply(*H, wk, r, v);
 }
 
+// Solve with the hierarchy's solver: FCG (1), CGHS (0), or the s-step CG for CGS (2),
+// PIPELINED_CGS (3) and CGS_CUBLAS (4), as solve() dispatches (solver/solve.cu:11-51).
 int orc_solve(void* h, const double* b, double* x, int* niter, double* delta0, double* exit_res)
 {
-    SolveInfo si = fcg(*(Hierarchy*)h, b, x);
+    const Hierarchy& H = *(Hierarchy*)h;
+    SolveInfo si = H.prm.solver == 1 ? fcg(H, b, x) : H.prm.solver == 0 ? cghs(H, b, x) : sstep_cg(H, b, x);
     *niter = si.niter;
     *delta0 = si.delta0;
     *exit_res = si.exit_res;

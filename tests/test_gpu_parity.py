@@ -255,10 +255,10 @@ def test_error_paths(bx, cuda):
     with pytest.raises(bx.BcmgxError) as e:
         bx.prec_setup(A.indptr, c, A.data, fcg(bx))
     assert e.value.code == -1
-    # unsupported solver / preconditioner
+    # invalid solver / unsupported preconditioner
     with pytest.raises(bx.BcmgxError) as e:
-        bx.prec_setup(A.indptr, A.indices, A.data, fcg(bx, solver="CGHS"))
-    assert e.value.code == -2
+        bx.prec_setup(A.indptr, A.indices, A.data, fcg(bx, solver=7))
+    assert e.value.code == -1
     with pytest.raises(bx.BcmgxError) as e:
         bx.prec_setup(A.indptr, A.indices, A.data, fcg(bx, preconditioner="AFSAI"))
     assert e.value.code == -2

@@ -87,3 +87,30 @@ def test_hierarchy_shape_50(oracle):
     x, info = H.solve(b)
     assert info["retv"] == 0
     assert np.linalg.norm(x - x_star) / np.linalg.norm(x_star) < 1e-6
+
+
+@pytest.mark.parametrize("solver,s", [("CGHS", 1), ("CGS", 1), ("CGS", 3), ("PIPELINED_CGS", 2)])
+@pytest.mark.parametrize("pre", ["BCMG", "L1_JACOBI", "NONE"])
+def test_oracle_krylov_solvers(oracle, solver, s, pre):
+    """The oracle's CGHS and s-step CG reach rtol 1e-8 on a 7-point Poisson system, agree with a
+    direct solve, and (s = 1) take the iterations of the oracle's FCG: with a symmetric
+    preconditioner the three are the same method."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spl
+    M = oracle.Matrix.lap3d(7, 16, 16, 16, 1, 1, 1)
+    row, col, val = M.csr()
+    A = sp.csr_matrix((val, col, row))
+    n = A.shape[0]
+    b = A @ np.random.default_rng(1).uniform(-1, 1, n)
+    xs = spl.spsolve(A.tocsc(), b)
+    H = oracle.Hierarchy(oracle.Matrix.from_csr(row, col, val), oracle.params(rtol=1e-8, solver=solver,
+                                                                               preconditioner=pre, sstep=s))
+    x, info = H.solve(b)
+    assert info["retv"] == 0
+    assert np.linalg.norm(b - A @ x) < 1e-8 * np.linalg.norm(b)
+    assert np.linalg.norm(x - xs) / np.linalg.norm(xs) < 1e-6
+    if s == 1:
+        Hf = oracle.Hierarchy(oracle.Matrix.from_csr(row, col, val), oracle.params(rtol=1e-8, solver="FCG",
+                                                                                    preconditioner=pre))
+        _, fi = Hf.solve(b)
+        assert abs(fi["niter"] - info["niter"]) <= 1

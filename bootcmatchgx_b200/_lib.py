@@ -85,6 +85,7 @@ SIGNATURES = {
     "bcmgx_batch_free": (C.c_int, [_vp]),
     "bcmgx_hierarchy_get_info": (C.c_int, [_vp, C.POINTER(HierarchyInfo)]),
     "bcmgx_hierarchy_get_level": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),
+    "bcmgx_hierarchy_get_afsai": (C.c_int, [_vp, _i64p, _vp, _vp, _vp]),
     "bcmgx_hierarchy_get_prolongator": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),
     "bcmgx_hierarchy_get_sweep": (C.c_int, [_vp, C.c_int, _ip, _ip, _ip, _ip, _vp, _vp, _vp, _vp]),
     "bcmgx_prec_apply": (C.c_int, [_vp, _vp, _vp, C.c_int]),

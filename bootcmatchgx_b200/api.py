@@ -244,6 +244,16 @@ class Hierarchy:
                 "num_sweep_records": hi.num_sweep_records, "setup_ms": hi.setup_ms,
                 "tpr": list(hi.tpr[:nl])}
 
+    def afsai_factor(self):
+        """The AFSAI factor G (CSR row, col, val) of an AFSAI hierarchy."""
+        z = C.c_int64()
+        check(lib().bcmgx_hierarchy_get_afsai(self.h, C.byref(z), None, None, None), "get_afsai")
+        row = np.empty(self.n + 1, np.int32)
+        col = np.empty(z.value, np.int32)
+        val = np.empty(z.value, np.float64)
+        check(lib().bcmgx_hierarchy_get_afsai(self.h, C.byref(z), _ptr(row), _ptr(col), _ptr(val)), "get_afsai")
+        return row, col, val
+
     def level(self, l):
         inf = self.info()
         n, z = inf["n"][l], inf["nnz"][l]

@@ -63,10 +63,8 @@ static void check_params(const bcmgx_params* p)
     BCMGX_REQUIRE(p->error == 0, BCMGX_ERR_INVALID_INPUT, "settings carry an error flag (unsupported legacy option)");
     BCMGX_REQUIRE(p->solver >= BCMGX_SOLVER_CGHS && p->solver < BCMGX_SOLVER_INVALID, BCMGX_ERR_INVALID_INPUT,
         "invalid solver");
-    BCMGX_REQUIRE(p->preconditioner == BCMGX_PREC_BCMG || p->preconditioner == BCMGX_PREC_NONE ||
-            p->preconditioner == BCMGX_PREC_L1_JACOBI,
-        BCMGX_ERR_UNSUPPORTED, std::string("preconditioner ") + prec_name(p->preconditioner) +
-            " is not implemented (BCMG, L1_JACOBI or NONE)");
+    BCMGX_REQUIRE(p->preconditioner >= BCMGX_PREC_NONE && p->preconditioner < BCMGX_PREC_INVALID, BCMGX_ERR_INVALID_INPUT,
+        "invalid preconditioner");
     if (p->solver == BCMGX_SOLVER_CGS || p->solver == BCMGX_SOLVER_PIPELINED_CGS || p->solver == BCMGX_SOLVER_CGS_CUBLAS)
         BCMGX_REQUIRE(p->sstep >= 1 && p->sstep <= 8, BCMGX_ERR_INVALID_INPUT, "sstep must be 1..8");
     if (p->preconditioner == BCMGX_PREC_L1_JACOBI)
@@ -193,6 +191,9 @@ bcmgx_hierarchy::~bcmgx_hierarchy()
     krylov = nullptr;
     l1d.release();
     l1tmp.release();
+    afsai_G = bcmgx::DevCsr();
+    afsai_GT = bcmgx::DevCsr();
+    afsai_tmp.release();
     lv.clear();
     b.release();
     xv.release();
@@ -485,6 +486,22 @@ int bcmgx_hierarchy_get_level(const bcmgx_hierarchy* h, int l, int* row, int* co
         if (row) BCMGX_CUDA(cudaMemcpyAsync(row, A.row.p, sizeof(int) * ((size_t)A.n + 1), cudaMemcpyDeviceToHost, s));
         if (col) BCMGX_CUDA(cudaMemcpyAsync(col, A.col.p, sizeof(int) * A.nnz, cudaMemcpyDeviceToHost, s));
         if (val) BCMGX_CUDA(cudaMemcpyAsync(val, A.val.p, sizeof(double) * A.nnz, cudaMemcpyDeviceToHost, s));
+        BCMGX_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int bcmgx_hierarchy_get_afsai(const bcmgx_hierarchy* h, int64_t* nnz, int* row, int* col, double* val)
+{
+    return guarded([&] {
+        BCMGX_REQUIRE(h && nnz, BCMGX_ERR_INVALID_INPUT, "NULL argument");
+        BCMGX_REQUIRE(h->prm.preconditioner == BCMGX_PREC_AFSAI, BCMGX_ERR_INVALID_INPUT, "not an AFSAI hierarchy");
+        DeviceScope ds(h->device);
+        const DevCsr& G = h->afsai_G;
+        cudaStream_t s = h->stream;
+        *nnz = G.nnz;
+        if (row) BCMGX_CUDA(cudaMemcpyAsync(row, G.row.p, sizeof(int) * ((size_t)G.n + 1), cudaMemcpyDeviceToHost, s));
+        if (col) BCMGX_CUDA(cudaMemcpyAsync(col, G.col.p, sizeof(int) * G.nnz, cudaMemcpyDeviceToHost, s));
+        if (val) BCMGX_CUDA(cudaMemcpyAsync(val, G.val.p, sizeof(double) * G.nnz, cudaMemcpyDeviceToHost, s));
         BCMGX_CUDA(cudaStreamSynchronize(s));
     });
 }

@@ -191,6 +191,9 @@ struct bcmgx_hierarchy {
     bcmgx::KrylovWork* krylov = nullptr;   // solvers other than FCG
     // standalone l1-Jacobi preconditioner: divisor a_ii + sum_{j != i} |a_ij| and a sweep buffer
     bcmgx::DBuf<double> l1d, l1tmp;
+    // AFSAI preconditioner: the factor G of the scaled matrix, its transpose, and G r
+    bcmgx::DevCsr afsai_G, afsai_GT;
+    bcmgx::DBuf<double> afsai_tmp;
     ~bcmgx_hierarchy();
 };
 
@@ -230,6 +233,9 @@ void ensure_solve_workspace(bcmgx_hierarchy* H);
 int fcg_solve(bcmgx_hierarchy* H, const double* b_dev, double* x_dev, bcmgx_solve_info* info);
 void prec_apply_dev(bcmgx_hierarchy* H, const double* r, double* v);
 void prec_apply_impl(bcmgx_hierarchy* H, const double* r, double* v, const int* skip);
+// AFSAI preconditioner (afsai.cu): set-up of G and G^T, application v = G^T G r.
+void afsai_build_dev(bcmgx_hierarchy* H);
+void afsai_apply(bcmgx_hierarchy* H, const double* r, double* v, const int* skip);
 // CGHS or the s-step CG (krylov.cu), for every solver but FCG.
 int krylov_solve(bcmgx_hierarchy* H, const double* b, double* x, bcmgx_solve_info* info);
 // FP64 row operations on level-0-like matrices with the autotuned shape; skip: see k_rowop.

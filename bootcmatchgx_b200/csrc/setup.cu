@@ -166,7 +166,7 @@ __global__ void k_scan_down(const int* __restrict__ in, int* __restrict__ out, l
 
 // Exclusive prefix sum of in[0..n) into out[0..n); when with_total, out[n] = total.
 // Returns the total (synchronises the stream).
-static long long scan_exclusive(const int* in, int* out, long n, bool with_total, cudaStream_t s)
+long long scan_exclusive(const int* in, int* out, long n, bool with_total, cudaStream_t s)
 {
     const int ntiles = std::max(1, (int)((n + kScanTile - 1) / kScanTile));
     DBuf<long long> tiles, tot;
@@ -1007,6 +1007,7 @@ void build_hierarchy(bcmgx_hierarchy* H, const bcmgx_csr* Ain)
     H->ftcoarse = 1;
     // AMG::BuildData::setMaxCoarseSize, AMG.cu:238-241
     H->maxcoarsesize = (int)(40 * std::pow((double)L0n, 1.0 / 3.0));
+    if (P.preconditioner == BCMGX_PREC_AFSAI) afsai_build_dev(H);
     if (P.preconditioner == BCMGX_PREC_L1_JACOBI) {
         H->l1d.alloc(L0n, s);
         note_launch(); k_l1_divisor<<<gs_grid(L0n), 256, 0, s>>>(L0n, A.row.p, A.col.p, A.val.p, H->l1d.p);

@@ -496,6 +496,10 @@ void prec_apply_impl(bcmgx_hierarchy* H, const double* r, double* v, const int* 
         l1jacobi_apply(H, r, v, skip);
         return;
     }
+    if (H->prm.preconditioner == BCMGX_PREC_AFSAI) {
+        afsai_apply(H, r, v, skip);
+        return;
+    }
     if (H->prm.preconditioner != BCMGX_PREC_BCMG) {
         note_launch();
         auto k = k_convert<double, double>;

@@ -158,6 +158,10 @@ int bcmgx_solve_adjoint(bcmgx_hierarchy* h, const double* g, const double* x, do
 int bcmgx_free(bcmgx_hierarchy* h);
 
 int bcmgx_hierarchy_get_info(const bcmgx_hierarchy* h, bcmgx_hierarchy_info* info);
+/* The AFSAI factor G of an AFSAI hierarchy (the preconditioner is G^T G): *nnz is set; the
+ * n + 1 row offsets, columns and values are copied to the host arrays that are not NULL.
+ * Inspection of afsai_setup's Aprec (preconditioner/afsai/afsai.cu:1016-1019). */
+int bcmgx_hierarchy_get_afsai(const bcmgx_hierarchy* h, int64_t* nnz, int* row, int* col, double* val);
 /* Copies level l's matrix to host arrays sized from bcmgx_hierarchy_get_info. */
 int bcmgx_hierarchy_get_level(const bcmgx_hierarchy* h, int l, int* row, int* col, double* val);
 /* Copies level l's composite prolongator (column agg[i], value p[i] of row i; l < levels-1) and

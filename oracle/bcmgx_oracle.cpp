@@ -99,6 +99,7 @@ struct Hierarchy {
     double op_cmplx = 0, op_wcmplx = 0, avg_cratio = 1;
     std::vector<int> grid_sweeps;
     std::vector<double> l1d;   // standalone l1-Jacobi divisor a_ii + sum_{j != i} |a_ij| (L1_JACOBI)
+    Csr G, GT;                 // AFSAI factor and its transpose (AFSAI)
 };
 
 // ------------------------------------------------------------------------------------------
@@ -535,6 +536,204 @@ void build_restriction(Level& L, int nc)
     }
 }
 
+// ---- AFSAI (adaptive factorized sparse approximate inverse) ---------------------------------
+// Restates afsai_setup (preconditioner/afsai/afsai.cu:287-1090) at np = 1 with its kernels
+// (kapGradCUDA_WiP.cu, d_gFSA.cu, choldc.cu, scalar_product_atomicAdd.h): 30 steps of one new
+// entry per row of the lower-triangular factor G of the diagonally scaled matrix, chosen by the
+// largest |gradient| (ties: the smallest column), each step solving the row's small SPD system
+// (packed U^T U Cholesky, cudacholdcMix); a row stops when its Kaporin term changes by less than
+// 1e-3 relative or stops growing. Applied as v = G^T (G r) (afsai_apply, :1092-1103).
+constexpr int kAfsaiSteps = 30;
+constexpr double kAfsaiEps = 0.001;
+
+// solve U^T U x = b in place of b, U upper-packed (column j holds rows 0..j) with the diagonal
+// stored inverted; false when a pivot is not positive (cudacholdcMix, choldc.cu)
+bool afsai_chol_solve(double* l, double* x, int n)
+{
+    int ooffi = 0;
+    for (int i = 0; i < n; i++) {
+        int ooffj = ooffi;
+        for (int j = i; j < n; j++) {
+            double sum = l[i + ooffj];
+            for (int k = 0; k < i; k++) sum -= l[ooffi + k] * l[ooffj + k];
+            if (i == j) {
+                if (sum <= 0.0) return false;
+                l[ooffj + i] = 1. / std::sqrt(sum);
+            } else {
+                l[ooffj + i] = sum * l[ooffi + i];
+            }
+            ooffj += (j + 1);
+        }
+        ooffi += (i + 1);
+    }
+    ooffi = 0;
+    for (int i = 0; i < n; i++) {
+        double sum = x[i];
+        for (int j = i - 1; j >= 0; j--) sum -= l[ooffi + j] * x[j];
+        x[i] = sum * l[ooffi + i];
+        ooffi += (i + 1);
+    }
+    ooffi = n * (n - 1) / 2;
+    for (int i = n - 1; i >= 0; i--) {
+        double sum = x[i];
+        int ooffj = ooffi + i;
+        for (int j = i + 1; j < n; j++) {
+            sum -= l[ooffj + i + 1] * x[j];
+            ooffj += (j + 1);
+        }
+        x[i] = sum * l[ooffi + i];
+        ooffi -= i;
+    }
+    return true;
+}
+
+// One row of G: pattern cols (ascending, all < i) and coefficients, plus the Kaporin term.
+void afsai_row(const Csr& S, int i, std::vector<int>& iwn, std::vector<double>& x, double& dk)
+{
+    iwn.clear();
+    x.clear();
+    dk = 0.0;
+    double dk_old = 0.0;
+    std::vector<double> M, b;
+    for (int step = 0; step < kAfsaiSteps; step++) {
+        const int m = (int)iwn.size();
+        // gradient g_c = S(i, c) + sum_k x_k S(iwn_k, c) over columns c < i; merge of sorted rows
+        std::vector<int> pos(m + 1), end(m + 1), rows(m + 1);
+        std::vector<double> fac(m + 1);
+        rows[0] = i;
+        fac[0] = 1.0;
+        for (int k = 0; k < m; k++) {
+            rows[k + 1] = iwn[k];
+            fac[k + 1] = x[k];
+        }
+        for (int k = 0; k <= m; k++) {
+            pos[k] = S.row[rows[k]];
+            end[k] = S.row[rows[k] + 1];
+        }
+        int best = -1, iw = 0;
+        double bestv = 0.0;
+        for (;;) {
+            int c = INT32_MAX;
+            for (int k = 0; k <= m; k++)
+                if (pos[k] < end[k] && S.col[pos[k]] < c) c = S.col[pos[k]];
+            if (c >= i) break;
+            double g = 0.0;
+            for (int k = 0; k <= m; k++)
+                if (pos[k] < end[k] && S.col[pos[k]] == c) {
+                    g += S.val[pos[k]] * fac[k];
+                    pos[k]++;
+                }
+            while (iw < m && iwn[iw] < c) iw++;
+            if (iw < m && iwn[iw] == c) continue;   // already in the pattern
+            if (std::fabs(g) > bestv) {
+                bestv = std::fabs(g);
+                best = c;
+            }
+        }
+        if (best < 0) break;   // no new entry: the row is done
+        iwn.insert(std::lower_bound(iwn.begin(), iwn.end(), best), best);
+        const int n = m + 1;
+        // the row's system: M = S(iwn, iwn) upper-packed, b = -S(i, iwn)
+        M.assign(n * (n + 1) / 2, 0.0);
+        b.assign(n, 0.0);
+        for (int r = 0; r < n; r++) {
+            const int row = iwn[r];
+            int jj = S.row[row];
+            const int je = S.row[row + 1];
+            for (int cidx = r; cidx < n; cidx++) {
+                while (jj < je && S.col[jj] < iwn[cidx]) jj++;
+                if (jj == je) break;
+                if (S.col[jj] == iwn[cidx]) M[cidx * (cidx + 1) / 2 + r] = S.val[jj];
+            }
+        }
+        for (int jj = S.row[i], r = 0; jj < S.row[i + 1] && r < n && S.col[jj] < i;) {
+            if (iwn[r] > S.col[jj]) jj++;
+            else if (iwn[r] == S.col[jj]) { b[r] = -S.val[jj]; jj++; r++; }
+            else r++;
+        }
+        x = b;
+        if (!afsai_chol_solve(M.data(), x.data(), n)) {   // not reached for SPD matrices
+            x.assign(n, 0.0);
+            dk = 0.0;
+            break;
+        }
+        double d = 0.0;
+        for (int k = 0; k < n; k++) d += b[k] * x[k];
+        dk = d;
+        const bool conv = std::fabs(dk - dk_old) < kAfsaiEps * dk_old || dk == 0.0;
+        dk_old = dk;
+        if (conv) break;
+    }
+}
+
+// G (lower triangular, diagonal last in each row) of the scaled matrix
+Csr afsai_build(const Csr& A)
+{
+    const int n = A.n;
+    std::vector<double> d(n);
+    for (int i = 0; i < n; i++)
+        for (int j = A.row[i]; j < A.row[i + 1]; j++)
+            if (A.col[j] == i) d[i] = 1.0 / std::sqrt(A.val[j]);
+    Csr S = A;
+    std::vector<double> sdiag(n, 0.0);
+    for (int i = 0; i < n; i++)
+        for (int j = A.row[i]; j < A.row[i + 1]; j++) {
+            S.val[j] = (A.val[j] * d[A.col[j]]) * d[i];
+            if (A.col[j] == i) sdiag[i] = S.val[j];
+        }
+    std::vector<std::vector<int>> cols(n);
+    std::vector<std::vector<double>> vals(n);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int i = 0; i < n; i++) {
+        std::vector<int> iwn;
+        std::vector<double> x;
+        double dk;
+        afsai_row(S, i, iwn, x, dk);
+        const double sf = sdiag[i] - dk;
+        if (sf > 0.0) {
+            const double s = 1.0 / std::sqrt(sf);
+            for (size_t k = 0; k < iwn.size(); k++) {
+                cols[i].push_back(iwn[k]);
+                vals[i].push_back(s * x[k]);
+            }
+            cols[i].push_back(i);
+            vals[i].push_back(s);
+        } else {
+            cols[i].push_back(i);
+            vals[i].push_back(1.0);
+        }
+    }
+    Csr G;
+    G.n = G.m = n;
+    G.row.assign(n + 1, 0);
+    for (int i = 0; i < n; i++) G.row[i + 1] = G.row[i] + (int)cols[i].size();
+    for (int i = 0; i < n; i++) {
+        G.col.insert(G.col.end(), cols[i].begin(), cols[i].end());
+        G.val.insert(G.val.end(), vals[i].begin(), vals[i].end());
+    }
+    return G;
+}
+
+Csr transpose(const Csr& G)
+{
+    Csr T;
+    T.n = G.m;
+    T.m = G.n;
+    T.row.assign(T.n + 1, 0);
+    for (int c : G.col) T.row[c + 1]++;
+    for (int i = 0; i < T.n; i++) T.row[i + 1] += T.row[i];
+    T.col.resize(G.col.size());
+    T.val.resize(G.col.size());
+    std::vector<int> fill(T.row.begin(), T.row.end() - 1);
+    for (int i = 0; i < G.n; i++)
+        for (int j = G.row[i]; j < G.row[i + 1]; j++) {
+            const int t = fill[G.col[j]]++;
+            T.col[t] = i;
+            T.val[t] = G.val[j];
+        }
+    return T;
+}
+
 // Hierarchy construction. Restates bcmg_setup (bcmg.cu:12-49) -> Bootstrap::bootstrap with one
 // hierarchy (bootstrap.cu:11-46) -> adaptiveCoarsening (matchingAggregation.cu:287-466) ->
 // matchingAggregation (matchingAggregation.cu:106-269), with the parameters of
@@ -560,6 +759,10 @@ Hierarchy* build(const Csr& A0, const Params& prm, bool record)
             }
             H->l1d[i] = d + off;
         }
+    }
+    if (prm.preconditioner == 3) {
+        H->G = afsai_build(A0);
+        H->GT = transpose(H->G);
     }
     if (prm.preconditioner != 2) return H;
     const int sweepnumber = prm.aggrsweeps + 1;
@@ -705,6 +908,12 @@ void prec_apply(const Hierarchy& H, Work& wk, const double* r, double* v)
         // l1jacobi_apply (l1jacobi.cu:513-523): l1jacsweeps sweeps from v (zero at every call site)
         std::vector<double> tmp(n);
         l1jacobi(H.prm.l1jacsweeps, H.lv[0].A, H.l1d, r, v, tmp.data());
+        return;
+    }
+    if (H.prm.preconditioner == 3) {
+        std::vector<double> t(n);
+        spmv(H.G, r, t.data());
+        spmv(H.GT, t.data(), v);
         return;
     }
     if (H.prm.preconditioner != 2) {
@@ -1228,6 +1437,9 @@ void* orc_setup(void* h, const orc_params* p, int record)
 }
 
 void orc_hier_free(void* h) { delete (Hierarchy*)h; }
+
+// The AFSAI factor G (n rows) of an AFSAI hierarchy; row/col/val sized from orc_matrix_info.
+void* orc_hier_afsai(void* h) { return &((Hierarchy*)h)->G; }
 
 int orc_hier_levels(void* h) { return (int)((Hierarchy*)h)->lv.size(); }
 

@@ -66,6 +66,8 @@ def lib():
         L.orc_hier_level_info.argtypes = [vp, C.c_int, ip, C.POINTER(C.c_long)]
         L.orc_hier_level_matrix.restype = vp
         L.orc_hier_level_matrix.argtypes = [vp, C.c_int]
+        L.orc_hier_afsai.restype = vp
+        L.orc_hier_afsai.argtypes = [vp]
         L.orc_hier_level_prolongator.argtypes = [vp, C.c_int, vp, vp, vp]
         L.orc_hier_num_records.argtypes = [vp]
         L.orc_hier_record.argtypes = [vp, C.c_int, ip, ip, ip, ip]
@@ -222,6 +224,10 @@ class Hierarchy:
         v = np.zeros_like(r)
         lib().orc_vcycle(self.h, _p(r), _p(v))
         return v
+
+    def afsai_factor(self):
+        """The AFSAI factor G of an AFSAI hierarchy as CSR arrays."""
+        return Matrix(lib().orc_hier_afsai(self.h), owned=False).csr()
 
     def solve(self, b, x0=None):
         b = np.ascontiguousarray(b, dtype=np.float64)

@@ -1,6 +1,6 @@
 """The reference's other Krylov solvers (CGHS, the s-step CG behind CGS / PIPELINED_CGS /
-CGS_CUBLAS) and the standalone l1-Jacobi preconditioner, against the oracle's restatements of
-cghs/CG_HS.cu, cgs/CGs.cu and l1jacobi/l1jacobi.cu."""
+CGS_CUBLAS) and preconditioners (standalone l1-Jacobi, AFSAI), against the oracle's
+restatements of cghs/CG_HS.cu, cgs/CGs.cu, l1jacobi/l1jacobi.cu and afsai/afsai.cu."""
 import numpy as np
 import pytest
 
@@ -21,7 +21,7 @@ def _oracle_params(oracle, **kw):
 
 
 @pytest.mark.parametrize("case", [("lap7", (20, 20, 20)), ("lap27", (14, 14, 14)), ("diff", (16, 2))])
-@pytest.mark.parametrize("pre", ["BCMG", "L1_JACOBI", "NONE"])
+@pytest.mark.parametrize("pre", ["BCMG", "L1_JACOBI", "AFSAI", "NONE"])
 @pytest.mark.parametrize("solver,s", SOLVERS)
 def test_solver_matches_oracle(bx, oracle, cuda, case, pre, solver, s):
     """Status, iterations within +-1 (2 % for runs of hundreds of unpreconditioned iterations,
@@ -106,9 +106,34 @@ def test_graph_and_stream_drivers_agree(bx, cuda, solver, s, pre):
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][2], out[1][2])
 
 
+@pytest.mark.parametrize("case", [("lap7", (12, 12, 12)), ("lap27", (10, 9, 8)), ("diff", (12, 2)),
+                                  ("rand", (2000, 0.004, 8))])
+def test_afsai_factor_bit_exact(bx, oracle, cuda, case):
+    """The AFSAI factor G (pattern and values) equals the oracle's restatement bit for bit:
+    every step is separately rounded on both sides, and ties in the gradient go to the smallest
+    column on both. Its application G^T G r agrees to rounding."""
+    A = as_csr(bx, case)
+    kw = dict(solver="FCG", preconditioner="AFSAI")
+    h = bx.prec_setup(A.indptr, A.indices, A.data, _params(bx, **kw))
+    Ho = oracle.Hierarchy(oracle.Matrix.from_csr(A.indptr, A.indices, A.data), _oracle_params(oracle, **kw))
+    row, col, val = h.afsai_factor()
+    ro, co, vo = Ho.afsai_factor()
+    assert np.array_equal(row, ro) and np.array_equal(col, co)
+    assert np.array_equal(val, vo)
+    assert (np.diff(row) <= 31).all() and (np.diff(row) >= 1).all()
+    r = np.random.default_rng(9).uniform(-1, 1, A.shape[0])
+    v, vo_ = h.prec_apply(r), Ho.vcycle(r)
+    assert np.linalg.norm(v - vo_) / np.linalg.norm(vo_) < 1e-13
+
+
 def test_solver_parameter_errors(bx, cuda):
     A = as_csr(bx, ("lap7", (6, 6, 6)))
-    for kw, code in ((dict(preconditioner="AFSAI"), -2), (dict(solver="CGS", sstep=9), -1),
+    B = A.copy()
+    B.data[B.indices == np.repeat(np.arange(B.shape[0]), np.diff(B.indptr))] *= -1.0
+    with pytest.raises(bx.BcmgxError) as e:
+        bx.prec_setup(B.indptr, B.indices, B.data, _params(bx, preconditioner="AFSAI"))
+    assert e.value.code == -1 and "diagonal" in str(e.value)
+    for kw, code in ((dict(preconditioner=9), -1), (dict(solver="CGS", sstep=9), -1),
                      (dict(solver="CGS", sstep=0), -1), (dict(preconditioner="L1_JACOBI", l1jacsweeps=0), -1)):
         with pytest.raises(bx.BcmgxError) as e:
             bx.prec_setup(A.indptr, A.indices, A.data, _params(bx, **kw))

@@ -260,8 +260,8 @@ def test_error_paths(bx, cuda):
         bx.prec_setup(A.indptr, A.indices, A.data, fcg(bx, solver=7))
     assert e.value.code == -1
     with pytest.raises(bx.BcmgxError) as e:
-        bx.prec_setup(A.indptr, A.indices, A.data, fcg(bx, preconditioner="AFSAI"))
-    assert e.value.code == -2
+        bx.prec_setup(A.indptr, A.indices, A.data, fcg(bx, preconditioner=9))
+    assert e.value.code == -1
     # itnlim reached: status NO_CONVERGENCE, retv -1 as SolverOut
     h = bx.prec_setup(A.indptr, A.indices, A.data, fcg(bx, rtol=1e-14, itnlim=2))
     x, info = h.solve(np.ones(n))

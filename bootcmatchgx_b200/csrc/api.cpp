@@ -3,6 +3,8 @@
 #include "internal.h"
 
 #include <atomic>
+#include <map>
+#include <mutex>
 #include <thread>
 #include <cstdlib>
 #include <cmath>
@@ -92,6 +94,36 @@ static int solve_dispatch(bcmgx_hierarchy* h, const double* b, double* x, bcmgx_
     return h->prm.solver == BCMGX_SOLVER_FCG ? fcg_solve(h, b, x, info) : krylov_solve(h, b, x, info);
 }
 
+static std::mutex g_pin_mu;
+static std::multimap<size_t, void*> g_pin_free;
+constexpr size_t kPinHeader = 64;   // the block's size, stored in front of the returned pointer
+
+void* pinned_alloc(size_t bytes)
+{
+    const size_t b = (bytes + 63) & ~(size_t)63;
+    {
+        std::lock_guard<std::mutex> g(g_pin_mu);
+        auto it = g_pin_free.find(b);
+        if (it != g_pin_free.end()) {
+            void* p = it->second;
+            g_pin_free.erase(it);
+            return p;
+        }
+    }
+    void* base = nullptr;
+    BCMGX_CUDA(cudaMallocHost(&base, b + kPinHeader));
+    *(size_t*)base = b;
+    return (char*)base + kPinHeader;
+}
+
+void pinned_free(void* p)
+{
+    if (!p) return;
+    const size_t b = *(size_t*)((char*)p - kPinHeader);
+    std::lock_guard<std::mutex> g(g_pin_mu);
+    g_pin_free.emplace(b, p);
+}
+
 // Builds one hierarchy (the body of bcmgx_setup). own_stream forces a library-owned stream even
 // when params name one (batch set-ups run concurrently, one stream each).
 static bcmgx_hierarchy* setup_one(const bcmgx_csr* A, const bcmgx_params* p, int device, bool own_stream)
@@ -173,8 +205,8 @@ bcmgx_batch::~bcmgx_batch()
     states_ptr.release();
     states.release();
     if (stream) cudaStreamSynchronize(stream);
-    if (states_host) cudaFreeHost(states_host);
-    if (copies_host) cudaFreeHost(copies_host);
+    bcmgx::pinned_free(states_host);
+    bcmgx::pinned_free(copies_host);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (own)
@@ -210,7 +242,7 @@ bcmgx_hierarchy::~bcmgx_hierarchy()
     gb.release();
     gx.release();
     if (stream) cudaStreamSynchronize(stream);
-    if (st_host) cudaFreeHost(st_host);
+    bcmgx::pinned_free(st_host);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     for (auto& e : ev_it)

@@ -23,6 +23,11 @@ struct Error : std::exception {
 };
 
 void set_last_error(const std::string& s);
+// Page-locked host blocks for the small host mirrors of device state. Released blocks are kept
+// for reuse until the process exits: returning page-locked memory to the system can stall the
+// calling thread for a long time, and solves are often set up and torn down repeatedly.
+void* pinned_alloc(size_t bytes);
+void pinned_free(void* p);
 // counts every kernel launch of the library (reported by bcmgx_launch_count)
 void note_launch();
 void note_launches(long long k);
@@ -99,6 +104,7 @@ struct DevCsr {
     DBuf<int> row, col;
     DBuf<double> val;
     DBuf<float> val32;
+    DBuf<short> dcol; // col - row as int16 when every entry is within 32767 of the diagonal, else empty
     int tpr = 0;      // threads per row for SpMV / smoother (autotuned)
 };
 

@@ -343,7 +343,7 @@ struct KrylovWork {
     ~KrylovWork()
     {
         if (graph) cudaGraphExecDestroy(graph);
-        if (st_host) cudaFreeHost(st_host);
+        pinned_free(st_host);
     }
 };
 
@@ -379,7 +379,7 @@ KrylovWork& krylov_work(bcmgx_hierarchy* H)
     }
     wk.part.alloc((size_t)num_sms() * kBlocksPerSM * 2 * kMaxS, s);
     wk.st.alloc(1, s);
-    BCMGX_CUDA(cudaMallocHost((void**)&wk.st_host, 2 * sizeof(KryState)));
+    wk.st_host = (KryState*)pinned_alloc(2 * sizeof(KryState));
     return wk;
 }
 

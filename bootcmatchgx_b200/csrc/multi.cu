@@ -276,7 +276,7 @@ struct MultiWork {
     ~MultiWork()
     {
         if (graph) cudaGraphExecDestroy(graph);
-        if (st_host) cudaFreeHost(st_host);
+        pinned_free(st_host);
     }
 };
 
@@ -336,7 +336,7 @@ void ensure_multi(bcmgx_hierarchy* H, MultiWork& wk, int K)
     wk.Q.alloc(nk, s);
     wk.part.alloc((size_t)num_sms() * kBlkBlocksPerSM * 3 * 32, s);
     wk.st.alloc(1, s);
-    if (!wk.st_host) BCMGX_CUDA(cudaMallocHost((void**)&wk.st_host, 2 * sizeof(BlockState)));
+    if (!wk.st_host) wk.st_host = (BlockState*)pinned_alloc(2 * sizeof(BlockState));
 }
 
 // grid of a row-slot SpMM kernel over n rows (at most kBlkBlocksPerSM blocks per SM: the size

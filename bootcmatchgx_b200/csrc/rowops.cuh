@@ -11,11 +11,17 @@ namespace bcmgx {
 
 enum RowOp { OP_AXPBY = 0, OP_RESID = 1, OP_JACOBI = 2 };
 
+// Column index of entry j: int32 columns as stored, or int16 offsets from the row (a level whose
+// entries all lie within 32767 of the diagonal keeps this compact copy of its columns, which
+// cuts the index stream of every row kernel in half).
+__device__ __forceinline__ int col_at(const int* __restrict__ col, int j, int) { return ld_stream(col + j); }
+__device__ __forceinline__ int col_at(const short* __restrict__ dcol, int j, int r) { return r + (int)__ldcs(dcol + j); }
+
 // Partial dot product of one row over the lanes of a sub-warp. Entries are taken in batches of
 // K per lane: all K column and value loads are issued, then all K gathers of x, then the K
 // multiply-adds, so a row of up to K*S entries costs one round of memory latency per lane.
-template <int S, typename AT, typename VT, typename XT>
-__device__ __forceinline__ AT row_partial(int b, int e, int lane, const int* __restrict__ col,
+template <int S, typename AT, typename VT, typename XT, typename IT>
+__device__ __forceinline__ AT row_partial(int b, int e, int lane, int r, const IT* __restrict__ col,
     const VT* __restrict__ val, const XT* __restrict__ x)
 {
     constexpr int K = 8;
@@ -27,7 +33,7 @@ __device__ __forceinline__ AT row_partial(int b, int e, int lane, const int* __r
 #pragma unroll
         for (int k = 0; k < K; k++) {
             const int j = j0 + k * S;
-            c[k] = j < e ? ld_stream(col + j) : -1;
+            c[k] = j < e ? col_at(col, j, r) : -1;
             v[k] = j < e ? ld_stream(val + j) : VT(0);
         }
 #pragma unroll
@@ -41,8 +47,8 @@ __device__ __forceinline__ AT row_partial(int b, int e, int lane, const int* __r
 // y = alpha*A*x + beta*y (OP_AXPBY), y = f - A*x (OP_RESID) or one l1-Jacobi sweep
 // y = ((f - A*x) / M) + x (OP_JACOBI, the update of _jacobi_it_full<0>, l1jacobi.cu:345-379).
 // Grid-stride over rows; all lanes of a sub-warp stay converged for the shuffles.
-template <int S, int OP, typename VT, typename XT, typename FT, typename MT, typename YT>
-__global__ void __launch_bounds__(256) k_rowop(int n, const int* __restrict__ row, const int* __restrict__ col,
+template <int S, int OP, typename VT, typename XT, typename FT, typename MT, typename YT, typename IT>
+__global__ void __launch_bounds__(256) k_rowop(int n, const int* __restrict__ row, const IT* __restrict__ col,
     const VT* __restrict__ val, const XT* __restrict__ x, const FT* __restrict__ f, const MT* __restrict__ M,
     YT* __restrict__ y, double alpha, double beta, const int* __restrict__ skip)
 {
@@ -56,7 +62,7 @@ __global__ void __launch_bounds__(256) k_rowop(int n, const int* __restrict__ ro
         const long r0 = base + sub;
         const int r = (int)r0;
         AT s = 0;
-        if (r0 < n) s = row_partial<S, AT>(__ldg(row + r), __ldg(row + r + 1), lane, col, val, x);
+        if (r0 < n) s = row_partial<S, AT>(__ldg(row + r), __ldg(row + r + 1), lane, r, col, val, x);
         s = subwarp_sum<S>(s);
         if (r0 < n && lane == 0) {
             if (OP == OP_AXPBY) {

@@ -387,6 +387,27 @@ __global__ void k_rank(int n, const int* __restrict__ row, const int* __restrict
     const int lane = threadIdx.x & 31;
     for (long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32; r < n; r += (long)gridDim.x * blockDim.x / 32) {
         const int b = row[r], e = row[r + 1];
+        if (e - b <= 32) {
+            // the whole row in registers (lane = entry): ranks by shuffles, no reloads
+            const int t = b + lane;
+            const bool in = t < e;
+            const int ct = in ? col[t] : -1;
+            const double wt = in ? W[t] : 0.0;
+            const bool el = in && ct != r && wt > 0.0;
+            const unsigned elig = __ballot_sync(0xffffffffu, el);
+            int rk = 0;
+            for (int k = 0; k < e - b; k++) {
+                const int ck = __shfl_sync(0xffffffffu, ct, k);
+                const double wk = __shfl_sync(0xffffffffu, wt, k);
+                rk += (((elig >> k) & 1u) && (wk > wt || (wk == wt && ck > ct))) ? 1 : 0;
+            }
+            if (in) {
+                rank[t] = el ? rk : -1;
+                if (el) ordj[b + rk] = t;
+            }
+            if (lane == 0) degE[r] = __popc(elig);
+            continue;
+        }
         int cnt = 0;
         for (int t0 = b; t0 < e; t0 += 32) {
             const int t = t0 + lane;
@@ -569,8 +590,8 @@ __global__ void k_make_p(int n, const int* __restrict__ M, const double* __restr
 // sort by key, each group of equal J is (AP)_{f0,J} = sum of its f0 terms and (AP)_{f1,J}
 // likewise (<= 2 terms each), and C_IJ = p_f0 (AP)_{f0,J} + p_f1 (AP)_{f1,J}: the values
 // nsparse forms for A*P and then R*(AP) (kernel_spgemm_hash_d.cu:792-799), since a sum of at most
-// two rounded terms does not depend on their order. FILL = false counts the entries of row I.
-template <bool FILL>
+// two rounded terms does not depend on their order. Row I is written at I * cap (padded) and its
+// length at Crow[I]; a compaction then forms the CSR matrix.
 __global__ void k_galerkin(int nc, const int* __restrict__ fine0, const int* __restrict__ fine1, const int* __restrict__ agg,
     const double* __restrict__ p, const int* __restrict__ Arow, const int* __restrict__ Acol, const double* __restrict__ Aval,
     int* __restrict__ Crow, int* __restrict__ Ccol, double* __restrict__ Cval, int cap, int* err)
@@ -605,7 +626,7 @@ __global__ void k_galerkin(int nc, const int* __restrict__ fine0, const int* __r
         }
         __syncwarp();
         const double p0 = p[f0], p1 = f1 >= 0 ? p[f1] : 0.0;
-        const int outbase = FILL ? Crow[I] : 0;
+        const long outbase = (long)I * cap;
         int nheads = 0;
         for (int base = 0; base < cnt; base += 32) {
             const int s = base + lane;
@@ -616,7 +637,7 @@ __global__ void k_galerkin(int nc, const int* __restrict__ fine0, const int* __r
                 head = (s == 0) || ((int)(key[sidx[s - 1]] >> 32) != J);
             }
             const unsigned hm = __ballot_sync(0xffffffffu, head);
-            if (FILL && head) {
+            if (head) {
                 double ap0 = 0.0, ap1 = 0.0;
                 int n0 = 0, n1 = 0;
                 for (int g = s; g < cnt; g++) {
@@ -635,14 +656,28 @@ __global__ void k_galerkin(int nc, const int* __restrict__ fine0, const int* __r
                 if (n0 && n1) cv = __dadd_rn(__dmul_rn(p0, ap0), __dmul_rn(p1, ap1));
                 else if (n0) cv = __dmul_rn(p0, ap0);
                 else cv = __dmul_rn(p1, ap1);
-                const int o = outbase + nheads + __popc(hm & ((1u << lane) - 1u));
+                const long o = outbase + nheads + __popc(hm & ((1u << lane) - 1u));
                 Ccol[o] = J;
                 Cval[o] = cv;
             }
             nheads += __popc(hm);
         }
-        if (!FILL && lane == 0) Crow[I] = nheads;
+        if (lane == 0) Crow[I] = nheads;
         __syncwarp();
+    }
+}
+
+// padded rows (I * cap) -> CSR; one warp per row
+__global__ void k_compact_rows(int nc, int cap, const int* __restrict__ rowptr, const int* __restrict__ pcol,
+    const double* __restrict__ pval, int* __restrict__ col, double* __restrict__ val)
+{
+    const int lane = threadIdx.x & 31;
+    for (long I = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32; I < nc; I += (long)gridDim.x * blockDim.x / 32) {
+        const int b = rowptr[I], len = rowptr[I + 1] - b;
+        for (int t = lane; t < len; t += 32) {
+            col[b + t] = pcol[I * (long)cap + t];
+            val[b + t] = pval[I * (long)cap + t];
+        }
     }
 }
 
@@ -895,33 +930,69 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
         "coarse row too long for the Galerkin kernel (" + std::to_string(cap) + " candidate entries)");
     int wpb = (int)std::min<size_t>(8, std::max<size_t>(1, (48 * 1024) / per_warp));
     size_t smem = per_warp * wpb;
-    if (smem > 48 * 1024) {
-        BCMGX_CUDA(cudaFuncSetAttribute(k_galerkin<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        BCMGX_CUDA(cudaFuncSetAttribute(k_galerkin<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    }
+    if (smem > 48 * 1024)
+        BCMGX_CUDA(cudaFuncSetAttribute(k_galerkin, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int g = (int)std::max<long>(1, std::min<long>(((long)nc + wpb - 1) / wpb, (long)num_sms() * 32));
     DevCsr& C = out.C;
     C.n = C.m = nc;
     C.row.alloc((size_t)nc + 1, s);
-    DBuf<int> counts;
+    // one pass into padded rows (cap entries each), then prefix sum and compaction
+    DBuf<int> counts, pcol;
+    DBuf<double> pval;
     counts.alloc(std::max(nc, 1), s);
-    note_launch(); k_galerkin<false><<<g, wpb * 32, smem, s>>>(nc, fine0.p, fine1.p, out.agg.p, out.p.p, A.row.p, A.col.p, A.val.p,
-        counts.p, nullptr, nullptr, cap, err.p);
+    pcol.alloc(std::max<size_t>((size_t)nc * cap, 1), s);
+    pval.alloc(std::max<size_t>((size_t)nc * cap, 1), s);
+    note_launch(); k_galerkin<<<g, wpb * 32, smem, s>>>(nc, fine0.p, fine1.p, out.agg.p, out.p.p, A.row.p, A.col.p, A.val.p,
+        counts.p, pcol.p, pval.p, cap, err.p);
     BCMGX_CHECK_LAUNCH();
     C.nnz = scan_exclusive(counts.p, C.row.p, nc, true, s);
     C.col.alloc(std::max<int64_t>(C.nnz, 1), s);
     C.val.alloc(std::max<int64_t>(C.nnz, 1), s);
-    note_launch(); k_galerkin<true><<<g, wpb * 32, smem, s>>>(nc, fine0.p, fine1.p, out.agg.p, out.p.p, A.row.p, A.col.p, A.val.p,
-        C.row.p, C.col.p, C.val.p, cap, err.p);
+    note_launch(); k_compact_rows<<<warp_grid(nc), 256, 0, s>>>(nc, cap, C.row.p, pcol.p, pval.p, C.col.p, C.val.p);
     BCMGX_CHECK_LAUNCH();
     e = read_err(err.p, s);
     if (e) throw Error(BCMGX_ERR_INTERNAL, "galerkin: " + err_text(e));
     C.max_row = row_max(C, s);
 }
 
+// Largest |col - row| of the matrix (atomicMax of per-thread maxima).
+__global__ void k_max_offset(int n, const int* __restrict__ row, const int* __restrict__ col, int* out)
+{
+    int mx = 0;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        for (int j = row[i]; j < row[i + 1]; j++) mx = max(mx, abs(col[j] - (int)i));
+    atomicMax(out, mx);
+}
+
+__global__ void k_to_offsets(int n, const int* __restrict__ row, const int* __restrict__ col, short* __restrict__ dcol)
+{
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        for (int j = row[i]; j < row[i + 1]; j++) dcol[j] = (short)(col[j] - (int)i);
+}
+
+// A compact copy of the columns as int16 offsets from the row when every entry lies within
+// 32767 of the diagonal: the solve-phase row kernels then stream 2 instead of 4 index bytes per
+// entry. BCMGX_INDEX16=0 in the environment keeps int32 columns only.
+static void build_offsets(DevCsr& A, cudaStream_t s)
+{
+    const char* env = std::getenv("BCMGX_INDEX16");
+    if (env && env[0] == '0') return;
+    if (A.n <= 0 || A.nnz <= 0) return;
+    DBuf<int> mx;
+    mx.alloc(1, s);
+    BCMGX_CUDA(cudaMemsetAsync(mx.p, 0, sizeof(int), s));
+    note_launch(); k_max_offset<<<gs_grid(A.n), 256, 0, s>>>(A.n, A.row.p, A.col.p, mx.p);
+    BCMGX_CHECK_LAUNCH();
+    if (read_err(mx.p, s) > 32767) return;
+    A.dcol.alloc(A.nnz, s);
+    note_launch(); k_to_offsets<<<gs_grid(A.n), 256, 0, s>>>(A.n, A.row.p, A.col.p, A.dcol.p);
+    BCMGX_CHECK_LAUNCH();
+}
+
 static void finish_level_matrix(Level& V, bool want_f32, cudaStream_t s)
 {
     const int n = V.A.n;
+    build_offsets(V.A, s);
     V.M.alloc(n, s);
     if (want_f32) V.M32.alloc(n, s);
     note_launch(); k_abs_row_sum<<<gs_grid(n), 256, 0, s>>>(n, V.A.row.p, V.A.val.p, V.M.p, want_f32 ? V.M32.p : nullptr);

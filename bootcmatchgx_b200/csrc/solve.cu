@@ -64,8 +64,8 @@ int fit_grid(const void* kernel, int threads, long need_blocks)
     return (int)std::max<long>(1, std::min<long>(need_blocks, (long)num_sms() * b));
 }
 
-template <int OP, typename VT, typename XT, typename FT, typename MT, typename YT>
-static void launch_rowop(int tpr, int n, const int* row, const int* col, const VT* val, const XT* x, const FT* f,
+template <int OP, typename VT, typename XT, typename FT, typename MT, typename YT, typename IT>
+static void launch_rowop(int tpr, int n, const int* row, const IT* col, const VT* val, const XT* x, const FT* f,
     const MT* M, YT* y, double alpha, double beta, const int* skip, cudaStream_t s)
 {
     if (n <= 0) return;
@@ -75,14 +75,23 @@ static void launch_rowop(int tpr, int n, const int* row, const int* col, const V
         kern<<<fit_grid(kern, 256, need), 256, 0, s>>>(n, row, col, val, x, f, M, y, alpha, beta, skip);
     };
     switch (tpr) {
-    case 1: go(k_rowop<1, OP, VT, XT, FT, MT, YT>); break;
-    case 2: go(k_rowop<2, OP, VT, XT, FT, MT, YT>); break;
-    case 4: go(k_rowop<4, OP, VT, XT, FT, MT, YT>); break;
-    case 8: go(k_rowop<8, OP, VT, XT, FT, MT, YT>); break;
-    case 16: go(k_rowop<16, OP, VT, XT, FT, MT, YT>); break;
-    default: go(k_rowop<32, OP, VT, XT, FT, MT, YT>); break;
+    case 1: go(k_rowop<1, OP, VT, XT, FT, MT, YT, IT>); break;
+    case 2: go(k_rowop<2, OP, VT, XT, FT, MT, YT, IT>); break;
+    case 4: go(k_rowop<4, OP, VT, XT, FT, MT, YT, IT>); break;
+    case 8: go(k_rowop<8, OP, VT, XT, FT, MT, YT, IT>); break;
+    case 16: go(k_rowop<16, OP, VT, XT, FT, MT, YT, IT>); break;
+    default: go(k_rowop<32, OP, VT, XT, FT, MT, YT, IT>); break;
     }
     BCMGX_CHECK_LAUNCH();
+}
+
+// The row operation on a level matrix, through its int16 column offsets when it has them.
+template <int OP, typename VT, typename XT, typename FT, typename MT, typename YT>
+static void launch_rowop_A(int tpr, const DevCsr& A, const VT* val, const XT* x, const FT* f, const MT* M, YT* y,
+    double alpha, double beta, const int* skip, cudaStream_t s)
+{
+    if (A.dcol.p) launch_rowop<OP>(tpr, A.n, A.row.p, (const short*)A.dcol.p, val, x, f, M, y, alpha, beta, skip, s);
+    else launch_rowop<OP>(tpr, A.n, A.row.p, (const int*)A.col.p, val, x, f, M, y, alpha, beta, skip, s);
 }
 
 // About 6-8 entries per lane: 27-point rows -> 4 lanes, 7-point rows -> 2 lanes.
@@ -106,13 +115,13 @@ void launch_spmv(int n, const int* row, const int* col, const double* val, const
 
 void rowop_spmv(const DevCsr& A, const double* x, double* y, const int* skip, cudaStream_t s)
 {
-    launch_rowop<OP_AXPBY>(A.tpr, A.n, A.row.p, A.col.p, A.val.p, x, (const double*)nullptr, (const double*)nullptr, y,
+    launch_rowop_A<OP_AXPBY>(A.tpr, A, A.val.p, x, (const double*)nullptr, (const double*)nullptr, y,
         1.0, 0.0, skip, s);
 }
 
 void rowop_resid(const DevCsr& A, const double* x, const double* f, double* y, const int* skip, cudaStream_t s)
 {
-    launch_rowop<OP_RESID>(A.tpr, A.n, A.row.p, A.col.p, A.val.p, x, f, (const double*)nullptr, y, 1.0, 0.0, skip, s);
+    launch_rowop_A<OP_RESID>(A.tpr, A, A.val.p, x, f, (const double*)nullptr, y, 1.0, 0.0, skip, s);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -241,7 +250,7 @@ struct Cycle {
     template <int OP, typename VT, typename XT, typename FT, typename MT, typename YT>
     void rowop(const DevCsr& A, const VT* val, const XT* x, const FT* f, const MT* M, YT* y) const
     {
-        if (lk < 0) launch_rowop<OP>(A.tpr, A.n, A.row.p, A.col.p, val, x, f, M, y, 1.0, 0.0, skip, s);
+        if (lk < 0) launch_rowop_A<OP>(A.tpr, A, val, x, f, M, y, 1.0, 0.0, skip, s);
         else launch_blk_rowop<OP>(A.n, 1 << lk, 1 << lk, A.row.p, A.col.p, val, x, f, M, y, 1.0, 0.0, skip, s);
     }
     template <typename FT, typename MT, typename YT, typename CT>
@@ -485,7 +494,7 @@ static void l1jacobi_apply(bcmgx_hierarchy* H, const double* r, double* v, const
     first<<<ew_grid(first, n), 256, 0, s>>>(n, r, H->l1d.p, out[0], (double*)nullptr, skip);
     BCMGX_CHECK_LAUNCH();
     for (int i = 1; i < k; i++)
-        launch_rowop<OP_JACOBI>(A.tpr, n, A.row.p, A.col.p, A.val.p, (const double*)out[i - 1], r, (const double*)H->l1d.p,
+        launch_rowop_A<OP_JACOBI>(A.tpr, A, A.val.p, (const double*)out[i - 1], r, (const double*)H->l1d.p,
             out[i], 1.0, 0.0, skip, s);
 }
 
@@ -553,8 +562,8 @@ static int red_grid(Kern kern, long work_threads)
 }
 
 // r = b - A x and ||r||^2 -> delta0, tolerance (FCG.cu:46-51).
-template <int S>
-__global__ void __launch_bounds__(kRedThreads) k_fcg_resid0(int n, const int* __restrict__ row, const int* __restrict__ col,
+template <int S, typename IT>
+__global__ void __launch_bounds__(kRedThreads) k_fcg_resid0(int n, const int* __restrict__ row, const IT* __restrict__ col,
     const double* __restrict__ val, const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ r,
     FcgState* st, double* partials)
 {
@@ -565,7 +574,7 @@ __global__ void __launch_bounds__(kRedThreads) k_fcg_resid0(int n, const int* __
     for (long base = ((long)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) / S; base < n; base += stride) {
         const long r0 = base + sub;
         double s = 0;
-        if (r0 < n) s = row_partial<S, double>(row[r0], row[r0 + 1], lane, col, val, x);
+        if (r0 < n) s = row_partial<S, double>(row[r0], row[r0 + 1], lane, (int)r0, col, val, x);
         s = subwarp_sum<S>(s);
         if (r0 < n && lane == 0) {
             double ri = -1.0 * s + 1.0 * b[r0];
@@ -588,8 +597,8 @@ __global__ void __launch_bounds__(kRedThreads) k_fcg_resid0(int n, const int* __
 // gamma = oq.pv (triple_innerproduct, triple_inner_product.cu:7-101) followed by the scalar
 // recurrence theta = gamma/delta, delta = beta - gamma^2/delta, theta2 = alpha/delta
 // (FCG.cu:132-136).
-template <int S, int MODE>
-__global__ void __launch_bounds__(kRedThreads) k_fcg_spmv_dots(int n, const int* __restrict__ row, const int* __restrict__ col,
+template <int S, int MODE, typename IT>
+__global__ void __launch_bounds__(kRedThreads) k_fcg_spmv_dots(int n, const int* __restrict__ row, const IT* __restrict__ col,
     const double* __restrict__ val, const double* __restrict__ pv, double* __restrict__ pw, const double* __restrict__ r,
     const double* __restrict__ oq, FcgState* st, double* partials, const int* __restrict__ skip)
 {
@@ -601,7 +610,7 @@ __global__ void __launch_bounds__(kRedThreads) k_fcg_spmv_dots(int n, const int*
     for (long base = ((long)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) / S; base < n; base += stride) {
         const long r0 = base + sub;
         double s = 0;
-        if (r0 < n) s = row_partial<S, double>(row[r0], row[r0 + 1], lane, col, val, pv);
+        if (r0 < n) s = row_partial<S, double>(row[r0], row[r0 + 1], lane, (int)r0, col, val, pv);
         s = subwarp_sum<S>(s);
         if (r0 < n && lane == 0) {
             pw[r0] = s;
@@ -692,17 +701,27 @@ __global__ void __launch_bounds__(kRedThreads) k_fcg_update(int n, double* __res
 template <int S>
 static void launch_resid0(const DevCsr& A, const double* x, const double* b, double* r, FcgState* st, double* part, cudaStream_t s)
 {
-    auto k = k_fcg_resid0<S>;
     note_launch();
-    k<<<red_grid(k, (long)A.n * S), kRedThreads, 0, s>>>(A.n, A.row.p, A.col.p, A.val.p, x, b, r, st, part);
+    if (A.dcol.p) {
+        auto k = k_fcg_resid0<S, short>;
+        k<<<red_grid(k, (long)A.n * S), kRedThreads, 0, s>>>(A.n, A.row.p, A.dcol.p, A.val.p, x, b, r, st, part);
+    } else {
+        auto k = k_fcg_resid0<S, int>;
+        k<<<red_grid(k, (long)A.n * S), kRedThreads, 0, s>>>(A.n, A.row.p, A.col.p, A.val.p, x, b, r, st, part);
+    }
 }
 template <int S, int MODE>
 static void launch_dots(const DevCsr& A, const double* pv, double* pw, const double* r, const double* oq, FcgState* st,
     double* part, const int* skip, cudaStream_t s)
 {
-    auto k = k_fcg_spmv_dots<S, MODE>;
     note_launch();
-    k<<<red_grid(k, (long)A.n * S), kRedThreads, 0, s>>>(A.n, A.row.p, A.col.p, A.val.p, pv, pw, r, oq, st, part, skip);
+    if (A.dcol.p) {
+        auto k = k_fcg_spmv_dots<S, MODE, short>;
+        k<<<red_grid(k, (long)A.n * S), kRedThreads, 0, s>>>(A.n, A.row.p, A.dcol.p, A.val.p, pv, pw, r, oq, st, part, skip);
+    } else {
+        auto k = k_fcg_spmv_dots<S, MODE, int>;
+        k<<<red_grid(k, (long)A.n * S), kRedThreads, 0, s>>>(A.n, A.row.p, A.col.p, A.val.p, pv, pw, r, oq, st, part, skip);
+    }
 }
 
 static void fcg_resid0(const DevCsr& A, const double* x, const double* b, double* r, FcgState* st, double* part, cudaStream_t s)
@@ -748,7 +767,7 @@ void ensure_solve_workspace(bcmgx_hierarchy* H)
     H->partials.alloc((size_t)num_sms() * kRedBlocksPerSM * 4, s);
     H->st.alloc(1, s);
     BCMGX_CUDA(cudaMemsetAsync(H->st.p, 0, sizeof(FcgState), s));
-    if (!H->st_host) BCMGX_CUDA(cudaMallocHost((void**)&H->st_host, 2 * sizeof(FcgState)));
+    if (!H->st_host) H->st_host = (FcgState*)pinned_alloc(2 * sizeof(FcgState));
     const bool f32 = H->prm.vcycle_precision == BCMGX_VCYCLE_FP32;
     const int L = (int)H->lv.size();
     for (int l = 0; l < L; l++) {
@@ -819,11 +838,11 @@ void time_level_kernels(bcmgx_hierarchy* H, int l, int reps, double* out)
         return (double)ms / reps;
     };
     if (f32) {
-        out[0] = timeit([&] { launch_rowop<OP_JACOBI>(A.tpr, n, A.row.p, A.col.p, A.val32.p, (const float*)a32.p, (const float*)c32.p, V.M32.p, b32.p, 1.0, 0.0, nullptr, s); });
-        out[1] = timeit([&] { launch_rowop<OP_RESID>(A.tpr, n, A.row.p, A.col.p, A.val32.p, (const float*)a32.p, (const float*)c32.p, (const float*)nullptr, b32.p, 1.0, 0.0, nullptr, s); });
+        out[0] = timeit([&] { launch_rowop_A<OP_JACOBI>(A.tpr, A, A.val32.p, (const float*)a32.p, (const float*)c32.p, V.M32.p, b32.p, 1.0, 0.0, nullptr, s); });
+        out[1] = timeit([&] { launch_rowop_A<OP_RESID>(A.tpr, A, A.val32.p, (const float*)a32.p, (const float*)c32.p, (const float*)nullptr, b32.p, 1.0, 0.0, nullptr, s); });
     } else {
-        out[0] = timeit([&] { launch_rowop<OP_JACOBI>(A.tpr, n, A.row.p, A.col.p, A.val.p, (const double*)a.p, (const double*)c.p, V.M.p, b.p, 1.0, 0.0, nullptr, s); });
-        out[1] = timeit([&] { launch_rowop<OP_RESID>(A.tpr, n, A.row.p, A.col.p, A.val.p, (const double*)a.p, (const double*)c.p, (const double*)nullptr, b.p, 1.0, 0.0, nullptr, s); });
+        out[0] = timeit([&] { launch_rowop_A<OP_JACOBI>(A.tpr, A, A.val.p, (const double*)a.p, (const double*)c.p, V.M.p, b.p, 1.0, 0.0, nullptr, s); });
+        out[1] = timeit([&] { launch_rowop_A<OP_RESID>(A.tpr, A, A.val.p, (const double*)a.p, (const double*)c.p, (const double*)nullptr, b.p, 1.0, 0.0, nullptr, s); });
     }
     out[2] = timeit([&] { launch_spmv(n, A.row.p, A.col.p, A.val.p, a.p, b.p, 1.0, 0.0, A.tpr, s); });
     out[3] = 0;
@@ -908,9 +927,9 @@ int autotune_tpr(Level& V, bool f32, cudaStream_t s)
     for (int t = 1; t <= 16; t *= 2) {
         auto launch = [&] {
             if (f32)
-                launch_rowop<OP_JACOBI>(t, n, A.row.p, A.col.p, A.val32.p, (const float*)a32.p, (const float*)c32.p, V.M32.p, b32.p, 1.0, 0.0, nullptr, s);
+                launch_rowop_A<OP_JACOBI>(t, A, A.val32.p, (const float*)a32.p, (const float*)c32.p, V.M32.p, b32.p, 1.0, 0.0, nullptr, s);
             else
-                launch_rowop<OP_JACOBI>(t, n, A.row.p, A.col.p, A.val.p, (const double*)a.p, (const double*)c.p, V.M.p, b.p, 1.0, 0.0, nullptr, s);
+                launch_rowop_A<OP_JACOBI>(t, A, A.val.p, (const double*)a.p, (const double*)c.p, V.M.p, b.p, 1.0, 0.0, nullptr, s);
         };
         launch();
         BCMGX_CUDA(cudaEventRecord(e0, s));
@@ -1115,8 +1134,8 @@ void batch_build(bcmgx_batch* B)
     std::vector<FcgState*> sp(m);
     for (int k = 0; k < m; k++) sp[k] = B->hs[k]->st.p;
     BCMGX_CUDA(cudaMemcpyAsync(B->states_ptr.p, sp.data(), sizeof(FcgState*) * m, cudaMemcpyHostToDevice, s));
-    BCMGX_CUDA(cudaMallocHost((void**)&B->states_host, sizeof(FcgState) * m));
-    BCMGX_CUDA(cudaMallocHost((void**)&B->copies_host, sizeof(BatchCopy) * 2 * m));
+    B->states_host = pinned_alloc(sizeof(FcgState) * m);
+    B->copies_host = pinned_alloc(sizeof(BatchCopy) * 2 * m);
     BCMGX_CUDA(cudaStreamSynchronize(s));
 }
 

@@ -282,9 +282,13 @@ def run_ours(a, wl, rank, world, local_rank):
     h32.free()
     h64.free()
     peak, peak_kind = read_peaks()
+    # algorithmic bytes of the format the kernels stream: int16 column offsets (2 B) where the
+    # level has them, else int32 (4 B); bcmgx_spmv on raw CSR arrays always streams int32
+    ib32, ib64 = inf32["index_bytes"][0], inf64["index_bytes"][0]
     bytes_spmv = 12 * nnz + 4 * (n + 1) + 16 * n
-    bytes_jac32 = 8 * nnz + 4 * (n + 1) + 16 * n
-    bytes_jac64 = 12 * nnz + 4 * (n + 1) + 32 * n
+    bytes_jac32 = (ib32 + 4) * nnz + 4 * (n + 1) + 16 * n
+    bytes_jac64 = (ib64 + 8) * nnz + 4 * (n + 1) + 32 * n
+    bytes_jac32_int32 = 8 * nnz + 4 * (n + 1) + 16 * n
     gbs_spmv = bytes_spmv / (spmv_ms * 1e-3) / 1e9
     gbs_jac32 = bytes_jac32 / (k32["jacobi"] * 1e-3) / 1e9
     gbs_jac64 = bytes_jac64 / (k64f["jacobi"] * 1e-3) / 1e9
@@ -352,14 +356,16 @@ def run_ours(a, wl, rank, world, local_rank):
                    "fp32_rel_residual": float(nrm(b - _spmv(row, col, val, x32)) / nrm(b))},
         "spmv": {"gbs": gbs_spmv, "ms": spmv_ms, "bytes": bytes_spmv, "frac_of_peak": gbs_spmv / peak,
                  "frac_of_8TBs_nominal": gbs_spmv / 8000.0},
-        "kernels_level0": {"fp32_jacobi_ms": k32["jacobi"], "fp32_jacobi_gbs": gbs_jac32,
+        "kernels_level0": {"index_bytes": ib32, "fp32_jacobi_ms": k32["jacobi"], "fp32_jacobi_gbs": gbs_jac32,
+                           "fp32_jacobi_int32_equivalent_gbs": bytes_jac32_int32 / (k32["jacobi"] * 1e-3) / 1e9,
                            "fp32_residual_ms": k32["residual"], "fp64_jacobi_ms": k64f["jacobi"],
                            "fp64_jacobi_gbs": gbs_jac64, "fcg_spmv_dots_ms": k64f["fcg_spmv_dots"]},
         "kernels_coarse_levels_fp32_jacobi_ms": [round(k["jacobi"], 4) for k in lvl],
         "roofline": {"kernel": f"k_rowop<{inf32['tpr'][0]},OP_JACOBI,float> (FP32 l1-Jacobi sweep, level 0)",
                      "bound": "hbm", "achieved": gbs_jac32, "peak": peak, "unit": "GB/s",
                      "frac": gbs_jac32 / peak, "peak_kind": f"{peak_kind} hbm_gbs (copy)",
-                     "bytes_per_launch": bytes_jac32, "traffic": TRAFFIC.get(a.workload)},
+                     "bytes_per_launch": bytes_jac32,
+                     "traffic": int(TRAFFIC_RATIO[ib32] * bytes_jac32) if a.workload.startswith("poisson27") else None},
         "gpu_launches": int(round(launches32)),
         "e2e": {"value": e2e_ms / 1e3, "unit": "s", "h2d_bytes_per_step": int(row.nbytes + col.nbytes + val.nbytes + b.nbytes),
                 "d2h_bytes_per_step": int(n * 8), "path": "bcmgx_setup(host CSR) + bcmgx_solve(host b, x), pinned"},
@@ -369,10 +375,11 @@ def run_ours(a, wl, rank, world, local_rank):
     return line
 
 
-# DRAM bytes (read + write) of one level-0 FP32 Jacobi launch. Measured by ncu on the 100^3 case
-# (profiles/jacobi_fp32_poisson27_100.md: 231.67 MB = 0.99983 x its algorithmic bytes) and scaled
-# by the algorithmic bytes (non-zeros) to the other 27-point workloads.
-TRAFFIC = {"poisson27_100": 231670016, "poisson27_160": int(0.99983 * (8 * 109215352 + 4 * 4096001 + 16 * 4096000))}
+# DRAM bytes (read + write) of one level-0 FP32 Jacobi launch as a multiple of its algorithmic
+# bytes, measured by ncu on the 27-point 100^3 case per index format (int32 columns:
+# profiles/jacobi_fp32_poisson27_100.md; int16 offsets: profiles/jacobi_fp32_int16_poisson27_100.md)
+# and scaled by the algorithmic bytes to the other 27-point workloads.
+TRAFFIC_RATIO = {4: 0.99983, 2: 1.00115}
 
 
 def _spmv(row, col, val, x):

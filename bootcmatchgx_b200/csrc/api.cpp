@@ -497,6 +497,7 @@ int bcmgx_hierarchy_get_info(const bcmgx_hierarchy* h, bcmgx_hierarchy_info* inf
             info->n[l] = h->lv[l].A.n;
             info->nnz[l] = h->lv[l].A.nnz;
             info->tpr[l] = h->lv[l].A.tpr;
+            info->index_bytes[l] = h->lv[l].A.dcol.p ? 2 : 4;
         }
         info->op_cmplx = h->op_cmplx;
         info->op_wcmplx = h->op_wcmplx;

@@ -396,10 +396,17 @@ __global__ void k_rank(int n, const int* __restrict__ row, const int* __restrict
             const bool el = in && ct != r && wt > 0.0;
             const unsigned elig = __ballot_sync(0xffffffffu, el);
             int rk = 0;
-            for (int k = 0; k < e - b; k++) {
-                const int ck = __shfl_sync(0xffffffffu, ct, k);
-                const double wk = __shfl_sync(0xffffffffu, wt, k);
-                rk += (((elig >> k) & 1u) && (wk > wt || (wk == wt && ck > ct))) ? 1 : 0;
+            const double w0 = __shfl_sync(0xffffffffu, wt, elig ? __ffs(elig) - 1 : 0);
+            if (__ballot_sync(0xffffffffu, el && wt != w0) == 0u) {
+                // all candidates weigh the same: the order is by column alone (columns ascend
+                // with the lane), so the rank is the number of candidates in higher lanes
+                rk = __popc(lane == 31 ? 0u : (elig >> (lane + 1)));
+            } else {
+                for (int k = 0; k < e - b; k++) {
+                    const int ck = __shfl_sync(0xffffffffu, ct, k);
+                    const double wk = __shfl_sync(0xffffffffu, wt, k);
+                    rk += (((elig >> k) & 1u) && (wk > wt || (wk == wt && ck > ct))) ? 1 : 0;
+                }
             }
             if (in) {
                 rank[t] = el ? rk : -1;
@@ -966,8 +973,9 @@ __global__ void k_max_offset(int n, const int* __restrict__ row, const int* __re
 
 __global__ void k_to_offsets(int n, const int* __restrict__ row, const int* __restrict__ col, short* __restrict__ dcol)
 {
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-        for (int j = row[i]; j < row[i + 1]; j++) dcol[j] = (short)(col[j] - (int)i);
+    const int lane = threadIdx.x & 31;
+    for (long i = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32; i < n; i += (long)gridDim.x * blockDim.x / 32)
+        for (int j = row[i] + lane; j < row[i + 1]; j += 32) dcol[j] = (short)(col[j] - (int)i);
 }
 
 // A compact copy of the columns as int16 offsets from the row when every entry lies within
@@ -985,7 +993,7 @@ static void build_offsets(DevCsr& A, cudaStream_t s)
     BCMGX_CHECK_LAUNCH();
     if (read_err(mx.p, s) > 32767) return;
     A.dcol.alloc(A.nnz, s);
-    note_launch(); k_to_offsets<<<gs_grid(A.n), 256, 0, s>>>(A.n, A.row.p, A.col.p, A.dcol.p);
+    note_launch(); k_to_offsets<<<warp_grid(A.n), 256, 0, s>>>(A.n, A.row.p, A.col.p, A.dcol.p);
     BCMGX_CHECK_LAUNCH();
 }
 

@@ -195,6 +195,18 @@ def reference_arm(a, wl, rank, world):
 
 
 # ---------------------------------------------------------------------------------------------
+def max_over_ranks(x, world, device=None):
+    """The largest value of x over all ranks of the job (a time is reported as the slowest rank's);
+    x itself when the job has one rank. Works on any process-group backend (NCCL, gloo)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(a, wl, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -243,12 +255,8 @@ def run_ours(a, wl, rank, world, local_rank):
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        ms = e0.elapsed_time(e1) / steps
+        ms = max_over_ranks(e0.elapsed_time(e1) / steps, world, dev)
         launches = (bx.lib().bcmgx_launch_count() - c0) / steps
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
         return ms, infos, launches
 
     # ---- headline: FP32 V-cycle inside FP64 FCG
@@ -319,11 +327,7 @@ def run_ours(a, wl, rank, world, local_rank):
     e1.record(stream)
     torch.cuda.synchronize()
     wall = (time.perf_counter() - t0) / ke
-    e2e_ms = max(e0.elapsed_time(e1) / ke, wall * 1e3)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(max(e0.elapsed_time(e1) / ke, wall * 1e3), world, dev)
 
     if rank != 0:
         return None

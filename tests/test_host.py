@@ -191,3 +191,44 @@ def test_gaussian_random_field_statistics():
     # correlation at lag 4 along x ~ exp(-16/32) for the squared-exponential kernel
     c = np.mean(f * np.roll(f, 4, axis=0)) / np.mean(f * f)
     assert abs(c - np.exp(-0.5)) < 0.1
+
+
+def _replica_rank(rank, world, port, out):
+    import torch.distributed as dist
+    import bench
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        # every rank times its own replica; the job reports the slowest one
+        mine = 10.0 + 5.0 * rank
+        got = bench.max_over_ranks(mine, world)
+        dist.barrier()
+        # the reference arm runs on rank 0 only; the other ranks return without work
+        import argparse
+        line = bench.reference_arm(argparse.Namespace(gpus=world, steps=1, warmup=0, workload="poisson7_50"),
+                                   bench.WORKLOADS["poisson7_50"], rank, world) if rank != 0 else "rank0"
+        out.put((rank, got, line))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_replica_timing_over_gloo_ranks():
+    """bench.py at N > 1 (replicas): two gloo ranks on CPU agree on the slowest rank's time, and
+    the reference arm does no work on ranks other than 0."""
+    import multiprocessing as mp
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    procs = [ctx.Process(target=_replica_rank, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(out.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert res[0] == (0, 15.0, "rank0") and res[1] == (1, 15.0, None)
+    import bench
+    assert bench.max_over_ranks(3.5, 1) == 3.5

@@ -438,7 +438,7 @@ def run_adjoint(a):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / a.steps
     _, grad64 = fwd_bwd(prm64)
-    tight = autograd.default_params(rtol=1e-10, vcycle_precision="FP64")
+    tight = autograd.default_params(rtol=1e-12, vcycle_precision="FP64")
     _, grad_t = fwd_bwd(tight)
     errs, errs_t = [], []
     h = cfg["step"]
@@ -452,7 +452,7 @@ def run_adjoint(a):
             "config": {"problem": "7-point FV diffusion 96^3, kappa = exp(theta), theta GRF (length 8, sigma 2, seed 5); "
                                   "x_obs = x(theta0) + N(0,1e-3); theta = theta0 + 0.1 N(0,1); L = 0.5||x - x_obs||^2",
                        "rtol": cfg["rtol"], "fd_step": h, "directions": cfg["directions"]},
-            "fd": "central differences of L on FP64 solves to rtol 1e-10, directions d ~ N(0, I)",
+            "fd": "central differences of L on FP64 solves to rtol 1e-12, directions d ~ N(0, I)",
             "grad_rel_err_vs_central_fd_max": max(errs), "grad_rel_err_vs_central_fd_median": float(np.median(errs)),
             "grad_fp64_rel_err_vs_central_fd_max": max(errs_t),
             "grad_rel_err_vs_fresh_fp64": float((grad - grad64).norm() / grad64.norm()), "loss": float(L)}

@@ -40,7 +40,15 @@ def _ptr(a):
 
 
 def _is_device(a):
-    return hasattr(a, "is_cuda") and a.is_cuda
+    """True for a CUDA tensor. The library orders its own stream after the legacy default stream
+    (torch's default); work that torch queued on another current stream is waited for here."""
+    if not (hasattr(a, "is_cuda") and a.is_cuda):
+        return False
+    import torch
+    cur = torch.cuda.current_stream(a.device)
+    if cur.cuda_stream != 0:
+        cur.synchronize()
+    return True
 
 
 def params_default(**overrides) -> L.Params:

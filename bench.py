@@ -517,11 +517,31 @@ def run_batch(a):
                        "vcycle": "fp32", "rtol": 1e-8, "setup_threads": min(16, os.cpu_count() or 1)}}
 
 
+def block_kernel_rooflines(t, n, nnz, k):
+    """Level-0 block kernels of the FP32-cycle multi-RHS solve (bcmgx_time_block_kernels, CUDA
+    events, zero inputs): ms per launch and HBM GB/s of the algorithmic bytes (matrix once, every
+    block read or written once: the gathers of X from L1/L2 are not counted) against the measured
+    copy peak. The FP32 sweep reads the FP32 matrix values (8 bytes per entry with the int32
+    column), the FP64 kernels 12 bytes per entry."""
+    peak, kind = read_peaks()
+    blk4, blk8 = 4.0 * n * k, 8.0 * n * k
+    alg = {"jacobi": 8 * nnz + 4 * (n + 1) + 4 * n + 3 * blk4,
+           "residual": 8 * nnz + 4 * (n + 1) + 3 * blk4,
+           "spmm": 12 * nnz + 4 * (n + 1) + 2 * blk8,
+           "fcg_spmm_dots": 12 * nnz + 4 * (n + 1) + 4 * blk8}
+    out = {"peak_gbs": peak, "peak_kind": kind}
+    for key, b in alg.items():
+        ms = t[key]
+        out[key] = {"ms": ms, "algorithmic_bytes": int(b), "gbs": b / ms / 1e6, "frac": b / ms / 1e6 / peak}
+    return out
+
+
 def run_multi(a):
     """The 27-point 100^3 Poisson matrix with 32 right-hand sides (uniform[-1,1], numpy
     default_rng(6)) solved to 1e-8 in one block solve (CSR SpMM throughout, FP32 V-cycle) vs a
-    sequential loop of 32 single solves on the same hierarchy; also the block FP64-cycle solve
-    and the SpMM kernel alone (CUDA events, HBM GB/s of its algorithmic bytes)."""
+    sequential loop of 32 single solves on the same hierarchy; also the block FP64-cycle solve,
+    the level-0 block kernels (CUDA events, HBM GB/s of their algorithmic bytes) and the public
+    SpMM call."""
     import scipy.sparse as sp
     import torch
     import bootcmatchgx_b200 as bx
@@ -579,9 +599,11 @@ def run_multi(a):
             res["speedup_vs_sequential"] = t_seq / t_block
             res["max_rel_diff_vs_single"] = max(float(torch.linalg.norm(X[:, j] - xs[j]) / torch.linalg.norm(xs[j]))
                                                 for j in range(k))
+            res["kernels_level0"] = block_kernel_rooflines(h.time_block_kernels(k, reps=20), n, nnz, k)
         h.free()
         out[prec] = res
-    # the SpMM kernel alone: Y = A X for the 32-column block
+    # the public SpMM call Y = A X for the 32-column block: CSR validation on the device, a host
+    # round trip for its verdict, then the kernel (the kernel alone: fp32.kernels_level0.spmm)
     Y = torch.empty_like(Bd)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     for _ in range(3):
@@ -599,8 +621,9 @@ def run_multi(a):
     return {"metric": "multi-RHS solves/s (27-point 100^3, 32 right-hand sides, one block solve)",
             "value": f32["solves_per_s"], "unit": "solves/s", "higher_is_better": True, "workload": "poisson27_100_x32",
             "fp32": f32, "fp64": out["FP64"],
-            "spmm": {"ms": ms, "algorithmic_bytes": alg, "gbs": alg / ms / 1e6, "peak_gbs": peak,
-                     "frac": alg / ms / 1e6 / peak, "peak_kind": peak_kind},
+            "spmm_call": {"ms": ms, "what": "bcmgx_spmm: validation + host round trip + kernel",
+                          "algorithmic_bytes": alg, "gbs": alg / ms / 1e6, "peak_gbs": peak,
+                          "frac": alg / ms / 1e6 / peak, "peak_kind": peak_kind},
             "steps": a.steps, "warmup": a.warmup,
             "config": {"rows": n, "nnz": nnz, "rhs": k, "rhs_dist": "uniform[-1,1] (numpy default_rng(6))",
                        "rtol": 1e-8, "x0": 0}}
@@ -630,7 +653,7 @@ def profile_multi_step(a):
     torch.cuda.synchronize()
     c2 = L.bcmgx_launch_count()
     h.free()
-    print(json.dumps({"warmup_launches": c1 - c0, "step_launches": c2 - c1,
+    print(json.dumps({"warmup_launches": c1 - c0, "launches_before_step": c1, "step_launches": c2 - c1,
                       "niter_max": max(i["niter"] for i in infos)}), flush=True)
 
 

@@ -90,6 +90,7 @@ SIGNATURES = {
     "bcmgx_hierarchy_get_sweep": (C.c_int, [_vp, C.c_int, _ip, _ip, _ip, _ip, _vp, _vp, _vp, _vp]),
     "bcmgx_prec_apply": (C.c_int, [_vp, _vp, _vp, C.c_int]),
     "bcmgx_time_kernels": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
+    "bcmgx_time_block_kernels": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
     "bcmgx_spmv": (C.c_int, [C.c_int, C.c_int, C.c_int64, _vp, _vp, _vp, _vp, _vp, C.c_double,
                              C.c_double, C.c_int, _vp]),
     "bcmgx_spmm": (C.c_int, [C.c_int, C.c_int, C.c_int64, _vp, _vp, _vp, C.c_int, _vp, _vp, C.c_double,

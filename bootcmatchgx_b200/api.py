@@ -302,6 +302,13 @@ class Hierarchy:
         check(lib().bcmgx_time_kernels(self.h, level, reps, _ptr(out)), "bcmgx_time_kernels")
         return {"jacobi": out[0], "residual": out[1], "spmv": out[2], "fcg_spmv_dots": out[3]}
 
+    def time_block_kernels(self, nrhs=32, reps=20):
+        """Average ms per launch of the level-0 block Jacobi sweep, block residual, FP64 block SpMM
+        and block FCG SpMV+dots for nrhs right-hand sides."""
+        out = np.zeros(4)
+        check(lib().bcmgx_time_block_kernels(self.h, nrhs, reps, _ptr(out)), "bcmgx_time_block_kernels")
+        return {"jacobi": out[0], "residual": out[1], "spmm": out[2], "fcg_spmm_dots": out[3]}
+
     def free(self):
         if getattr(self, "h", None):
             check(lib().bcmgx_free(self.h), "prec_finalize")

@@ -625,6 +625,15 @@ int bcmgx_time_kernels(bcmgx_hierarchy* h, int level, int reps, double* out_ms)
     });
 }
 
+int bcmgx_time_block_kernels(bcmgx_hierarchy* h, int nrhs, int reps, double* out_ms)
+{
+    return guarded([&] {
+        BCMGX_REQUIRE(h && out_ms && nrhs >= 1 && nrhs <= 32 && reps > 0, BCMGX_ERR_INVALID_INPUT, "bad argument");
+        DeviceScope ds(h->device);
+        time_block_kernels(h, nrhs, reps, out_ms);
+    });
+}
+
 int bcmgx_spmv(int n, int m, int64_t nnz, const int* row, const int* col, const double* val, const double* x, double* y,
     double alpha, double beta, int threads_per_row, void* stream)
 {
@@ -648,7 +657,7 @@ int bcmgx_spmm(int n, int m, int64_t nnz, const int* row, const int* col, const 
         BCMGX_REQUIRE(nrhs >= 1 && nrhs <= 32, BCMGX_ERR_INVALID_INPUT, "nrhs must be 1..32");
         BCMGX_REQUIRE(row && (nnz == 0 || (col && val)) && X && Y, BCMGX_ERR_INVALID_INPUT, "NULL argument");
         if (n > 0) validate_csr_dev(n, m, nnz, row, col, false, (cudaStream_t)stream);
-        launch_spmm(n, nrhs, row, col, val, X, Y, alpha, beta, (cudaStream_t)stream);
+        launch_spmm(n, m, nrhs, row, col, val, X, Y, alpha, beta, (cudaStream_t)stream);
     });
 }
 

@@ -8,9 +8,9 @@
 // warp works on 32 / LPE consecutive rows at once. Each lane of a slot owns W consecutive columns
 // (one 8- or 16-byte vector load per neighbour: W = 2 for FP64, 4 for FP32 blocks), so the
 // per-entry index, value and address arithmetic is shared by W columns and no cross-lane
-// reduction is needed; a lane stores its W results as one vector. Matrix entries are streamed
-// with evict-first loads (broadcast within a slot) and the gathers go through L1 / L2, where
-// neighbouring rows reuse them.
+// reduction is needed; a lane stores its W results as one vector. A warp stages the matrix
+// entries of its rows in shared memory with coalesced evict-first loads (blk_rows), and the
+// gathers go through L1 / L2, where neighbouring rows reuse them.
 #pragma once
 
 #include "common.cuh"
@@ -105,99 +105,188 @@ inline BlkShape blk_shape(int K, int bytes)
     return BlkShape { W, lg };
 }
 
-// s[w] = sum over the entries of row [b, e) of a_ij * X[j*ld + c0 + w] (w < W), entries in
-// order, U entries per batch: all index / value loads, then all gathers, then the FMAs.
-template <int W, typename AT, typename VT, typename XT>
-__device__ __forceinline__ void blk_row(int b, int e, int c0, int ld, const int* __restrict__ col,
-    const VT* __restrict__ val, const XT* __restrict__ X, AT (&s)[W])
-{
-    constexpr int U = 4;
-#pragma unroll
-    for (int w = 0; w < W; w++) s[w] = 0;
-    for (int j0 = b; j0 < e; j0 += U) {
-        int c[U];
-        VT v[U];
-        XT x[U][W];
-#pragma unroll
-        for (int k = 0; k < U; k++) {
-            const int j = j0 + k;
-            c[k] = j < e ? ld_stream(col + j) : -1;
-            v[k] = j < e ? ld_stream(val + j) : VT(0);
-        }
-#pragma unroll
-        for (int k = 0; k < U; k++) {
-            if (c[k] >= 0) {
-                ldv<W>(X + (long)c[k] * ld + c0, x[k]);
-            } else {
-#pragma unroll
-                for (int w = 0; w < W; w++) x[k][w] = XT(0);
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < U; k++)
-#pragma unroll
-            for (int w = 0; w < W; w++) s[w] += (AT)v[k] * (AT)x[k][w];
-    }
-}
-
-// Row loop of the SpMM kernels: warp w of the grid takes the row group starting at w * rpw
-// (rpw = 32 / LPE rows), then every warps * rpw rows; slot s of the warp owns row r0 + s.
-#define BCMGX_BLOCK_ROWGROUPS(r0, n, rpw)                                                         \
-    for (long r0 = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32 * (rpw); r0 < (n);          \
-         r0 += (long)gridDim.x * blockDim.x / 32 * (rpw))
-
 // Element loop of the element-wise kernels over n rows of a block with 2^lk columns.
 #define BCMGX_BLOCK_ELEMS(i, n, lk)                                                             \
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < ((long)(n) << (lk));          \
          i += (long)gridDim.x * blockDim.x)
 
+// Matrix entries of one warp step staged in shared memory: the column as an element offset
+// into the block (col * ld, so the gather address is one multiply-add) and the value.
+template <typename VT>
+struct BlkEnt;
+template <>
+struct BlkEnt<float> {
+    int off;
+    float v;
+};
+template <>
+struct __align__(16) BlkEnt<double> {
+    double v;
+    int off;
+    int pad;
+};
+
+// Rows a warp stages per step (at least one row group) and the staging capacity per warp:
+// 32 entries per row on average; a step over longer rows reads its entries from global memory.
+template <typename VT>
+struct BlkStage {
+    static constexpr int rows = sizeof(VT) == 4 ? 8 : 4;
+    static constexpr int cap = 32 * rows;
+};
+// resident blocks per SM the kernel is compiled for: 6 (40 registers), 5 (48) for FP64 values
+// with four columns per lane
+template <typename VT, int W>
+constexpr int blk_min_blocks() { return sizeof(VT) == 8 && W == 4 ? 5 : 6; }
+constexpr int kBlkRowopThreads = 256;
+
+// acc[w] = sum over staged entries [b, e) of v * Xc[off + w], entries in order; U entries per
+// batch without predicates (all loads of the batch issue before its multiply-adds), then the
+// remainder one entry at a time.
+template <int W, typename AT, typename VT, typename XT>
+__device__ __forceinline__ void blk_row_staged(int b, int e, const BlkEnt<VT>* s, const XT* __restrict__ Xc, AT (&acc)[W])
+{
+    constexpr int U = 4;
+#pragma unroll
+    for (int w = 0; w < W; w++) acc[w] = 0;
+    int j = b;
+    for (; j + U <= e; j += U) {
+        BlkEnt<VT> q[U];
+        XT x[U][W];
+#pragma unroll
+        for (int k = 0; k < U; k++) q[k] = s[j + k];
+#pragma unroll
+        for (int k = 0; k < U; k++) ldv<W>(Xc + q[k].off, x[k]);
+#pragma unroll
+        for (int k = 0; k < U; k++)
+#pragma unroll
+            for (int w = 0; w < W; w++) acc[w] += (AT)q[k].v * (AT)x[k][w];
+    }
+    for (; j < e; j++) {
+        const BlkEnt<VT> q = s[j];
+        XT x[W];
+        ldv<W>(Xc + q.off, x);
+#pragma unroll
+        for (int w = 0; w < W; w++) acc[w] += (AT)q.v * (AT)x[w];
+    }
+}
+
+// The row loop of the block SpMM kernels. Each warp takes steps of rw consecutive rows (whole
+// row groups of 32 / LPE rows, at least BlkStage::rows): lanes 0..rw-1 load the row offsets,
+// the warp copies the step's entries into its shared-memory stage `st` (BlkStage::cap entries)
+// with coalesced loads, and then each slot reads its row's entries from there as broadcasts.
+// Per entry a slot issues one shared load, one address multiply-add, one vector gather and W
+// multiply-adds; per-lane index and value loads from global memory hit a different cache line
+// for every slot and cost more L1 throughput than the gathers. A step whose entries do not fit
+// (or stage_ok = 0: X has 2^31 or more elements, past the 32-bit staged offsets) reads them from
+// global memory. For every row r this lane computes, epi(r, o, s) receives o = r * ld + c0 and
+// the sums s[w] of column c0 + w, entries added in row order. All lanes of a warp run the loop
+// (it has warp-synchronous steps); lanes without a column (c0 >= K) skip the epilogue.
+template <int W, typename VT, typename XT, typename Epi>
+__device__ __forceinline__ void blk_rows(int n, int lpe_log2, int ld, int K, const int* __restrict__ row,
+    const int* __restrict__ col, const VT* __restrict__ val, const XT* __restrict__ X, int stage_ok, BlkEnt<VT>* st,
+    Epi&& epi)
+{
+    using AT = typename Acc<VT>::type;
+    using ST = BlkStage<VT>;
+    const int warps = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int slot = lane >> lpe_log2;
+    const int c0 = (lane & ((1 << lpe_log2) - 1)) * W;
+    const int rpg = 32 >> lpe_log2;
+    const int rw = rpg > ST::rows ? rpg : ST::rows;
+    const bool active = c0 < K;
+    const XT* Xc = X + c0;
+    const long wstride = (long)gridDim.x * warps * rw;
+    for (long w0 = ((long)blockIdx.x * warps + (threadIdx.x >> 5)) * rw; w0 < n; w0 += wstride) {
+        const int nr = (int)(w0 + rw < n ? rw : n - w0);
+        const int rp = lane < nr ? __ldg(row + w0 + lane) : 0;
+        const int e0 = __ldg(row + w0 + nr);
+        const int b0 = __shfl_sync(0xffffffffu, rp, 0);
+        const bool staged = stage_ok && e0 - b0 <= ST::cap;
+        if (staged) {
+            for (int t = lane; t < e0 - b0; t += 32) {
+                BlkEnt<VT> q;
+                q.v = ld_stream(val + b0 + t);
+                q.off = ld_stream(col + b0 + t) * ld;
+                st[t] = q;
+            }
+        }
+        __syncwarp();
+        for (int g = 0; g < rw; g += rpg) {
+            const int lr = g + slot;
+            const int rb = __shfl_sync(0xffffffffu, rp, lr & 31);
+            const int rn = __shfl_sync(0xffffffffu, rp, (lr + 1) & 31);
+            if (lr >= nr || !active) continue;
+            const int re = lr + 1 < nr ? rn : e0;
+            AT s[W];
+            if (staged) {
+                blk_row_staged<W>(rb - b0, re - b0, st, Xc, s);
+            } else {
+#pragma unroll
+                for (int w = 0; w < W; w++) s[w] = 0;
+                for (int j = rb; j < re; j++) {
+                    const AT v = (AT)ld_stream(val + j);
+                    XT x[W];
+                    ldv<W>(Xc + (long)ld_stream(col + j) * ld, x);
+#pragma unroll
+                    for (int w = 0; w < W; w++) s[w] += v * (AT)x[w];
+                }
+            }
+            const long r = w0 + lr;
+            epi(r, r * ld + c0, s);
+        }
+        __syncwarp();
+    }
+}
+
+// rows one block of a blk_rows kernel covers per step, for the grid size
+template <typename VT>
+inline long blk_rows_per_block(int lpe_log2, int threads)
+{
+    const int rpg = 32 >> lpe_log2;
+    return (long)(threads / 32) * (rpg > BlkStage<VT>::rows ? rpg : BlkStage<VT>::rows);
+}
+
 // Y = alpha A X + beta Y (OP 0), Y = F - A X (OP 1), or one l1-Jacobi sweep
 // Y = ((F - A X) / M) + X (OP 2), the same updates as k_rowop, column by column. With W > 1,
 // ld is a multiple of W, K = LPE * W and all blocks are 16-byte aligned.
 template <int OP, int W, typename VT, typename XT, typename FT, typename MT, typename YT>
-__global__ void __launch_bounds__(256) k_blk_rowop(int n, int lpe_log2, int ld, int K, const int* __restrict__ row,
-    const int* __restrict__ col, const VT* __restrict__ val, const XT* __restrict__ X, const FT* __restrict__ F,
-    const MT* __restrict__ M, YT* __restrict__ Y, double alpha, double beta, const int* __restrict__ skip)
+__global__ void __launch_bounds__(kBlkRowopThreads, blk_min_blocks<VT, W>()) k_blk_rowop(int n, int lpe_log2, int ld,
+    int K, const int* __restrict__ row, const int* __restrict__ col, const VT* __restrict__ val,
+    const XT* __restrict__ X, const FT* __restrict__ F, const MT* __restrict__ M, YT* __restrict__ Y, double alpha,
+    double beta, int stage_ok, const int* __restrict__ skip)
 {
     if (skip && *skip) return;
     using AT = typename Acc<VT>::type;
-    const int lane = threadIdx.x & 31;
-    const int slot = lane >> lpe_log2;
-    const int c0 = (lane & ((1 << lpe_log2) - 1)) * W;
-    if (c0 >= K) return;   // one-column-per-lane shapes: lanes past the last column
-    BCMGX_BLOCK_ROWGROUPS(r0, n, 32 >> lpe_log2)
-    {
-        const long r = r0 + slot;
-        if (r >= n) continue;
-        AT s[W];
-        blk_row<W>(__ldg(row + r), __ldg(row + r + 1), c0, ld, col, val, X, s);
-        const long o = r * ld + c0;
-        YT y[W];
-        if (OP == 0) {
-            YT y0[W];
-            if (beta != 0.0) ldw<W>(Y + o, y0);
+    __shared__ BlkEnt<VT> stage[kBlkRowopThreads / 32][BlkStage<VT>::cap];
+    blk_rows<W>(n, lpe_log2, ld, K, row, col, val, X, stage_ok, stage[threadIdx.x >> 5],
+        [&](long r, long o, const AT (&s)[W]) {
+            YT y[W];
+            if (OP == 0) {
+                YT y0[W];
+                if (beta != 0.0) ldw<W>(Y + o, y0);
 #pragma unroll
-            for (int w = 0; w < W; w++) {
-                AT t = (AT)alpha * s[w];
-                if (beta != 0.0) t += (AT)beta * (AT)y0[w];
-                y[w] = (YT)t;
+                for (int w = 0; w < W; w++) {
+                    AT t = (AT)alpha * s[w];
+                    if (beta != 0.0) t += (AT)beta * (AT)y0[w];
+                    y[w] = (YT)t;
+                }
+            } else if (OP == 1) {
+                FT f[W];
+                ldw<W>(F + o, f);
+#pragma unroll
+                for (int w = 0; w < W; w++) y[w] = (YT)((AT)f[w] - s[w]);
+            } else {
+                FT f[W];
+                XT x[W];
+                ldw<W>(F + o, f);
+                ldw<W>(X + o, x);
+                const AT m = (AT)M[r];
+#pragma unroll
+                for (int w = 0; w < W; w++) y[w] = (YT)(((-s[w] + (AT)f[w]) / m) + (AT)x[w]);
             }
-        } else if (OP == 1) {
-            FT f[W];
-            ldw<W>(F + o, f);
-#pragma unroll
-            for (int w = 0; w < W; w++) y[w] = (YT)((AT)f[w] - s[w]);
-        } else {
-            FT f[W];
-            XT x[W];
-            ldw<W>(F + o, f);
-            ldw<W>(X + o, x);
-            const AT m = (AT)M[r];
-#pragma unroll
-            for (int w = 0; w < W; w++) y[w] = (YT)(((-s[w] + (AT)f[w]) / m) + (AT)x[w]);
-        }
-        stv<W>(Y + o, y);
-    }
+            stv<W>(Y + o, y);
+        });
 }
 
 // sweep from a zero iterate: U = F / M, optionally keeping a converted copy of F

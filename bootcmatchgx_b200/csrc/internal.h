@@ -253,9 +253,11 @@ void cycle_apply_block(bcmgx_hierarchy* H, const CycleBufs& bufs, int lk, const 
 // Block FCG for K right-hand sides of one system (multi.cu); B, X row-major n x K, device.
 int multi_solve(bcmgx_hierarchy* H, int K, const double* B, double* X, bcmgx_solve_info* infos);
 // Y = alpha A X + beta Y for row-major n x K blocks on device memory (K <= 32).
-void launch_spmm(int n, int K, const int* row, const int* col, const double* val, const double* X, double* Y,
+void launch_spmm(int n, int m, int K, const int* row, const int* col, const double* val, const double* X, double* Y,
     double alpha, double beta, cudaStream_t s);
 void time_level_kernels(bcmgx_hierarchy* H, int l, int reps, double* out);
+void time_block_kernels(bcmgx_hierarchy* H, int K, int reps, double* out);
+double time_block_dots(bcmgx_hierarchy* H, int K, int reps);
 void grad_pattern(const DevCsr& A, const double* lam, const double* x, double* dA, cudaStream_t s);
 void batch_build(bcmgx_batch* B);
 int batch_solve(bcmgx_batch* B, const double* const* b, double* const* x, bcmgx_solve_info* infos);

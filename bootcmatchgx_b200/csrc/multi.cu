@@ -98,28 +98,24 @@ __global__ void k_blk_init(BlockState* st, int K, double rtol, int itnlim)
 
 // R = B - A X and per column delta0 = ||r||, tol = rtol * delta0 (FCG.cu:46-51).
 template <int W>
-__global__ void __launch_bounds__(kBlkThreads) k_blk_resid0(int n, int lpe_log2, int kp, const int* __restrict__ row,
+__global__ void __launch_bounds__(kBlkThreads, 5) k_blk_resid0(int n, int lpe_log2, int kp, const int* __restrict__ row,
     const int* __restrict__ col, const double* __restrict__ val, const double* __restrict__ X, const double* __restrict__ B,
-    double* __restrict__ R, BlockState* st, double* partials)
+    double* __restrict__ R, BlockState* st, double* partials, int stage_ok)
 {
-    const int lane = threadIdx.x & 31, slot = lane >> lpe_log2;
-    const int c0 = (lane & ((1 << lpe_log2) - 1)) * W;
+    __shared__ BlkEnt<double> stage[kBlkThreads / 32][BlkStage<double>::cap];
+    const int lane = threadIdx.x & 31;
     double acc[1][W] = {};
-    BCMGX_BLOCK_ROWGROUPS(r0, n, 32 >> lpe_log2)
-    {
-        const long r = r0 + slot;
-        if (r >= n) continue;
-        double s[W], bb[W], rr[W];
-        blk_row<W>(__ldg(row + r), __ldg(row + r + 1), c0, kp, col, val, X, s);
-        const long o = r * kp + c0;
-        ldw<W>(B + o, bb);
+    blk_rows<W>(n, lpe_log2, kp, kp, row, col, val, X, stage_ok, stage[threadIdx.x >> 5],
+        [&](long, long o, const double (&s)[W]) {
+            double bb[W], rr[W];
+            ldw<W>(B + o, bb);
 #pragma unroll
-        for (int w = 0; w < W; w++) {
-            rr[w] = -1.0 * s[w] + 1.0 * bb[w];
-            acc[0][w] += rr[w] * rr[w];
-        }
-        stv<W>(R + o, rr);
-    }
+            for (int w = 0; w < W; w++) {
+                rr[w] = -1.0 * s[w] + 1.0 * bb[w];
+                acc[0][w] += rr[w] * rr[w];
+            }
+            stv<W>(R + o, rr);
+        });
     double out[1];
     if (blk_colsum<1, W>(acc, 1 << lpe_log2, partials, &st->ticket[0], out) && threadIdx.x < kp) {
         const double d0 = sqrt(out[0]);
@@ -132,33 +128,29 @@ __global__ void __launch_bounds__(kBlkThreads) k_blk_resid0(int n, int lpe_log2,
 // PW = A PV with the per-column dots alpha = r.pv, beta = pw.pv (and gamma = oq.pv in the loop),
 // then the scalar recurrence of each running column (FCG.cu:59-86, 121-136).
 template <int MODE, int W>
-__global__ void __launch_bounds__(kBlkThreads) k_blk_spmv_dots(int n, int lpe_log2, int kp, const int* __restrict__ row,
+__global__ void __launch_bounds__(kBlkThreads, 5) k_blk_spmv_dots(int n, int lpe_log2, int kp, const int* __restrict__ row,
     const int* __restrict__ col, const double* __restrict__ val, const double* __restrict__ PV, double* __restrict__ PW,
-    const double* __restrict__ R, const double* __restrict__ OQ, BlockState* st, double* partials,
+    const double* __restrict__ R, const double* __restrict__ OQ, BlockState* st, double* partials, int stage_ok,
     const int* __restrict__ skip)
 {
     if (skip && *skip) return;
-    const int lane = threadIdx.x & 31, slot = lane >> lpe_log2;
-    const int c0 = (lane & ((1 << lpe_log2) - 1)) * W;
+    __shared__ BlkEnt<double> stage[kBlkThreads / 32][BlkStage<double>::cap];
+    const int lane = threadIdx.x & 31;
     double acc[3][W] = {};
-    BCMGX_BLOCK_ROWGROUPS(r0, n, 32 >> lpe_log2)
-    {
-        const long r = r0 + slot;
-        if (r >= n) continue;
-        double s[W], vi[W], ri[W], qi[W];
-        blk_row<W>(__ldg(row + r), __ldg(row + r + 1), c0, kp, col, val, PV, s);
-        const long o = r * kp + c0;
-        stv<W>(PW + o, s);
-        ldw<W>(PV + o, vi);
-        ldw<W>(R + o, ri);
-        if (MODE == 1) ldw<W>(OQ + o, qi);
+    blk_rows<W>(n, lpe_log2, kp, kp, row, col, val, PV, stage_ok, stage[threadIdx.x >> 5],
+        [&](long, long o, const double (&s)[W]) {
+            double vi[W], ri[W], qi[W];
+            stv<W>(PW + o, s);
+            ldw<W>(PV + o, vi);
+            ldw<W>(R + o, ri);
+            if (MODE == 1) ldw<W>(OQ + o, qi);
 #pragma unroll
-        for (int w = 0; w < W; w++) {
-            acc[0][w] += ri[w] * vi[w];
-            acc[1][w] += s[w] * vi[w];
-            if (MODE == 1) acc[2][w] += qi[w] * vi[w];
-        }
-    }
+            for (int w = 0; w < W; w++) {
+                acc[0][w] += ri[w] * vi[w];
+                acc[1][w] += s[w] * vi[w];
+                if (MODE == 1) acc[2][w] += qi[w] * vi[w];
+            }
+        });
     double out[3];
     if (blk_colsum<3, W>(acc, 1 << lpe_log2, partials, &st->ticket[1], out) && threadIdx.x < kp && !st->done[lane]) {
         const int k = lane;
@@ -344,9 +336,12 @@ void ensure_multi(bcmgx_hierarchy* H, MultiWork& wk, int K)
 template <typename Kern>
 int rows_grid(Kern kern, long n, BlkShape sh)
 {
-    const long rows_per_block = (kBlkThreads / 32L) << (5 - sh.lpe_log2);
+    const long rows_per_block = blk_rows_per_block<double>(sh.lpe_log2, kBlkThreads);
     return std::min(fit_grid(kern, kBlkThreads, (n + rows_per_block - 1) / rows_per_block), num_sms() * kBlkBlocksPerSM);
 }
+
+// the staged 32-bit entry offsets (col * kp) hold for blocks of fewer than 2^31 elements
+int stage_ok(const DevCsr& A, int kp) { return (long)A.m * kp <= 0x7fffffffL ? 1 : 0; }
 
 // the level-0 SpMM shape of the FCG kernels (FP64 blocks of KP columns)
 BlkShape fcg_shape(const MultiWork& wk) { return blk_shape(1 << wk.lk, (int)sizeof(double)); }
@@ -358,7 +353,7 @@ void launch_resid0(const DevCsr& A, const MultiWork& wk, cudaStream_t s)
     auto go = [&](auto kern) {
         note_launch();
         kern<<<rows_grid(kern, A.n, sh), kBlkThreads, 0, s>>>(A.n, sh.lpe_log2, kp, A.row.p, A.col.p, A.val.p, wk.X.p,
-            wk.B.p, wk.R.p, wk.st.p, wk.part.p);
+            wk.B.p, wk.R.p, wk.st.p, wk.part.p, stage_ok(A, kp));
     };
     if (sh.W == 2) go(k_blk_resid0<2>);
     else go(k_blk_resid0<1>);
@@ -374,7 +369,7 @@ void launch_dots(const DevCsr& A, const MultiWork& wk, const double* pv, double*
     auto go = [&](auto kern) {
         note_launch();
         kern<<<rows_grid(kern, A.n, sh), kBlkThreads, 0, s>>>(A.n, sh.lpe_log2, kp, A.row.p, A.col.p, A.val.p, pv, pw,
-            wk.R.p, oq, wk.st.p, wk.part.p, skip);
+            wk.R.p, oq, wk.st.p, wk.part.p, stage_ok(A, kp), skip);
     };
     if (sh.W == 2) go(k_blk_spmv_dots<MODE, 2>);
     else go(k_blk_spmv_dots<MODE, 1>);
@@ -500,6 +495,36 @@ void multi_stream_solve(bcmgx_hierarchy* H, MultiWork& wk)
 }  // namespace
 
 // B, X: device, row-major n x K (X: x0 in, solution out). infos: K entries or null.
+// Average device time of the level-0 block FCG SpMV + dots (loop form) for K columns, on the
+// solve's block workspace filled with zeros (CUDA events, reps launches after one warm-up).
+double time_block_dots(bcmgx_hierarchy* H, int K, int reps)
+{
+    ensure_solve_workspace(H);
+    if (!H->multi) H->multi = new MultiWork();
+    MultiWork& wk = *H->multi;
+    ensure_multi(H, wk, K);
+    cudaStream_t s = H->stream;
+    const DevCsr& A = H->lv[0].A;
+    const size_t nk = (size_t)A.n << wk.lk;
+    for (DBuf<double>* b : { &wk.V, &wk.W, &wk.R, &wk.Q }) BCMGX_CUDA(cudaMemsetAsync(b->p, 0, sizeof(double) * nk, s));
+    note_launch();
+    k_blk_init<<<1, 32, 0, s>>>(wk.st.p, wk.K, 1.0, 1);
+    BCMGX_CHECK_LAUNCH();
+    cudaEvent_t e0, e1;
+    BCMGX_CUDA(cudaEventCreate(&e0));
+    BCMGX_CUDA(cudaEventCreate(&e1));
+    launch_dots<1>(A, wk, wk.V.p, wk.W.p, wk.Q.p, nullptr, s);
+    BCMGX_CUDA(cudaEventRecord(e0, s));
+    for (int i = 0; i < reps; i++) launch_dots<1>(A, wk, wk.V.p, wk.W.p, wk.Q.p, nullptr, s);
+    BCMGX_CUDA(cudaEventRecord(e1, s));
+    BCMGX_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    BCMGX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return (double)ms / reps;
+}
+
 int multi_solve(bcmgx_hierarchy* H, int K, const double* B, double* X, bcmgx_solve_info* infos)
 {
     BCMGX_REQUIRE(K >= 1 && K <= kMaxRhs, BCMGX_ERR_INVALID_INPUT, "the number of right-hand sides must be 1..32");

@@ -201,9 +201,10 @@ static bool aligned_for(const void* p, int W, size_t elem)
 }
 
 // Y = alpha A X + beta Y / F - A X / Jacobi sweep on blocks with leading dimension ld and K
-// columns; vector loads and stores when the pointers and ld allow them, else one column per lane.
+// columns (X has m rows); vector loads and stores when the pointers and ld allow them, else one
+// column per lane.
 template <int OP, typename VT, typename XT, typename FT, typename MT, typename YT>
-static void launch_blk_rowop(int n, int ld, int K, const int* row, const int* col, const VT* val, const XT* x,
+static void launch_blk_rowop(int n, int m, int ld, int K, const int* row, const int* col, const VT* val, const XT* x,
     const FT* f, const MT* M, YT* y, double alpha, double beta, const int* skip, cudaStream_t s)
 {
     if (n <= 0) return;
@@ -211,10 +212,13 @@ static void launch_blk_rowop(int n, int ld, int K, const int* row, const int* co
     if (sh.W > 1 && (ld % sh.W != 0 || !aligned_for(x, sh.W, sizeof(XT)) || !aligned_for(y, sh.W, sizeof(YT)) ||
                         !aligned_for(f, sh.W, sizeof(FT))))
         sh = BlkShape { 1, ceil_log2(K) };
-    const long need = ((long)n + (8L << (5 - sh.lpe_log2)) - 1) / (8L << (5 - sh.lpe_log2));   // 8 warps x rows per warp
+    const long per_block = blk_rows_per_block<VT>(sh.lpe_log2, kBlkRowopThreads);
+    const long need = ((long)n + per_block - 1) / per_block;
+    const int stage_ok = (long)m * ld <= 0x7fffffffL ? 1 : 0;
     auto go = [&](auto kern) {
         note_launch();
-        kern<<<fit_grid(kern, 256, need), 256, 0, s>>>(n, sh.lpe_log2, ld, K, row, col, val, x, f, M, y, alpha, beta, skip);
+        kern<<<fit_grid(kern, kBlkRowopThreads, need), kBlkRowopThreads, 0, s>>>(n, sh.lpe_log2, ld, K, row, col, val, x,
+            f, M, y, alpha, beta, stage_ok, skip);
     };
     if constexpr (sizeof(XT) == 4) {
         if (sh.W == 4) {
@@ -251,7 +255,7 @@ struct Cycle {
     void rowop(const DevCsr& A, const VT* val, const XT* x, const FT* f, const MT* M, YT* y) const
     {
         if (lk < 0) launch_rowop_A<OP>(A.tpr, A, val, x, f, M, y, 1.0, 0.0, skip, s);
-        else launch_blk_rowop<OP>(A.n, 1 << lk, 1 << lk, A.row.p, A.col.p, val, x, f, M, y, 1.0, 0.0, skip, s);
+        else launch_blk_rowop<OP>(A.n, A.m, 1 << lk, 1 << lk, A.row.p, A.col.p, val, x, f, M, y, 1.0, 0.0, skip, s);
     }
     template <typename FT, typename MT, typename YT, typename CT>
     void first(int n, const FT* f, const MT* M, YT* u, CT* fcopy) const
@@ -297,7 +301,7 @@ struct Cycle {
     void restrict_to(int nc, const Level& V, const WT* rval, const RT* res, OT* out) const
     {
         if (lk >= 0) {
-            launch_blk_rowop<OP_AXPBY>(nc, 1 << lk, 1 << lk, V.rptr.p, V.ridx.p, rval, res, (const OT*)nullptr,
+            launch_blk_rowop<OP_AXPBY>(nc, V.A.n, 1 << lk, 1 << lk, V.rptr.p, V.ridx.p, rval, res, (const OT*)nullptr,
                 (const OT*)nullptr, out, 1.0, 0.0, skip, s);
             return;
         }
@@ -534,10 +538,10 @@ void cycle_apply_block(bcmgx_hierarchy* H, const CycleBufs& bufs, int lk, const 
     c.run(0, Vec { (void*)r, false }, Vec(), Vec { v, false });
 }
 
-void launch_spmm(int n, int K, const int* row, const int* col, const double* val, const double* X, double* Y,
+void launch_spmm(int n, int m, int K, const int* row, const int* col, const double* val, const double* X, double* Y,
     double alpha, double beta, cudaStream_t s)
 {
-    launch_blk_rowop<OP_AXPBY>(n, K, K, row, col, val, X, (const double*)nullptr, (const double*)nullptr, Y, alpha,
+    launch_blk_rowop<OP_AXPBY>(n, m, K, K, row, col, val, X, (const double*)nullptr, (const double*)nullptr, Y, alpha,
         beta, nullptr, s);
 }
 
@@ -854,6 +858,66 @@ void time_level_kernels(bcmgx_hierarchy* H, int l, int reps, double* out)
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+}
+
+// Average device time (CUDA events on the hierarchy's stream, reps launches after one warm-up)
+// of the level-0 block kernels for blocks of KP columns (K rounded up to a power of two, the
+// multi-right-hand-side solve's padded width): out[0] one block l1-Jacobi sweep in the cycle's
+// precision, out[1] the block residual, out[2] the FP64 block SpMM Y = A X, out[3] the block
+// FCG SpMV + per-column dots (time_block_dots). Inputs are zero blocks.
+void time_block_kernels(bcmgx_hierarchy* H, int K, int reps, double* out)
+{
+    ensure_solve_workspace(H);
+    cudaStream_t s = H->stream;
+    Level& V = H->lv[0];
+    const DevCsr& A = V.A;
+    const int L = (int)H->lv.size();
+    const bool f32 = H->prm.vcycle_precision == BCMGX_VCYCLE_FP32 && L > 1;
+    const int kp = 1 << ceil_log2(K);
+    const size_t nk = (size_t)A.n * kp;
+    DBuf<double> x, f, y;
+    x.alloc(nk, s);
+    y.alloc(nk, s);
+    BCMGX_CUDA(cudaMemsetAsync(x.p, 0, sizeof(double) * nk, s));
+    cudaEvent_t e0, e1;
+    BCMGX_CUDA(cudaEventCreate(&e0));
+    BCMGX_CUDA(cudaEventCreate(&e1));
+    auto timeit = [&](auto&& launch) {
+        launch();
+        BCMGX_CUDA(cudaEventRecord(e0, s));
+        for (int i = 0; i < reps; i++) launch();
+        BCMGX_CUDA(cudaEventRecord(e1, s));
+        BCMGX_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        BCMGX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        return (double)ms / reps;
+    };
+    if (f32) {
+        DBuf<float> x32, f32b, y32;
+        x32.alloc(nk, s);
+        f32b.alloc(nk, s);
+        y32.alloc(nk, s);
+        BCMGX_CUDA(cudaMemsetAsync(x32.p, 0, sizeof(float) * nk, s));
+        BCMGX_CUDA(cudaMemsetAsync(f32b.p, 0, sizeof(float) * nk, s));
+        out[0] = timeit([&] { launch_blk_rowop<OP_JACOBI>(A.n, A.m, kp, kp, A.row.p, A.col.p, A.val32.p,
+                                  (const float*)x32.p, (const float*)f32b.p, V.M32.p, y32.p, 1.0, 0.0, nullptr, s); });
+        out[1] = timeit([&] { launch_blk_rowop<OP_RESID>(A.n, A.m, kp, kp, A.row.p, A.col.p, A.val32.p,
+                                  (const float*)x32.p, (const float*)f32b.p, (const float*)nullptr, y32.p, 1.0, 0.0, nullptr, s); });
+        BCMGX_CUDA(cudaStreamSynchronize(s));
+    } else {
+        f.alloc(nk, s);
+        BCMGX_CUDA(cudaMemsetAsync(f.p, 0, sizeof(double) * nk, s));
+        out[0] = timeit([&] { launch_blk_rowop<OP_JACOBI>(A.n, A.m, kp, kp, A.row.p, A.col.p, A.val.p,
+                                  (const double*)x.p, (const double*)f.p, V.M.p, y.p, 1.0, 0.0, nullptr, s); });
+        out[1] = timeit([&] { launch_blk_rowop<OP_RESID>(A.n, A.m, kp, kp, A.row.p, A.col.p, A.val.p,
+                                  (const double*)x.p, (const double*)f.p, (const double*)nullptr, y.p, 1.0, 0.0, nullptr, s); });
+    }
+    out[2] = timeit([&] { launch_blk_rowop<OP_AXPBY>(A.n, A.m, kp, kp, A.row.p, A.col.p, A.val.p, (const double*)x.p,
+                              (const double*)nullptr, (const double*)nullptr, y.p, 1.0, 0.0, nullptr, s); });
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    BCMGX_CUDA(cudaStreamSynchronize(s));
+    out[3] = time_block_dots(H, K, reps);
 }
 
 // Threads-per-row autotuner: for a level with at least kTuneMinRows rows, one l1-Jacobi sweep

@@ -188,6 +188,12 @@ int bcmgx_prec_apply(bcmgx_hierarchy* h, const double* r, double* v, int on_devi
  * precision, out[1] the residual, out[2] the FP64 SpMV, out[3] the fused FCG SpMV + dots
  * (level 0 only). No counterpart in the reference: the measurement hook of the benchmarks. */
 int bcmgx_time_kernels(bcmgx_hierarchy* h, int level, int reps, double* out_ms);
+/* The same for the level-0 block kernels of a solve with nrhs (1..32) right-hand sides (blocks of
+ * nrhs rounded up to a power of two columns): out[0] one block l1-Jacobi sweep in the cycle's
+ * precision, out[1] the block residual, out[2] the FP64 block SpMM, out[3] the block FCG SpMV +
+ * per-column dots. Allocates the multi-right-hand-side workspace. No counterpart in the
+ * reference (its solve takes one vector). */
+int bcmgx_time_block_kernels(bcmgx_hierarchy* h, int nrhs, int reps, double* out_ms);
 
 /* ---- batched solves (no counterpart in the reference) ------------------------------------ */
 /* Many independent systems solved together: their set-ups run concurrently (nthreads host

@@ -10,9 +10,11 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("k", [1, 5, 32])
-@pytest.mark.parametrize("case", [("lap27", (14, 13, 12)), ("rand", (3000, 0.004, 3))])
+@pytest.mark.parametrize("case", [("lap27", (14, 13, 12)), ("rand", (3000, 0.004, 3)), ("rand", (1500, 0.04, 4))])
 def test_spmm_matches_scipy(bx, cuda, case, k):
-    """Y = alpha A X + beta Y against scipy in FP64 (entries summed in row order: 1e-14 relative)."""
+    """Y = alpha A X + beta Y against scipy in FP64 (entries summed in row order: 1e-14 relative).
+    The last matrix has about 60 entries per row, more than a warp step stages in shared memory,
+    so its products read the entries from global memory."""
     import torch
     A = as_csr(bx, case)
     n = A.shape[0]
@@ -125,3 +127,18 @@ def test_multi_graph_and_stream_drivers_agree(bx, cuda, prec):
         out[g] = (X, [i["niter"] for i in infos])
     assert out[0][1] == out[1][1]
     assert np.array_equal(out[0][0], out[1][0])
+
+
+def test_block_kernel_timing_hook(bx, cuda):
+    """bcmgx_time_block_kernels times the four level-0 block kernels; a solve afterwards is unchanged."""
+    A = as_csr(bx, ("lap27", (20, 20, 20)))
+    B = np.random.default_rng(8).uniform(-1, 1, (A.shape[0], 5))
+    p = bx.params_default(solver="FCG", rtol=1e-9, dispnorm=0, vcycle_precision="FP32")
+    h = bx.prec_setup(A.indptr, A.indices, A.data, p)
+    X0, _ = h.solve_multi(B)
+    t = h.time_block_kernels(5, reps=3)
+    assert all(t[key] > 0 for key in ("jacobi", "residual", "spmm", "fcg_spmm_dots")), t
+    X1, _ = h.solve_multi(B)
+    assert np.array_equal(X0, X1)
+    with pytest.raises(bx.BcmgxError):
+        h.time_block_kernels(33)

@@ -133,19 +133,24 @@ struct BlkStage {
     static constexpr int rows = sizeof(VT) == 4 ? 8 : 4;
     static constexpr int cap = 32 * rows;
 };
-// resident blocks per SM the kernel is compiled for: 6 (40 registers), 5 (48) for FP64 values
-// with four columns per lane
+// resident blocks per SM the kernel is compiled for: 5 (48 registers) for four columns per
+// lane, else 6 (40 registers)
 template <typename VT, int W>
-constexpr int blk_min_blocks() { return sizeof(VT) == 8 && W == 4 ? 5 : 6; }
+constexpr int blk_min_blocks() { return W == 4 ? 5 : 6; }
 constexpr int kBlkRowopThreads = 256;
 
 // acc[w] = sum over staged entries [b, e) of v * Xc[off + w], entries in order; U entries per
 // batch without predicates (all loads of the batch issue before its multiply-adds), then the
 // remainder one entry at a time.
+// Entries per batch: 3 keeps the batch's loads in registers at the 40-48 register budget (4
+// spills; on 32-column blocks of the 27-point 100^3 matrix, 3 was 4-8 % faster than 4 and 2)
+#ifndef BCMGX_BLK_BATCH
+#define BCMGX_BLK_BATCH 3
+#endif
 template <int W, typename AT, typename VT, typename XT>
 __device__ __forceinline__ void blk_row_staged(int b, int e, const BlkEnt<VT>* s, const XT* __restrict__ Xc, AT (&acc)[W])
 {
-    constexpr int U = 4;
+    constexpr int U = BCMGX_BLK_BATCH;
 #pragma unroll
     for (int w = 0; w < W; w++) acc[w] = 0;
     int j = b;

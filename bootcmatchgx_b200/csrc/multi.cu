@@ -98,7 +98,7 @@ __global__ void k_blk_init(BlockState* st, int K, double rtol, int itnlim)
 
 // R = B - A X and per column delta0 = ||r||, tol = rtol * delta0 (FCG.cu:46-51).
 template <int W>
-__global__ void __launch_bounds__(kBlkThreads, 5) k_blk_resid0(int n, int lpe_log2, int kp, const int* __restrict__ row,
+__global__ void __launch_bounds__(kBlkThreads, 4) k_blk_resid0(int n, int lpe_log2, int kp, const int* __restrict__ row,
     const int* __restrict__ col, const double* __restrict__ val, const double* __restrict__ X, const double* __restrict__ B,
     double* __restrict__ R, BlockState* st, double* partials, int stage_ok)
 {
@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(kBlkThreads, 5) k_blk_resid0(int n, int lpe_lo
 // PW = A PV with the per-column dots alpha = r.pv, beta = pw.pv (and gamma = oq.pv in the loop),
 // then the scalar recurrence of each running column (FCG.cu:59-86, 121-136).
 template <int MODE, int W>
-__global__ void __launch_bounds__(kBlkThreads, 5) k_blk_spmv_dots(int n, int lpe_log2, int kp, const int* __restrict__ row,
+__global__ void __launch_bounds__(kBlkThreads, 4) k_blk_spmv_dots(int n, int lpe_log2, int kp, const int* __restrict__ row,
     const int* __restrict__ col, const double* __restrict__ val, const double* __restrict__ PV, double* __restrict__ PW,
     const double* __restrict__ R, const double* __restrict__ OQ, BlockState* st, double* partials, int stage_ok,
     const int* __restrict__ skip)

@@ -685,7 +685,7 @@ int bcmgx_suitor_matching(int n, int64_t nnz, const int* row, const int* col, co
         validate_csr_dev(n, n, nnz, row, col, false, s);
         DBuf<int> tpos;
         tpos.alloc(nnz, s);
-        tpos_dev(n, row, col, tpos.p, s);
+        tpos_dev(n, nnz, row, col, tpos.p, s);
         suitor_dev(n, nnz, row, col, W, tpos.p, M, s);
         BCMGX_CUDA(cudaStreamSynchronize(s));
     });

@@ -290,27 +290,71 @@ __global__ void k_diag_c(int n, const int* __restrict__ row, const int* __restri
     }
 }
 
+// Row loop of the matching kernels: a sub-warp of S lanes (a power of two, 4..32, from the
+// average row length) owns a row and its lanes stride over the row's entries, so a warp keeps
+// 32 / S rows in flight; each lane takes its entries in batches of kSetupBatch, issuing all loads
+// of a batch before the loads that depend on them.
+constexpr int kSetupBatch = 4;
+#define BCMGX_SUBWARP_ROWS(r, n, S)                                                                  \
+    for (long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) / (S); r < (n);                      \
+         r += (long)gridDim.x * blockDim.x / (S))
+
+// lanes per row for the matching kernels: about 4 entries per lane
+static int setup_subwarp(long n, int64_t nnz)
+{
+    const double avg = n > 0 ? (double)nnz / (double)n : 1.0;
+    return avg <= 12 ? 4 : avg <= 40 ? 8 : avg <= 96 ? 16 : 32;
+}
+
 // Position of the transposed entry: tpos[j] for a_rc is the index of a_cr in row c (-1 if the
-// pattern has no a_cr); the diagonal maps to itself. One warp per row.
+// pattern has no a_cr); the diagonal maps to itself. The binary searches of a lane's batch run
+// in lock step, one round of independent loads per halving.
+template <int S>
 __global__ void k_tpos(int n, const int* __restrict__ row, const int* __restrict__ col, int* __restrict__ tpos)
 {
-    const int lane = threadIdx.x & 31;
-    for (long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32; r < n; r += (long)gridDim.x * blockDim.x / 32) {
-        const int b = row[r], e = row[r + 1];
-        for (int j = b + lane; j < e; j += 32) {
-            const int c = col[j];
-            if (c == r) {
-                tpos[j] = j;
-                continue;
+    constexpr int U = kSetupBatch;
+    const int lane = threadIdx.x & (S - 1);
+    BCMGX_SUBWARP_ROWS(r, n, S)
+    {
+        const int b = __ldg(row + r), e = __ldg(row + r + 1);
+        for (int j0 = b + lane; j0 < e; j0 += U * S) {
+            int c[U], lo[U], hi[U], end[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) c[u] = j0 + u * S < e ? __ldg(col + j0 + u * S) : -1;
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const bool srch = c[u] >= 0 && c[u] != (int)r;
+                lo[u] = srch ? __ldg(row + c[u]) : 0;
+                end[u] = srch ? __ldg(row + c[u] + 1) : 0;
+                hi[u] = end[u];
             }
-            int lo = row[c], hi = row[c + 1];
-            const int end = hi;
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (col[mid] < (int)r) lo = mid + 1;
-                else hi = mid;
+            for (int step = 0; step < 32; step++) {
+                int cm[U];
+                bool any = false;
+#pragma unroll
+                for (int u = 0; u < U; u++)
+                    if (lo[u] < hi[u]) {
+                        any = true;
+                        cm[u] = __ldg(col + ((lo[u] + hi[u]) >> 1));
+                    }
+                if (!any) break;
+#pragma unroll
+                for (int u = 0; u < U; u++)
+                    if (lo[u] < hi[u]) {
+                        const int mid = (lo[u] + hi[u]) >> 1;
+                        if (cm[u] < (int)r) lo[u] = mid + 1;
+                        else hi[u] = mid;
+                    }
             }
-            tpos[j] = (lo < end && col[lo] == (int)r) ? lo : -1;
+            int hit[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) hit[u] = c[u] >= 0 && c[u] != (int)r && lo[u] < end[u] ? __ldg(col + lo[u]) : -1;
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int j = j0 + u * S;
+                if (c[u] < 0) continue;
+                tpos[j] = c[u] == (int)r ? j : (hit[u] == (int)r ? lo[u] : -1);
+            }
         }
     }
 }
@@ -329,18 +373,34 @@ __device__ __forceinline__ double ahat(double a, double Cr, double Cc, double wr
 
 // min over all off-diagonal |a_hat| (find_Max_Min with AbsMin, matching.cu:188-217). The bit
 // pattern of a non-negative double orders like its value, so atomicMin on it is exact.
+template <int S>
 __global__ void k_ahat_min(int n, const int* __restrict__ row, const int* __restrict__ col, const double* __restrict__ val,
     const double* __restrict__ w, const double* __restrict__ C, unsigned long long* min_bits)
 {
-    const int lane = threadIdx.x & 31;
+    constexpr int U = kSetupBatch;
+    const int lane = threadIdx.x & (S - 1);
     double mn = DBL_MAX;
-    for (long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32; r < n; r += (long)gridDim.x * blockDim.x / 32) {
-        const int b = row[r], e = row[r + 1];
-        const double Cr = C[r], wr = w[r];
-        for (int j = b + lane; j < e; j += 32) {
-            const int c = col[j];
-            if (c == r) continue;
-            mn = fmin(mn, fabs(ahat(val[j], Cr, C[c], wr, w[c])));
+    BCMGX_SUBWARP_ROWS(r, n, S)
+    {
+        const int b = __ldg(row + r), e = __ldg(row + r + 1);
+        const double Cr = __ldg(C + r), wr = __ldg(w + r);
+        for (int j0 = b + lane; j0 < e; j0 += U * S) {
+            int c[U];
+            double a[U], Cc[U], wc[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const bool in = j0 + u * S < e;
+                c[u] = in ? __ldg(col + j0 + u * S) : (int)r;
+                a[u] = in ? __ldg(val + j0 + u * S) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                Cc[u] = c[u] != (int)r ? __ldg(C + c[u]) : 0.0;
+                wc[u] = c[u] != (int)r ? __ldg(w + c[u]) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++)
+                if (c[u] != (int)r) mn = fmin(mn, fabs(ahat(a[u], Cr, Cc[u], wr, wc[u])));
         }
     }
     unsigned long long bits = (unsigned long long)__double_as_longlong(mn);
@@ -348,29 +408,51 @@ __global__ void k_ahat_min(int n, const int* __restrict__ row, const int* __rest
         unsigned long long other = __shfl_xor_sync(0xffffffffu, bits, o);
         bits = other < bits ? other : bits;
     }
-    if (lane == 0) atomicMin(min_bits, bits);
+    if ((threadIdx.x & 31) == 0) atomicMin(min_bits, bits);
 }
 
 // W = log(|a_hat|), or log(SUITOR_EPS / (0.999 min)) where a_hat == 0 (_make_w,
 // matching.cu:219-229); a lower entry takes the value of its upper counterpart
 // (_write_T_warp, matching.cu:29-64), i.e. is computed from a_cr. Diagonal slots are 0.
+template <int S>
 __global__ void k_logw(int n, const int* __restrict__ row, const int* __restrict__ col, const double* __restrict__ val,
     const double* __restrict__ w, const double* __restrict__ C, const int* __restrict__ tpos, double zero_sub,
     double* __restrict__ W)
 {
-    const int lane = threadIdx.x & 31;
-    for (long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32; r < n; r += (long)gridDim.x * blockDim.x / 32) {
-        const int b = row[r], e = row[r + 1];
-        const double Cr = C[r], wr = w[r];
-        for (int j = b + lane; j < e; j += 32) {
-            const int c = col[j];
-            if (c == r) {
-                W[j] = 0.0;
-                continue;
+    constexpr int U = kSetupBatch;
+    const int lane = threadIdx.x & (S - 1);
+    BCMGX_SUBWARP_ROWS(r, n, S)
+    {
+        const int b = __ldg(row + r), e = __ldg(row + r + 1);
+        const double Cr = __ldg(C + r), wr = __ldg(w + r);
+        for (int j0 = b + lane; j0 < e; j0 += U * S) {
+            int c[U], src[U];
+            double a[U], Cc[U], wc[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int j = j0 + u * S;
+                c[u] = j < e ? __ldg(col + j) : -1;
+                src[u] = j < e ? __ldg(tpos + j) : -1;
             }
-            const int src = (c < r && tpos[j] >= 0) ? tpos[j] : j;
-            const double s = fabs(ahat(val[src], Cr, C[c], wr, w[c]));
-            W[j] = log(s != 0.0 ? s : zero_sub);
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const bool off = c[u] >= 0 && c[u] != (int)r;
+                src[u] = (c[u] < (int)r && src[u] >= 0) ? src[u] : j0 + u * S;
+                a[u] = off ? __ldg(val + src[u]) : 0.0;
+                Cc[u] = off ? __ldg(C + c[u]) : 0.0;
+                wc[u] = off ? __ldg(w + c[u]) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int j = j0 + u * S;
+                if (c[u] < 0) continue;
+                if (c[u] == (int)r) {
+                    W[j] = 0.0;
+                    continue;
+                }
+                const double sa = fabs(ahat(a[u], Cr, Cc[u], wr, wc[u]));
+                W[j] = log(sa != 0.0 ? sa : zero_sub);
+            }
         }
     }
 }
@@ -445,23 +527,49 @@ __global__ void k_rank(int n, const int* __restrict__ row, const int* __restrict
 // Preference records: pref[row[v] + k] = {k-th candidate y of v, v's offer value at y}, where
 // the offer value is degE[y] - (rank of v in y's list), or 0 when y does not rank v (no
 // transposed entry: the pair is never proposed). rinfo[v] = {row[v], degE[v]}.
+template <int S>
 __global__ void k_pref(int n, const int* __restrict__ row, const int* __restrict__ col, const int* __restrict__ ordj,
     const int* __restrict__ rank, const int* __restrict__ tpos, const int* __restrict__ degE, int2* __restrict__ pref,
     int2* __restrict__ rinfo)
 {
-    const int lane = threadIdx.x & 31;
-    for (long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32; r < n; r += (long)gridDim.x * blockDim.x / 32) {
-        const int b = row[r], dE = degE[r];
-        for (int k = lane; k < dE; k += 32) {
-            const int j = ordj[b + k];
-            const int y = col[j];
-            const int tj = tpos[j];
-            const int ry = tj >= 0 ? rank[tj] : -1;
-            pref[b + k] = make_int2(y, ry >= 0 ? degE[y] - ry : 0);
+    constexpr int U = kSetupBatch;
+    const int lane = threadIdx.x & (S - 1);
+    BCMGX_SUBWARP_ROWS(r, n, S)
+    {
+        const int b = __ldg(row + r), dE = __ldg(degE + r);
+        for (int k0 = lane; k0 < dE; k0 += U * S) {
+            int j[U], y[U], tj[U], ry[U], dy[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) j[u] = k0 + u * S < dE ? __ldg(ordj + b + k0 + u * S) : -1;
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                y[u] = j[u] >= 0 ? __ldg(col + j[u]) : 0;
+                tj[u] = j[u] >= 0 ? __ldg(tpos + j[u]) : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                ry[u] = tj[u] >= 0 ? __ldg(rank + tj[u]) : -1;
+                dy[u] = j[u] >= 0 ? __ldg(degE + y[u]) : 0;
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++)
+                if (j[u] >= 0) pref[b + k0 + u * S] = make_int2(y[u], ry[u] >= 0 ? dy[u] - ry[u] : 0);
         }
         if (lane == 0) rinfo[r] = make_int2(b, dE);
     }
 }
+
+// launch of a matching kernel K<S> for the lanes-per-row choice S of setup_subwarp
+#define BCMGX_SUBWARP_LAUNCH(K, S, n, s, ...)                                                      \
+    do {                                                                                           \
+        note_launch();                                                                             \
+        switch (S) {                                                                               \
+        case 4: K<4><<<gs_grid((long)(n) * 4), 256, 0, s>>>(__VA_ARGS__); break;                   \
+        case 8: K<8><<<gs_grid((long)(n) * 8), 256, 0, s>>>(__VA_ARGS__); break;                   \
+        case 16: K<16><<<gs_grid((long)(n) * 16), 256, 0, s>>>(__VA_ARGS__); break;                \
+        default: K<32><<<gs_grid((long)(n) * 32), 256, 0, s>>>(__VA_ARGS__); break;                \
+        }                                                                                          \
+    } while (0)
 
 // Lock-free suitor. A vertex proposes to its candidates in preference order; y keeps the best
 // suitor by atomicMax on its offer word (set_suitor/find_Candidate, suitor.cu:51-147, with the
@@ -787,9 +895,10 @@ void edge_weights_dev(int n, int64_t nnz, const int* row, const int* col, const 
     BCMGX_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), s));
     const double dmax = DBL_MAX;
     BCMGX_CUDA(cudaMemcpyAsync(mn.p, &dmax, sizeof(double), cudaMemcpyHostToDevice, s));
+    const int S = setup_subwarp(n, nnz);
     note_launch(); k_diag_c<<<gs_grid(n), 256, 0, s>>>(n, row, col, val, w, C.p, err.p);
-    note_launch(); k_tpos<<<warp_grid(n), 256, 0, s>>>(n, row, col, tpos);
-    note_launch(); k_ahat_min<<<warp_grid(n), 256, 0, s>>>(n, row, col, val, w, C.p, mn.p);
+    BCMGX_SUBWARP_LAUNCH(k_tpos, S, n, s, n, row, col, tpos);
+    BCMGX_SUBWARP_LAUNCH(k_ahat_min, S, n, s, n, row, col, val, w, C.p, mn.p);
     BCMGX_CHECK_LAUNCH();
     double m = 0;
     BCMGX_CUDA(cudaMemcpyAsync(&m, mn.p, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -797,7 +906,7 @@ void edge_weights_dev(int n, int64_t nnz, const int* row, const int* col, const 
     if (e) throw Error(BCMGX_ERR_INVALID_INPUT, "edge weights: " + err_text(e));
     if (std::fabs(m) < DBL_EPSILON) m = DBL_EPSILON;   // toMaximumProductMatrix, matching.cu:243-245
     const double zero_sub = kSuitorEps / (0.999 * m);
-    note_launch(); k_logw<<<warp_grid(n), 256, 0, s>>>(n, row, col, val, w, C.p, tpos, zero_sub, W);
+    BCMGX_SUBWARP_LAUNCH(k_logw, S, n, s, n, row, col, val, w, C.p, tpos, zero_sub, W);
     BCMGX_CHECK_LAUNCH();
     if (min_out_host) *min_out_host = m;
 }
@@ -816,9 +925,9 @@ void validate_csr_dev(int n, int m, int64_t nnz, const int* row, const int* col,
     if (e) throw Error(BCMGX_ERR_INVALID_INPUT, "input matrix: " + err_text(e));
 }
 
-void tpos_dev(int n, const int* row, const int* col, int* tpos, cudaStream_t s)
+void tpos_dev(int n, int64_t nnz, const int* row, const int* col, int* tpos, cudaStream_t s)
 {
-    note_launch(); k_tpos<<<warp_grid(n), 256, 0, s>>>(n, row, col, tpos);
+    BCMGX_SUBWARP_LAUNCH(k_tpos, setup_subwarp(n, nnz), n, s, n, row, col, tpos);
     BCMGX_CHECK_LAUNCH();
 }
 
@@ -838,7 +947,7 @@ void suitor_dev(int n, int64_t nnz, const int* row, const int* col, const double
     note_launch(); k_rank<<<warp_grid(n), 256, 0, s>>>(n, row, col, W, rank.p, ordj.p, degE.p);
     pref.alloc(z, s);
     rinfo.alloc(n, s);
-    note_launch(); k_pref<<<warp_grid(n), 256, 0, s>>>(n, row, col, ordj.p, rank.p, tpos, degE.p, pref.p, rinfo.p);
+    BCMGX_SUBWARP_LAUNCH(k_pref, setup_subwarp(n, nnz), n, s, n, row, col, ordj.p, rank.p, tpos, degE.p, pref.p, rinfo.p);
     BCMGX_CHECK_LAUNCH();
     rank.release();
     ordj.release();
@@ -1246,18 +1355,16 @@ static void edge_weights_noalloc(int n, int64_t nnz, const int* row, const int* 
     if (e) throw Error(BCMGX_ERR_INVALID_INPUT, "input matrix: " + err_text(e));
     note_launch();
     k_diag_c<<<gs_grid(n), 256, 0, s>>>(n, row, col, val, w, C, err);
-    note_launch();
-    k_tpos<<<warp_grid(n), 256, 0, s>>>(n, row, col, tpos);
-    note_launch();
-    k_ahat_min<<<warp_grid(n), 256, 0, s>>>(n, row, col, val, w, C, minb);
+    const int S = setup_subwarp(n, nnz);
+    BCMGX_SUBWARP_LAUNCH(k_tpos, S, n, s, n, row, col, tpos);
+    BCMGX_SUBWARP_LAUNCH(k_ahat_min, S, n, s, n, row, col, val, w, C, minb);
     BCMGX_CHECK_LAUNCH();
     double m = 0;
     BCMGX_CUDA(cudaMemcpyAsync(&m, minb, sizeof(double), cudaMemcpyDeviceToHost, s));
     e = read_err(err, s);
     if (e) throw Error(BCMGX_ERR_INVALID_INPUT, "edge weights: " + err_text(e));
     if (std::fabs(m) < DBL_EPSILON) m = DBL_EPSILON;
-    note_launch();
-    k_logw<<<warp_grid(n), 256, 0, s>>>(n, row, col, val, w, C, tpos, kSuitorEps / (0.999 * m), W);
+    BCMGX_SUBWARP_LAUNCH(k_logw, S, n, s, n, row, col, val, w, C, tpos, kSuitorEps / (0.999 * m), W);
     BCMGX_CHECK_LAUNCH();
     BCMGX_CUDA(cudaStreamSynchronize(s));
     if (min_out) *min_out = m;

@@ -207,6 +207,51 @@ def max_over_ranks(x, world, device=None):
     return float(t.item())
 
 
+def time_vcycle(h, r, stream, reps=10):
+    """ms of one preconditioner application v = B r (the V-cycle) on device vectors, CUDA events
+    on the hierarchy's stream, after one warm-up application."""
+    import torch
+    h.prec_apply(r)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        h.prec_apply(r)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def vcycle_bytes(inf, pre, post, coarse):
+    """Algorithmic bytes of one FP32 V-cycle as the kernels run it: on every level but the last,
+    pre + post - 1 l1-Jacobi sweeps over the FP32 matrix (the first pre-sweep starts from zero and
+    reads no matrix), the residual, the restriction R r (one entry per fine row) and the
+    prolongation x += p x_c[agg]; the coarsest level runs `coarse` FP64 sweeps (the first from
+    zero). Matrix entries
+    count index_bytes + value bytes, vectors 4 bytes (8 on the coarsest level); level 0 also reads
+    the FP64 residual and writes the FP64 output."""
+    n, z, ib = inf["n"], inf["nnz"], inf["index_bytes"]
+    total = 0
+    for l in range(len(n) - 1):
+        nl, zl, nc = n[l], z[l], n[l + 1]
+        sweep = (ib[l] + 4) * zl + 4 * (nl + 1) + 16 * nl
+        total += (pre + post - 1) * sweep + 12 * nl
+        total += (ib[l] + 4) * zl + 4 * (nl + 1) + 12 * nl
+        total += 4 * (nc + 1) + 8 * nl + 4 * nl + 4 * nc
+        total += 8 * nl + 4 * nc + 8 * nl
+        if l == 0:
+            total += 8 * nl + 4 * nl
+    nL, zL = n[-1], z[-1]
+    total += (coarse - 1) * ((ib[-1] + 8) * zL + 4 * (nL + 1) + 32 * nL) + 24 * nL
+    return int(total)
+
+
+def vcycle_roofline(ms, inf, p, peak, peak_kind):
+    b = vcycle_bytes(inf, p.prerelax_sweeps, p.postrelax_sweeps, p.relaxnumber_coarse)
+    return {"ms": ms, "algorithmic_bytes": b, "gbs": b / ms / 1e6, "frac": b / ms / 1e6 / peak,
+            "peak": peak, "peak_kind": f"{peak_kind} hbm_gbs (copy)",
+            "what": "one FP32 V-cycle (bcmgx_prec_apply on device vectors), CUDA events"}
+
+
 def run_ours(a, wl, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -283,6 +328,7 @@ def run_ours(a, wl, rank, world, local_rank):
     # ---- kernel figures on kept hierarchies (same stream, CUDA events)
     h32, _, inf32 = step("FP32", keep=True)
     k32 = h32.time_kernels(0, reps=20)
+    vc_ms = time_vcycle(h32, d_b, stream)
     h64, _, inf64 = step("FP64", keep=True)
     k64f = h64.time_kernels(0, reps=20)
     spmv_ms = k64f["spmv"]
@@ -357,6 +403,7 @@ def run_ours(a, wl, rank, world, local_rank):
                    "fp64_vs_xstar": None if xs is None else float(nrm(x64 - xs) / nrm(xs)),
                    "fp32_vs_fp64_tight": float(nrm(x32 - xt) / nrm(xt)),
                    "fp64_vs_fp64_tight": float(nrm(x64 - xt) / nrm(xt)),
+                   "fp32_vs_fp64": float(nrm(x32 - x64) / nrm(x64)),
                    "fp32_rel_residual": float(nrm(b - _spmv(row, col, val, x32)) / nrm(b))},
         "spmv": {"gbs": gbs_spmv, "ms": spmv_ms, "bytes": bytes_spmv, "frac_of_peak": gbs_spmv / peak,
                  "frac_of_8TBs_nominal": gbs_spmv / 8000.0},
@@ -365,6 +412,7 @@ def run_ours(a, wl, rank, world, local_rank):
                            "fp32_residual_ms": k32["residual"], "fp64_jacobi_ms": k64f["jacobi"],
                            "fp64_jacobi_gbs": gbs_jac64, "fcg_spmv_dots_ms": k64f["fcg_spmv_dots"]},
         "kernels_coarse_levels_fp32_jacobi_ms": [round(k["jacobi"], 4) for k in lvl],
+        "vcycle": vcycle_roofline(vc_ms, inf32, params("FP32"), peak, peak_kind),
         "roofline": {"kernel": f"k_rowop<{inf32['tpr'][0]},OP_JACOBI,float> (FP32 l1-Jacobi sweep, level 0)",
                      "bound": "hbm", "achieved": gbs_jac32, "peak": peak, "unit": "GB/s",
                      "frac": gbs_jac32 / peak, "peak_kind": f"{peak_kind} hbm_gbs (copy)",

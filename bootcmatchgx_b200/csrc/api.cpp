@@ -686,7 +686,7 @@ int bcmgx_suitor_matching(int n, int64_t nnz, const int* row, const int* col, co
         DBuf<int> tpos;
         tpos.alloc(nnz, s);
         tpos_dev(n, nnz, row, col, tpos.p, s);
-        suitor_dev(n, nnz, row, col, W, tpos.p, M, s);
+        suitor_dev(n, nnz, row, col, W, tpos.p, M, 0, s);
         BCMGX_CUDA(cudaStreamSynchronize(s));
     });
 }

@@ -279,7 +279,7 @@ void edge_weights_dev(int n, int64_t nnz, const int* row, const int* col, const 
     const double* w, double* W, int* tpos, double* min_out_host, cudaStream_t s);
 void validate_csr_dev(int n, int m, int64_t nnz, const int* row, const int* col, bool need_diag, cudaStream_t s);
 void tpos_dev(int n, int64_t nnz, const int* row, const int* col, int* tpos, cudaStream_t s);
-void suitor_dev(int n, int64_t nnz, const int* row, const int* col, const double* W, const int* tpos,
-    int* M, cudaStream_t s);
+void suitor_dev(int n, int64_t nnz, const int* row, const int* col, const double* W, const int* tpos, int* M, int max_row,
+    cudaStream_t s);
 
 }  // namespace bcmgx

@@ -10,8 +10,9 @@
 // bit-identical to the CPU restatement. Integer results (matching, aggregates, sizes) do not
 // depend on thread scheduling:
 //  * the suitor matching is lock-free: every vertex ranks its neighbours once, offers are
-//    32-bit ranks combined with atomicMax, and each vertex's search pointer only moves forward,
-//    so the work is bounded by nnz and the result is the greedy matching of the edge order;
+//    ranks combined with atomicMax (64-bit words that also name the proposer), and each
+//    vertex's search pointer only moves forward, so the work is bounded by nnz and the result
+//    is the greedy matching of the edge order;
 //  * aggregates are numbered by prefix sums (pairs by master id, then singletons by id);
 //  * every Galerkin entry is a sum of at most two rounded products, formed in a fixed order.
 #include "internal.h"
@@ -615,6 +616,55 @@ __global__ void k_suitor(int n, const int2* __restrict__ rinfo, const int2* __re
     }
 }
 
+// The same suitor with 64-bit offer words [offer value (16 bits) | proposer v (32) | index of y in
+// v's list (16)], for rows of fewer than 65536 entries. Offer values at y differ between
+// proposers, so atomicMax orders the words as it orders the offer values and the matching is
+// the same; but the word a proposal displaces names the old suitor d and its position at y, so
+// d resumes at once instead of after two dependent lookups, and the proposal needs no load of
+// the current offer first. Each step of a displacement chain is then three dependent memory
+// operations (row info, preference record, atomic) instead of seven.
+__global__ void k_suitor_w(int n, const int2* __restrict__ rinfo, const int2* __restrict__ pref,
+    unsigned long long* offer, long long budget, int* err, int descending)
+{
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+        int cur = descending ? (int)(n - 1 - t) : (int)t;
+        int k = 0;
+        long long steps = 0;
+        while (cur >= 0) {
+            const int2 ci = __ldg(rinfo + cur);
+            int next = -1, nextk = 0;
+            for (; k < ci.y; k++) {
+                if (++steps > budget) {
+                    atomicOr(err, ERR_SUITOR_BUDGET);
+                    return;
+                }
+                const int2 pr = __ldg(pref + ci.x + k);
+                if (pr.y == 0) continue;
+                const unsigned long long mine = ((unsigned long long)(unsigned)pr.y << 48) |
+                    ((unsigned long long)(unsigned)cur << 16) | (unsigned long long)(unsigned)k;
+                const unsigned long long old = atomicMax(offer + pr.x, mine);
+                if (old < mine) {
+                    if (old != 0ull) {
+                        next = (int)((old >> 16) & 0xffffffffull);
+                        nextk = (int)(old & 0xffffull) + 1;
+                    }
+                    break;
+                }
+            }
+            cur = next;
+            k = nextk;
+        }
+    }
+}
+
+__global__ void k_suitor_result_w(int n, const unsigned long long* __restrict__ offer, int* __restrict__ M)
+{
+    for (long y = (long)blockIdx.x * blockDim.x + threadIdx.x; y < n; y += (long)gridDim.x * blockDim.x) {
+        const unsigned long long o = offer[y];
+        M[y] = o ? (int)((o >> 16) & 0xffffffffull) : -1;
+    }
+}
+
 // M[y] = suitor of y, or -1 (the suitors array the reference returns, suitor.cu:303-329).
 __global__ void k_suitor_result(int n, const int2* __restrict__ rinfo, const int2* __restrict__ pref,
     const unsigned* __restrict__ offer, int* __restrict__ M)
@@ -873,15 +923,16 @@ static int read_err(const int* err, cudaStream_t s)
     return e;
 }
 
-static int row_max(const DevCsr& A, cudaStream_t s)
+static int row_max_raw(int n, const int* row, cudaStream_t s)
 {
     DBuf<int> mx;
     mx.alloc(1, s);
     BCMGX_CUDA(cudaMemsetAsync(mx.p, 0, sizeof(int), s));
-    note_launch(); k_row_max<<<gs_grid(A.n), 256, 0, s>>>(A.n, A.row.p, mx.p);
+    note_launch(); k_row_max<<<gs_grid(n), 256, 0, s>>>(n, row, mx.p);
     BCMGX_CHECK_LAUNCH();
     return read_err(mx.p, s);
 }
+static int row_max(const DevCsr& A, cudaStream_t s) { return row_max_raw(A.n, A.row.p, s); }
 
 void edge_weights_dev(int n, int64_t nnz, const int* row, const int* col, const double* val, const double* w, double* W,
     int* tpos, double* min_out_host, cudaStream_t s)
@@ -931,19 +982,28 @@ void tpos_dev(int n, int64_t nnz, const int* row, const int* col, int* tpos, cud
     BCMGX_CHECK_LAUNCH();
 }
 
-void suitor_dev(int n, int64_t nnz, const int* row, const int* col, const double* W, const int* tpos, int* M, cudaStream_t s)
+void suitor_dev(int n, int64_t nnz, const int* row, const int* col, const double* W, const int* tpos, int* M, int max_row,
+    cudaStream_t s)
 {
+    if (max_row <= 0) max_row = row_max_raw(n, row, s);
+    const bool wide = max_row < 65536;
     DBuf<int> rank, ordj, degE, err;
     DBuf<int2> pref, rinfo;
     DBuf<unsigned> offer;
+    DBuf<unsigned long long> offer_w;
     const int64_t z = std::max<int64_t>(nnz, 1);
     rank.alloc(z, s);
     ordj.alloc(z, s);
     degE.alloc(n, s);
-    offer.alloc(n, s);
     err.alloc(1, s);
     BCMGX_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), s));
-    BCMGX_CUDA(cudaMemsetAsync(offer.p, 0, sizeof(unsigned) * n, s));
+    if (wide) {
+        offer_w.alloc(n, s);
+        BCMGX_CUDA(cudaMemsetAsync(offer_w.p, 0, sizeof(unsigned long long) * n, s));
+    } else {
+        offer.alloc(n, s);
+        BCMGX_CUDA(cudaMemsetAsync(offer.p, 0, sizeof(unsigned) * n, s));
+    }
     note_launch(); k_rank<<<warp_grid(n), 256, 0, s>>>(n, row, col, W, rank.p, ordj.p, degE.p);
     pref.alloc(z, s);
     rinfo.alloc(n, s);
@@ -956,8 +1016,14 @@ void suitor_dev(int n, int64_t nnz, const int* row, const int* col, const double
         const char* e = std::getenv("BCMGX_SUITOR_ASC");
         asc = (e && std::atoi(e) > 0) ? 1 : 0;
     }
-    note_launch(); k_suitor<<<ceil_div(n, 128), 128, 0, s>>>(n, rinfo.p, pref.p, offer.p, (long long)nnz + n + 1024, err.p, asc ? 0 : 1);
-    note_launch(); k_suitor_result<<<gs_grid(n), 256, 0, s>>>(n, rinfo.p, pref.p, offer.p, M);
+    const long long budget = (long long)nnz + n + 1024;
+    if (wide) {
+        note_launch(); k_suitor_w<<<ceil_div(n, 128), 128, 0, s>>>(n, rinfo.p, pref.p, offer_w.p, budget, err.p, asc ? 0 : 1);
+        note_launch(); k_suitor_result_w<<<gs_grid(n), 256, 0, s>>>(n, offer_w.p, M);
+    } else {
+        note_launch(); k_suitor<<<ceil_div(n, 128), 128, 0, s>>>(n, rinfo.p, pref.p, offer.p, budget, err.p, asc ? 0 : 1);
+        note_launch(); k_suitor_result<<<gs_grid(n), 256, 0, s>>>(n, rinfo.p, pref.p, offer.p, M);
+    }
     note_launch(); k_check_symmetric<<<gs_grid(n), 256, 0, s>>>(n, M, err.p);
     BCMGX_CHECK_LAUNCH();
     int e = read_err(err.p, s);
@@ -988,7 +1054,7 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
     }
     {
         PhaseTimer pt(H, "suitor");
-        suitor_dev(n, nnz, A.row.p, A.col.p, W.p, tpos.p, M.p, s);
+        suitor_dev(n, nnz, A.row.p, A.col.p, W.p, tpos.p, M.p, A.max_row, s);
     }
     PhaseTimer pt_p(H, "makeP+galerkin");
     W.release();

@@ -766,6 +766,13 @@ __global__ void k_galerkin(int nc, const int* __restrict__ fine0, const int* __r
     unsigned long long* key = (unsigned long long*)smem + (size_t)wid * cap;
     double* tv = (double*)(smem + (size_t)wpb * cap * 8) + (size_t)wid * cap;
     int* sidx = (int*)(smem + (size_t)wpb * cap * 16) + (size_t)wid * cap;
+    // the 32-bit-key form keeps its keys and sorted keys in the warp's key[] bytes, its products in
+    // tv and the sorted products in a region of its own after sidx (warps of a block may take
+    // different forms at the same time)
+    unsigned* key32 = (unsigned*)key;
+    unsigned* skey32 = key32 + cap;
+    double* sval = (double*)(smem + (size_t)wpb * cap * 20) + (size_t)wid * cap;
+    const bool narrow = nc < (1 << 25);
     for (long I = (long)blockIdx.x * wpb + wid; I < nc; I += (long)gridDim.x * wpb) {
         const int f0 = fine0[I], f1 = fine1[I];
         const int b0 = Arow[f0], d0 = Arow[f0 + 1] - b0;
@@ -773,6 +780,66 @@ __global__ void k_galerkin(int nc, const int* __restrict__ fine0, const int* __r
         const int cnt = d0 + d1;
         if (cnt > cap) {
             if (lane == 0) atomicOr(err, ERR_GALERKIN_CAP);
+            continue;
+        }
+        if (narrow && cnt <= 128) {
+            // keys (J << 7) | t are distinct and order like (J, source row, position): a 32-bit
+            // rank sort that writes each key and its product straight to its sorted slot
+            for (int t = lane; t < cnt; t += 32) {
+                const int j = t < d0 ? b0 + t : b1 + (t - d0);
+                const int c = Acol[j];
+                key32[t] = ((unsigned)agg[c] << 7) | (unsigned)t;
+                tv[t] = __dmul_rn(Aval[j], p[c]);
+            }
+            __syncwarp();
+            for (int t = lane; t < cnt; t += 32) {
+                const unsigned kt = key32[t];
+                int pos = 0;
+#pragma unroll 8
+                for (int u = 0; u < cnt; u++) pos += key32[u] < kt ? 1 : 0;
+                skey32[pos] = kt;
+                sval[pos] = tv[t];
+            }
+            __syncwarp();
+            const double p0 = p[f0], p1 = f1 >= 0 ? p[f1] : 0.0;
+            const long outbase = (long)I * cap;
+            int nheads = 0;
+            for (int base = 0; base < cnt; base += 32) {
+                const int sidx0 = base + lane;
+                bool head = false;
+                int J = -1;
+                if (sidx0 < cnt) {
+                    J = (int)(skey32[sidx0] >> 7);
+                    head = (sidx0 == 0) || ((int)(skey32[sidx0 - 1] >> 7) != J);
+                }
+                const unsigned hm = __ballot_sync(0xffffffffu, head);
+                if (head) {
+                    double ap0 = 0.0, ap1 = 0.0;
+                    int n0 = 0, n1 = 0;
+                    for (int g = sidx0; g < cnt; g++) {
+                        const unsigned kk = skey32[g];
+                        if ((int)(kk >> 7) != J) break;
+                        const double tt = sval[g];
+                        if ((int)(kk & 127u) < d0) {
+                            ap0 = n0 == 0 ? tt : __dadd_rn(ap0, tt);
+                            n0++;
+                        } else {
+                            ap1 = n1 == 0 ? tt : __dadd_rn(ap1, tt);
+                            n1++;
+                        }
+                    }
+                    double cv;
+                    if (n0 && n1) cv = __dadd_rn(__dmul_rn(p0, ap0), __dmul_rn(p1, ap1));
+                    else if (n0) cv = __dmul_rn(p0, ap0);
+                    else cv = __dmul_rn(p1, ap1);
+                    const long o = outbase + nheads + __popc(hm & ((1u << lane) - 1u));
+                    Ccol[o] = J;
+                    Cval[o] = cv;
+                }
+                nheads += __popc(hm);
+            }
+            if (lane == 0) Crow[I] = nheads;
+            __syncwarp();
             continue;
         }
         for (int t = lane; t < cnt; t += 32) {
@@ -1106,7 +1173,7 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
     // Galerkin: count, prefix sum, fill
     const int amax = A.max_row > 0 ? A.max_row : row_max(A, s);
     const int cap = std::max(2 * amax, 32);
-    const size_t per_warp = (size_t)cap * 20;
+    const size_t per_warp = (size_t)cap * 28;
     const size_t smem_limit = 200 * 1024;
     BCMGX_REQUIRE(per_warp <= smem_limit, BCMGX_ERR_UNSUPPORTED,
         "coarse row too long for the Galerkin kernel (" + std::to_string(cap) + " candidate entries)");

@@ -279,7 +279,15 @@ void edge_weights_dev(int n, int64_t nnz, const int* row, const int* col, const 
     const double* w, double* W, int* tpos, double* min_out_host, cudaStream_t s);
 void validate_csr_dev(int n, int m, int64_t nnz, const int* row, const int* col, bool need_diag, cudaStream_t s);
 void tpos_dev(int n, int64_t nnz, const int* row, const int* col, int* tpos, cudaStream_t s);
+// The edge weights formed inside the rank kernel (rows of at most 32 entries): the inputs of
+// k_logw's expression instead of the stored weights.
+struct FusedWeights {
+    const double* val = nullptr;
+    const double* w = nullptr;
+    const double* C = nullptr;
+    double zero_sub = 0.0;
+};
 void suitor_dev(int n, int64_t nnz, const int* row, const int* col, const double* W, const int* tpos, int* M, int max_row,
-    cudaStream_t s);
+    cudaStream_t s, const FusedWeights* fw = nullptr);
 
 }  // namespace bcmgx

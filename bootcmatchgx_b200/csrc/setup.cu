@@ -464,6 +464,59 @@ __global__ void k_logw(int n, const int* __restrict__ row, const int* __restrict
 
 // Per row: rank of every candidate (off-diagonal, W > 0) in the row's preference order,
 // (W, column) descending (find_Candidate, suitor.cu:80-147); ordj lists the entries by rank.
+// Ranks of a row of at most 32 entries held in registers (lane = entry t = b + lane, column ct
+// and weight wt; ct = -1 past the row): ranks by shuffles, no reloads.
+__device__ __forceinline__ void rank_row32(long r, int b, int e, int ct, double wt, int* __restrict__ rank,
+    int* __restrict__ ordj, int* __restrict__ degE)
+{
+    const int lane = threadIdx.x & 31;
+    const int t = b + lane;
+    const bool in = t < e;
+    const bool el = in && ct != r && wt > 0.0;
+    const unsigned elig = __ballot_sync(0xffffffffu, el);
+    int rk = 0;
+    const double w0 = __shfl_sync(0xffffffffu, wt, elig ? __ffs(elig) - 1 : 0);
+    if (__ballot_sync(0xffffffffu, el && wt != w0) == 0u) {
+        // all candidates weigh the same: the order is by column alone (columns ascend with the
+        // lane), so the rank is the number of candidates in higher lanes
+        rk = __popc(lane == 31 ? 0u : (elig >> (lane + 1)));
+    } else {
+        for (int k = 0; k < e - b; k++) {
+            const int ck = __shfl_sync(0xffffffffu, ct, k);
+            const double wk = __shfl_sync(0xffffffffu, wt, k);
+            rk += (((elig >> k) & 1u) && (wk > wt || (wk == wt && ck > ct))) ? 1 : 0;
+        }
+    }
+    if (in) {
+        rank[t] = el ? rk : -1;
+        if (el) ordj[b + rk] = t;
+    }
+    if (lane == 0) degE[r] = __popc(elig);
+}
+
+// k_rank for a matrix whose rows all have at most 32 entries, with every entry's weight formed
+// in registers by k_logw's expression (same operations, same rounding) instead of read from W:
+// the weights are never stored.
+__global__ void k_rank_w(int n, const int* __restrict__ row, const int* __restrict__ col, const double* __restrict__ val,
+    const double* __restrict__ w, const double* __restrict__ C, const int* __restrict__ tpos, double zero_sub,
+    int* __restrict__ rank, int* __restrict__ ordj, int* __restrict__ degE)
+{
+    const int lane = threadIdx.x & 31;
+    for (long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32; r < n; r += (long)gridDim.x * blockDim.x / 32) {
+        const int b = __ldg(row + r), e = __ldg(row + r + 1);
+        const int t = b + lane;
+        const int ct = t < e ? __ldg(col + t) : -1;
+        double wt = 0.0;
+        if (ct >= 0 && ct != (int)r) {
+            const int tp = __ldg(tpos + t);
+            const int src = (ct < (int)r && tp >= 0) ? tp : t;
+            const double sa = fabs(ahat(__ldg(val + src), __ldg(C + r), __ldg(C + ct), __ldg(w + r), __ldg(w + ct)));
+            wt = log(sa != 0.0 ? sa : zero_sub);
+        }
+        rank_row32(r, b, e, ct, wt, rank, ordj, degE);
+    }
+}
+
 __global__ void k_rank(int n, const int* __restrict__ row, const int* __restrict__ col, const double* __restrict__ W,
     int* __restrict__ rank, int* __restrict__ ordj, int* __restrict__ degE)
 {
@@ -471,31 +524,9 @@ __global__ void k_rank(int n, const int* __restrict__ row, const int* __restrict
     for (long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32; r < n; r += (long)gridDim.x * blockDim.x / 32) {
         const int b = row[r], e = row[r + 1];
         if (e - b <= 32) {
-            // the whole row in registers (lane = entry): ranks by shuffles, no reloads
             const int t = b + lane;
             const bool in = t < e;
-            const int ct = in ? col[t] : -1;
-            const double wt = in ? W[t] : 0.0;
-            const bool el = in && ct != r && wt > 0.0;
-            const unsigned elig = __ballot_sync(0xffffffffu, el);
-            int rk = 0;
-            const double w0 = __shfl_sync(0xffffffffu, wt, elig ? __ffs(elig) - 1 : 0);
-            if (__ballot_sync(0xffffffffu, el && wt != w0) == 0u) {
-                // all candidates weigh the same: the order is by column alone (columns ascend
-                // with the lane), so the rank is the number of candidates in higher lanes
-                rk = __popc(lane == 31 ? 0u : (elig >> (lane + 1)));
-            } else {
-                for (int k = 0; k < e - b; k++) {
-                    const int ck = __shfl_sync(0xffffffffu, ct, k);
-                    const double wk = __shfl_sync(0xffffffffu, wt, k);
-                    rk += (((elig >> k) & 1u) && (wk > wt || (wk == wt && ck > ct))) ? 1 : 0;
-                }
-            }
-            if (in) {
-                rank[t] = el ? rk : -1;
-                if (el) ordj[b + rk] = t;
-            }
-            if (lane == 0) degE[r] = __popc(elig);
+            rank_row32(r, b, e, in ? col[t] : -1, in ? W[t] : 0.0, rank, ordj, degE);
             continue;
         }
         int cnt = 0;
@@ -1001,32 +1032,41 @@ static int row_max_raw(int n, const int* row, cudaStream_t s)
 }
 static int row_max(const DevCsr& A, cudaStream_t s) { return row_max_raw(A.n, A.row.p, s); }
 
-void edge_weights_dev(int n, int64_t nnz, const int* row, const int* col, const double* val, const double* w, double* W,
-    int* tpos, double* min_out_host, cudaStream_t s)
+// The inputs of the edge weights: C_r (into C, n doubles), the transposed positions and the
+// substitute log argument SUITOR_EPS / (0.999 min |a_hat|) for a_hat == 0; returns it and, when
+// min_out_host is set, the minimum.
+static double edge_prep_dev(int n, int64_t nnz, const int* row, const int* col, const double* val, const double* w,
+    double* C, int* tpos, double* min_out_host, cudaStream_t s)
 {
-    DBuf<double> C;
     DBuf<unsigned long long> mn;
     DBuf<int> err;
-    C.alloc(n, s);
     mn.alloc(1, s);
     err.alloc(1, s);
     BCMGX_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), s));
     const double dmax = DBL_MAX;
     BCMGX_CUDA(cudaMemcpyAsync(mn.p, &dmax, sizeof(double), cudaMemcpyHostToDevice, s));
     const int S = setup_subwarp(n, nnz);
-    note_launch(); k_diag_c<<<gs_grid(n), 256, 0, s>>>(n, row, col, val, w, C.p, err.p);
+    note_launch(); k_diag_c<<<gs_grid(n), 256, 0, s>>>(n, row, col, val, w, C, err.p);
     BCMGX_SUBWARP_LAUNCH(k_tpos, S, n, s, n, row, col, tpos);
-    BCMGX_SUBWARP_LAUNCH(k_ahat_min, S, n, s, n, row, col, val, w, C.p, mn.p);
+    BCMGX_SUBWARP_LAUNCH(k_ahat_min, S, n, s, n, row, col, val, w, C, mn.p);
     BCMGX_CHECK_LAUNCH();
     double m = 0;
     BCMGX_CUDA(cudaMemcpyAsync(&m, mn.p, sizeof(double), cudaMemcpyDeviceToHost, s));
     int e = read_err(err.p, s);
     if (e) throw Error(BCMGX_ERR_INVALID_INPUT, "edge weights: " + err_text(e));
     if (std::fabs(m) < DBL_EPSILON) m = DBL_EPSILON;   // toMaximumProductMatrix, matching.cu:243-245
-    const double zero_sub = kSuitorEps / (0.999 * m);
-    BCMGX_SUBWARP_LAUNCH(k_logw, S, n, s, n, row, col, val, w, C.p, tpos, zero_sub, W);
-    BCMGX_CHECK_LAUNCH();
     if (min_out_host) *min_out_host = m;
+    return kSuitorEps / (0.999 * m);
+}
+
+void edge_weights_dev(int n, int64_t nnz, const int* row, const int* col, const double* val, const double* w, double* W,
+    int* tpos, double* min_out_host, cudaStream_t s)
+{
+    DBuf<double> C;
+    C.alloc(n, s);
+    const double zero_sub = edge_prep_dev(n, nnz, row, col, val, w, C.p, tpos, min_out_host, s);
+    BCMGX_SUBWARP_LAUNCH(k_logw, setup_subwarp(n, nnz), n, s, n, row, col, val, w, C.p, tpos, zero_sub, W);
+    BCMGX_CHECK_LAUNCH();
 }
 
 void validate_csr_dev(int n, int m, int64_t nnz, const int* row, const int* col, bool need_diag, cudaStream_t s)
@@ -1050,9 +1090,10 @@ void tpos_dev(int n, int64_t nnz, const int* row, const int* col, int* tpos, cud
 }
 
 void suitor_dev(int n, int64_t nnz, const int* row, const int* col, const double* W, const int* tpos, int* M, int max_row,
-    cudaStream_t s)
+    cudaStream_t s, const FusedWeights* fw)
 {
     if (max_row <= 0) max_row = row_max_raw(n, row, s);
+    if (fw && max_row > 32) throw Error(BCMGX_ERR_INTERNAL, "weights formed in the rank kernel need rows of <= 32 entries");
     const bool wide = max_row < 65536;
     DBuf<int> rank, ordj, degE, err;
     DBuf<int2> pref, rinfo;
@@ -1071,7 +1112,12 @@ void suitor_dev(int n, int64_t nnz, const int* row, const int* col, const double
         offer.alloc(n, s);
         BCMGX_CUDA(cudaMemsetAsync(offer.p, 0, sizeof(unsigned) * n, s));
     }
-    note_launch(); k_rank<<<warp_grid(n), 256, 0, s>>>(n, row, col, W, rank.p, ordj.p, degE.p);
+    if (fw) {
+        note_launch();
+        k_rank_w<<<warp_grid(n), 256, 0, s>>>(n, row, col, fw->val, fw->w, fw->C, tpos, fw->zero_sub, rank.p, ordj.p, degE.p);
+    } else {
+        note_launch(); k_rank<<<warp_grid(n), 256, 0, s>>>(n, row, col, W, rank.p, ordj.p, degE.p);
+    }
     pref.alloc(z, s);
     rinfo.alloc(n, s);
     BCMGX_SUBWARP_LAUNCH(k_pref, setup_subwarp(n, nnz), n, s, n, row, col, ordj.p, rank.p, tpos, degE.p, pref.p, rinfo.p);
@@ -1110,21 +1156,36 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
     cudaStream_t s = H->stream;
     const int n = A.n;
     const int64_t nnz = A.nnz;
-    DBuf<double> W;
+    DBuf<double> W, Cd;
     DBuf<int> tpos, M, fm, fs, pofs, sofs, err;
-    W.alloc(std::max<int64_t>(nnz, 1), s);
     tpos.alloc(std::max<int64_t>(nnz, 1), s);
     M.alloc(n, s);
-    {
-        PhaseTimer pt(H, "weights");
-        edge_weights_dev(n, nnz, A.row.p, A.col.p, A.val.p, w, W.p, tpos.p, nullptr, s);
-    }
-    {
+    const int amax0 = A.max_row > 0 ? A.max_row : row_max(A, s);
+    if (amax0 <= 32) {
+        // rows of at most 32 entries: the rank kernel forms the edge weights itself
+        Cd.alloc(n, s);
+        FusedWeights fw;
+        {
+            PhaseTimer pt(H, "weights");
+            fw.zero_sub = edge_prep_dev(n, nnz, A.row.p, A.col.p, A.val.p, w, Cd.p, tpos.p, nullptr, s);
+        }
+        fw.val = A.val.p;
+        fw.w = w;
+        fw.C = Cd.p;
         PhaseTimer pt(H, "suitor");
-        suitor_dev(n, nnz, A.row.p, A.col.p, W.p, tpos.p, M.p, A.max_row, s);
+        suitor_dev(n, nnz, A.row.p, A.col.p, nullptr, tpos.p, M.p, amax0, s, &fw);
+    } else {
+        W.alloc(std::max<int64_t>(nnz, 1), s);
+        {
+            PhaseTimer pt(H, "weights");
+            edge_weights_dev(n, nnz, A.row.p, A.col.p, A.val.p, w, W.p, tpos.p, nullptr, s);
+        }
+        PhaseTimer pt(H, "suitor");
+        suitor_dev(n, nnz, A.row.p, A.col.p, W.p, tpos.p, M.p, amax0, s);
     }
     PhaseTimer pt_p(H, "makeP+galerkin");
     W.release();
+    Cd.release();
     tpos.release();
     fm.alloc(n, s);
     fs.alloc(n, s);

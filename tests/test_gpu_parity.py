@@ -138,10 +138,13 @@ def test_weights_and_matching(bx, oracle, cuda, case):
 
 
 @pytest.mark.parametrize("case", [("lap7", (20, 20, 20)), ("lap27", (16, 16, 16)), ("lap7", (9, 30, 7)),
-                                  ("rand", (3000, 0.003, 5)), ("diff", (14, 9))])
+                                  ("rand", (3000, 0.003, 5)), ("diff", (14, 9)), ("rand", (1500, 0.05, 9))])
 def test_hierarchy_bit_exact(bx, oracle, cuda, case):
     """Every sweep's matching, aggregates, prolongator values and weight vector, every level's
-    matrix and the composite prolongators equal the oracle's bit for bit."""
+    matrix and the composite prolongators equal the oracle's bit for bit. The last matrix has
+    about 150 entries per row: its sweeps store the edge weights (rows over 32 entries), run the
+    matching kernels on whole warps and the Galerkin product with 64-bit keys (over 128 candidate
+    entries per coarse row)."""
     A = as_csr(bx, case)
     h = bx.prec_setup(A.indptr, A.indices, A.data, fcg(bx, record_sweeps=1))
     Ao = oracle.Matrix.from_csr(A.indptr, A.indices, A.data)
@@ -305,3 +308,28 @@ def test_graph_and_stream_drivers_agree(bx, cuda, case, prec):
         out[g] = (x1, i1["niter"], x2, i2["niter"])
     assert out[0][1] == out[1][1] and out[0][3] == out[1][3]
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][2], out[1][2])
+
+
+def test_suitor_with_a_row_of_65536_entries(bx, oracle, cuda):
+    """A row of 70,000 entries (an arrowhead pattern over a chain) takes the suitor with 32-bit
+    offer words; its matching on given symmetric weights equals the oracle's greedy matching.
+    Most weights of the long row are <= 0 (no candidates), so its ranking stays short."""
+    import torch
+    n = 70000
+    rng = np.random.default_rng(21)
+    i = np.arange(n - 1)
+    chain = sp.coo_matrix((np.ones(n - 1), (i, i + 1)), shape=(n, n))
+    arrow = sp.coo_matrix((np.ones(n - 2), (np.zeros(n - 2, int), np.arange(2, n))), shape=(n, n))
+    U = (chain + arrow).tocsr()
+    U.data = rng.uniform(-2.0, 2.0, U.nnz)
+    U[0, 2:] = -np.abs(U[0, 2:].toarray())
+    U[0, rng.choice(np.arange(2, n), 100, replace=False)] = rng.uniform(0.5, 2.0, 100)
+    W = (U + U.T + sp.identity(n)).tocsr()   # symmetric weights on a symmetric pattern, with a diagonal
+    W.sort_indices()
+    assert np.diff(W.indptr).max() >= 65536
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(cuda)
+    Mg = bx.suitor_matching(d(W.indptr.astype(np.int32)), d(W.indices.astype(np.int32)), d(W.data)).cpu().numpy()
+    Mo = oracle.Matrix.from_csr(W.indptr, W.indices, np.ones(W.nnz)).match(W.data, 0)
+    assert np.array_equal(Mg, Mo)
+    m = Mg >= 0
+    assert m.sum() > n // 2 and np.all(Mg[Mg[m]] == np.nonzero(m)[0])

@@ -19,10 +19,11 @@ __device__ __forceinline__ int col_at(const short* __restrict__ dcol, int j, int
 
 // Partial dot product of one row over the lanes of a sub-warp. Entries are taken in batches of
 // K per lane: all K column and value loads are issued, then all K gathers of x, then the K
-// multiply-adds, so a row of up to K*S entries costs one round of memory latency per lane.
-template <int S, typename AT, typename VT, typename XT, typename IT>
+// multiply-adds, so a row of up to K*S entries costs one round of memory latency per lane. The
+// gathers use the read-only path unless RO is false (x written earlier by the same kernel).
+template <int S, typename AT, bool RO = true, typename VT, typename XT, typename IT>
 __device__ __forceinline__ AT row_partial(int b, int e, int lane, int r, const IT* __restrict__ col,
-    const VT* __restrict__ val, const XT* __restrict__ x)
+    const VT* __restrict__ val, const XT* x)
 {
     constexpr int K = 8;
     AT s = 0;
@@ -37,7 +38,7 @@ __device__ __forceinline__ AT row_partial(int b, int e, int lane, int r, const I
             v[k] = j < e ? ld_stream(val + j) : VT(0);
         }
 #pragma unroll
-        for (int k = 0; k < K; k++) xv[k] = c[k] >= 0 ? ld_ro(x + c[k]) : XT(0);
+        for (int k = 0; k < K; k++) xv[k] = c[k] >= 0 ? (RO ? ld_ro(x + c[k]) : x[c[k]]) : XT(0);
 #pragma unroll
         for (int k = 0; k < K; k++) s += (AT)v[k] * (AT)xv[k];
     }

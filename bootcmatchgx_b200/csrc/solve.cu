@@ -12,6 +12,7 @@
 // FP32 V-cycle (vcycle_precision = FP32): levels 0..L-2 run on FP32 matrix values and vectors;
 // the coarsest level, the outer residual, the dots and the direction updates stay FP64.
 #include "internal.h"
+#include <type_traits>
 #include "rowops.cuh"
 #include "blockops.cuh"
 
@@ -138,6 +139,45 @@ __global__ void k_first_sweep(int n, const FT* __restrict__ f, const MT* __restr
         AT fi = (AT)f[i];
         if (fcopy) fcopy[i] = (CT)fi;
         u[i] = (YT)(fi / (AT)M[i]);
+    }
+}
+
+// k l1-Jacobi sweeps of a small level in one block of kChainThreads threads: the sweeps of
+// Cycle::chain (the first from a zero iterate when src is null), each followed by a block-wide
+// barrier, so a chain is one launch instead of k. Sweep i writes out[i]: out[k-1] = dst, and
+// out[i] = q0 for even k-2-i, q1 otherwise (the ping-pong order of chain). The row arithmetic is
+// k_first_sweep's and k_rowop<S, OP_JACOBI>'s, so the iterates are the same; vectors written by
+// the block are gathered with coherent loads.
+constexpr int kChainThreads = 1024;
+constexpr long kChainMaxNnz = 65536;   // larger levels keep one launch per sweep
+
+template <int S, typename T, typename IT>
+__global__ void __launch_bounds__(kChainThreads) k_chain_block(int n, const int* __restrict__ row, const IT* __restrict__ col,
+    const T* __restrict__ val, const T* __restrict__ f, const T* __restrict__ M, const T* src, T* dst, T* q0, T* q1, int k,
+    const int* __restrict__ skip)
+{
+    if (skip && *skip) return;
+    using AT = typename Acc<T>::type;
+    using WT = typename Wider<T>::type;
+    const int lane = threadIdx.x & (S - 1);
+    const int sub = (threadIdx.x & 31) / S;
+    const int rows_per_step = blockDim.x / S;
+    const T* in = src;
+    for (int i = 0; i < k; i++) {
+        T* out = i == k - 1 ? dst : (((k - 2 - i) & 1) == 0 ? q0 : q1);
+        if (in == nullptr) {
+            for (int r = threadIdx.x; r < n; r += blockDim.x) out[r] = (T)((WT)f[r] / (WT)M[r]);
+        } else {
+            for (int base = (threadIdx.x & ~31) / S; base < n; base += rows_per_step) {
+                const int r = base + sub;
+                AT sum = 0;
+                if (r < n) sum = row_partial<S, AT, false>(__ldg(row + r), __ldg(row + r + 1), lane, r, col, val, in);
+                sum = subwarp_sum<S>(sum);
+                if (r < n && lane == 0) out[r] = (T)(((-sum + (AT)f[r]) / (AT)M[r]) + (AT)in[r]);
+            }
+        }
+        __syncthreads();
+        in = out;
     }
 }
 
@@ -386,6 +426,7 @@ struct Cycle {
             copy(src, other, n);
             src = other;
         }
+        if (chain_in_block(l, k, f, src, dst, A, Bf, fcopy)) return;
         Vec fl = f;
         for (int i = 0; i < k; i++) {
             if (i == 0 && src.p == nullptr) {
@@ -395,6 +436,47 @@ struct Cycle {
                 sweep(l, fl, i == 0 ? src : out[i - 1], out[i]);
             }
         }
+    }
+
+    // A chain of k >= 2 sweeps on a small single-vector level whose vectors all have the level's
+    // precision runs as one k_chain_block launch; returns false otherwise.
+    bool chain_in_block(int l, int k, Vec f, Vec src, Vec dst, Vec A, Vec Bf, Vec fcopy) const
+    {
+        const Level& V = lv(l);
+        const DevCsr& Am = V.A;
+        const bool f32 = lf32(l);
+        if (lk >= 0 || k < 2 || fcopy.p || Am.nnz > kChainMaxNnz) return false;
+        for (const Vec& v : { f, dst, A, Bf })
+            if (v.f32 != f32) return false;
+        if (src.p && src.f32 != f32) return false;
+        const Vec q0 = (dst == A) ? Bf : A;
+        const Vec q1 = (q0 == A) ? Bf : A;
+        auto go = [&](auto kern, auto val, auto M, auto* tp, auto* colp) {
+            using T = std::remove_pointer_t<decltype(tp)>;
+            note_launch();
+            kern<<<1, kChainThreads, 0, s>>>(Am.n, Am.row.p, colp, val, (const T*)f.p, M, (const T*)src.p, (T*)dst.p,
+                (T*)q0.p, (T*)q1.p, k, skip);
+            BCMGX_CHECK_LAUNCH();
+        };
+        auto dispatch = [&](auto* tp, auto val, auto M) {
+            using T = std::remove_pointer_t<decltype(tp)>;
+            auto with_col = [&](auto* colp) {
+                using IT = std::remove_const_t<std::remove_pointer_t<decltype(colp)>>;
+                switch (Am.tpr) {
+                case 1: go(k_chain_block<1, T, IT>, val, M, tp, colp); break;
+                case 2: go(k_chain_block<2, T, IT>, val, M, tp, colp); break;
+                case 4: go(k_chain_block<4, T, IT>, val, M, tp, colp); break;
+                case 8: go(k_chain_block<8, T, IT>, val, M, tp, colp); break;
+                case 16: go(k_chain_block<16, T, IT>, val, M, tp, colp); break;
+                default: go(k_chain_block<32, T, IT>, val, M, tp, colp); break;
+                }
+            };
+            if (Am.dcol.p) with_col((const short*)Am.dcol.p);
+            else with_col((const int*)Am.col.p);
+        };
+        if (f32) dispatch((float*)nullptr, (const float*)Am.val32.p, (const float*)V.M32.p);
+        else dispatch((double*)nullptr, (const double*)Am.val.p, (const double*)V.M.p);
+        return true;
     }
 
     // One cycle on level l for right-hand side f, starting from x_cur (nullptr: zero),

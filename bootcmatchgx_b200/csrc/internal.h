@@ -188,6 +188,7 @@ struct bcmgx_hierarchy {
     bcmgx::DBuf<double> hist;           // residual history, one entry per iteration
     cudaEvent_t ev_it[2] = { nullptr, nullptr };
     cudaEvent_t ev_in = nullptr;        // orders the library's stream after the caller's (after_caller)
+    bool chain_in_block = false;        // small levels' sweep chains as one-block kernels (batch graphs)
     // captured solve (CUDA graph) and its own b / x buffers
     cudaGraphExec_t iter_graph = nullptr;
     bcmgx::DBuf<double> gb, gx;

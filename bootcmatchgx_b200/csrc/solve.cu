@@ -438,14 +438,17 @@ struct Cycle {
         }
     }
 
-    // A chain of k >= 2 sweeps on a small single-vector level whose vectors all have the level's
-    // precision runs as one k_chain_block launch; returns false otherwise.
+    // While the batch graph is captured (H->chain_in_block), a chain of k >= 2 sweeps on a small
+    // single-vector level whose vectors all have the level's precision runs as one k_chain_block
+    // launch; returns false otherwise. A solve that has the GPU to itself keeps one launch per
+    // sweep: one block works through a level far slower than a grid does, and only when hundreds
+    // of systems run side by side is the number of kernels the bound.
     bool chain_in_block(int l, int k, Vec f, Vec src, Vec dst, Vec A, Vec Bf, Vec fcopy) const
     {
         const Level& V = lv(l);
         const DevCsr& Am = V.A;
         const bool f32 = lf32(l);
-        if (lk >= 0 || k < 2 || fcopy.p || Am.nnz > kChainMaxNnz) return false;
+        if (!H->chain_in_block || lk >= 0 || k < 2 || fcopy.p || Am.nnz > kChainMaxNnz) return false;
         for (const Vec& v : { f, dst, A, Bf })
             if (v.f32 != f32) return false;
         if (src.p && src.f32 != f32) return false;
@@ -1268,7 +1271,9 @@ void batch_build(bcmgx_batch* B)
     BCMGX_CUDA(cudaGraphCreate(&g, 0));
     for (bcmgx_hierarchy* H : B->hs) {
         ensure_solve_workspace(H);
+        H->chain_in_block = true;   // many systems share the GPU: fewer, longer kernels per system
         add_solve_to_graph(H, g);
+        H->chain_in_block = false;
     }
     BCMGX_CUDA(cudaGraphInstantiate(&B->exec, g, 0));
     BCMGX_CUDA(cudaGraphDestroy(g));

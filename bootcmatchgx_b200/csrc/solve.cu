@@ -149,7 +149,7 @@ __global__ void k_first_sweep(int n, const FT* __restrict__ f, const MT* __restr
 // k_first_sweep's and k_rowop<S, OP_JACOBI>'s, so the iterates are the same; vectors written by
 // the block are gathered with coherent loads.
 constexpr int kChainThreads = 1024;
-constexpr long kChainMaxNnz = 65536;   // larger levels keep one launch per sweep
+constexpr long kChainMaxNnz = 65536;   // larger levels keep one launch per sweep (32768: -2 %, 262144: -9 % on the batch benchmark)
 
 template <int S, typename T, typename IT>
 __global__ void __launch_bounds__(kChainThreads) k_chain_block(int n, const int* __restrict__ row, const IT* __restrict__ col,

@@ -250,7 +250,8 @@ int krylov_solve(bcmgx_hierarchy* H, const double* b, double* x, bcmgx_solve_inf
 void rowop_spmv(const DevCsr& A, const double* x, double* y, const int* skip, cudaStream_t s);
 void rowop_resid(const DevCsr& A, const double* x, const double* f, double* y, const int* skip, cudaStream_t s);
 // One V-cycle on 2^lk right-hand sides (row-major n0 x 2^lk blocks) with block buffers `bufs`.
-void cycle_apply_block(bcmgx_hierarchy* H, const CycleBufs& bufs, int lk, const double* r, double* v, const int* skip);
+void cycle_apply_block(bcmgx_hierarchy* H, const CycleBufs& bufs, int lk, const double* r, double* v, double* scratch,
+    const int* skip);
 // Block FCG for K right-hand sides of one system (multi.cu); B, X row-major n x K, device.
 int multi_solve(bcmgx_hierarchy* H, int K, const double* B, double* X, bcmgx_solve_info* infos);
 // Y = alpha A X + beta Y for row-major n x K blocks on device memory (K <= 32).

@@ -261,6 +261,7 @@ struct MultiWork {
     std::vector<DBuf<unsigned char>> raw;   // cycle buffers
     CycleBufs cyc;
     DBuf<double> B, X, R, V, W, D, Q, part;
+    DBuf<double> P;                         // scratch block of the l1-Jacobi / AFSAI preconditioners
     DBuf<BlockState> st;
     BlockState* st_host = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -327,6 +328,8 @@ void ensure_multi(bcmgx_hierarchy* H, MultiWork& wk, int K)
     wk.D.alloc(nk, s);
     wk.Q.alloc(nk, s);
     wk.part.alloc((size_t)num_sms() * kBlkBlocksPerSM * 3 * 32, s);
+    const int pc = H->prm.preconditioner;
+    if (pc == BCMGX_PREC_L1_JACOBI || pc == BCMGX_PREC_AFSAI) wk.P.alloc(nk, s);
     wk.st.alloc(1, s);
     if (!wk.st_host) wk.st_host = (BlockState*)pinned_alloc(2 * sizeof(BlockState));
 }
@@ -392,7 +395,7 @@ void blk_startup(bcmgx_hierarchy* H, MultiWork& wk)
     k_blk_init<<<1, 32, 0, s>>>(wk.st.p, wk.K, H->prm.rtol, H->prm.itnlim);
     BCMGX_CHECK_LAUNCH();
     launch_resid0(A, wk, s);
-    cycle_apply_block(H, wk.cyc, wk.lk, wk.R.p, wk.V.p, nullptr);
+    cycle_apply_block(H, wk.cyc, wk.lk, wk.R.p, wk.V.p, wk.P.p, nullptr);
     launch_dots<0>(A, wk, wk.V.p, wk.W.p, nullptr, nullptr, s);
     note_launch();
     k_blk_update0<<<elem_grid(k_blk_update0, A.n, wk.lk), kBlkThreads, 0, s>>>(A.n, wk.lk, wk.V.p, wk.W.p, wk.X.p, wk.R.p, wk.D.p, wk.Q.p,
@@ -409,7 +412,7 @@ void blk_iteration(bcmgx_hierarchy* H, MultiWork& wk, bool even, const int* skip
     double* pw = even ? wk.W.p : wk.Q.p;
     const double* od = even ? wk.D.p : wk.V.p;
     const double* oq = even ? wk.Q.p : wk.W.p;
-    cycle_apply_block(H, wk.cyc, wk.lk, wk.R.p, pv, skip);
+    cycle_apply_block(H, wk.cyc, wk.lk, wk.R.p, pv, wk.P.p, skip);
     launch_dots<1>(A, wk, pv, pw, oq, skip, s);
     note_launch();
     k_blk_update<<<elem_grid(k_blk_update, A.n, wk.lk), kBlkThreads, 0, s>>>(A.n, wk.lk, pv, od, wk.X.p, pw, oq, wk.R.p, wk.st.p,

@@ -609,9 +609,40 @@ void prec_apply_impl(bcmgx_hierarchy* H, const double* r, double* v, const int* 
     c.run(0, Vec { (void*)r, false }, Vec(), Vec { v, false });
 }
 
-void cycle_apply_block(bcmgx_hierarchy* H, const CycleBufs& bufs, int lk, const double* r, double* v, const int* skip)
+// The preconditioner on a block of 2^lk right-hand sides (scratch: an n x 2^lk block, needed by
+// l1-Jacobi and AFSAI): the block V-cycle, the standalone l1-Jacobi sweeps (l1jacobi_apply on
+// every column: the first from zero, the last into v), AFSAI's G^T (G r) as two block SpMMs
+// (afsai_apply), or the identity.
+void cycle_apply_block(bcmgx_hierarchy* H, const CycleBufs& bufs, int lk, const double* r, double* v, double* scratch,
+    const int* skip)
 {
     const int n0 = H->lv[0].A.n;
+    const int kp = 1 << lk;
+    cudaStream_t s = H->stream;
+    if (H->prm.preconditioner == BCMGX_PREC_L1_JACOBI) {
+        const DevCsr& A = H->lv[0].A;
+        const int k = H->prm.l1jacsweeps;
+        std::vector<double*> out(k);
+        out[k - 1] = v;
+        for (int i = k - 2; i >= 0; i--) out[i] = (out[i + 1] == v) ? scratch : v;
+        auto first = k_blk_first_sweep<double, double, double, double>;
+        note_launch();
+        first<<<ew_grid(first, (long)n0 << lk), 256, 0, s>>>(n0, lk, r, H->l1d.p, out[0], (double*)nullptr, skip);
+        BCMGX_CHECK_LAUNCH();
+        for (int i = 1; i < k; i++)
+            launch_blk_rowop<OP_JACOBI>(n0, n0, kp, kp, A.row.p, A.col.p, A.val.p, (const double*)out[i - 1], r,
+                (const double*)H->l1d.p, out[i], 1.0, 0.0, skip, s);
+        return;
+    }
+    if (H->prm.preconditioner == BCMGX_PREC_AFSAI) {
+        const DevCsr& G = H->afsai_G;
+        const DevCsr& GT = H->afsai_GT;
+        launch_blk_rowop<OP_AXPBY>(n0, n0, kp, kp, G.row.p, G.col.p, G.val.p, r, (const double*)nullptr,
+            (const double*)nullptr, scratch, 1.0, 0.0, skip, s);
+        launch_blk_rowop<OP_AXPBY>(n0, n0, kp, kp, GT.row.p, GT.col.p, GT.val.p, (const double*)scratch,
+            (const double*)nullptr, (const double*)nullptr, v, 1.0, 0.0, skip, s);
+        return;
+    }
     if (H->prm.preconditioner != BCMGX_PREC_BCMG) {
         note_launch();
         auto k = k_blk_convert<double, double>;

@@ -153,8 +153,10 @@ int bcmgx_solve(bcmgx_hierarchy* h, const double* b, double* x, int on_device, b
 /* Solves A X = B for nrhs <= 32 right-hand sides at once (B, X row-major n x nrhs: entry (i, k)
  * at i*nrhs + k; X holds x0 on entry). Every sparse product is a CSR SpMM over the block, and
  * every column runs the FCG recurrence with its own scalars and stopping test; infos has nrhs
- * entries (or is NULL). No counterpart in the reference (its solve takes one vector,
- * solve.cu:11-51); column k gives the result of bcmgx_solve on column k up to rounding. */
+ * entries (or is NULL). The preconditioner is the hierarchy's own: the BCMG V-cycle, l1-Jacobi
+ * sweeps, the AFSAI product G^T G, or none, each applied to the whole block. No counterpart in the
+ * reference (its solve takes one vector, solve.cu:11-51); column k gives the result of bcmgx_solve
+ * on column k up to rounding. */
 int bcmgx_solve_multi(bcmgx_hierarchy* h, int nrhs, const double* B, double* X, int on_device,
     bcmgx_solve_info* infos);
 /* Adjoint of x = A^{-1} b for a loss L(x): given g = dL/dx, solves A lambda = g with the same

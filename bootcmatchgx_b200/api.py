@@ -375,7 +375,7 @@ class Batch:
         if rc not in (L.OK, L.ERR_NO_CONVERGENCE):
             raise BcmgxError(rc, "batch solve", L.last_error())
         return xs, [{"niter": i.niter, "retv": i.retv, "exit_res": i.exit_res, "delta0": i.delta0,
-                     "solve_ms": i.solve_ms} for i in infos]
+                     "solve_ms": i.solve_ms, "status": rc} for i in infos]
 
     def free(self):
         if getattr(self, "h", None):

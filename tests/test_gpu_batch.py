@@ -46,6 +46,25 @@ def test_batch_matches_single_solves(bx, cuda, prec):
     B.free()
 
 
+@pytest.mark.parametrize("pre", ["L1_JACOBI", "AFSAI", "NONE"])
+def test_batch_other_preconditioners(bx, cuda, pre):
+    """The standalone l1-Jacobi and AFSAI preconditioners (and none) in a batch: every system gives
+    bit for bit the iterations and solution of its own single solve."""
+    import torch
+    systems = _systems(bx, 5, 8)
+    p = bx.params_default(solver="FCG", preconditioner=pre, rtol=1e-8, dispnorm=0, l1jacsweeps=2)
+    B = bx.Batch(systems, p, nthreads=2)
+    rng = np.random.default_rng(9)
+    bs = [torch.from_numpy(rng.uniform(-1, 1, r.size - 1)).to(cuda) for r, _, _ in systems]
+    xs, infos = B.solve(bs)
+    for k, (row, col, val) in enumerate(systems):
+        x, info = bx.prec_setup(row, col, val, p).solve(bs[k])
+        assert infos[k]["status"] == 0
+        assert info["niter"] == infos[k]["niter"]
+        assert torch.equal(x, xs[k])
+    B.free()
+
+
 def test_batch_setup_error_is_reported(bx, cuda):
     systems = _systems(bx, 3, 6)
     r, c, v = systems[1]

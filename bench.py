@@ -382,6 +382,7 @@ def run_ours(a, wl, rank, world, local_rank):
     setup64 = float(np.mean([i[1]["setup_ms"] for i in infos64]))
     solve64 = float(np.mean([i[0]["solve_ms"] for i in infos64]))
     nrm = np.linalg.norm
+    tpr0 = inf32["tpr"][0]   # level 0's threads-per-row code: negative for the staged kernel
     line = {
         "metric": METRIC, "value": ms32 / 1e3, "unit": "s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms32, "higher_is_better": False, "scaling": "weak",
@@ -413,11 +414,13 @@ def run_ours(a, wl, rank, world, local_rank):
                            "fp64_jacobi_gbs": gbs_jac64, "fcg_spmv_dots_ms": k64f["fcg_spmv_dots"]},
         "kernels_coarse_levels_fp32_jacobi_ms": [round(k["jacobi"], 4) for k in lvl],
         "vcycle": vcycle_roofline(vc_ms, inf32, params("FP32"), peak, peak_kind),
-        "roofline": {"kernel": f"k_rowop<{inf32['tpr'][0]},OP_JACOBI,float> (FP32 l1-Jacobi sweep, level 0)",
+        "roofline": {"kernel": (f"k_rowop_staged<{-tpr0},OP_JACOBI,float>" if tpr0 < 0 else f"k_rowop<{tpr0},OP_JACOBI,float>")
+                     + " (FP32 l1-Jacobi sweep, level 0)",
                      "bound": "hbm", "achieved": gbs_jac32, "peak": peak, "unit": "GB/s",
                      "frac": gbs_jac32 / peak, "peak_kind": f"{peak_kind} hbm_gbs (copy)",
                      "bytes_per_launch": bytes_jac32,
-                     "traffic": int(TRAFFIC_RATIO[ib32] * bytes_jac32) if a.workload.startswith("poisson27") else None},
+                     "traffic": (int(TRAFFIC_RATIO[(ib32, tpr0 < 0)] * bytes_jac32)
+                                 if a.workload.startswith("poisson27") and (ib32, tpr0 < 0) in TRAFFIC_RATIO else None)},
         "gpu_launches": int(round(launches32)),
         "e2e": {"value": e2e_ms / 1e3, "unit": "s", "h2d_bytes_per_step": int(row.nbytes + col.nbytes + val.nbytes + b.nbytes),
                 "d2h_bytes_per_step": int(n * 8), "path": "bcmgx_setup(host CSR) + bcmgx_solve(host b, x), pinned"},
@@ -428,10 +431,11 @@ def run_ours(a, wl, rank, world, local_rank):
 
 
 # DRAM bytes (read + write) of one level-0 FP32 Jacobi launch as a multiple of its algorithmic
-# bytes, measured by ncu on the 27-point 100^3 case per index format (int32 columns:
-# profiles/jacobi_fp32_poisson27_100.md; int16 offsets: profiles/jacobi_fp32_int16_poisson27_100.md)
-# and scaled by the algorithmic bytes to the other 27-point workloads.
-TRAFFIC_RATIO = {4: 0.99983, 2: 1.00115}
+# bytes, measured by ncu on the 27-point 100^3 case per (index bytes, staged kernel) (int32 columns:
+# profiles/jacobi_fp32_poisson27_100.md; int16 offsets: profiles/jacobi_fp32_int16_poisson27_100.md;
+# staged, int16: profiles/jacobi_fp32_staged_poisson27_100.md) and scaled by the algorithmic bytes
+# to the other 27-point workloads.
+TRAFFIC_RATIO = {(4, False): 0.99983, (2, False): 1.00115, (2, True): 1.01173}
 
 
 def _spmv(row, col, val, x):

@@ -174,15 +174,21 @@ static bcmgx_hierarchy* setup_one(const bcmgx_csr* A, const bcmgx_params* p, int
     BCMGX_CUDA(cudaEventCreate(&e0));
     BCMGX_CUDA(cudaEventCreate(&e1));
     BCMGX_CUDA(cudaEventRecord(e0, H->stream));
+    stage_fault_init();
     build_hierarchy(H.get(), A);
     const char* force = std::getenv("BCMGX_TPR");
     const int L = (int)H->lv.size();
     for (int l = 0; l < L; l++) {
         Level& V = H->lv[l];
         const bool f32 = p->vcycle_precision == BCMGX_VCYCLE_FP32 && l < L - 1;
-        if (force) V.A.tpr = std::atoi(force);
-        else if (p->autotune) V.A.tpr = autotune_tpr(V, f32, H->stream);
-        else V.A.tpr = default_tpr(V.A.n, V.A.nnz);
+        int code;
+        if (force) code = std::atoi(force);
+        else if (p->autotune) code = autotune_tpr(V, f32, H->stream);
+        else code = default_tpr(V.A.n, V.A.nnz);
+        // negative: the staged kernel with -code threads per row (2, 4 or 8)
+        V.A.staged = code < 0;
+        V.A.tpr = code < 0 ? -code : code;
+        if (V.A.tpr < 1) V.A.tpr = default_tpr(V.A.n, V.A.nnz);
     }
     BCMGX_CUDA(cudaEventRecord(e1, H->stream));
     BCMGX_CUDA(cudaEventSynchronize(e1));
@@ -190,6 +196,7 @@ static bcmgx_hierarchy* setup_one(const bcmgx_csr* A, const bcmgx_params* p, int
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    stage_fault_check();
     H->setup_ms = ms;
     return H.release();
 }
@@ -392,6 +399,7 @@ int bcmgx_batch_solve(bcmgx_batch* B, const double* const* b, double* const* x, 
         status = batch_solve(B, b, x, infos);
         if (status == BCMGX_ERR_NO_CONVERGENCE) set_last_error("batch solve: a system reached itnlim");
         if (status == BCMGX_ERR_NOT_SPD) set_last_error("batch solve: FCG breakdown in a system");
+        stage_fault_check();
     });
     return rc != BCMGX_OK ? rc : status;
 }
@@ -427,6 +435,7 @@ int bcmgx_solve(bcmgx_hierarchy* h, const double* b, double* x, int on_device, b
         }
         if (status == BCMGX_ERR_NO_CONVERGENCE) set_last_error("itnlim reached before the tolerance");
         if (status == BCMGX_ERR_NOT_SPD) set_last_error("FCG breakdown: non-positive or non-finite curvature");
+        stage_fault_check();
     });
     return rc != BCMGX_OK ? rc : status;
 }
@@ -456,6 +465,7 @@ int bcmgx_solve_multi(bcmgx_hierarchy* h, int nrhs, const double* B, double* X, 
         }
         if (status == BCMGX_ERR_NO_CONVERGENCE) set_last_error("itnlim reached before the tolerance (some column)");
         if (status == BCMGX_ERR_NOT_SPD) set_last_error("FCG breakdown in some column: non-positive or non-finite curvature");
+        stage_fault_check();
     });
     return rc != BCMGX_OK ? rc : status;
 }
@@ -495,6 +505,7 @@ int bcmgx_solve_adjoint(bcmgx_hierarchy* h, const double* g, const double* x, do
             BCMGX_CUDA(cudaStreamSynchronize(s));
         }
         if (status == BCMGX_ERR_NO_CONVERGENCE) set_last_error("adjoint solve: itnlim reached before the tolerance");
+        stage_fault_check();
     });
     return rc != BCMGX_OK ? rc : status;
 }
@@ -517,7 +528,7 @@ int bcmgx_hierarchy_get_info(const bcmgx_hierarchy* h, bcmgx_hierarchy_info* inf
         for (int l = 0; l < info->num_levels && l < BCMGX_MAX_LEVELS; l++) {
             info->n[l] = h->lv[l].A.n;
             info->nnz[l] = h->lv[l].A.nnz;
-            info->tpr[l] = h->lv[l].A.tpr;
+            info->tpr[l] = h->lv[l].A.staged ? -h->lv[l].A.tpr : h->lv[l].A.tpr;
             info->index_bytes[l] = h->lv[l].A.dcol.p ? 2 : 4;
         }
         info->op_cmplx = h->op_cmplx;
@@ -613,6 +624,7 @@ int bcmgx_prec_apply(bcmgx_hierarchy* h, const double* r, double* v, int on_devi
             BCMGX_CUDA(cudaMemcpyAsync(v, vd.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
             BCMGX_CUDA(cudaStreamSynchronize(s));
         }
+        stage_fault_check();
     });
 }
 
@@ -622,6 +634,7 @@ int bcmgx_time_kernels(bcmgx_hierarchy* h, int level, int reps, double* out_ms)
         BCMGX_REQUIRE(h && out_ms && level >= 0 && level < (int)h->lv.size() && reps > 0, BCMGX_ERR_INVALID_INPUT, "bad argument");
         DeviceScope ds(h->device);
         time_level_kernels(h, level, reps, out_ms);
+        stage_fault_check();
     });
 }
 

@@ -77,7 +77,9 @@ struct DBuf {
         s = stream;
         n = count;
         if (count == 0) return;
-        cudaError_t e = cudaMallocAsync((void**)&p, count * sizeof(T), stream);
+        // 64 bytes past the end: bulk copies of 16-byte granules (staged.cuh) may round the end
+        // of a range up without leaving the allocation
+        cudaError_t e = cudaMallocAsync((void**)&p, count * sizeof(T) + 64, stream);
         if (e != cudaSuccess) {
             p = nullptr;
             n = 0;
@@ -106,6 +108,7 @@ struct DevCsr {
     DBuf<float> val32;
     DBuf<short> dcol; // col - row as int16 when every entry is within 32767 of the diagonal, else empty
     int tpr = 0;      // threads per row for SpMV / smoother (autotuned)
+    bool staged = false;  // row kernels stream the entries through shared-memory stages (staged.cuh)
 };
 
 struct Level {
@@ -274,6 +277,8 @@ inline int fit_grid(void (*kernel)(A...), int threads, long need_blocks)
 
 // ---- kernels usable on raw device memory (kernels.cu) ----
 int autotune_tpr(Level& V, bool f32, cudaStream_t s);
+void stage_fault_init();
+void stage_fault_check();
 int default_tpr(int n, int64_t nnz);
 void launch_spmv(int n, const int* row, const int* col, const double* val, const double* x, double* y,
     double alpha, double beta, int tpr, cudaStream_t s);

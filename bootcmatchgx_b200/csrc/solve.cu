@@ -14,6 +14,7 @@
 #include "internal.h"
 #include <type_traits>
 #include "rowops.cuh"
+#include "staged.cuh"
 #include "blockops.cuh"
 
 #include <algorithm>
@@ -86,11 +87,81 @@ static void launch_rowop(int tpr, int n, const int* row, const IT* col, const VT
     BCMGX_CHECK_LAUNCH();
 }
 
-// The row operation on a level matrix, through its int16 column offsets when it has them.
+// Fault word of the staged row kernels, in mapped pinned host memory: nonzero when one of their
+// waits on a shared-memory stage gave up. The entry points read it after their final stream
+// synchronisation (stage_fault_check), so the check costs no copy.
+static int* g_stage_fault = nullptr;
+static std::once_flag g_stage_fault_once;
+
+void stage_fault_init()
+{
+    std::call_once(g_stage_fault_once, [] {
+        void* p = nullptr;
+        BCMGX_CUDA(cudaHostAlloc(&p, sizeof(int), cudaHostAllocMapped | cudaHostAllocPortable));
+        *(volatile int*)p = 0;
+        g_stage_fault = (int*)p;
+    });
+}
+
+void stage_fault_check()
+{
+    if (g_stage_fault && *(volatile int*)g_stage_fault) {
+        const int code = *(volatile int*)g_stage_fault;
+        *(volatile int*)g_stage_fault = 0;
+        throw Error(BCMGX_ERR_TIMEOUT, "staged row kernel: a wait on a shared-memory stage gave up (code " +
+            std::to_string(code) + ")");
+    }
+}
+
+static bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
+
+// The staged form of launch_rowop (staged.cuh): one resident wave of blocks over tiles of R rows.
+template <int S, int OP, typename VT, typename XT, typename FT, typename MT, typename YT, typename IT>
+static void launch_staged(int n, int64_t nnz, const int* row, const IT* col, const VT* val, const XT* x, const FT* f,
+    const MT* M, YT* y, double alpha, double beta, const int* skip, cudaStream_t s)
+{
+    using C = StageCfg<VT, IT>;
+    auto kern = k_rowop_staged<S, OP, VT, XT, FT, MT, YT, IT>;
+    static const int per_sm = [kern] {
+        BCMGX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, kStageThreads, C::SMEM) != cudaSuccess || b < 1) {
+            (void)cudaGetLastError();
+            b = 1;
+        }
+        return b;
+    }();
+    stage_fault_init();
+    const int R = stage_tile_rows<VT, IT>(n, nnz, S);
+    const long ntiles = ((long)n + R - 1) / R;
+    const int grid = (int)std::min<long>(ntiles, (long)per_sm * num_sms());
+    note_launch();
+    kern<<<grid, kStageThreads, C::SMEM, s>>>(n, R, row, col, val, x, f, M, y, alpha, beta, skip, g_stage_fault);
+    BCMGX_CHECK_LAUNCH();
+}
+
+// The row operation on a level matrix, through its int16 column offsets when it has them, and
+// through the staged kernel when the level's tuning chose it (stage: -1 follows A.staged, 0 / 1
+// force it off / on). The staged kernel exists for 2, 4 and 8 threads per row.
 template <int OP, typename VT, typename XT, typename FT, typename MT, typename YT>
 static void launch_rowop_A(int tpr, const DevCsr& A, const VT* val, const XT* x, const FT* f, const MT* M, YT* y,
-    double alpha, double beta, const int* skip, cudaStream_t s)
+    double alpha, double beta, const int* skip, cudaStream_t s, int stage = -1)
 {
+    if (A.n <= 0) return;
+    const bool staged = (stage < 0 ? A.staged : stage > 0) && (tpr == 2 || tpr == 4 || tpr == 8) &&
+        aligned16(A.row.p) && aligned16(val) && aligned16(A.dcol.p ? (const void*)A.dcol.p : (const void*)A.col.p);
+    if (staged) {
+        auto go = [&](auto* colp) {
+            switch (tpr) {
+            case 2: launch_staged<2, OP>(A.n, A.nnz, A.row.p, colp, val, x, f, M, y, alpha, beta, skip, s); break;
+            case 4: launch_staged<4, OP>(A.n, A.nnz, A.row.p, colp, val, x, f, M, y, alpha, beta, skip, s); break;
+            default: launch_staged<8, OP>(A.n, A.nnz, A.row.p, colp, val, x, f, M, y, alpha, beta, skip, s); break;
+            }
+        };
+        if (A.dcol.p) go((const short*)A.dcol.p);
+        else go((const int*)A.col.p);
+        return;
+    }
     if (A.dcol.p) launch_rowop<OP>(tpr, A.n, A.row.p, (const short*)A.dcol.p, val, x, f, M, y, alpha, beta, skip, s);
     else launch_rowop<OP>(tpr, A.n, A.row.p, (const int*)A.col.p, val, x, f, M, y, alpha, beta, skip, s);
 }
@@ -1038,10 +1109,13 @@ void time_block_kernels(bcmgx_hierarchy* H, int K, int reps, double* out)
 
 // Threads-per-row autotuner: for a level with at least kTuneMinRows rows, one l1-Jacobi sweep
 // in the cycle's precision is timed (CUDA events, 3 launches after a warm-up) for every
-// candidate 1..16 and the fastest is kept. Results are cached per (rows, nnz, precision) for
-// the life of the process, so repeated set-ups of same-shaped matrices reuse them; when the
-// environment variable BCMGX_TUNE_CACHE names a file, the cache is also read from it at the
-// first use and every new result is appended to it (one "rows nnz precision tpr" line each).
+// candidate 1..16 of the plain kernel and 2, 4, 8 of the staged one, and the fastest is kept.
+// The result is a code: the threads per row, negative for the staged kernel (the two kernels
+// sum a row in the same order, so that choice does not change results). Codes are cached per
+// (rows, nnz, precision) for the life of the process, so repeated set-ups of same-shaped
+// matrices reuse them; when the environment variable BCMGX_TUNE_CACHE names a file, the cache is
+// also read from it at the first use and every new result is appended to it (one "rows nnz
+// precision code" line each).
 constexpr int kTuneMinRows = 20000;
 static std::mutex g_tune_mu;
 static std::map<std::tuple<int, int64_t, int>, int> g_tune_cache;
@@ -1058,7 +1132,8 @@ static void tune_cache_load()
     long long z;
     int n, prec, t;
     while (std::fscanf(f, "%d %lld %d %d", &n, &z, &prec, &t) == 4)
-        if (t == 1 || t == 2 || t == 4 || t == 8 || t == 16 || t == 32) g_tune_cache[std::make_tuple(n, (int64_t)z, prec)] = t;
+        if (t == 1 || t == 2 || t == 4 || t == 8 || t == 16 || t == 32 || t == -2 || t == -4 || t == -8)
+            g_tune_cache[std::make_tuple(n, (int64_t)z, prec)] = t;
     std::fclose(f);
 }
 
@@ -1104,12 +1179,14 @@ int autotune_tpr(Level& V, bool f32, cudaStream_t s)
     BCMGX_CUDA(cudaEventCreate(&e1));
     int best = default_tpr(n, A.nnz);
     float best_ms = 1e30f;
-    for (int t = 1; t <= 16; t *= 2) {
+    // candidates: 1..16 threads per row, then the staged kernel with 2, 4 and 8 (coded negative)
+    for (int t : {1, 2, 4, 8, 16, -2, -4, -8}) {
+        const int tp = t < 0 ? -t : t, stage = t < 0 ? 1 : 0;
         auto launch = [&] {
             if (f32)
-                launch_rowop_A<OP_JACOBI>(t, A, A.val32.p, (const float*)a32.p, (const float*)c32.p, V.M32.p, b32.p, 1.0, 0.0, nullptr, s);
+                launch_rowop_A<OP_JACOBI>(tp, A, A.val32.p, (const float*)a32.p, (const float*)c32.p, V.M32.p, b32.p, 1.0, 0.0, nullptr, s, stage);
             else
-                launch_rowop_A<OP_JACOBI>(t, A, A.val.p, (const double*)a.p, (const double*)c.p, V.M.p, b.p, 1.0, 0.0, nullptr, s);
+                launch_rowop_A<OP_JACOBI>(tp, A, A.val.p, (const double*)a.p, (const double*)c.p, V.M.p, b.p, 1.0, 0.0, nullptr, s, stage);
         };
         launch();
         BCMGX_CUDA(cudaEventRecord(e0, s));

@@ -123,7 +123,8 @@ typedef struct bcmgx_hierarchy_info {
     double op_cmplx, op_wcmplx, avg_cratio;
     int maxcoarsesize, ftcoarse, num_sweep_records;
     double setup_ms;         /* device time of the set-up (CUDA events) */
-    int tpr[BCMGX_MAX_LEVELS];   /* threads per row the solve kernels use on each level */
+    int tpr[BCMGX_MAX_LEVELS];   /* threads per row the solve kernels use on each level; negative: the
+                                    staged kernel (matrix entries through shared memory) with -tpr */
     int index_bytes[BCMGX_MAX_LEVELS]; /* column index bytes the solve kernels stream per entry
                                           (2: int16 offsets from the diagonal, 4: int32) */
 } bcmgx_hierarchy_info;

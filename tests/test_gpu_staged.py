@@ -1,0 +1,123 @@
+"""The staged row kernels (matrix entries streamed through shared-memory stages by bulk async
+copies, staged.cuh) against the plain row kernels (rowops.cuh). With the same threads per row both
+sum every row in the same order, so whole set-ups and solves must agree bit for bit. The
+environment variable BCMGX_TPR forces the kernel on every level: S for the plain kernel, -S for the
+staged one."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from test_gpu_parity import as_csr, fcg
+
+pytestmark = pytest.mark.gpu
+
+
+def far_columns(n, seed):
+    """SPD, each row coupled to its neighbours and to the row n/2 away: column offsets beyond
+    int16, so level 0 keeps int32 columns."""
+    rng = np.random.default_rng(seed)
+    i = np.arange(n)
+    rows = np.concatenate([i, i, i])
+    cols = np.concatenate([(i + 1) % n, (i - 1) % n, (i + n // 2) % n])
+    B = sp.csr_matrix((-rng.uniform(0.5, 1.5, rows.size), (rows, cols)), shape=(n, n))
+    B = (B + B.T).tocsr()
+    d = np.asarray(abs(B).sum(axis=1)).ravel() + 0.1
+    A = (B + sp.diags(d)).tocsr()
+    A.sort_indices()
+    return A
+
+
+def arrow(n, k, seed):
+    """SPD tridiagonal band plus k dense rows and columns: the tiles holding the dense rows have
+    more entries than a shared-memory stage and are read from global memory."""
+    rng = np.random.default_rng(seed)
+    i = np.arange(n - 1)
+    B = sp.csr_matrix((-rng.uniform(0.5, 1.5, n - 1), (i, i + 1)), shape=(n, n)).tolil()
+    for r in rng.choice(n, k, replace=False):
+        B[r, :] = -rng.uniform(0, 0.01, n)
+    B = B.tocsr()
+    B.setdiag(0)
+    B.eliminate_zeros()
+    B = (B + B.T).tocsr()
+    d = np.asarray(abs(B).sum(axis=1)).ravel() + 0.5
+    A = (B + sp.diags(d)).tocsr()
+    A.sort_indices()
+    return A
+
+
+def matrix(bx, case):
+    kind, arg = case
+    if kind == "far":
+        return far_columns(*arg)
+    if kind == "arrow":
+        return arrow(*arg)
+    return as_csr(bx, case)
+
+
+def setup_solve(bx, monkeypatch, A, b, code, **kw):
+    monkeypatch.setenv("BCMGX_TPR", str(code))
+    try:
+        h = bx.prec_setup(A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data, fcg(bx, **kw))
+    finally:
+        monkeypatch.delenv("BCMGX_TPR")
+    x, info = h.solve(b.copy())
+    hi = h.info()
+    h.free()
+    return x, info, hi
+
+
+CASES = [("lap27", (23, 17, 19)), ("lap7", (40, 33, 31)), ("diff", (24, 3)), ("rand", (5000, 0.01, 2, True)),
+         ("far", (80000, 4)), ("arrow", (3000, 4, 5))]
+
+
+@pytest.mark.parametrize("prec", ["FP64", "FP32"])
+@pytest.mark.parametrize("S", [2, 4, 8])
+@pytest.mark.parametrize("case", CASES)
+def test_staged_solve_bit_identical(bx, cuda, monkeypatch, case, S, prec):
+    """Every level on the staged kernel with S threads per row gives the plain kernel's
+    iterations and solution bit for bit (set-up, V-cycle sweeps and residuals, FCG residual)."""
+    A = matrix(bx, case)
+    n = A.shape[0]
+    b = A @ np.random.default_rng(3).uniform(-1, 1, n)
+    x0, i0, h0 = setup_solve(bx, monkeypatch, A, b, S, vcycle_precision=prec, rtol=1e-8)
+    x1, i1, h1 = setup_solve(bx, monkeypatch, A, b, -S, vcycle_precision=prec, rtol=1e-8)
+    assert h0["tpr"] == [S] * h0["num_levels"] and h1["tpr"] == [-S] * h1["num_levels"]
+    if case[0] == "far":
+        assert h0["index_bytes"][0] == 4
+    assert i0["status"] == 0 and i1["status"] == 0
+    assert i0["niter"] == i1["niter"]
+    assert np.array_equal(x0, x1)
+    assert np.linalg.norm(b - A @ x1) <= 1e-8 * np.linalg.norm(b) * 1.0001
+
+
+def test_staged_in_batch_graph(bx, cuda, monkeypatch):
+    """The staged kernel inside the batch graph (captured launches) gives the plain kernel's
+    single-solve results bit for bit."""
+    import torch
+    from test_gpu_batch import _systems
+    systems = _systems(bx, 4, 21, lo=20, hi=34)
+    p = bx.params_default(solver="FCG", preconditioner="BCMG", rtol=1e-8, dispnorm=0, vcycle_precision="FP32")
+    monkeypatch.setenv("BCMGX_TPR", "-4")
+    B = bx.Batch(systems, p, nthreads=2)
+    monkeypatch.setenv("BCMGX_TPR", "4")
+    singles = [bx.prec_setup(r, c, v, p) for r, c, v in systems]
+    monkeypatch.delenv("BCMGX_TPR")
+    rng = np.random.default_rng(8)
+    bs = [torch.from_numpy(rng.uniform(-1, 1, r.size - 1)).to(cuda) for r, _, _ in systems]
+    xs, infos = B.solve(bs)
+    for k, h in enumerate(singles):
+        x, info = h.solve(bs[k])
+        assert info["niter"] == infos[k]["niter"]
+        assert torch.equal(x, xs[k])
+        h.free()
+    B.free()
+
+
+def test_autotuned_codes_are_reported(bx, cuda):
+    """With the autotuner on (the default), every level reports a threads-per-row code of the
+    plain (1..32) or the staged (-2, -4, -8) kernel."""
+    A = as_csr(bx, ("lap27", (40, 40, 40)))
+    h = bx.prec_setup(A.indptr, A.indices, A.data, fcg(bx, vcycle_precision="FP32"))
+    for t in h.info()["tpr"]:
+        assert t in (1, 2, 4, 8, 16, 32, -2, -4, -8)
+    h.free()

@@ -1373,15 +1373,36 @@ __global__ void k_batch_states(int m, FcgState* const* __restrict__ st, FcgState
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) out[k] = *st[k];
 }
 
+// While one system's solve is captured into the batch graph: sweep chains of small levels as one
+// block (fewer, longer kernels per system), and the plain row kernels instead of the staged ones
+// (a staged kernel's resident grid of large shared-memory blocks would hold the SMs that the other
+// systems' branches run on). The hierarchy's own settings come back when the capture ends.
+struct BatchCaptureMode {
+    bcmgx_hierarchy* H;
+    std::vector<char> staged;
+    explicit BatchCaptureMode(bcmgx_hierarchy* h) : H(h)
+    {
+        H->chain_in_block = true;
+        for (Level& V : H->lv) {
+            staged.push_back(V.A.staged ? 1 : 0);
+            V.A.staged = false;
+        }
+    }
+    ~BatchCaptureMode()
+    {
+        H->chain_in_block = false;
+        for (size_t l = 0; l < staged.size(); l++) H->lv[l].A.staged = staged[l] != 0;
+    }
+};
+
 void batch_build(bcmgx_batch* B)
 {
     cudaGraph_t g = nullptr;
     BCMGX_CUDA(cudaGraphCreate(&g, 0));
     for (bcmgx_hierarchy* H : B->hs) {
         ensure_solve_workspace(H);
-        H->chain_in_block = true;   // many systems share the GPU: fewer, longer kernels per system
+        BatchCaptureMode mode(H);
         add_solve_to_graph(H, g);
-        H->chain_in_block = false;
     }
     BCMGX_CUDA(cudaGraphInstantiate(&B->exec, g, 0));
     BCMGX_CUDA(cudaGraphDestroy(g));

@@ -90,16 +90,16 @@ def test_staged_solve_bit_identical(bx, cuda, monkeypatch, case, S, prec):
     assert np.linalg.norm(b - A @ x1) <= 1e-8 * np.linalg.norm(b) * 1.0001
 
 
-def test_staged_in_batch_graph(bx, cuda, monkeypatch):
-    """The staged kernel inside the batch graph (captured launches) gives the plain kernel's
-    single-solve results bit for bit."""
+def test_staged_hierarchies_in_batch_graph(bx, cuda, monkeypatch):
+    """Hierarchies set up for the staged kernel: the batch graph captures the plain row kernels
+    (side by side with other systems), their single solves (also graph-captured) the staged ones;
+    both give the same results bit for bit, and the batch leaves the hierarchies staged."""
     import torch
     from test_gpu_batch import _systems
     systems = _systems(bx, 4, 21, lo=20, hi=34)
     p = bx.params_default(solver="FCG", preconditioner="BCMG", rtol=1e-8, dispnorm=0, vcycle_precision="FP32")
     monkeypatch.setenv("BCMGX_TPR", "-4")
     B = bx.Batch(systems, p, nthreads=2)
-    monkeypatch.setenv("BCMGX_TPR", "4")
     singles = [bx.prec_setup(r, c, v, p) for r, c, v in systems]
     monkeypatch.delenv("BCMGX_TPR")
     rng = np.random.default_rng(8)
@@ -110,6 +110,9 @@ def test_staged_in_batch_graph(bx, cuda, monkeypatch):
         assert info["niter"] == infos[k]["niter"]
         assert torch.equal(x, xs[k])
         h.free()
+    assert B.hierarchy(0).info()["tpr"][0] == -4
+    x1, i1 = B.hierarchy(0).solve(bs[0])
+    assert i1["niter"] == infos[0]["niter"] and torch.equal(x1, xs[0])
     B.free()
 
 

@@ -275,6 +275,15 @@ inline int fit_grid(void (*kernel)(A...), int threads, long need_blocks)
     return fit_grid((const void*)kernel, threads, need_blocks);
 }
 
+// Raises the kernel's dynamic shared-memory limit on the current device to at least `bytes`
+// (never lowers it, so concurrent set-ups on other threads keep the room their launches need).
+void ensure_smem_limit(const void* kernel, size_t bytes);
+template <typename... A>
+inline void ensure_smem_limit(void (*kernel)(A...), size_t bytes)
+{
+    ensure_smem_limit((const void*)kernel, bytes);
+}
+
 // ---- kernels usable on raw device memory (kernels.cu) ----
 int autotune_tpr(Level& V, bool f32, cudaStream_t s);
 void stage_fault_init();

@@ -786,11 +786,16 @@ __global__ void k_make_p(int n, const int* __restrict__ M, const double* __restr
 // sort by key, each group of equal J is (AP)_{f0,J} = sum of its f0 terms and (AP)_{f1,J}
 // likewise (<= 2 terms each), and C_IJ = p_f0 (AP)_{f0,J} + p_f1 (AP)_{f1,J}: the values
 // nsparse forms for A*P and then R*(AP) (kernel_spgemm_hash_d.cu:792-799), since a sum of at most
-// two rounded terms does not depend on their order. Row I is written at I * cap (padded) and its
-// length at Crow[I]; a compaction then forms the CSR matrix.
-__global__ void k_galerkin(int nc, const int* __restrict__ fine0, const int* __restrict__ fine1, const int* __restrict__ agg,
-    const double* __restrict__ p, const int* __restrict__ Arow, const int* __restrict__ Acol, const double* __restrict__ Aval,
-    int* __restrict__ Crow, int* __restrict__ Ccol, double* __restrict__ Cval, int cap, int* err)
+// two rounded terms does not depend on their order. Row I is written from off[I] (the prefix sum
+// of the rows' candidate counts, which bound their lengths) and its length at Crow[I]; a
+// compaction then forms the CSR matrix. cap is the candidates a warp's shared memory holds: a
+// row with more is appended to long_rows (for a second launch with room for it, over that list:
+// rows = long_rows, nc its length), or flagged as an error when long_rows is NULL.
+__global__ void k_galerkin(int nc, const int* __restrict__ rows, const int* __restrict__ fine0, const int* __restrict__ fine1,
+    const int* __restrict__ agg, const double* __restrict__ p, const int* __restrict__ Arow, const int* __restrict__ Acol,
+    const double* __restrict__ Aval, const int* __restrict__ off, int* __restrict__ Crow, int* __restrict__ Ccol,
+    double* __restrict__ Cval, int cap, int* __restrict__ long_rows, int* __restrict__ nlong, int* __restrict__ long_max,
+    int* err)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int wpb = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -804,13 +809,21 @@ __global__ void k_galerkin(int nc, const int* __restrict__ fine0, const int* __r
     unsigned* skey32 = key32 + cap;
     double* sval = (double*)(smem + (size_t)wpb * cap * 20) + (size_t)wid * cap;
     const bool narrow = nc < (1 << 25);
-    for (long I = (long)blockIdx.x * wpb + wid; I < nc; I += (long)gridDim.x * wpb) {
+    for (long k = (long)blockIdx.x * wpb + wid; k < nc; k += (long)gridDim.x * wpb) {
+        const int I = rows ? rows[k] : (int)k;
         const int f0 = fine0[I], f1 = fine1[I];
         const int b0 = Arow[f0], d0 = Arow[f0 + 1] - b0;
         const int b1 = f1 >= 0 ? Arow[f1] : 0, d1 = f1 >= 0 ? Arow[f1 + 1] - b1 : 0;
         const int cnt = d0 + d1;
         if (cnt > cap) {
-            if (lane == 0) atomicOr(err, ERR_GALERKIN_CAP);
+            if (lane == 0) {
+                if (long_rows) {
+                    long_rows[atomicAdd(nlong, 1)] = I;
+                    atomicMax(long_max, cnt);
+                } else {
+                    atomicOr(err, ERR_GALERKIN_CAP);
+                }
+            }
             continue;
         }
         if (narrow && cnt <= 128) {
@@ -833,7 +846,7 @@ __global__ void k_galerkin(int nc, const int* __restrict__ fine0, const int* __r
             }
             __syncwarp();
             const double p0 = p[f0], p1 = f1 >= 0 ? p[f1] : 0.0;
-            const long outbase = (long)I * cap;
+            const long outbase = off[I];
             int nheads = 0;
             for (int base = 0; base < cnt; base += 32) {
                 const int sidx0 = base + lane;
@@ -889,7 +902,7 @@ __global__ void k_galerkin(int nc, const int* __restrict__ fine0, const int* __r
         }
         __syncwarp();
         const double p0 = p[f0], p1 = f1 >= 0 ? p[f1] : 0.0;
-        const long outbase = (long)I * cap;
+        const long outbase = off[I];
         int nheads = 0;
         for (int base = 0; base < cnt; base += 32) {
             const int s = base + lane;
@@ -930,16 +943,26 @@ __global__ void k_galerkin(int nc, const int* __restrict__ fine0, const int* __r
     }
 }
 
-// padded rows (I * cap) -> CSR; one warp per row
-__global__ void k_compact_rows(int nc, int cap, const int* __restrict__ rowptr, const int* __restrict__ pcol,
+// Number of candidate entries of every coarse row: the entries of its fine rows.
+__global__ void k_galerkin_counts(int nc, const int* __restrict__ fine0, const int* __restrict__ fine1,
+    const int* __restrict__ Arow, int* __restrict__ cnt)
+{
+    for (long I = (long)blockIdx.x * blockDim.x + threadIdx.x; I < nc; I += (long)gridDim.x * blockDim.x) {
+        const int f0 = fine0[I], f1 = fine1[I];
+        cnt[I] = (Arow[f0 + 1] - Arow[f0]) + (f1 >= 0 ? Arow[f1 + 1] - Arow[f1] : 0);
+    }
+}
+
+// rows written from off[I] -> CSR; one warp per row
+__global__ void k_compact_rows(int nc, const int* __restrict__ off, const int* __restrict__ rowptr, const int* __restrict__ pcol,
     const double* __restrict__ pval, int* __restrict__ col, double* __restrict__ val)
 {
     const int lane = threadIdx.x & 31;
     for (long I = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32; I < nc; I += (long)gridDim.x * blockDim.x / 32) {
         const int b = rowptr[I], len = rowptr[I + 1] - b;
         for (int t = lane; t < len; t += 32) {
-            col[b + t] = pcol[I * (long)cap + t];
-            val[b + t] = pval[I * (long)cap + t];
+            col[b + t] = pcol[(long)off[I] + t];
+            val[b + t] = pval[(long)off[I] + t];
         }
     }
 }
@@ -1231,34 +1254,63 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
     fs.release();
     pofs.release();
     sofs.release();
-    // Galerkin: count, prefix sum, fill
+    // Galerkin: each coarse row's candidate count (the entries of its fine rows) and their prefix
+    // sum, which places the row's output (the counts add up to nnz(A), so the scratch is nnz(A)
+    // entries whatever the row lengths); the product of the rows that fit kGalCap candidates per
+    // warp, then of the longer ones (listed by the first launch) with one warp per block and shared
+    // memory for the longest; then compaction.
     const int amax = A.max_row > 0 ? A.max_row : row_max(A, s);
-    const int cap = std::max(2 * amax, 32);
-    const size_t per_warp = (size_t)cap * 28;
+    constexpr int kGalCap = 512;
+    constexpr size_t kGalBytes = 28;   // shared-memory bytes per candidate (keys, products, sort)
     const size_t smem_limit = 200 * 1024;
-    BCMGX_REQUIRE(per_warp <= smem_limit, BCMGX_ERR_UNSUPPORTED,
-        "coarse row too long for the Galerkin kernel (" + std::to_string(cap) + " candidate entries)");
-    int wpb = (int)std::min<size_t>(8, std::max<size_t>(1, (48 * 1024) / per_warp));
-    size_t smem = per_warp * wpb;
-    if (smem > 48 * 1024)
-        BCMGX_CUDA(cudaFuncSetAttribute(k_galerkin, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int g = (int)std::max<long>(1, std::min<long>(((long)nc + wpb - 1) / wpb, (long)num_sms() * 32));
+    const int cap1 = std::min(std::max(2 * amax, 32), kGalCap);
     DevCsr& C = out.C;
     C.n = C.m = nc;
     C.row.alloc((size_t)nc + 1, s);
-    // one pass into padded rows (cap entries each), then prefix sum and compaction
-    DBuf<int> counts, pcol;
+    DBuf<int> cand, off, counts, pcol, longr, lstat;
     DBuf<double> pval;
-    counts.alloc(std::max(nc, 1), s);
-    pcol.alloc(std::max<size_t>((size_t)nc * cap, 1), s);
-    pval.alloc(std::max<size_t>((size_t)nc * cap, 1), s);
-    note_launch(); k_galerkin<<<g, wpb * 32, smem, s>>>(nc, fine0.p, fine1.p, out.agg.p, out.p.p, A.row.p, A.col.p, A.val.p,
-        counts.p, pcol.p, pval.p, cap, err.p);
+    cand.alloc(std::max(nc, 1), s);
+    off.alloc((size_t)nc + 1, s);
+    note_launch(); k_galerkin_counts<<<gs_grid(nc), 256, 0, s>>>(nc, fine0.p, fine1.p, A.row.p, cand.p);
     BCMGX_CHECK_LAUNCH();
+    const long long total = scan_exclusive(cand.p, off.p, nc, true, s);
+    cand.release();
+    counts.alloc(std::max(nc, 1), s);
+    pcol.alloc(std::max<size_t>((size_t)total, 1), s);
+    pval.alloc(std::max<size_t>((size_t)total, 1), s);
+    const bool may_be_long = 2 * amax > cap1;
+    if (may_be_long) {
+        longr.alloc(std::max(nc, 1), s);
+        lstat.alloc(2, s);
+        BCMGX_CUDA(cudaMemsetAsync(lstat.p, 0, 2 * sizeof(int), s));
+    }
+    auto galerkin = [&](const int* rows, int nrows, int cap, bool list_long) {
+        const size_t per_warp = (size_t)cap * kGalBytes;
+        const int wpb = (int)std::min<size_t>(8, std::max<size_t>(1, (48 * 1024) / per_warp));
+        const size_t smem = per_warp * wpb;
+        ensure_smem_limit(k_galerkin, smem);
+        const int g = (int)std::max<long>(1, std::min<long>(((long)nrows + wpb - 1) / wpb, (long)num_sms() * 32));
+        note_launch();
+        k_galerkin<<<g, wpb * 32, smem, s>>>(nrows, rows, fine0.p, fine1.p, out.agg.p, out.p.p, A.row.p, A.col.p,
+            A.val.p, off.p, counts.p, pcol.p, pval.p, cap, list_long ? longr.p : nullptr,
+            list_long ? lstat.p : nullptr, list_long ? lstat.p + 1 : nullptr, err.p);
+        BCMGX_CHECK_LAUNCH();
+    };
+    galerkin(nullptr, nc, cap1, may_be_long);
+    if (may_be_long) {
+        int st[2] = { 0, 0 };
+        BCMGX_CUDA(cudaMemcpyAsync(st, lstat.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+        BCMGX_CUDA(cudaStreamSynchronize(s));
+        if (st[0] > 0) {
+            BCMGX_REQUIRE((size_t)st[1] * kGalBytes <= smem_limit, BCMGX_ERR_UNSUPPORTED,
+                "coarse row too long for the Galerkin kernel (" + std::to_string(st[1]) + " candidate entries)");
+            galerkin(longr.p, st[0], st[1], false);
+        }
+    }
     C.nnz = scan_exclusive(counts.p, C.row.p, nc, true, s);
     C.col.alloc(std::max<int64_t>(C.nnz, 1), s);
     C.val.alloc(std::max<int64_t>(C.nnz, 1), s);
-    note_launch(); k_compact_rows<<<warp_grid(nc), 256, 0, s>>>(nc, cap, C.row.p, pcol.p, pval.p, C.col.p, C.val.p);
+    note_launch(); k_compact_rows<<<warp_grid(nc), 256, 0, s>>>(nc, off.p, C.row.p, pcol.p, pval.p, C.col.p, C.val.p);
     BCMGX_CHECK_LAUNCH();
     e = read_err(err.p, s);
     if (e) throw Error(BCMGX_ERR_INTERNAL, "galerkin: " + err_text(e));

@@ -40,6 +40,20 @@ int num_sms()
     return sms;
 }
 
+void ensure_smem_limit(const void* kernel, size_t bytes)
+{
+    if (bytes <= 48 * 1024) return;
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, size_t> set;
+    int dev = 0;
+    BCMGX_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> g(mu);
+    size_t& cur = set[std::make_pair(dev, kernel)];
+    if (bytes <= cur) return;
+    BCMGX_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    cur = bytes;
+}
+
 // Grid of a grid-stride kernel: the blocks its work needs, but no more than fit on the GPU at
 // once for this kernel (its registers and shared memory decide how many blocks an SM holds; the
 // figure is queried once per kernel and cached). Every block is then resident from the start: a
@@ -122,8 +136,8 @@ static void launch_staged(int n, int64_t nnz, const int* row, const IT* col, con
 {
     using C = StageCfg<VT, IT>;
     auto kern = k_rowop_staged<S, OP, VT, XT, FT, MT, YT, IT>;
+    ensure_smem_limit(kern, C::SMEM);
     static const int per_sm = [kern] {
-        BCMGX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
         int b = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, kStageThreads, C::SMEM) != cudaSuccess || b < 1) {
             (void)cudaGetLastError();

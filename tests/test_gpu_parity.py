@@ -40,6 +40,23 @@ def random_spd(n, density, seed, ragged=False):
     return A
 
 
+def arrow(n, k, seed):
+    """SPD tridiagonal band plus k dense rows and columns (rows of n entries)."""
+    rng = np.random.default_rng(seed)
+    i = np.arange(n - 1)
+    B = sp.csr_matrix((-rng.uniform(0.5, 1.5, n - 1), (i, i + 1)), shape=(n, n)).tolil()
+    for r in rng.choice(n, k, replace=False):
+        B[r, :] = -rng.uniform(0, 0.01, n)
+    B = B.tocsr()
+    B.setdiag(0)
+    B.eliminate_zeros()
+    B = (B + B.T).tocsr()
+    d = np.asarray(abs(B).sum(axis=1)).ravel() + 0.5
+    A = (B + sp.diags(d)).tocsr()
+    A.sort_indices()
+    return A
+
+
 def heterogeneous(bx, n, seed):
     rng = np.random.default_rng(seed)
     kappa = np.exp(1.5 * rng.normal(size=n ** 3))
@@ -55,6 +72,9 @@ def as_csr(bx, case):
         r, c, v = bx.laplacian_3d(27, *arg)
     elif kind == "rand":
         A = random_spd(*arg)
+        r, c, v = A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data
+    elif kind == "arrow":
+        A = arrow(*arg)
         r, c, v = A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data
     else:
         A = heterogeneous(bx, *arg)
@@ -138,13 +158,15 @@ def test_weights_and_matching(bx, oracle, cuda, case):
 
 
 @pytest.mark.parametrize("case", [("lap7", (20, 20, 20)), ("lap27", (16, 16, 16)), ("lap7", (9, 30, 7)),
-                                  ("rand", (3000, 0.003, 5)), ("diff", (14, 9)), ("rand", (1500, 0.05, 9))])
+                                  ("rand", (3000, 0.003, 5)), ("diff", (14, 9)), ("rand", (1500, 0.05, 9)),
+                                  ("arrow", (3000, 4, 5))])
 def test_hierarchy_bit_exact(bx, oracle, cuda, case):
     """Every sweep's matching, aggregates, prolongator values and weight vector, every level's
-    matrix and the composite prolongators equal the oracle's bit for bit. The last matrix has
+    matrix and the composite prolongators equal the oracle's bit for bit. The sixth matrix has
     about 150 entries per row: its sweeps store the edge weights (rows over 32 entries), run the
     matching kernels on whole warps and the Galerkin product with 64-bit keys (over 128 candidate
-    entries per coarse row)."""
+    entries per coarse row). The last has 4 dense rows of 3000 entries: the coarse rows holding
+    them exceed a warp's 512 candidates in the first Galerkin launch and go to the second."""
     A = as_csr(bx, case)
     h = bx.prec_setup(A.indptr, A.indices, A.data, fcg(bx, record_sweeps=1))
     Ao = oracle.Matrix.from_csr(A.indptr, A.indices, A.data)
@@ -170,6 +192,31 @@ def test_hierarchy_bit_exact(bx, oracle, cuda, case):
     st = Ho.stats()
     assert gi["maxcoarsesize"] == st["maxcoarsesize"] and gi["ftcoarse"] == st["ftcoarse"]
     assert abs(gi["op_cmplx"] - st["op_cmplx"]) < 1e-12
+
+
+def test_long_row_in_a_large_matrix(bx, oracle, cuda):
+    """A 7-point 100^3 Laplacian with one row coupled to 2000 others: the Galerkin scratch is the
+    fine matrix's entries (not the coarse rows times the longest row, which here would be 24 GB),
+    the levels match the oracle's sizes and the solve reaches the tolerance."""
+    r, c, v = bx.laplacian_3d(7, 100, 100, 100)
+    n = r.size - 1
+    rng = np.random.default_rng(4)
+    k = 12345
+    cols = rng.choice(np.setdiff1d(np.arange(n), [k]), 2000, replace=False)
+    B = sp.csr_matrix((-0.01 * np.ones(2000), (np.full(2000, k), cols)), shape=(n, n))
+    B = (B + B.T).tocsr()
+    A = (sp.csr_matrix((v, c, r), shape=(n, n)) + B + sp.diags(np.asarray(abs(B).sum(axis=1)).ravel())).tocsr()
+    A.sort_indices()
+    row, col = A.indptr.astype(np.int32), A.indices.astype(np.int32)
+    h = bx.prec_setup(row, col, A.data, fcg(bx, rtol=1e-8))
+    Ho = oracle.Hierarchy(oracle.Matrix.from_csr(row, col, A.data), oracle.params())
+    gi = h.info()
+    assert [(n_, z) for n_, z in zip(gi["n"], gi["nnz"])] == Ho.level_sizes()
+    b = A @ rng.uniform(-1, 1, n)
+    x, info = h.solve(b)
+    assert info["status"] == 0
+    assert np.linalg.norm(b - A @ x) <= 1e-8 * np.linalg.norm(b) * 1.0001
+    h.free()
 
 
 @pytest.mark.parametrize("cycle", ["V_CYCLE", "H_CYCLE", "W_CYCLE", "VARIABLE_V_CYCLE"])

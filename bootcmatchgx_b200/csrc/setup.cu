@@ -18,6 +18,8 @@
 #include "internal.h"
 #include "common.cuh"
 
+#include <cub/device/device_segmented_sort.cuh>
+
 #include <algorithm>
 #include <cfloat>
 #include <chrono>
@@ -943,6 +945,103 @@ __global__ void k_galerkin(int nc, const int* __restrict__ rows, const int* __re
     }
 }
 
+// Coarse rows longer than a warp's shared memory holds: their candidates in global memory, one
+// block per row, the (J, source row, position) keys of k_galerkin at seg[k] onwards.
+__global__ void k_galerkin_long_fill(int nrows, const int* __restrict__ rows, const int* __restrict__ fine0,
+    const int* __restrict__ fine1, const int* __restrict__ agg, const double* __restrict__ p, const int* __restrict__ Arow,
+    const int* __restrict__ Acol, const double* __restrict__ Aval, const int* __restrict__ seg,
+    unsigned long long* __restrict__ key, double* __restrict__ tv)
+{
+    for (int k = blockIdx.x; k < nrows; k += gridDim.x) {
+        const int I = rows[k];
+        const int f0 = fine0[I], f1 = fine1[I];
+        const int b0 = Arow[f0], d0 = Arow[f0 + 1] - b0;
+        const int b1 = f1 >= 0 ? Arow[f1] : 0, d1 = f1 >= 0 ? Arow[f1 + 1] - b1 : 0;
+        const long o = seg[k];
+        for (int t = threadIdx.x; t < d0 + d1; t += blockDim.x) {
+            const int j = t < d0 ? b0 + t : b1 + (t - d0);
+            const int c = Acol[j];
+            const unsigned src = t < d0 ? 0u : 1u;
+            key[o + t] = ((unsigned long long)(unsigned)agg[c] << 32) | ((unsigned long long)src << 31) | (unsigned)t;
+            tv[o + t] = __dmul_rn(Aval[j], p[c]);
+        }
+    }
+}
+
+// The long rows' sorted candidates -> their entries of C, with k_galerkin's sums: one block per
+// row walks its candidates in chunks of blockDim, marks the first of every J, and numbers the
+// marks by a block-wide scan of the warps' ballots.
+__global__ void __launch_bounds__(1024) k_galerkin_long_rows(int nrows, const int* __restrict__ rows,
+    const int* __restrict__ fine0, const int* __restrict__ fine1, const double* __restrict__ p, const int* __restrict__ seg,
+    const unsigned long long* __restrict__ key, const double* __restrict__ tv, const int* __restrict__ off,
+    int* __restrict__ Crow, int* __restrict__ Ccol, double* __restrict__ Cval)
+{
+    __shared__ int wsum[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int k = blockIdx.x; k < nrows; k += gridDim.x) {
+        const int I = rows[k];
+        const int f0 = fine0[I], f1 = fine1[I];
+        const long o = seg[k];
+        const int cnt = seg[k + 1] - seg[k];
+        const double p0 = p[f0], p1 = f1 >= 0 ? p[f1] : 0.0;
+        int nheads = 0;
+        for (int base = 0; base < cnt; base += blockDim.x) {
+            const int g = base + threadIdx.x;
+            bool head = false;
+            int J = -1;
+            if (g < cnt) {
+                J = (int)(key[o + g] >> 32);
+                head = g == 0 || (int)(key[o + g - 1] >> 32) != J;
+            }
+            const unsigned hm = __ballot_sync(0xffffffffu, head);
+            if (lane == 0) wsum[wid] = __popc(hm);
+            __syncthreads();
+            int before = 0, chunk = 0;
+            for (int w = 0; w < nw; w++) {
+                before += w < wid ? wsum[w] : 0;
+                chunk += wsum[w];
+            }
+            if (head) {
+                double ap0 = 0.0, ap1 = 0.0;
+                int n0 = 0, n1 = 0;
+                for (int h = g; h < cnt; h++) {
+                    const unsigned long long kk = key[o + h];
+                    if ((int)(kk >> 32) != J) break;
+                    const double tt = tv[o + h];
+                    if (((kk >> 31) & 1ull) == 0) {
+                        ap0 = n0 == 0 ? tt : __dadd_rn(ap0, tt);
+                        n0++;
+                    } else {
+                        ap1 = n1 == 0 ? tt : __dadd_rn(ap1, tt);
+                        n1++;
+                    }
+                }
+                double cv;
+                if (n0 && n1) cv = __dadd_rn(__dmul_rn(p0, ap0), __dmul_rn(p1, ap1));
+                else if (n0) cv = __dmul_rn(p0, ap0);
+                else cv = __dmul_rn(p1, ap1);
+                const long d = (long)off[I] + nheads + before + __popc(hm & ((1u << lane) - 1u));
+                Ccol[d] = J;
+                Cval[d] = cv;
+            }
+            nheads += chunk;
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) Crow[I] = nheads;
+    }
+}
+
+// Candidate count of each listed row (as k_galerkin_counts, over a list).
+__global__ void k_galerkin_list_counts(int nrows, const int* __restrict__ rows, const int* __restrict__ fine0,
+    const int* __restrict__ fine1, const int* __restrict__ Arow, int* __restrict__ cnt)
+{
+    for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < nrows; k += (long)gridDim.x * blockDim.x) {
+        const int I = rows[k];
+        const int f0 = fine0[I], f1 = fine1[I];
+        cnt[k] = (Arow[f0 + 1] - Arow[f0]) + (f1 >= 0 ? Arow[f1 + 1] - Arow[f1] : 0);
+    }
+}
+
 // Number of candidate entries of every coarse row: the entries of its fine rows.
 __global__ void k_galerkin_counts(int nc, const int* __restrict__ fine0, const int* __restrict__ fine1,
     const int* __restrict__ Arow, int* __restrict__ cnt)
@@ -1284,7 +1383,9 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
         lstat.alloc(2, s);
         BCMGX_CUDA(cudaMemsetAsync(lstat.p, 0, 2 * sizeof(int), s));
     }
-    auto galerkin = [&](const int* rows, int nrows, int cap, bool list_long) {
+    // one launch of k_galerkin over `rows` (all coarse rows when NULL) with room for cap candidates
+    // per warp; longer rows go to `list` (count and longest in stat[0], stat[1]) when it is given
+    auto galerkin = [&](const int* rows, int nrows, int cap, int* list, int* stat) {
         const size_t per_warp = (size_t)cap * kGalBytes;
         const int wpb = (int)std::min<size_t>(8, std::max<size_t>(1, (48 * 1024) / per_warp));
         const size_t smem = per_warp * wpb;
@@ -1292,19 +1393,64 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
         const int g = (int)std::max<long>(1, std::min<long>(((long)nrows + wpb - 1) / wpb, (long)num_sms() * 32));
         note_launch();
         k_galerkin<<<g, wpb * 32, smem, s>>>(nrows, rows, fine0.p, fine1.p, out.agg.p, out.p.p, A.row.p, A.col.p,
-            A.val.p, off.p, counts.p, pcol.p, pval.p, cap, list_long ? longr.p : nullptr,
-            list_long ? lstat.p : nullptr, list_long ? lstat.p + 1 : nullptr, err.p);
+            A.val.p, off.p, counts.p, pcol.p, pval.p, cap, list, stat, stat ? stat + 1 : nullptr, err.p);
         BCMGX_CHECK_LAUNCH();
     };
-    galerkin(nullptr, nc, cap1, may_be_long);
+    auto read2 = [&](const int* d, int (&h)[2]) {
+        BCMGX_CUDA(cudaMemcpyAsync(h, d, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+        BCMGX_CUDA(cudaStreamSynchronize(s));
+    };
+    galerkin(nullptr, nc, cap1, may_be_long ? longr.p : nullptr, may_be_long ? lstat.p : nullptr);
     if (may_be_long) {
         int st[2] = { 0, 0 };
-        BCMGX_CUDA(cudaMemcpyAsync(st, lstat.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
-        BCMGX_CUDA(cudaStreamSynchronize(s));
+        read2(lstat.p, st);
         if (st[0] > 0) {
-            BCMGX_REQUIRE((size_t)st[1] * kGalBytes <= smem_limit, BCMGX_ERR_UNSUPPORTED,
-                "coarse row too long for the Galerkin kernel (" + std::to_string(st[1]) + " candidate entries)");
-            galerkin(longr.p, st[0], st[1], false);
+            const int capmax = (int)(smem_limit / kGalBytes);
+            const bool very_long = st[1] > capmax;
+            DBuf<int> longr2, lstat2;
+            if (very_long) {
+                longr2.alloc(st[0], s);
+                lstat2.alloc(2, s);
+                BCMGX_CUDA(cudaMemsetAsync(lstat2.p, 0, 2 * sizeof(int), s));
+            }
+            galerkin(longr.p, st[0], std::min(st[1], capmax), very_long ? longr2.p : nullptr,
+                very_long ? lstat2.p : nullptr);
+            if (very_long) {
+                // rows beyond a block's shared memory: candidates in global memory, sorted per row
+                // by key with CUB's segmented sort, then summed and written by one block per row
+                int st2[2] = { 0, 0 };
+                read2(lstat2.p, st2);
+                const int n3 = st2[0];
+                DBuf<int> cnt3, seg;
+                cnt3.alloc(n3, s);
+                seg.alloc((size_t)n3 + 1, s);
+                note_launch();
+                k_galerkin_list_counts<<<gs_grid(n3), 256, 0, s>>>(n3, longr2.p, fine0.p, fine1.p, A.row.p, cnt3.p);
+                BCMGX_CHECK_LAUNCH();
+                const long long total3 = scan_exclusive(cnt3.p, seg.p, n3, true, s);
+                DBuf<unsigned long long> k_in, k_out;
+                DBuf<double> v_in, v_out;
+                k_in.alloc((size_t)total3, s);
+                k_out.alloc((size_t)total3, s);
+                v_in.alloc((size_t)total3, s);
+                v_out.alloc((size_t)total3, s);
+                const int g3 = std::min(n3, num_sms() * 4);
+                note_launch();
+                k_galerkin_long_fill<<<g3, 256, 0, s>>>(n3, longr2.p, fine0.p, fine1.p, out.agg.p, out.p.p, A.row.p,
+                    A.col.p, A.val.p, seg.p, k_in.p, v_in.p);
+                BCMGX_CHECK_LAUNCH();
+                size_t tmp_bytes = 0;
+                BCMGX_CUDA(cub::DeviceSegmentedSort::SortPairs(nullptr, tmp_bytes, k_in.p, k_out.p, v_in.p, v_out.p,
+                    (int)total3, n3, seg.p, seg.p + 1, s));
+                DBuf<unsigned char> tmp;
+                tmp.alloc(std::max<size_t>(tmp_bytes, 1), s);
+                BCMGX_CUDA(cub::DeviceSegmentedSort::SortPairs(tmp.p, tmp_bytes, k_in.p, k_out.p, v_in.p, v_out.p,
+                    (int)total3, n3, seg.p, seg.p + 1, s));
+                note_launch();
+                k_galerkin_long_rows<<<std::min(n3, num_sms() * 2), 1024, 0, s>>>(n3, longr2.p, fine0.p, fine1.p,
+                    out.p.p, seg.p, k_out.p, v_out.p, off.p, counts.p, pcol.p, pval.p);
+                BCMGX_CHECK_LAUNCH();
+            }
         }
     }
     C.nnz = scan_exclusive(counts.p, C.row.p, nc, true, s);

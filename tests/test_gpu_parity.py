@@ -159,14 +159,16 @@ def test_weights_and_matching(bx, oracle, cuda, case):
 
 @pytest.mark.parametrize("case", [("lap7", (20, 20, 20)), ("lap27", (16, 16, 16)), ("lap7", (9, 30, 7)),
                                   ("rand", (3000, 0.003, 5)), ("diff", (14, 9)), ("rand", (1500, 0.05, 9)),
-                                  ("arrow", (3000, 4, 5))])
+                                  ("arrow", (3000, 4, 5)), ("arrow", (10000, 3, 7))])
 def test_hierarchy_bit_exact(bx, oracle, cuda, case):
     """Every sweep's matching, aggregates, prolongator values and weight vector, every level's
     matrix and the composite prolongators equal the oracle's bit for bit. The sixth matrix has
     about 150 entries per row: its sweeps store the edge weights (rows over 32 entries), run the
     matching kernels on whole warps and the Galerkin product with 64-bit keys (over 128 candidate
-    entries per coarse row). The last has 4 dense rows of 3000 entries: the coarse rows holding
-    them exceed a warp's 512 candidates in the first Galerkin launch and go to the second."""
+    entries per coarse row). The arrow matrices have dense rows of 3000 and 10000 entries: the
+    coarse rows holding them exceed a warp's 512 candidates in the first Galerkin launch and go to
+    the second (one warp per block), and those over a block's 7314 to the global-memory path
+    (candidates sorted per row with CUB's segmented sort)."""
     A = as_csr(bx, case)
     h = bx.prec_setup(A.indptr, A.indices, A.data, fcg(bx, record_sweeps=1))
     Ao = oracle.Matrix.from_csr(A.indptr, A.indices, A.data)

@@ -97,13 +97,22 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity
         if (global_ns() - t0 > 1000000000ull) return false;
     }
 }
-// Global -> shared bulk copy of `bytes` (multiple of 16, both addresses 16-byte aligned),
-// completing as transaction bytes on mbarrier `bar`.
-__device__ __forceinline__ void bulk_to_smem(void* dst, const void* src, unsigned bytes, unsigned long long* bar)
+// L2 policy for data read once per pass: evict first, so that the gathered vectors stay in L2.
+__device__ __forceinline__ unsigned long long l2_evict_first()
 {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                 ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar))
-                 : "memory");
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+// Global -> shared bulk copy of `bytes` (multiple of 16, both addresses 16-byte aligned),
+// completing as transaction bytes on mbarrier `bar`, with L2 policy `pol`.
+__device__ __forceinline__ void bulk_to_smem(void* dst, const void* src, unsigned bytes, unsigned long long* bar,
+    unsigned long long pol)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;"
+        ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(pol)
+        : "memory");
 }
 
 __device__ __forceinline__ int col_of(short v, int r) { return r + (int)v; }
@@ -157,6 +166,7 @@ __global__ void __launch_bounds__(kStageThreads) k_rowop_staged(int n, int R, co
     if (warp == kStageWarps) {
         // producer: one thread issues the copies of every tile of this block, NS tiles ahead
         if (l32 != 0) return;
+        const unsigned long long pol = l2_evict_first();
         int it = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
             const int st = it % NS;
@@ -173,10 +183,10 @@ __global__ void __launch_bounds__(kStageThreads) k_rowop_staged(int n, int R, co
             meta[st][1] = fits ? 1 : 0;
             const unsigned bytes = (unsigned)nrp * 4u + (fits ? (unsigned)cnt * (unsigned)C::kEntry : 0u);
             mbar_expect_tx(&full[st], bytes);
-            bulk_to_smem(base, row + t0, (unsigned)nrp * 4u, &full[st]);
+            bulk_to_smem(base, row + t0, (unsigned)nrp * 4u, &full[st], pol);
             if (fits && cnt > 0) {
-                bulk_to_smem(base + C::COLS, col + a0, (unsigned)cnt * (unsigned)sizeof(IT), &full[st]);
-                bulk_to_smem(base + C::VALS, val + a0, (unsigned)cnt * (unsigned)sizeof(VT), &full[st]);
+                bulk_to_smem(base + C::COLS, col + a0, (unsigned)cnt * (unsigned)sizeof(IT), &full[st], pol);
+                bulk_to_smem(base + C::VALS, val + a0, (unsigned)cnt * (unsigned)sizeof(VT), &full[st], pol);
             }
         }
         // the copies still in flight land before the block's shared memory is released

@@ -31,7 +31,7 @@ extern "C" {
 #define BCMGX_ERR_UNSUPPORTED (-2)     /* option the reference has but this path does not run  */
 #define BCMGX_ERR_NO_CONVERGENCE (-3)  /* itnlim reached (the reference's SolverOut.retv = -1) */
 #define BCMGX_ERR_CUDA (-4)            /* a CUDA runtime call failed                           */
-#define BCMGX_ERR_TIMEOUT (-5)         /* a bounded device loop hit its iteration limit        */
+#define BCMGX_ERR_TIMEOUT (-5)         /* a bounded device loop or wait hit its limit          */
 #define BCMGX_ERR_OOM (-6)             /* device or host allocation failed                     */
 #define BCMGX_ERR_NOT_SPD (-7)         /* FCG met a non-positive curvature / non-finite value  */
 #define BCMGX_ERR_INTERNAL (-8)

@@ -185,7 +185,7 @@ static bcmgx_hierarchy* setup_one(const bcmgx_csr* A, const bcmgx_params* p, int
         if (force) code = std::atoi(force);
         else if (p->autotune) code = autotune_tpr(V, f32, H->stream);
         else code = default_tpr(V.A.n, V.A.nnz);
-        // negative: the staged kernel with -code threads per row (2, 4 or 8)
+        // negative: the staged kernel with -code threads per row (1, 2, 4 or 8)
         V.A.staged = code < 0;
         V.A.tpr = code < 0 ? -code : code;
         if (V.A.tpr < 1) V.A.tpr = default_tpr(V.A.n, V.A.nnz);

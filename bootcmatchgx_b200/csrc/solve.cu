@@ -156,17 +156,18 @@ static void launch_staged(int n, int64_t nnz, const int* row, const IT* col, con
 
 // The row operation on a level matrix, through its int16 column offsets when it has them, and
 // through the staged kernel when the level's tuning chose it (stage: -1 follows A.staged, 0 / 1
-// force it off / on). The staged kernel exists for 2, 4 and 8 threads per row.
+// force it off / on). The staged kernel exists for 1, 2, 4 and 8 threads per row.
 template <int OP, typename VT, typename XT, typename FT, typename MT, typename YT>
 static void launch_rowop_A(int tpr, const DevCsr& A, const VT* val, const XT* x, const FT* f, const MT* M, YT* y,
     double alpha, double beta, const int* skip, cudaStream_t s, int stage = -1)
 {
     if (A.n <= 0) return;
-    const bool staged = (stage < 0 ? A.staged : stage > 0) && (tpr == 2 || tpr == 4 || tpr == 8) &&
+    const bool staged = (stage < 0 ? A.staged : stage > 0) && (tpr == 1 || tpr == 2 || tpr == 4 || tpr == 8) &&
         aligned16(A.row.p) && aligned16(val) && aligned16(A.dcol.p ? (const void*)A.dcol.p : (const void*)A.col.p);
     if (staged) {
         auto go = [&](auto* colp) {
             switch (tpr) {
+            case 1: launch_staged<1, OP>(A.n, A.nnz, A.row.p, colp, val, x, f, M, y, alpha, beta, skip, s); break;
             case 2: launch_staged<2, OP>(A.n, A.nnz, A.row.p, colp, val, x, f, M, y, alpha, beta, skip, s); break;
             case 4: launch_staged<4, OP>(A.n, A.nnz, A.row.p, colp, val, x, f, M, y, alpha, beta, skip, s); break;
             default: launch_staged<8, OP>(A.n, A.nnz, A.row.p, colp, val, x, f, M, y, alpha, beta, skip, s); break;
@@ -1123,7 +1124,7 @@ void time_block_kernels(bcmgx_hierarchy* H, int K, int reps, double* out)
 
 // Threads-per-row autotuner: for a level with at least kTuneMinRows rows, one l1-Jacobi sweep
 // in the cycle's precision is timed (CUDA events, 3 launches after a warm-up) for every
-// candidate 1..16 of the plain kernel and 2, 4, 8 of the staged one, and the fastest is kept.
+// candidate 1..16 of the plain kernel and 1, 2, 4, 8 of the staged one, and the fastest is kept.
 // The result is a code: the threads per row, negative for the staged kernel (the two kernels
 // sum a row in the same order, so that choice does not change results). Codes are cached per
 // (rows, nnz, precision) for the life of the process, so repeated set-ups of same-shaped
@@ -1146,7 +1147,7 @@ static void tune_cache_load()
     long long z;
     int n, prec, t;
     while (std::fscanf(f, "%d %lld %d %d", &n, &z, &prec, &t) == 4)
-        if (t == 1 || t == 2 || t == 4 || t == 8 || t == 16 || t == 32 || t == -2 || t == -4 || t == -8)
+        if (t == 1 || t == 2 || t == 4 || t == 8 || t == 16 || t == 32 || t == -1 || t == -2 || t == -4 || t == -8)
             g_tune_cache[std::make_tuple(n, (int64_t)z, prec)] = t;
     std::fclose(f);
 }
@@ -1193,8 +1194,8 @@ int autotune_tpr(Level& V, bool f32, cudaStream_t s)
     BCMGX_CUDA(cudaEventCreate(&e1));
     int best = default_tpr(n, A.nnz);
     float best_ms = 1e30f;
-    // candidates: 1..16 threads per row, then the staged kernel with 2, 4 and 8 (coded negative)
-    for (int t : {1, 2, 4, 8, 16, -2, -4, -8}) {
+    // candidates: 1..16 threads per row, then the staged kernel with 1, 2, 4 and 8 (coded negative)
+    for (int t : {1, 2, 4, 8, 16, -1, -2, -4, -8}) {
         const int tp = t < 0 ? -t : t, stage = t < 0 ? 1 : 0;
         auto launch = [&] {
             if (f32)

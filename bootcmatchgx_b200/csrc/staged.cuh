@@ -26,7 +26,7 @@ namespace bcmgx {
 
 constexpr int kStageWarps = 12;                  // consumer warps per block (+1 producer warp)
 constexpr int kStageThreads = (kStageWarps + 1) * 32;
-constexpr int kStageMaxRows = kStageWarps * 16;  // rows per tile at most: one per sub-warp of 2 lanes
+constexpr int kStageMaxRows = kStageWarps * 32;  // rows per tile at most: one per lane (S = 1)
 constexpr int kStageRowSlots = kStageMaxRows + 8;
 
 // Shared-memory budget per value / index type: 4 stages of 18 KB for 6-byte entries (3 blocks

@@ -53,7 +53,7 @@ CASES = [("lap27", (23, 17, 19)), ("lap7", (40, 33, 31)), ("diff", (24, 3)), ("r
 
 
 @pytest.mark.parametrize("prec", ["FP64", "FP32"])
-@pytest.mark.parametrize("S", [2, 4, 8])
+@pytest.mark.parametrize("S", [1, 2, 4, 8])
 @pytest.mark.parametrize("case", CASES)
 def test_staged_solve_bit_identical(bx, cuda, monkeypatch, case, S, prec):
     """Every level on the staged kernel with S threads per row gives the plain kernel's
@@ -100,9 +100,9 @@ def test_staged_hierarchies_in_batch_graph(bx, cuda, monkeypatch):
 
 def test_autotuned_codes_are_reported(bx, cuda):
     """With the autotuner on (the default), every level reports a threads-per-row code of the
-    plain (1..32) or the staged (-2, -4, -8) kernel."""
+    plain (1..32) or the staged (-1, -2, -4, -8) kernel."""
     A = as_csr(bx, ("lap27", (40, 40, 40)))
     h = bx.prec_setup(A.indptr, A.indices, A.data, fcg(bx, vcycle_precision="FP32"))
     for t in h.info()["tpr"]:
-        assert t in (1, 2, 4, 8, 16, 32, -2, -4, -8)
+        assert t in (1, 2, 4, 8, 16, 32, -1, -2, -4, -8)
     h.free()

@@ -28,6 +28,7 @@
 namespace bcmgx {
 
 long long scan_exclusive(const int* in, int* out, long n, bool with_total, cudaStream_t s);
+void scan_exclusive_dev(const int* in, int* out, long n, cudaStream_t s);
 int num_sms();
 
 namespace {
@@ -295,7 +296,7 @@ void afsai_build_dev(bcmgx_hierarchy* H)
     note_launch(); k_count_cols<<<grid_for(G.nnz, 256), 256, 0, s>>>(G.nnz, G.col.p, cnt.p);
     BCMGX_CHECK_LAUNCH();
     T.row.alloc((size_t)n + 1, s);
-    scan_exclusive(cnt.p, T.row.p, n, true, s);
+    scan_exclusive_dev(cnt.p, T.row.p, n, s);
     fill.alloc((size_t)n + 1, s);
     BCMGX_CUDA(cudaMemcpyAsync(fill.p, T.row.p, sizeof(int) * ((size_t)n + 1), cudaMemcpyDeviceToDevice, s));
     T.col.alloc(T.nnz, s);

@@ -38,7 +38,7 @@ constexpr double kCoarseRatioThreshold = 1.2;           // matchingAggregation.c
 
 enum : int {
     ERR_ROW0 = 1, ERR_ROWN = 2, ERR_ROWORDER = 4, ERR_COLRANGE = 8, ERR_COLSORT = 16, ERR_NODIAG = 32,
-    ERR_SUITOR_BUDGET = 64, ERR_ASYM_MATCH = 128, ERR_BADW = 256, ERR_GALERKIN_CAP = 512,
+    ERR_SUITOR_BUDGET = 64, ERR_ASYM_MATCH = 128, ERR_BADW = 256, ERR_GALERKIN_CAP = 512, ERR_GALERKIN_OFS = 1024,
 };
 
 // Optional phase timing of the set-up (environment BCMGX_PROFILE=1): the stream is synchronised
@@ -134,7 +134,8 @@ __global__ void k_scan_tiles(const int* __restrict__ in, long n, long long* tile
     if (threadIdx.x == 0) tile_sums[blockIdx.x] = tot;
 }
 
-__global__ void k_scan_top(long long* tile_sums, int ntiles, long long* total)
+// total: the sum (64-bit); out_total, when given: the sum as the int32 entry after the scan
+__global__ void k_scan_top(long long* tile_sums, int ntiles, long long* total, int* out_total)
 {
     long long carry = 0;
     for (int b0 = 0; b0 < ntiles; b0 += blockDim.x) {
@@ -145,7 +146,10 @@ __global__ void k_scan_top(long long* tile_sums, int ntiles, long long* total)
         if (i < ntiles) tile_sums[i] = carry + ex;
         carry += tot;
     }
-    if (threadIdx.x == 0) *total = carry;
+    if (threadIdx.x == 0) {
+        *total = carry;
+        if (out_total) *out_total = carry <= 0x7fffffffLL ? (int)carry : -1;
+    }
 }
 
 __global__ void k_scan_down(const int* __restrict__ in, int* __restrict__ out, long n, const long long* tile_offs)
@@ -169,27 +173,39 @@ __global__ void k_scan_down(const int* __restrict__ in, int* __restrict__ out, l
 
 // Exclusive prefix sum of in[0..n) into out[0..n); when with_total, out[n] = total.
 // Returns the total (synchronises the stream).
-long long scan_exclusive(const int* in, int* out, long n, bool with_total, cudaStream_t s)
+// Exclusive scan of n ints into out (and the total into out[n] when with_total), on the device;
+// tot receives the 64-bit total.
+static void scan_launch(const int* in, int* out, long n, bool with_total, long long* tot, cudaStream_t s)
 {
     const int ntiles = std::max(1, (int)((n + kScanTile - 1) / kScanTile));
-    DBuf<long long> tiles, tot;
+    DBuf<long long> tiles;
     tiles.alloc(ntiles, s);
-    tot.alloc(1, s);
     if (n > 0) { note_launch(); k_scan_tiles<<<ntiles, kScanThreads, 0, s>>>(in, n, tiles.p); }
     else BCMGX_CUDA(cudaMemsetAsync(tiles.p, 0, sizeof(long long), s));
-    note_launch(); k_scan_top<<<1, 1024, 0, s>>>(tiles.p, ntiles, tot.p);
+    note_launch(); k_scan_top<<<1, 1024, 0, s>>>(tiles.p, ntiles, tot, with_total ? out + n : nullptr);
     if (n > 0) { note_launch(); k_scan_down<<<ntiles, kScanThreads, 0, s>>>(in, out, n, tiles.p); }
     BCMGX_CHECK_LAUNCH();
+}
+
+long long scan_exclusive(const int* in, int* out, long n, bool with_total, cudaStream_t s)
+{
+    DBuf<long long> tot;
+    tot.alloc(1, s);
+    scan_launch(in, out, n, with_total, tot.p, s);
     long long total = 0;
     BCMGX_CUDA(cudaMemcpyAsync(&total, tot.p, sizeof(long long), cudaMemcpyDeviceToHost, s));
     BCMGX_CUDA(cudaStreamSynchronize(s));
     BCMGX_REQUIRE(total <= 0x7fffffffLL, BCMGX_ERR_UNSUPPORTED, "more than 2^31-1 entries (int32 offsets)");
-    if (with_total) {
-        int t32 = (int)total;
-        BCMGX_CUDA(cudaMemcpyAsync(out + n, &t32, sizeof(int), cudaMemcpyHostToDevice, s));
-        BCMGX_CUDA(cudaStreamSynchronize(s));
-    }
     return total;
+}
+
+// The same scan with the total only on the device (out[n]), for callers that know it already or
+// do not need it: no host synchronisation. The total must fit int32 (out[n] = -1 otherwise).
+void scan_exclusive_dev(const int* in, int* out, long n, cudaStream_t s)
+{
+    DBuf<long long> tot;
+    tot.alloc(1, s);
+    scan_launch(in, out, n, true, tot.p, s);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -795,9 +811,9 @@ __global__ void k_make_p(int n, const int* __restrict__ M, const double* __restr
 // rows = long_rows, nc its length), or flagged as an error when long_rows is NULL.
 __global__ void k_galerkin(int nc, const int* __restrict__ rows, const int* __restrict__ fine0, const int* __restrict__ fine1,
     const int* __restrict__ agg, const double* __restrict__ p, const int* __restrict__ Arow, const int* __restrict__ Acol,
-    const double* __restrict__ Aval, const int* __restrict__ off, int* __restrict__ Crow, int* __restrict__ Ccol,
-    double* __restrict__ Cval, int cap, int* __restrict__ long_rows, int* __restrict__ nlong, int* __restrict__ long_max,
-    int* err)
+    const double* __restrict__ Aval, const int* __restrict__ off, long long out_cap, int* __restrict__ Crow,
+    int* __restrict__ Ccol, double* __restrict__ Cval, int cap, int* __restrict__ long_rows, int* __restrict__ nlong,
+    int* __restrict__ long_max, int* err)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int wpb = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -817,6 +833,13 @@ __global__ void k_galerkin(int nc, const int* __restrict__ rows, const int* __re
         const int b0 = Arow[f0], d0 = Arow[f0 + 1] - b0;
         const int b1 = f1 >= 0 ? Arow[f1] : 0, d1 = f1 >= 0 ? Arow[f1 + 1] - b1 : 0;
         const int cnt = d0 + d1;
+        if (off[I] < 0 || (long long)off[I] + cnt > out_cap) {
+            if (lane == 0) {
+                atomicOr(err, ERR_GALERKIN_OFS);
+                Crow[I] = 0;
+            }
+            continue;
+        }
         if (cnt > cap) {
             if (lane == 0) {
                 if (long_rows) {
@@ -1132,6 +1155,7 @@ static std::string err_text(int e)
     if (e & ERR_ASYM_MATCH) s += "matching is not symmetric; ";
     if (e & ERR_BADW) s += "weight vector entry <= DBL_EPSILON; ";
     if (e & ERR_GALERKIN_CAP) s += "Galerkin row exceeds its shared-memory capacity; ";
+    if (e & ERR_GALERKIN_OFS) s += "Galerkin candidates exceed the fine matrix's entries; ";
     return s;
 }
 
@@ -1372,7 +1396,10 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
     off.alloc((size_t)nc + 1, s);
     note_launch(); k_galerkin_counts<<<gs_grid(nc), 256, 0, s>>>(nc, fine0.p, fine1.p, A.row.p, cand.p);
     BCMGX_CHECK_LAUNCH();
-    const long long total = scan_exclusive(cand.p, off.p, nc, true, s);
+    // the candidates of all coarse rows are the entries of A (every fine row is in one aggregate);
+    // k_galerkin checks each row's range against that before writing
+    scan_exclusive_dev(cand.p, off.p, nc, s);
+    const long long total = A.nnz;
     cand.release();
     counts.alloc(std::max(nc, 1), s);
     pcol.alloc(std::max<size_t>((size_t)total, 1), s);
@@ -1393,7 +1420,7 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
         const int g = (int)std::max<long>(1, std::min<long>(((long)nrows + wpb - 1) / wpb, (long)num_sms() * 32));
         note_launch();
         k_galerkin<<<g, wpb * 32, smem, s>>>(nrows, rows, fine0.p, fine1.p, out.agg.p, out.p.p, A.row.p, A.col.p,
-            A.val.p, off.p, counts.p, pcol.p, pval.p, cap, list, stat, stat ? stat + 1 : nullptr, err.p);
+            A.val.p, off.p, (long long)total, counts.p, pcol.p, pval.p, cap, list, stat, stat ? stat + 1 : nullptr, err.p);
         BCMGX_CHECK_LAUNCH();
     };
     auto read2 = [&](const int* d, int (&h)[2]) {
@@ -1523,7 +1550,7 @@ static void build_restriction(Level& V, int nc, bool want_f32, cudaStream_t s)
     note_launch(); k_count<<<gs_grid(n), 256, 0, s>>>(n, V.agg.p, cnt.p);
     BCMGX_CHECK_LAUNCH();
     V.rptr.alloc((size_t)nc + 1, s);
-    scan_exclusive(cnt.p, V.rptr.p, nc, true, s);
+    scan_exclusive_dev(cnt.p, V.rptr.p, nc, s);
     V.ridx.alloc(n, s);
     V.rval.alloc(n, s);
     if (want_f32) {

@@ -1341,10 +1341,18 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
     BCMGX_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), s));
     note_launch(); k_pair_flags<<<gs_grid(n), 256, 0, s>>>(n, M.p, w, fm.p, fs.p, err.p);
     BCMGX_CHECK_LAUNCH();
-    const long long npairs = scan_exclusive(fm.p, pofs.p, n, false, s);
-    const long long nsing = scan_exclusive(fs.p, sofs.p, n, false, s);
-    int e = read_err(err.p, s);
+    // both scans, then their totals and the error word in one round trip
+    DBuf<long long> tots;
+    tots.alloc(2, s);
+    scan_launch(fm.p, pofs.p, n, false, tots.p, s);
+    scan_launch(fs.p, sofs.p, n, false, tots.p + 1, s);
+    long long th[2] = { 0, 0 };
+    int e = 0;
+    BCMGX_CUDA(cudaMemcpyAsync(th, tots.p, 2 * sizeof(long long), cudaMemcpyDeviceToHost, s));
+    BCMGX_CUDA(cudaMemcpyAsync(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    BCMGX_CUDA(cudaStreamSynchronize(s));
     if (e) throw Error(BCMGX_ERR_INTERNAL, "aggregation: " + err_text(e));
+    const long long npairs = th[0], nsing = th[1];
     const int nc = (int)(npairs + nsing);
     out.nc = nc;
     DBuf<int> fine0, fine1;
@@ -1480,13 +1488,21 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
             }
         }
     }
-    C.nnz = scan_exclusive(counts.p, C.row.p, nc, true, s);
+    // row offsets of C; their total and the error word in one round trip
+    DBuf<long long> ctot;
+    ctot.alloc(1, s);
+    scan_launch(counts.p, C.row.p, nc, true, ctot.p, s);
+    long long cnnz = 0;
+    BCMGX_CUDA(cudaMemcpyAsync(&cnnz, ctot.p, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    BCMGX_CUDA(cudaMemcpyAsync(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    BCMGX_CUDA(cudaStreamSynchronize(s));
+    if (e) throw Error(BCMGX_ERR_INTERNAL, "galerkin: " + err_text(e));
+    BCMGX_REQUIRE(cnnz <= 0x7fffffffLL, BCMGX_ERR_UNSUPPORTED, "more than 2^31-1 entries (int32 offsets)");
+    C.nnz = cnnz;
     C.col.alloc(std::max<int64_t>(C.nnz, 1), s);
     C.val.alloc(std::max<int64_t>(C.nnz, 1), s);
     note_launch(); k_compact_rows<<<warp_grid(nc), 256, 0, s>>>(nc, off.p, C.row.p, pcol.p, pval.p, C.col.p, C.val.p);
     BCMGX_CHECK_LAUNCH();
-    e = read_err(err.p, s);
-    if (e) throw Error(BCMGX_ERR_INTERNAL, "galerkin: " + err_text(e));
     C.max_row = row_max(C, s);
 }
 

@@ -303,7 +303,9 @@ struct FusedWeights {
     const double* C = nullptr;
     double zero_sub = 0.0;
 };
+// err_out: when given, the matching's error bits go to that device word and are not read back
+// here (the caller reads them with its next round trip); otherwise they are checked on return.
 void suitor_dev(int n, int64_t nnz, const int* row, const int* col, const double* W, const int* tpos, int* M, int max_row,
-    cudaStream_t s, const FusedWeights* fw = nullptr);
+    cudaStream_t s, const FusedWeights* fw = nullptr, int* err_out = nullptr);
 
 }  // namespace bcmgx

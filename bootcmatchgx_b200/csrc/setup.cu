@@ -1236,7 +1236,7 @@ void tpos_dev(int n, int64_t nnz, const int* row, const int* col, int* tpos, cud
 }
 
 void suitor_dev(int n, int64_t nnz, const int* row, const int* col, const double* W, const int* tpos, int* M, int max_row,
-    cudaStream_t s, const FusedWeights* fw)
+    cudaStream_t s, const FusedWeights* fw, int* err_out)
 {
     if (max_row <= 0) max_row = row_max_raw(n, row, s);
     if (fw && max_row > 32) throw Error(BCMGX_ERR_INTERNAL, "weights formed in the rank kernel need rows of <= 32 entries");
@@ -1249,8 +1249,11 @@ void suitor_dev(int n, int64_t nnz, const int* row, const int* col, const double
     rank.alloc(z, s);
     ordj.alloc(z, s);
     degE.alloc(n, s);
-    err.alloc(1, s);
-    BCMGX_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), s));
+    if (!err_out) {
+        err.alloc(1, s);
+        BCMGX_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), s));
+    }
+    int* errp = err_out ? err_out : err.p;
     if (wide) {
         offer_w.alloc(n, s);
         BCMGX_CUDA(cudaMemsetAsync(offer_w.p, 0, sizeof(unsigned long long) * n, s));
@@ -1277,14 +1280,15 @@ void suitor_dev(int n, int64_t nnz, const int* row, const int* col, const double
     }
     const long long budget = (long long)nnz + n + 1024;
     if (wide) {
-        note_launch(); k_suitor_w<<<ceil_div(n, 128), 128, 0, s>>>(n, rinfo.p, pref.p, offer_w.p, budget, err.p, asc ? 0 : 1);
+        note_launch(); k_suitor_w<<<ceil_div(n, 128), 128, 0, s>>>(n, rinfo.p, pref.p, offer_w.p, budget, errp, asc ? 0 : 1);
         note_launch(); k_suitor_result_w<<<gs_grid(n), 256, 0, s>>>(n, offer_w.p, M);
     } else {
-        note_launch(); k_suitor<<<ceil_div(n, 128), 128, 0, s>>>(n, rinfo.p, pref.p, offer.p, budget, err.p, asc ? 0 : 1);
+        note_launch(); k_suitor<<<ceil_div(n, 128), 128, 0, s>>>(n, rinfo.p, pref.p, offer.p, budget, errp, asc ? 0 : 1);
         note_launch(); k_suitor_result<<<gs_grid(n), 256, 0, s>>>(n, rinfo.p, pref.p, offer.p, M);
     }
-    note_launch(); k_check_symmetric<<<gs_grid(n), 256, 0, s>>>(n, M, err.p);
+    note_launch(); k_check_symmetric<<<gs_grid(n), 256, 0, s>>>(n, M, errp);
     BCMGX_CHECK_LAUNCH();
+    if (err_out) return;
     int e = read_err(err.p, s);
     if (e) throw Error(e & ERR_SUITOR_BUDGET ? BCMGX_ERR_TIMEOUT : BCMGX_ERR_INTERNAL, "suitor matching: " + err_text(e));
 }
@@ -1306,6 +1310,9 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
     DBuf<int> tpos, M, fm, fs, pofs, sofs, err;
     tpos.alloc(std::max<int64_t>(nnz, 1), s);
     M.alloc(n, s);
+    // one error word for the matching and the aggregation, read with the pair / singleton totals
+    err.alloc(1, s);
+    BCMGX_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), s));
     const int amax0 = A.max_row > 0 ? A.max_row : row_max(A, s);
     if (amax0 <= 32) {
         // rows of at most 32 entries: the rank kernel forms the edge weights itself
@@ -1319,7 +1326,7 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
         fw.w = w;
         fw.C = Cd.p;
         PhaseTimer pt(H, "suitor");
-        suitor_dev(n, nnz, A.row.p, A.col.p, nullptr, tpos.p, M.p, amax0, s, &fw);
+        suitor_dev(n, nnz, A.row.p, A.col.p, nullptr, tpos.p, M.p, amax0, s, &fw, err.p);
     } else {
         W.alloc(std::max<int64_t>(nnz, 1), s);
         {
@@ -1327,7 +1334,7 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
             edge_weights_dev(n, nnz, A.row.p, A.col.p, A.val.p, w, W.p, tpos.p, nullptr, s);
         }
         PhaseTimer pt(H, "suitor");
-        suitor_dev(n, nnz, A.row.p, A.col.p, W.p, tpos.p, M.p, amax0, s);
+        suitor_dev(n, nnz, A.row.p, A.col.p, W.p, tpos.p, M.p, amax0, s, nullptr, err.p);
     }
     PhaseTimer pt_p(H, "makeP+galerkin");
     W.release();
@@ -1337,8 +1344,6 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
     fs.alloc(n, s);
     pofs.alloc(n, s);
     sofs.alloc(n, s);
-    err.alloc(1, s);
-    BCMGX_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), s));
     note_launch(); k_pair_flags<<<gs_grid(n), 256, 0, s>>>(n, M.p, w, fm.p, fs.p, err.p);
     BCMGX_CHECK_LAUNCH();
     // both scans, then their totals and the error word in one round trip
@@ -1351,7 +1356,7 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
     BCMGX_CUDA(cudaMemcpyAsync(th, tots.p, 2 * sizeof(long long), cudaMemcpyDeviceToHost, s));
     BCMGX_CUDA(cudaMemcpyAsync(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     BCMGX_CUDA(cudaStreamSynchronize(s));
-    if (e) throw Error(BCMGX_ERR_INTERNAL, "aggregation: " + err_text(e));
+    if (e) throw Error(e & ERR_SUITOR_BUDGET ? BCMGX_ERR_TIMEOUT : BCMGX_ERR_INTERNAL, "aggregation: " + err_text(e));
     const long long npairs = th[0], nsing = th[1];
     const int nc = (int)(npairs + nsing);
     out.nc = nc;
@@ -1488,13 +1493,22 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
             }
         }
     }
-    // row offsets of C; their total and the error word in one round trip
+    // row offsets of C; their total, the longest row and the error word in one round trip
     DBuf<long long> ctot;
+    DBuf<int> cmx;
     ctot.alloc(1, s);
+    cmx.alloc(1, s);
+    BCMGX_CUDA(cudaMemsetAsync(cmx.p, 0, sizeof(int), s));
     scan_launch(counts.p, C.row.p, nc, true, ctot.p, s);
+    if (nc > 0) {
+        note_launch(); k_row_max<<<gs_grid(nc), 256, 0, s>>>(nc, C.row.p, cmx.p);
+        BCMGX_CHECK_LAUNCH();
+    }
     long long cnnz = 0;
+    int cmax = 0;
     BCMGX_CUDA(cudaMemcpyAsync(&cnnz, ctot.p, sizeof(long long), cudaMemcpyDeviceToHost, s));
     BCMGX_CUDA(cudaMemcpyAsync(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    BCMGX_CUDA(cudaMemcpyAsync(&cmax, cmx.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     BCMGX_CUDA(cudaStreamSynchronize(s));
     if (e) throw Error(BCMGX_ERR_INTERNAL, "galerkin: " + err_text(e));
     BCMGX_REQUIRE(cnnz <= 0x7fffffffLL, BCMGX_ERR_UNSUPPORTED, "more than 2^31-1 entries (int32 offsets)");
@@ -1503,7 +1517,7 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
     C.val.alloc(std::max<int64_t>(C.nnz, 1), s);
     note_launch(); k_compact_rows<<<warp_grid(nc), 256, 0, s>>>(nc, off.p, C.row.p, pcol.p, pval.p, C.col.p, C.val.p);
     BCMGX_CHECK_LAUNCH();
-    C.max_row = row_max(C, s);
+    C.max_row = cmax;
 }
 
 // Largest |col - row| of the matrix (atomicMax of per-thread maxima).

@@ -103,7 +103,8 @@ static void launch_rowop(int tpr, int n, const int* row, const IT* col, const VT
 
 // Fault word of the staged row kernels, in mapped pinned host memory: nonzero when one of their
 // waits on a shared-memory stage gave up. The entry points read it after their final stream
-// synchronisation (stage_fault_check), so the check costs no copy.
+// synchronisation (stage_fault_check), so the check costs no copy. It is one word for the
+// process: with solves on several threads, the entry point that reads it first reports it.
 static int* g_stage_fault = nullptr;
 static std::once_flag g_stage_fault_once;
 

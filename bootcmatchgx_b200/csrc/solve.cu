@@ -101,6 +101,31 @@ static void launch_rowop(int tpr, int n, const int* row, const IT* col, const VT
     BCMGX_CHECK_LAUNCH();
 }
 
+// Deterministic values in [0.5, 1.5) for the vectors the timing hooks and the autotuner run the
+// kernels on: a zero vector makes every sweep divide a zero residual, and FP32 division leaves
+// its fast path for a zero numerator, so zero vectors time a case the solve does not see.
+template <typename T>
+__global__ void k_fill_probe(long n, T* __restrict__ a, unsigned salt)
+{
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        unsigned h = (unsigned)i * 0x9E3779B1u ^ salt;
+        h ^= h >> 15;
+        h *= 0x85EBCA77u;
+        h ^= h >> 13;
+        a[i] = (T)(0.5 + (double)(h & 0xFFFFFFu) / 16777216.0);
+    }
+}
+
+template <typename T>
+static void fill_probe(T* a, long n, unsigned salt, cudaStream_t s)
+{
+    if (n <= 0) return;
+    auto k = k_fill_probe<T>;
+    note_launch();
+    k<<<fit_grid(k, 256, (n + 255) / 256), 256, 0, s>>>(n, a, salt);
+    BCMGX_CHECK_LAUNCH();
+}
+
 // Fault word of the staged row kernels, in mapped pinned host memory: nonzero when one of their
 // waits on a shared-memory stage gave up. The entry points read it after their final stream
 // synchronisation (stage_fault_check), so the check costs no copy. It is one word for the
@@ -1022,14 +1047,14 @@ void time_level_kernels(bcmgx_hierarchy* H, int l, int reps, double* out)
     a.alloc(n, s);
     b.alloc(n, s);
     c.alloc(n, s);
-    BCMGX_CUDA(cudaMemsetAsync(a.p, 0, sizeof(double) * n, s));
-    BCMGX_CUDA(cudaMemsetAsync(c.p, 0, sizeof(double) * n, s));
+    fill_probe(a.p, n, 1u, s);
+    fill_probe(c.p, n, 2u, s);
     if (f32) {
         a32.alloc(n, s);
         b32.alloc(n, s);
         c32.alloc(n, s);
-        BCMGX_CUDA(cudaMemsetAsync(a32.p, 0, sizeof(float) * n, s));
-        BCMGX_CUDA(cudaMemsetAsync(c32.p, 0, sizeof(float) * n, s));
+        fill_probe(a32.p, n, 1u, s);
+        fill_probe(c32.p, n, 2u, s);
     }
     cudaEvent_t e0, e1;
     BCMGX_CUDA(cudaEventCreate(&e0));
@@ -1081,7 +1106,7 @@ void time_block_kernels(bcmgx_hierarchy* H, int K, int reps, double* out)
     DBuf<double> x, f, y;
     x.alloc(nk, s);
     y.alloc(nk, s);
-    BCMGX_CUDA(cudaMemsetAsync(x.p, 0, sizeof(double) * nk, s));
+    fill_probe(x.p, (long)nk, 1u, s);
     cudaEvent_t e0, e1;
     BCMGX_CUDA(cudaEventCreate(&e0));
     BCMGX_CUDA(cudaEventCreate(&e1));
@@ -1100,8 +1125,8 @@ void time_block_kernels(bcmgx_hierarchy* H, int K, int reps, double* out)
         x32.alloc(nk, s);
         f32b.alloc(nk, s);
         y32.alloc(nk, s);
-        BCMGX_CUDA(cudaMemsetAsync(x32.p, 0, sizeof(float) * nk, s));
-        BCMGX_CUDA(cudaMemsetAsync(f32b.p, 0, sizeof(float) * nk, s));
+        fill_probe(x32.p, (long)nk, 1u, s);
+        fill_probe(f32b.p, (long)nk, 2u, s);
         out[0] = timeit([&] { launch_blk_rowop<OP_JACOBI>(A.n, A.m, kp, kp, A.row.p, A.col.p, A.val32.p,
                                   (const float*)x32.p, (const float*)f32b.p, V.M32.p, y32.p, 1.0, 0.0, nullptr, s); });
         out[1] = timeit([&] { launch_blk_rowop<OP_RESID>(A.n, A.m, kp, kp, A.row.p, A.col.p, A.val32.p,
@@ -1109,7 +1134,7 @@ void time_block_kernels(bcmgx_hierarchy* H, int K, int reps, double* out)
         BCMGX_CUDA(cudaStreamSynchronize(s));
     } else {
         f.alloc(nk, s);
-        BCMGX_CUDA(cudaMemsetAsync(f.p, 0, sizeof(double) * nk, s));
+        fill_probe(f.p, (long)nk, 2u, s);
         out[0] = timeit([&] { launch_blk_rowop<OP_JACOBI>(A.n, A.m, kp, kp, A.row.p, A.col.p, A.val.p,
                                   (const double*)x.p, (const double*)f.p, V.M.p, y.p, 1.0, 0.0, nullptr, s); });
         out[1] = timeit([&] { launch_blk_rowop<OP_RESID>(A.n, A.m, kp, kp, A.row.p, A.col.p, A.val.p,
@@ -1181,14 +1206,14 @@ int autotune_tpr(Level& V, bool f32, cudaStream_t s)
         a32.alloc(n, s);
         b32.alloc(n, s);
         c32.alloc(n, s);
-        BCMGX_CUDA(cudaMemsetAsync(a32.p, 0, sizeof(float) * n, s));
-        BCMGX_CUDA(cudaMemsetAsync(c32.p, 0, sizeof(float) * n, s));
+        fill_probe(a32.p, n, 1u, s);
+        fill_probe(c32.p, n, 2u, s);
     } else {
         a.alloc(n, s);
         b.alloc(n, s);
         c.alloc(n, s);
-        BCMGX_CUDA(cudaMemsetAsync(a.p, 0, sizeof(double) * n, s));
-        BCMGX_CUDA(cudaMemsetAsync(c.p, 0, sizeof(double) * n, s));
+        fill_probe(a.p, n, 1u, s);
+        fill_probe(c.p, n, 2u, s);
     }
     cudaEvent_t e0, e1;
     BCMGX_CUDA(cudaEventCreate(&e0));

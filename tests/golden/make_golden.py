@@ -7,7 +7,11 @@ GPU box never runs this. It packs, without modification:
     BCMGX/launchAndCompare.mk:320-330), in the reference's rank-block-major row order;
   * BCMGX/src/test/data/mtx/lap3d_*.mtx (Matlab-generated Laplacians used by
     BCMGX/testGenerators.mk) as COO triplets;
-  * BCMGX/src/test/data/settings/{FCG_BCMG,FCG_BCMG.prova,sample}.properties as text.
+  * BCMGX/src/test/data/settings/{FCG_BCMG,FCG_BCMG.prova,sample}.properties as text;
+  * BCMGX/src/test/data/mtx/bcsstk09.mtx as text (the --matrix input of driverSolve, read by the
+    library's own MatrixMarket reader in the tests) and cmp/bcsstk09_sol.txt (its FCG+BCMG solution
+    of A x = 1, BCMGX/launchAndCompare.mk:136,207). The bcsstk13 / bcsstk24 solution files are all
+    zeros (their _aux.txt: FLAG = 1, ITER = 0) and pin nothing, so they are not packed.
 
 Usage: python tests/golden/make_golden.py [REFERENCE_ROOT]
 """
@@ -46,6 +50,9 @@ def main():
     for f in ("FCG_BCMG.properties", "FCG_BCMG.prova.properties", "sample.properties"):
         with open(os.path.join(DATA, "settings", f)) as fh:
             out["prop__" + f] = np.array(fh.read())
+    with open(os.path.join(DATA, "mtx", "bcsstk09.mtx")) as fh:
+        out["mtxtext__bcsstk09"] = np.array(fh.read())
+    out["sol__bcsstk09_sol"] = np.loadtxt(os.path.join(DATA, "cmp", "bcsstk09_sol.txt"))
     np.savez_compressed(OUT, **out)
     print("wrote", OUT, len(out), "arrays")
 

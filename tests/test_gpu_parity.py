@@ -102,6 +102,24 @@ def test_golden_solutions(bx, cuda, golden, st, PQR):
     assert np.linalg.norm(x - g) / np.linalg.norm(g) < 1e-5
 
 
+def test_bcsstk09_golden(bx, oracle, cuda, golden, tmp_path):
+    """bcsstk09 read by the library's MatrixMarket reader and solved on the GPU (A x = 1, FCG+BCMG)
+    reproduces BCMGX/src/test/data/cmp/bcsstk09_sol.txt within compareSolutions' 1e-5, in the
+    oracle's iterations (+-1)."""
+    path = tmp_path / "bcsstk09.mtx"
+    path.write_text(str(golden["mtxtext__bcsstk09"]))
+    row, col, val = bx.read_matrix_market(path)
+    n = row.size - 1
+    h = bx.prec_setup(row, col, val, fcg(bx))
+    x, info = h.solve(np.ones(n))
+    g = golden["sol__bcsstk09_sol"]
+    assert info["status"] == 0 and info["retv"] == 0
+    assert np.linalg.norm(x - g) / np.linalg.norm(g) < 1e-5
+    Ho = oracle.Hierarchy(oracle.Matrix.from_csr(row, col, val), oracle.params())
+    _, io = Ho.solve(np.ones(n))
+    assert abs(info["niter"] - io["niter"]) <= 1
+
+
 @pytest.mark.parametrize("tpr", [1, 2, 4, 8, 16, 32])
 @pytest.mark.parametrize("case", [("lap27", (12, 11, 10)), ("rand", (3000, 0.004, 1, True)), ("lap7", (1, 1, 1))])
 def test_spmv(bx, cuda, tpr, case):

@@ -114,3 +114,23 @@ def test_oracle_krylov_solvers(oracle, solver, s, pre):
                                                                                     preconditioner=pre))
         _, fi = Hf.solve(b)
         assert abs(fi["niter"] - info["niter"]) <= 1
+
+
+def test_bcsstk09_golden(oracle, golden, bx, tmp_path):
+    """The --matrix path of driverSolve on bcsstk09 (BCMGX/launchAndCompare.mk:136,207): the
+    library's MatrixMarket reader expands the symmetric file exactly as scipy does, and FCG+BCMG
+    on A x = 1 reproduces BCMGX/src/test/data/cmp/bcsstk09_sol.txt within compareSolutions' 1e-5."""
+    import scipy.io
+    path = tmp_path / "bcsstk09.mtx"
+    path.write_text(str(golden["mtxtext__bcsstk09"]))
+    row, col, val = bx.read_matrix_market(path)
+    n = row.size - 1
+    ref = scipy.io.mmread(str(path)).tocsr()
+    ref.sort_indices()
+    assert ref.shape == (n, n)
+    assert np.array_equal(row, ref.indptr) and np.array_equal(col, ref.indices) and np.array_equal(val, ref.data)
+    H = oracle.Hierarchy(oracle.Matrix.from_csr(row, col, val), oracle.params())
+    x, info = H.solve(np.ones(n))
+    g = golden["sol__bcsstk09_sol"]
+    assert info["retv"] == 0
+    assert np.linalg.norm(x - g) / np.linalg.norm(g) < 1e-5

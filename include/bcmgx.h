@@ -189,7 +189,9 @@ int bcmgx_prec_apply(bcmgx_hierarchy* h, const double* r, double* v, int on_devi
 /* Average device time (ms, CUDA events on the hierarchy's stream, `reps` launches after one
  * warm-up) of level `level`'s solve kernels: out[0] one l1-Jacobi sweep in the cycle's
  * precision, out[1] the residual, out[2] the FP64 SpMV, out[3] the fused FCG SpMV + dots
- * (level 0 only). No counterpart in the reference: the measurement hook of the benchmarks. */
+ * (level 0 only). The kernels run on fixed non-constant vectors (values in [0.5, 1.5)), as in a
+ * solve: on zero vectors every sweep divides zero residuals, which times slower. No counterpart
+ * in the reference: the measurement hook of the benchmarks. */
 int bcmgx_time_kernels(bcmgx_hierarchy* h, int level, int reps, double* out_ms);
 /* The same for the level-0 block kernels of a solve with nrhs (1..32) right-hand sides (blocks of
  * nrhs rounded up to a power of two columns): out[0] one block l1-Jacobi sweep in the cycle's

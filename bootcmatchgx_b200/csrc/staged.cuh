@@ -42,6 +42,9 @@ struct StageCfg {
     static constexpr int STAGE = VALS + CAP * (int)sizeof(VT);
     static constexpr int SMEM = NS * STAGE;
     static_assert(COLS % 16 == 0 && VALS % 16 == 0 && STAGE % 16 == 0, "stage layout must keep 16-byte granules");
+    static_assert(SMEM <= 227 * 1024, "the stage ring must fit a block's shared memory");
+    static_assert(CAP >= 64 * 8, "a stage must hold a useful tile");
+    static_assert((kStageMaxRows + 4) <= kStageRowSlots, "a tile's widened row offsets must fit their slots");
 };
 
 // Rows per tile for a matrix of n rows and nnz entries and S threads per row: the largest multiple

@@ -11,15 +11,23 @@ roofline figures, the end-to-end time through the C ABI with host buffers, and a
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
 Multi-GPU (torchrun, one process per GPU): each rank solves its own copy of the system
-(independent replicas, no collective on the data path); time = max over ranks.
+(independent replicas, no collective on the data path); time = max over ranks. The batched
+forms shard instead: rank r takes systems r, r + N, ... of the 256 (--batch) and a contiguous
+slice of the 32 right-hand-side columns (--multi).
 --impl reference times the reference algorithm's CPU restatement (oracle/, OpenMP) on rank 0.
 """
 from __future__ import annotations
 
+import os
+
+# OpenMP threads of the CPU legs (the oracle) pinned one per core; set before any OpenMP runtime
+# is loaded, since libgomp reads them once.
+os.environ.setdefault("OMP_PROC_BIND", "close")
+os.environ.setdefault("OMP_PLACES", "cores")
+
 import argparse
 import datetime
 import json
-import os
 import statistics
 import subprocess
 import sys
@@ -130,66 +138,132 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------------------------
-def cpu_baseline(wl, row, col, val, b, xs, max_seconds=30.0):
-    """The oracle (OpenMP C++ restatement of the same FCG+BCMG method) on this host: full
-    set-up, then FCG iterations until convergence or until the time budget; the solve time is
-    scaled to the iteration count of a converged run when the budget cuts it short."""
+def host_info():
+    """CPU model and CPU counts of this host (/proc/cpuinfo; lscpu need not be installed)."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        avail = len(os.sched_getaffinity(0))
+    except Exception:
+        avail = os.cpu_count() or 1
+    return {"cpu_model": model, "logical_cpus": os.cpu_count(), "cpus_available": avail,
+            "omp_proc_bind": os.environ.get("OMP_PROC_BIND"), "omp_places": os.environ.get("OMP_PLACES")}
+
+
+def diffusion_csr_numpy(nx, ny, nz, kappa):
+    """The 7-point FV diffusion matrix in numpy, with bcmgx_diffusion_7p's arithmetic and order
+    (cells x fastest, columns ascending, the diagonal summed over the faces -z, -y, -x, +x, +y,
+    +z): the reference arm builds its matrix without the product library."""
+    N = nx * ny * nz
+    r = np.arange(N)
+    gi, gj, gk = r % nx, (r // nx) % ny, r // (nx * ny)
+    k = np.asarray(kappa, dtype=np.float64).reshape(-1)
+    faces = [(0, 0, -1), (0, -1, 0), (-1, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1)]
+    cols = np.full((N, 7), -1, np.int64)
+    vals = np.zeros((N, 7))
+    diag = np.zeros(N)
+    for t, (dx, dy, dz) in enumerate(faces):
+        slot = t if t < 3 else t + 1
+        a, b_, c = gi + dx, gj + dy, gk + dz
+        inside = (a >= 0) & (a < nx) & (b_ >= 0) & (b_ < ny) & (c >= 0) & (c < nz)
+        j = np.where(inside, a + nx * (b_ + ny * c), 0)
+        kj = k[j]
+        tij = 2.0 * k * kj / (k + kj)
+        diag = diag + np.where(inside, tij, 2.0 * k)
+        cols[inside, slot] = j[inside]
+        vals[inside, slot] = -tij[inside]
+    cols[:, 3] = r
+    vals[:, 3] = diag
+    keep = cols >= 0
+    row = np.zeros(N + 1, np.int32)
+    row[1:] = np.cumsum(keep.sum(axis=1))
+    return row, cols[keep].astype(np.int32), vals[keep]
+
+
+def oracle_problem(wl):
+    """The workload built without the product library: the Laplacians by the oracle's generator
+    (the reference's row order) with b = A x* by the oracle's SpMV; the diffusion matrix by
+    diffusion_csr_numpy. Returns (oracle matrix, x* or None, b)."""
     from oracle import pyoracle as O
-    cores = os.cpu_count() or 1
-    O.num_threads(cores)
-    A = O.Matrix.from_csr(row, col, val)
+    if wl.get("kind") == "diffusion":
+        from bootcmatchgx_b200 import problems   # numpy only: loads no shared library
+        g = wl["grid"]
+        theta = problems.gaussian_random_field(g, length=8.0, sigma=2.0, seed=wl["theta_seed"])
+        row, col, val = diffusion_csr_numpy(*g, np.exp(theta).reshape(-1, order="F"))
+        b = np.random.default_rng(wl["rhs_seed"]).uniform(0.0, 1.0, row.size - 1)
+        return O.Matrix.from_csr(row, col, val), None, b
+    A = O.Matrix.lap3d(wl["stencil"], *wl["grid"])
+    n = A.info()[0]
+    xs = np.random.default_rng(wl["seed"]).uniform(-1.0, 1.0, n)
+    return A, xs, A.spmv(xs)
+
+
+def oracle_solve(O, A, b, rtol=RTOL):
+    """One full set-up + FCG solve by the oracle; returns (set-up s, solve s, x, info, levels)."""
     t0 = time.perf_counter()
-    H = O.Hierarchy(A, O.params(rtol=RTOL))
-    t_setup = time.perf_counter() - t0
-    t0 = time.perf_counter()
+    H = O.Hierarchy(A, O.params(rtol=rtol))
+    t1 = time.perf_counter()
     x, info = H.solve(b)
-    t_solve = time.perf_counter() - t0
-    return {"value": t_setup + t_solve, "unit": "s", "cores": cores, "kind": "port",
-            "sample": f"full set-up + full FCG solve ({info['niter']} iterations) of the same "
-                      f"workload with oracle/bcmgx_oracle.cpp, OMP threads={cores}",
-            "setup_s": t_setup, "solve_s": t_solve, "niter": info["niter"],
+    t2 = time.perf_counter()
+    return t1 - t0, t2 - t1, x, info, H.level_sizes()
+
+
+def cpu_baseline(wl, runs=5):
+    """The oracle (OpenMP C++ restatement of the same FCG+BCMG method) on this host's cores,
+    threads pinned one per core: `runs` full set-up + solve runs of the same workload, the
+    median reported. Also returns the oracle's solution and level sizes for the parity check."""
+    from oracle import pyoracle as O
+    hi = host_info()
+    cores = hi["cpus_available"]
+    O.num_threads(cores)
+    A, xs, b = oracle_problem(wl)
+    runs_out = [oracle_solve(O, A, b) for _ in range(runs)]
+    tot = [r[0] + r[1] for r in runs_out]
+    med = sorted(range(runs), key=lambda i: tot[i])[runs // 2]
+    ts, tv, x, info, levels = runs_out[med]
+    line = {"value": tot[med], "unit": "s", "cores": cores, "kind": "port",
+            "sample": f"median of {runs} full set-up + full FCG solve runs ({info['niter']} iterations) of "
+                      f"the same workload with oracle/bcmgx_oracle.cpp, OMP threads={cores} pinned one per core",
+            "runs_s": tot, "setup_s": ts, "solve_s": tv, "niter": info["niter"], "host": hi,
             "err_vs_xstar": None if xs is None else float(np.linalg.norm(x - xs) / np.linalg.norm(xs))}
+    return line, {"x": x, "niter": info["niter"], "levels": levels}
 
 
 def reference_arm(a, wl, rank, world):
     """--impl reference: the reference algorithm on the host cores (the reference itself has no
-    CPU implementation and its CUDA build needs MPI; the oracle port stands in)."""
+    CPU implementation, and its CUDA build needs MPI; the oracle port stands in). Every step,
+    warm-ups included, is one full set-up + FCG solve to 1e-8; nothing is extrapolated. The
+    problem is built by the oracle's own generator, so this arm loads no product code."""
     if rank != 0:
         return None
     from oracle import pyoracle as O
-    row, col, val, xs, b = build_problem(wl)
-    cores = os.cpu_count() or 1
+    hi = host_info()
+    cores = hi["cpus_available"]
     O.num_threads(cores)
-    A = O.Matrix.from_csr(row, col, val)
+    A, xs, b = oracle_problem(wl)
+    n, _, nnz = A.info()
     times, niter = [], None
-    budget = 240.0
-    t_start = time.perf_counter()
     for step in range(a.warmup + a.steps):
-        full = step == 0 or (time.perf_counter() - t_start) < budget / 2
-        t0 = time.perf_counter()
-        H = O.Hierarchy(A, O.params(rtol=RTOL, itnlim=2000 if (full or niter is None) else 3))
-        t1 = time.perf_counter()
-        x, info = H.solve(b)
-        t2 = time.perf_counter()
-        if info["retv"] == 0:
-            niter = info["niter"]
-            total = t2 - t0
-        else:   # bounded sample: set-up + 3 iterations, solve scaled to the converged count
-            total = (t1 - t0) + (t2 - t1) / info["niter"] * niter
+        ts, tv, x, info, _ = oracle_solve(O, A, b)
+        niter = info["niter"]
         if step >= a.warmup:
-            times.append(total)
-        del H
+            times.append(ts + tv)
     v = float(np.mean(times))
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": a.gpus,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": a.workload, "problem": wl["text"], "rtol": RTOL,
-                       "rows": int(row.size - 1), "nnz": int(col.size)},
-            "cpu_baseline": {"value": v, "unit": "s", "cores": cores, "kind": "port",
-                             "sample": "oracle/bcmgx_oracle.cpp (OpenMP restatement of FCG+BCMG): "
-                                       "set-up + FCG to 1e-8 per step; when the time budget is "
-                                       "spent a step is set-up + 3 iterations scaled to the "
-                                       f"converged count ({niter})"},
+            "config": {"workload": a.workload, "problem": wl["text"], "rtol": RTOL, "rows": int(n), "nnz": int(nnz)},
+            "median_s": float(np.median(times)), "niter": niter,
+            "cpu_baseline": {"value": v, "unit": "s", "cores": cores, "kind": "port", "host": hi,
+                             "sample": "oracle/bcmgx_oracle.cpp (OpenMP restatement of FCG+BCMG, threads pinned one "
+                                       f"per core): every step a full set-up + FCG solve to 1e-8 ({niter} iterations)"},
             "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     return line
 
@@ -304,8 +378,18 @@ def run_ours(a, wl, rank, world, local_rank):
         launches = (bx.lib().bcmgx_launch_count() - c0) / steps
         return ms, infos, launches
 
+    # ---- cold first calls: the first set-up of each form in this process runs the threads-per-row
+    # autotuner (its choices are then cached per matrix shape) and loads the kernels
+    cold = {}
+    for prec in ("FP32", "FP64"):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, info0, inf0 = step(prec)
+        torch.cuda.synchronize()
+        cold[prec.lower()] = {"setup_ms": inf0["setup_ms"], "solve_ms": info0["solve_ms"],
+                              "wall_ms": (time.perf_counter() - t0) * 1e3}
     # ---- headline: FP32 V-cycle inside FP64 FCG
-    for _ in range(a.warmup):
+    for _ in range(max(0, a.warmup - 1)):
         step("FP32")
     clocks = ClockSampler(local_rank)
     clocks.start()
@@ -314,7 +398,7 @@ def run_ours(a, wl, rank, world, local_rank):
     x32 = d_x.cpu().numpy().copy()
     # ---- plain FP64 form (same step, FP64 V-cycle)
     k64 = max(1, min(a.steps, 3))
-    for _ in range(a.warmup):
+    for _ in range(max(0, a.warmup - 1)):
         step("FP64")
     ms64, infos64, _ = timed("FP64", k64)
     x64 = d_x.cpu().numpy().copy()
@@ -376,7 +460,7 @@ def run_ours(a, wl, rank, world, local_rank):
     e2e_ms = max_over_ranks(max(e0.elapsed_time(e1) / ke, wall * 1e3), world, dev)
 
     if rank != 0:
-        return None
+        return None, None
     setup32 = float(np.mean([i[1]["setup_ms"] for i in infos32]))
     solve32 = float(np.mean([i[0]["solve_ms"] for i in infos32]))
     setup64 = float(np.mean([i[1]["setup_ms"] for i in infos64]))
@@ -421,20 +505,22 @@ def run_ours(a, wl, rank, world, local_rank):
                      "bytes_per_launch": bytes_jac32,
                      "traffic": (int(TRAFFIC_RATIO[(ib32, tpr0 < 0)] * bytes_jac32)
                                  if a.workload.startswith("poisson27") and (ib32, tpr0 < 0) in TRAFFIC_RATIO else None)},
+        "cold_first_call": dict(cold, what="the first set-up + solve of each form in the process (threads-per-row "
+                                "autotuner running, kernels loading); the timed steps reuse the tuned choices"),
         "gpu_launches": int(round(launches32)),
         "e2e": {"value": e2e_ms / 1e3, "unit": "s", "h2d_bytes_per_step": int(row.nbytes + col.nbytes + val.nbytes + b.nbytes),
                 "d2h_bytes_per_step": int(n * 8), "path": "bcmgx_setup(host CSR) + bcmgx_solve(host b, x), pinned"},
     }
     if clk:
         line["clocks"] = clk
-    return line
+    return line, {"x32": x32, "x64": x64}
 
 
 # DRAM bytes (read + write) of one level-0 FP32 Jacobi launch as a multiple of its algorithmic
-# bytes, measured by ncu on the 27-point 100^3 case per (index bytes, staged kernel) (int32 columns:
-# profiles/jacobi_fp32_poisson27_100.md; int16 offsets: profiles/jacobi_fp32_int16_poisson27_100.md;
-# staged, int16: profiles/jacobi_fp32_staged_poisson27_100.md) and scaled by the algorithmic bytes
-# to the other 27-point workloads.
+# bytes, per (index bytes, staged kernel): measured by ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum of single launches) on the 27-point 100^3 case, plain kernel with int32
+# columns, plain with int16 offsets, staged with int16 offsets; scaled by the algorithmic bytes to
+# the other 27-point workloads.
 TRAFFIC_RATIO = {(4, False): 0.99983, (2, False): 1.00115, (2, True): 1.01173}
 
 
@@ -444,15 +530,18 @@ def _spmv(row, col, val, x):
     return sp.csr_matrix((val, col, row), shape=(n, n)) @ x
 
 
-def run_adjoint(a):
+def run_adjoint(a, rank=0, world=1, local_rank=0, steps=None, warmup=None):
     """Differentiated solve (7-point FV diffusion 96^3, kappa = exp(theta)): forward FCG+BCMG to
     1e-10, backward = adjoint solve on the same hierarchy, chained to dL/dtheta by torch; the
     gradient is checked along random directions against FP64 central differences and against
-    the gradient of a fresh plain-FP64 solve."""
+    the gradient of a fresh plain-FP64 solve. At N > 1 every rank runs its own replica and the
+    time is the slowest rank's."""
     import torch
     import bootcmatchgx_b200 as bx
     from bootcmatchgx_b200 import autograd, problems
-    dev = torch.device("cuda", 0)
+    dev = torch.device("cuda", local_rank)
+    steps = a.steps if steps is None else steps
+    warmup = a.warmup if warmup is None else warmup
     cfg = ADJOINT
     g = cfg["grid"]
     n = g[0] * g[1] * g[2]
@@ -479,16 +568,16 @@ def run_adjoint(a):
             x = autograd.solve(asm.row, asm.col, asm.values(torch.exp(th)), b, p)
             return 0.5 * ((x - x_obs) ** 2).sum()
 
-    for _ in range(max(1, a.warmup)):
+    for _ in range(max(1, warmup)):
         fwd_bwd(prm)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    for _ in range(a.steps):
+    for _ in range(steps):
         L, grad = fwd_bwd(prm)
     e1.record()
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / a.steps
+    ms = max_over_ranks(e0.elapsed_time(e1) / steps, world, dev)
     _, grad64 = fwd_bwd(prm64)
     tight = autograd.default_params(rtol=1e-12, vcycle_precision="FP64")
     _, grad_t = fwd_bwd(tight)
@@ -501,6 +590,7 @@ def run_adjoint(a):
         errs_t.append(abs(float(fd - (grad_t * d).sum())) / abs(float(fd)))
     return {"metric": "differentiated solve: forward+backward s (FP32 V-cycle)", "value": ms / 1e3, "unit": "s",
             "higher_is_better": False, "workload": "diffusion7_96_adjoint", "rows": n, "nnz": int(asm.nnz),
+            "n_gpus": world, "steps": steps, "warmup": warmup,
             "config": {"problem": "7-point FV diffusion 96^3, kappa = exp(theta), theta GRF (length 8, sigma 2, seed 5); "
                                   "x_obs = x(theta0) + N(0,1e-3); theta = theta0 + 0.1 N(0,1); L = 0.5||x - x_obs||^2",
                        "rtol": cfg["rtol"], "fd_step": h, "directions": cfg["directions"]},
@@ -510,16 +600,21 @@ def run_adjoint(a):
             "grad_rel_err_vs_fresh_fp64": float((grad - grad64).norm() / grad64.norm()), "loss": float(L)}
 
 
-def run_batch(a):
+def run_batch(a, rank=0, world=1, local_rank=0, steps=None, warmup=None):
     """256 independent 7-point Poisson systems, box sides uniform in 10..46 (seed 4), diagonal shift
     uniform[0, 0.5], FP32 V-cycle, rhs uniform[-1,1]: one CUDA-graph launch for all solves vs a
-    sequential loop of single solves (same hierarchies, warm graphs)."""
+    sequential loop of single solves (same hierarchies, warm graphs). At N > 1 rank r takes
+    systems r, r + N, ... (bootcmatchgx_b200.replicas) on its own GPU, with no communication; the
+    time is the slowest rank's and the value counts all 256 systems."""
     import scipy.sparse as sp
     import torch
     import bootcmatchgx_b200 as bx
-    dev = torch.device("cuda", 0)
+    from bootcmatchgx_b200 import replicas
+    dev = torch.device("cuda", local_rank)
+    steps = a.steps if steps is None else steps
+    warmup = a.warmup if warmup is None else warmup
     rng = np.random.default_rng(4)
-    systems, rows = [], 0
+    systems, rhs, rows = [], [], 0
     for _ in range(256):
         dims = [int(d) for d in rng.integers(10, 47, size=3)]
         shift = rng.uniform(0.0, 0.5)
@@ -527,46 +622,55 @@ def run_batch(a):
         v = v + shift * (c == np.repeat(np.arange(r.size - 1), np.diff(r)))
         systems.append((r, c, v))
         rows += r.size - 1
-    bs = [torch.from_numpy(rng.uniform(-1, 1, r.size - 1)).to(dev) for r, _, _ in systems]
+    for r, _, _ in systems:
+        rhs.append(rng.uniform(-1, 1, r.size - 1))
+    mine = replicas.systems_of_rank(len(systems), rank, world)
+    sysm = [systems[k] for k in mine]
+    bs = [torch.from_numpy(rhs[k]).to(dev) for k in mine]
     p = bx.params_default(solver="FCG", preconditioner="BCMG", rtol=1e-8, dispnorm=0, vcycle_precision="FP32")
+    nthreads = min(16, os.cpu_count() or 1)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    B = bx.Batch(systems, p, nthreads=min(16, os.cpu_count() or 1))
+    B = bx.Batch(sysm, p, nthreads=nthreads)
     torch.cuda.synchronize()
-    t_setup = time.perf_counter() - t0
+    t_setup = max_over_ranks(time.perf_counter() - t0, world, dev)
     xs, infos = B.solve(bs)   # builds the graph
-    for _ in range(max(0, a.warmup - 1)):
+    for _ in range(max(0, warmup - 1)):
         B.solve(bs)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(a.steps):
+    for _ in range(steps):
         xs, infos = B.solve(bs)
     torch.cuda.synchronize()
-    t_batch = (time.perf_counter() - t0) / a.steps
-    hs = [B.hierarchy(k) for k in range(len(systems))]
+    t_batch = max_over_ranks((time.perf_counter() - t0) / steps, world, dev)
+    hs = [B.hierarchy(k) for k in range(len(sysm))]
     for k, h in enumerate(hs):   # warm each single-solve graph
         h.solve(bs[k])
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(a.steps):
+    for _ in range(steps):
         for k, h in enumerate(hs):
             h.solve(bs[k])
     torch.cuda.synchronize()
-    t_seq = (time.perf_counter() - t0) / a.steps
+    t_seq = max_over_ranks((time.perf_counter() - t0) / steps, world, dev)
     worst = 0.0
-    for k, (r, c, v) in enumerate(systems):
+    for k, (r, c, v) in enumerate(sysm):
         A = sp.csr_matrix((v, c, r), shape=(r.size - 1,) * 2)
         bb = bs[k].cpu().numpy()
         worst = max(worst, float(np.linalg.norm(bb - A @ xs[k].cpu().numpy()) / np.linalg.norm(bb)))
+    worst = max_over_ranks(worst, world, dev)
+    it_lo = -max_over_ranks(-min(i["niter"] for i in infos), world, dev)
+    it_hi = max_over_ranks(max(i["niter"] for i in infos), world, dev)
     B.free()
     return {"metric": "batched solves/s (256 uneven 7-point systems, one graph launch)", "value": 256 / t_batch,
-            "unit": "solves/s", "higher_is_better": True, "workload": "batch256_poisson7",
+            "unit": "solves/s", "higher_is_better": True, "workload": "batch256_poisson7", "n_gpus": world,
             "sequential_solves_per_s": 256 / t_seq, "speedup_vs_sequential": t_seq / t_batch,
             "batch_solve_ms": t_batch * 1e3, "sequential_ms": t_seq * 1e3, "setup_ms": t_setup * 1e3,
-            "total_rows": rows, "iters_min_max": [min(i["niter"] for i in infos), max(i["niter"] for i in infos)],
-            "max_rel_residual": worst, "steps": a.steps, "warmup": a.warmup,
+            "total_rows": rows, "iters_min_max": [int(it_lo), int(it_hi)],
+            "max_rel_residual": worst, "steps": steps, "warmup": warmup,
             "config": {"systems": 256, "sides": "uniform 10..46 (numpy default_rng(4))", "shift": "uniform[0,0.5]",
-                       "vcycle": "fp32", "rtol": 1e-8, "setup_threads": min(16, os.cpu_count() or 1)}}
+                       "vcycle": "fp32", "rtol": 1e-8, "setup_threads": nthreads,
+                       "parallelism": f"systems round robin over {world} GPU(s), one batch graph per GPU"}}
 
 
 def block_kernel_rooflines(t, n, nnz, k):
@@ -588,23 +692,32 @@ def block_kernel_rooflines(t, n, nnz, k):
     return out
 
 
-def run_multi(a):
+def run_multi(a, rank=0, world=1, local_rank=0, steps=None, warmup=None, kernels=True):
     """The 27-point 100^3 Poisson matrix with 32 right-hand sides (uniform[-1,1], numpy
     default_rng(6)) solved to 1e-8 in one block solve (CSR SpMM throughout, FP32 V-cycle) vs a
     sequential loop of 32 single solves on the same hierarchy; also the block FP64-cycle solve,
     the level-0 block kernels (CUDA events, HBM GB/s of their algorithmic bytes) and the public
-    SpMM call."""
+    SpMM call. At N > 1 rank r solves a contiguous slice of the 32 columns
+    (bootcmatchgx_b200.replicas) with its own hierarchy on its own GPU, with no communication;
+    times are the slowest rank's and the value counts all 32 columns."""
     import scipy.sparse as sp
     import torch
     import bootcmatchgx_b200 as bx
-    dev = torch.device("cuda", 0)
-    k = 32
+    from bootcmatchgx_b200 import replicas
+    dev = torch.device("cuda", local_rank)
+    steps = a.steps if steps is None else steps
+    warmup = a.warmup if warmup is None else warmup
+    ktot = 32
     row, col, val = bx.laplacian_3d(27, 100, 100, 100)
     n, nnz = row.size - 1, col.size
-    B = np.random.default_rng(6).uniform(-1.0, 1.0, (n, k))
+    Ball = np.random.default_rng(6).uniform(-1.0, 1.0, (n, ktot))
+    cols = replicas.columns_of_rank(ktot, rank, world)
+    k = len(cols)
+    B = np.ascontiguousarray(Ball[:, cols.start:cols.stop])
     d = [torch.from_numpy(x_).to(dev) for x_ in (row, col, val)]
     Bd = torch.from_numpy(B).to(dev)
     X = torch.zeros_like(Bd)
+    A = sp.csr_matrix((val, col, row), shape=(n, n))
     out = {}
     for prec in ("FP32", "FP64"):
         p = bx.params_default(solver="FCG", preconditioner="BCMG", rtol=1e-8, dispnorm=0, vcycle_precision=prec)
@@ -612,73 +725,76 @@ def run_multi(a):
         t0 = time.perf_counter()
         h = bx.Hierarchy(d[0], d[1], d[2], p)
         torch.cuda.synchronize()
-        t_setup = time.perf_counter() - t0
-        for _ in range(max(1, a.warmup)):
+        t_setup = max_over_ranks(time.perf_counter() - t0, world, dev)
+        for _ in range(max(1, warmup)):
             X.zero_()
             h.solve_multi(Bd, X)
         ts = []
-        for _ in range(a.steps):
+        for _ in range(steps):
             X.zero_()
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             _, infos = h.solve_multi(Bd, X)
             torch.cuda.synchronize()
             ts.append(time.perf_counter() - t0)
-        t_block = float(np.median(ts))
+        t_block = max_over_ranks(float(np.median(ts)), world, dev)
         Xh = X.cpu().numpy()
-        A = sp.csr_matrix((val, col, row), shape=(n, n))
         rel = np.linalg.norm(B - A @ Xh, axis=0) / np.linalg.norm(B, axis=0)
-        res = {"block_ms": t_block * 1e3, "solves_per_s": k / t_block, "setup_ms": t_setup * 1e3,
-               "iters_min_max": [min(i["niter"] for i in infos), max(i["niter"] for i in infos)],
-               "max_rel_residual": float(rel.max())}
+        res = {"block_ms": t_block * 1e3, "solves_per_s": ktot / t_block, "setup_ms": t_setup * 1e3,
+               "iters_min_max": [int(-max_over_ranks(-min(i["niter"] for i in infos), world, dev)),
+                                 int(max_over_ranks(max(i["niter"] for i in infos), world, dev))],
+               "max_rel_residual": max_over_ranks(float(rel.max()), world, dev)}
         if prec == "FP32":
             xs = [torch.zeros(n, dtype=torch.float64, device=dev) for _ in range(k)]
-            cols = [Bd[:, j].contiguous() for j in range(k)]
-            h.solve(cols[0], xs[0])   # builds the single-solve graph
+            colv = [Bd[:, j].contiguous() for j in range(k)]
+            h.solve(colv[0], xs[0])   # builds the single-solve graph
             ts = []
-            for _ in range(max(1, a.steps // 2)):
+            for _ in range(max(1, steps // 2)):
                 for x_ in xs:
                     x_.zero_()
                 torch.cuda.synchronize()
                 t0 = time.perf_counter()
                 for j in range(k):
-                    h.solve(cols[j], xs[j])
+                    h.solve(colv[j], xs[j])
                 torch.cuda.synchronize()
                 ts.append(time.perf_counter() - t0)
-            t_seq = float(np.median(ts))
+            t_seq = max_over_ranks(float(np.median(ts)), world, dev)
             res["sequential_ms"] = t_seq * 1e3
-            res["sequential_solves_per_s"] = k / t_seq
+            res["sequential_solves_per_s"] = ktot / t_seq
             res["speedup_vs_sequential"] = t_seq / t_block
-            res["max_rel_diff_vs_single"] = max(float(torch.linalg.norm(X[:, j] - xs[j]) / torch.linalg.norm(xs[j]))
-                                                for j in range(k))
-            res["kernels_level0"] = block_kernel_rooflines(h.time_block_kernels(k, reps=20), n, nnz, k)
+            res["max_rel_diff_vs_single"] = max_over_ranks(
+                max(float(torch.linalg.norm(X[:, j] - xs[j]) / torch.linalg.norm(xs[j])) for j in range(k)), world, dev)
+            if kernels:
+                res["kernels_level0"] = block_kernel_rooflines(h.time_block_kernels(k, reps=20), n, nnz, k)
         h.free()
         out[prec] = res
-    # the public SpMM call Y = A X for the 32-column block: CSR validation on the device, a host
-    # round trip for its verdict, then the kernel (the kernel alone: fp32.kernels_level0.spmm)
-    Y = torch.empty_like(Bd)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    for _ in range(3):
-        bx.spmm(d[0], d[1], d[2], Bd, Y)
-    reps = 20
-    e0.record()
-    for _ in range(reps):
-        bx.spmm(d[0], d[1], d[2], Bd, Y)
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / reps
-    alg = nnz * 12 + (n + 1) * 4 + 2 * n * k * 8
-    peak, peak_kind = read_peaks()
     f32 = out["FP32"]
-    return {"metric": "multi-RHS solves/s (27-point 100^3, 32 right-hand sides, one block solve)",
+    line = {"metric": "multi-RHS solves/s (27-point 100^3, 32 right-hand sides, one block solve)",
             "value": f32["solves_per_s"], "unit": "solves/s", "higher_is_better": True, "workload": "poisson27_100_x32",
-            "fp32": f32, "fp64": out["FP64"],
-            "spmm_call": {"ms": ms, "what": "bcmgx_spmm: validation + host round trip + kernel",
-                          "algorithmic_bytes": alg, "gbs": alg / ms / 1e6, "peak_gbs": peak,
-                          "frac": alg / ms / 1e6 / peak, "peak_kind": peak_kind},
-            "steps": a.steps, "warmup": a.warmup,
-            "config": {"rows": n, "nnz": nnz, "rhs": k, "rhs_dist": "uniform[-1,1] (numpy default_rng(6))",
-                       "rtol": 1e-8, "x0": 0}}
+            "n_gpus": world, "fp32": f32, "fp64": out["FP64"], "steps": steps, "warmup": warmup,
+            "config": {"rows": n, "nnz": nnz, "rhs": ktot, "rhs_dist": "uniform[-1,1] (numpy default_rng(6))",
+                       "rtol": 1e-8, "x0": 0,
+                       "parallelism": f"columns in contiguous slices over {world} GPU(s), one hierarchy per GPU"}}
+    if kernels and world == 1:
+        # the public SpMM call Y = A X for the 32-column block: CSR validation on the device, a host
+        # round trip for its verdict, then the kernel (the kernel alone: fp32.kernels_level0.spmm)
+        Y = torch.empty_like(Bd)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for _ in range(3):
+            bx.spmm(d[0], d[1], d[2], Bd, Y)
+        reps = 20
+        e0.record()
+        for _ in range(reps):
+            bx.spmm(d[0], d[1], d[2], Bd, Y)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        alg = nnz * 12 + (n + 1) * 4 + 2 * n * k * 8
+        peak, peak_kind = read_peaks()
+        line["spmm_call"] = {"ms": ms, "what": "bcmgx_spmm: validation + host round trip + kernel",
+                             "algorithmic_bytes": alg, "gbs": alg / ms / 1e6, "peak_gbs": peak,
+                             "frac": alg / ms / 1e6 / peak, "peak_kind": peak_kind}
+    return line
 
 
 def profile_multi_step(a):
@@ -739,6 +855,76 @@ def profile_step(a, wl):
     print(json.dumps({"warmup_launches": c1 - c0, "step_launches": c2 - c1, "niter": info["niter"]}), flush=True)
 
 
+def run_small(a, name, rank=0, world=1, local_rank=0, steps=10, warmup=3):
+    """A small workload (the 7-point 50^3 Poisson system by default: 125,000 rows, L2-resident)
+    through the same step as the headline: set-up + FCG solve to 1e-8, FP32 and FP64 V-cycles,
+    CUDA events, the slowest rank's time; rank 0 also compares the level sizes and iterations
+    with the oracle's (a fraction of a second on the host at this size)."""
+    import torch
+    import bootcmatchgx_b200 as bx
+    dev = torch.device("cuda", local_rank)
+    stream = torch.cuda.current_stream(dev)
+    wl = WORKLOADS[name]
+    row, col, val, xs, b = build_problem(wl)
+    d = [torch.from_numpy(x_).to(dev) for x_ in (row, col, val, b)]
+    x = torch.zeros(row.size - 1, dtype=torch.float64, device=dev)
+    out = {"workload": name, "rows": int(row.size - 1), "nnz": int(col.size), "steps": steps, "warmup": warmup,
+           "n_gpus": world}
+    for prec in ("FP32", "FP64"):
+        p = bx.params_default(solver="FCG", preconditioner="BCMG", rtol=RTOL, dispnorm=0, vcycle_precision=prec,
+                              stream=stream.cuda_stream)
+
+        def step():
+            h = bx.Hierarchy(d[0], d[1], d[2], p)
+            x.zero_()
+            _, info = h.solve(d[3], x)
+            inf = h.info()
+            h.free()
+            return info, inf
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        res = [step() for _ in range(steps)]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1) / steps, world, dev)
+        xh = x.cpu().numpy()
+        out[prec.lower()] = {"ms_per_step": ms, "setup_ms": float(np.mean([r[1]["setup_ms"] for r in res])),
+                             "solve_ms": float(np.mean([r[0]["solve_ms"] for r in res])), "niter": res[-1][0]["niter"],
+                             "err_vs_xstar": None if xs is None else float(np.linalg.norm(xh - xs) / np.linalg.norm(xs)),
+                             "levels": res[-1][1]["n"], "level_nnz": res[-1][1]["nnz"]}
+    if rank == 0:
+        from oracle import pyoracle as O
+        O.num_threads(host_info()["cpus_available"])
+        ts, tv, xo, io, lv = oracle_solve(O, O.Matrix.from_csr(row, col, val), b)
+        gl = list(zip(out["fp64"]["levels"], out["fp64"]["level_nnz"]))
+        out["parity"] = {"levels_equal": gl == [tuple(t) for t in lv], "niter_oracle": io["niter"],
+                         "niter_fp64": out["fp64"]["niter"], "oracle_s": ts + tv}
+    return out
+
+
+def secondary_configs(a, rank, world, local_rank):
+    """The other configurations, each in a bounded number of steps, as extra keys of the headline
+    line (every rank runs them in the same order, so that their max-over-ranks reductions pair
+    up): C1 (7-point 50^3), C5 (differentiated 96^3 diffusion), C4a (256 uneven systems in one
+    graph launch) and C4b (32 right-hand sides)."""
+    jobs = [("poisson7_50", lambda: run_small(a, "poisson7_50", rank, world, local_rank)),
+            ("adjoint_diffusion7_96", lambda: run_adjoint(a, rank, world, local_rank, steps=3, warmup=1)),
+            ("batch256_poisson7", lambda: run_batch(a, rank, world, local_rank, steps=3, warmup=2)),
+            ("poisson27_100_x32", lambda: run_multi(a, rank, world, local_rank, steps=3, warmup=1, kernels=False))]
+    out = {}
+    for name, fn in jobs:
+        t0 = time.perf_counter()
+        try:
+            out[name] = fn()
+        except Exception as e:   # reported in the line; the headline stands
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+        out[name]["wall_s"] = time.perf_counter() - t0
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -747,6 +933,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="poisson27_160", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true", help="leave out the other configurations' summaries")
     ap.add_argument("--adjoint", action="store_true", help="run the differentiated-solve configuration instead")
     ap.add_argument("--batch", action="store_true", help="run the batched-systems configuration instead")
     ap.add_argument("--multi", action="store_true", help="run the 32-right-hand-side configuration instead")
@@ -757,41 +944,55 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     wl = WORKLOADS[a.workload]
+    if a.impl == "reference":
+        line = reference_arm(a, wl, rank, world)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
     if a.profile_step:
         if a.multi:
             profile_multi_step(a)
         else:
             profile_step(a, wl)
         return
-    if a.adjoint:
-        print(json.dumps(run_adjoint(a)), flush=True)
-        return
-    if a.batch:
-        print(json.dumps(run_batch(a)), flush=True)
-        return
-    if a.multi:
-        print(json.dumps(run_multi(a)), flush=True)
-        return
-    if a.impl == "reference":
-        line = reference_arm(a, wl, rank, world)
-        if line is not None:
-            print(json.dumps(line), flush=True)
-        return
+    import torch
+    torch.cuda.set_device(local_rank)
     if world > 1:
-        import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    line = run_ours(a, wl, rank, world, local_rank)
-    if rank == 0 and line is not None:
-        if world == 1 and not a.no_cpu_baseline:
-            row, col, val, xs, b = build_problem(wl)
-            line["cpu_baseline"] = cpu_baseline(wl, row, col, val, b, xs)
-        print(json.dumps(line), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-        dist.destroy_process_group()
+    try:
+        line = None
+        if a.adjoint:
+            line = run_adjoint(a, rank, world, local_rank)
+        elif a.batch:
+            line = run_batch(a, rank, world, local_rank)
+        elif a.multi:
+            line = run_multi(a, rank, world, local_rank)
+        else:
+            line, extra = run_ours(a, wl, rank, world, local_rank)
+            if not a.no_secondary:
+                sec = secondary_configs(a, rank, world, local_rank)
+                if line is not None:
+                    line["secondary"] = sec
+            if rank == 0 and world == 1 and not a.no_cpu_baseline:
+                cb, ora = cpu_baseline(wl)
+                line["cpu_baseline"] = cb
+                x64 = extra["x64"]
+                gl = list(zip(line["breakdown"]["levels"], line["breakdown"]["level_nnz"]))
+                line["parity"] = {
+                    "levels_equal": gl == [tuple(t) for t in ora["levels"]],
+                    "level_sizes_oracle": ora["levels"], "niter_oracle": ora["niter"],
+                    "niter_fp64": line["fp64"]["niter"], "niter_fp32": line["breakdown"]["niter"],
+                    "fp64_rel_diff_vs_oracle_solution": float(np.linalg.norm(x64 - ora["x"]) / np.linalg.norm(ora["x"])),
+                    "fp32_rel_diff_vs_oracle_solution": float(np.linalg.norm(extra["x32"] - ora["x"]) / np.linalg.norm(ora["x"])),
+                    "what": "GPU hierarchy sizes, iterations and solutions against the oracle's run on the same inputs"}
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
 
 
 if __name__ == "__main__":

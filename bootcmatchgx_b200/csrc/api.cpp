@@ -13,6 +13,28 @@
 namespace bcmgx {
 
 static thread_local std::string g_last_error;
+thread_local long long t_fail_alloc_countdown = 0;
+
+// Arms the allocation-failure injection of the calling thread for one set-up (see internal.h)
+// and disarms it when the set-up returns or throws.
+struct FailAllocScope {
+    FailAllocScope()
+    {
+        const char* e = std::getenv("BCMGX_TEST_FAIL_ALLOC");
+        t_fail_alloc_countdown = (e && *e) ? std::max(0LL, std::atoll(e)) : 0;
+    }
+    ~FailAllocScope() { t_fail_alloc_countdown = 0; }
+};
+
+// A CUDA event owned for the duration of a scope.
+struct ScopedEvent {
+    cudaEvent_t e = nullptr;
+    ScopedEvent() { BCMGX_CUDA(cudaEventCreate(&e)); }
+    ~ScopedEvent()
+    {
+        if (e) cudaEventDestroy(e);
+    }
+};
 
 void set_last_error(const std::string& s) { g_last_error = s; }
 
@@ -144,6 +166,7 @@ static bcmgx_hierarchy* setup_one(const bcmgx_csr* A, const bcmgx_params* p, int
     BCMGX_REQUIRE(A->n > 0 && A->n == A->m, BCMGX_ERR_INVALID_INPUT, "matrix must be square with n > 0");
     BCMGX_REQUIRE(A->nnz > 0 && A->nnz <= 0x7fffffffLL, BCMGX_ERR_INVALID_INPUT, "nnz must be in [1, 2^31-1]");
     BCMGX_REQUIRE(A->row && A->col && A->val, BCMGX_ERR_INVALID_INPUT, "NULL CSR array");
+    FailAllocScope inject;
     std::unique_ptr<bcmgx_hierarchy> H(new bcmgx_hierarchy());
     H->prm = *p;
     int dev = device >= 0 ? device : p->device;
@@ -170,10 +193,8 @@ static bcmgx_hierarchy* setup_one(const bcmgx_csr* A, const bcmgx_params* p, int
     BCMGX_CUDA(cudaEventCreateWithFlags(&H->ev_it[1], cudaEventDisableTiming));
     BCMGX_CUDA(cudaEventCreateWithFlags(&H->ev_in, cudaEventDisableTiming));
     if (A->on_device) after_caller(H->stream, H->ev_in, H->own_stream);
-    cudaEvent_t e0, e1;
-    BCMGX_CUDA(cudaEventCreate(&e0));
-    BCMGX_CUDA(cudaEventCreate(&e1));
-    BCMGX_CUDA(cudaEventRecord(e0, H->stream));
+    ScopedEvent t0, t1;
+    BCMGX_CUDA(cudaEventRecord(t0.e, H->stream));
     stage_fault_init();
     build_hierarchy(H.get(), A);
     const char* force = std::getenv("BCMGX_TPR");
@@ -190,12 +211,10 @@ static bcmgx_hierarchy* setup_one(const bcmgx_csr* A, const bcmgx_params* p, int
         V.A.tpr = code < 0 ? -code : code;
         if (V.A.tpr < 1) V.A.tpr = default_tpr(V.A.n, V.A.nnz);
     }
-    BCMGX_CUDA(cudaEventRecord(e1, H->stream));
-    BCMGX_CUDA(cudaEventSynchronize(e1));
+    BCMGX_CUDA(cudaEventRecord(t1.e, H->stream));
+    BCMGX_CUDA(cudaEventSynchronize(t1.e));
     float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    cudaEventElapsedTime(&ms, t0.e, t1.e);
     stage_fault_check();
     H->setup_ms = ms;
     return H.release();

@@ -32,6 +32,11 @@ void pinned_free(void* p);
 void note_launch();
 void note_launches(long long k);
 long long launch_count();
+// Allocation-failure injection for the fault-path tests: while positive, every device allocation
+// of the calling thread counts it down, and the one that brings it to zero fails as out of
+// memory. bcmgx_setup arms it from the environment variable BCMGX_TEST_FAIL_ALLOC (k: fail the
+// k-th allocation of that set-up) and disarms it on return. Zero in production.
+extern thread_local long long t_fail_alloc_countdown;
 
 #define BCMGX_CUDA(call)                                                                       \
     do {                                                                                       \
@@ -77,6 +82,11 @@ struct DBuf {
         s = stream;
         n = count;
         if (count == 0) return;
+        if (t_fail_alloc_countdown > 0 && --t_fail_alloc_countdown == 0) {
+            n = 0;
+            throw Error(BCMGX_ERR_OOM, "device allocation of " + std::to_string(count * sizeof(T)) +
+                    " bytes failed (injected by BCMGX_TEST_FAIL_ALLOC)");
+        }
         // 64 bytes past the end: bulk copies of 16-byte granules (staged.cuh) may round the end
         // of a range up without leaving the allocation
         cudaError_t e = cudaMallocAsync((void**)&p, count * sizeof(T) + 64, stream);
@@ -267,6 +277,9 @@ void grad_pattern(const DevCsr& A, const double* lam, const double* x, double* d
 void batch_build(bcmgx_batch* B);
 int batch_solve(bcmgx_batch* B, const double* const* b, double* const* x, bcmgx_solve_info* infos);
 
+// Blocks of `kernel` resident per SM with `threads` threads and `smem` bytes of dynamic shared
+// memory on the current device (queried once per combination and device, then cached).
+int blocks_per_sm(const void* kernel, int threads, size_t smem);
 // Grid for a grid-stride kernel: min(need_blocks, blocks of this kernel resident on the GPU).
 int fit_grid(const void* kernel, int threads, long need_blocks);
 template <typename... A>

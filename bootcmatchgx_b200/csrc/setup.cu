@@ -1278,7 +1278,12 @@ void suitor_dev(int n, int64_t nnz, const int* row, const int* col, const double
         const char* e = std::getenv("BCMGX_SUITOR_ASC");
         asc = (e && std::atoi(e) > 0) ? 1 : 0;
     }
-    const long long budget = (long long)nnz + n + 1024;
+    // steps one proposal chain may take: every vertex's list position only moves forward, so no
+    // chain needs more than nnz + n. BCMGX_TEST_SUITOR_BUDGET overrides it (fault-path tests:
+    // a budget of 0 makes every chain give up at once and the set-up return BCMGX_ERR_TIMEOUT).
+    long long budget = (long long)nnz + n + 1024;
+    if (const char* tb = std::getenv("BCMGX_TEST_SUITOR_BUDGET"))
+        if (*tb) budget = std::max(0LL, std::atoll(tb));
     if (wide) {
         note_launch(); k_suitor_w<<<ceil_div(n, 128), 128, 0, s>>>(n, rinfo.p, pref.p, offer_w.p, budget, errp, asc ? 0 : 1);
         note_launch(); k_suitor_result_w<<<gs_grid(n), 256, 0, s>>>(n, offer_w.p, M);

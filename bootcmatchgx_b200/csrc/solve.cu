@@ -28,15 +28,34 @@
 
 namespace bcmgx {
 
+static int current_device()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        (void)cudaGetLastError();
+        dev = 0;
+    }
+    return dev;
+}
+
+// SM count of the current device (cached per device).
 int num_sms()
 {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
+    static std::mutex mu;
+    static std::unordered_map<int, int> cache;
+    const int dev = current_device();
+    {
+        std::lock_guard<std::mutex> g(mu);
+        auto it = cache.find(dev);
+        if (it != cache.end()) return it->second;
     }
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) {
+        (void)cudaGetLastError();
+        sms = 148;
+    }
+    std::lock_guard<std::mutex> g(mu);
+    cache[dev] = sms;
     return sms;
 }
 
@@ -56,27 +75,32 @@ void ensure_smem_limit(const void* kernel, size_t bytes)
 
 // Grid of a grid-stride kernel: the blocks its work needs, but no more than fit on the GPU at
 // once for this kernel (its registers and shared memory decide how many blocks an SM holds; the
-// figure is queried once per kernel and cached). Every block is then resident from the start: a
-// grid larger than one wave would leave its last blocks to run after the first wave has
-// finished all of its rows, on a mostly idle GPU.
-int fit_grid(const void* kernel, int threads, long need_blocks)
+// figure is queried once per kernel, block size, shared memory and device, and cached). Every
+// block is then resident from the start: a grid larger than one wave would leave its last blocks
+// to run after the first wave has finished all of its rows, on a mostly idle GPU.
+int blocks_per_sm(const void* kernel, int threads, size_t smem)
 {
     static std::mutex mu;
-    static std::unordered_map<const void*, int> per_sm;
-    int b = 0;
+    static std::map<std::tuple<int, const void*, int, size_t>, int> cache;
+    const auto key = std::make_tuple(current_device(), kernel, threads, smem);
     {
         std::lock_guard<std::mutex> g(mu);
-        auto it = per_sm.find(kernel);
-        if (it != per_sm.end()) b = it->second;
+        auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
     }
-    if (b == 0) {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, threads, 0) != cudaSuccess || b <= 0) {
-            (void)cudaGetLastError();
-            b = 1;
-        }
-        std::lock_guard<std::mutex> g(mu);
-        per_sm[kernel] = b;
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, threads, smem) != cudaSuccess || b <= 0) {
+        (void)cudaGetLastError();
+        b = 1;
     }
+    std::lock_guard<std::mutex> g(mu);
+    cache[key] = b;
+    return b;
+}
+
+int fit_grid(const void* kernel, int threads, long need_blocks)
+{
+    const int b = blocks_per_sm(kernel, threads, 0);
     return (int)std::max<long>(1, std::min<long>(need_blocks, (long)num_sms() * b));
 }
 
@@ -155,6 +179,18 @@ void stage_fault_check()
 
 static bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
 
+// Fault-path test hook of the staged kernels: BCMGX_TEST_STAGE_FAULT=<ns> in the environment makes
+// the launches that follow (the variable is read at every launch; a captured graph keeps the value
+// of its capture) drop block 0's first tile copy and wait at most <ns> for a stage, so that the
+// timeout path runs and the entry point returns BCMGX_ERR_TIMEOUT. Unset in production.
+static unsigned long long stage_test_wait_ns()
+{
+    const char* e = std::getenv("BCMGX_TEST_STAGE_FAULT");
+    if (!e || !*e) return 0;
+    const long long v = std::atoll(e);
+    return v > 0 ? (unsigned long long)v : 0ull;
+}
+
 // The staged form of launch_rowop (staged.cuh): one resident wave of blocks over tiles of R rows.
 template <int S, int OP, typename VT, typename XT, typename FT, typename MT, typename YT, typename IT>
 static void launch_staged(int n, int64_t nnz, const int* row, const IT* col, const VT* val, const XT* x, const FT* f,
@@ -163,20 +199,15 @@ static void launch_staged(int n, int64_t nnz, const int* row, const IT* col, con
     using C = StageCfg<VT, IT>;
     auto kern = k_rowop_staged<S, OP, VT, XT, FT, MT, YT, IT>;
     ensure_smem_limit(kern, C::SMEM);
-    static const int per_sm = [kern] {
-        int b = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, kStageThreads, C::SMEM) != cudaSuccess || b < 1) {
-            (void)cudaGetLastError();
-            b = 1;
-        }
-        return b;
-    }();
+    const int per_sm = blocks_per_sm((const void*)kern, kStageThreads, C::SMEM);
     stage_fault_init();
     const int R = stage_tile_rows<VT, IT>(n, nnz, S);
     const long ntiles = ((long)n + R - 1) / R;
     const int grid = (int)std::min<long>(ntiles, (long)per_sm * num_sms());
+    const unsigned long long test_ns = stage_test_wait_ns();
     note_launch();
-    kern<<<grid, kStageThreads, C::SMEM, s>>>(n, R, row, col, val, x, f, M, y, alpha, beta, skip, g_stage_fault);
+    kern<<<grid, kStageThreads, C::SMEM, s>>>(n, R, row, col, val, x, f, M, y, alpha, beta, skip, g_stage_fault,
+        test_ns ? test_ns : kStageWaitNs, test_ns ? 1 : 0);
     BCMGX_CHECK_LAUNCH();
 }
 

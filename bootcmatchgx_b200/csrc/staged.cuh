@@ -14,8 +14,12 @@
 // and its row offsets to multiples of 4, so the copies may read up to 7 entries and 3 row offsets
 // past the end of the arrays (every device buffer of the library carries 64 bytes of padding).
 // A tile whose widened range does not fit a stage is read from global memory instead. Every
-// wait on an mbarrier gives up after about one second and stores a nonzero code in *fault
-// (1: the producer waited for a free stage, 2: a consumer for a full one, 4: the final drain).
+// wait on an mbarrier gives up after a time limit and stores a nonzero code in *fault (1: the
+// producer waited for a free stage, 2: a consumer for a full one, 4: the final drain). The limit
+// is wait_ns (one second in production) for the first two; the drain, which must not let the
+// block exit while bulk copies into its shared memory are in flight, always waits up to one
+// second. A consumer warp decides to give up as a whole (every lane leaves the tile loop
+// together), so no shuffle runs with lanes that have left.
 #pragma once
 
 #include <algorithm>
@@ -89,15 +93,18 @@ __device__ __forceinline__ unsigned long long global_ns()
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-// Waits for the phase of parity `parity` to complete; false after about one second.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity)
+constexpr unsigned long long kStageWaitNs = 1000000000ull;   // one second
+
+// Waits for the phase of parity `parity` to complete; false after about limit_ns nanoseconds.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity,
+    unsigned long long limit_ns = kStageWaitNs)
 {
     if (mbar_try_wait(b, parity)) return true;
     const unsigned long long t0 = global_ns();
     for (;;) {
         for (int i = 0; i < 64; i++)
             if (mbar_try_wait(b, parity)) return true;
-        if (global_ns() - t0 > 1000000000ull) return false;
+        if (global_ns() - t0 > limit_ns) return false;
     }
 }
 // L2 policy for data read once per pass: evict first, so that the gathered vectors stay in L2.
@@ -144,11 +151,15 @@ __device__ __forceinline__ void row_operands(int r, const XT* __restrict__ x, co
 // tiles of R rows, tile t on block t mod gridDim.x, row i of a tile on consumer sub-warp i.
 // Launch with kStageThreads threads and StageCfg<VT, IT>::SMEM bytes of dynamic shared memory;
 // R = stage_tile_rows<VT, IT>(n, nnz, S): a multiple of 4, at most kStageWarps * 32 / S.
+// wait_ns: limit of the producer's and the consumers' stage waits (kStageWaitNs in production).
+// drop_first: a fault-path test hook; when set, block 0's producer issues no copy for its first
+// tile, so that the consumers' wait for that stage runs out (the drain skips that stage, which
+// has no copy in flight).
 template <int S, int OP, typename VT, typename XT, typename FT, typename MT, typename YT, typename IT>
 __global__ void __launch_bounds__(kStageThreads) k_rowop_staged(int n, int R, const int* __restrict__ row,
     const IT* __restrict__ col, const VT* __restrict__ val, const XT* __restrict__ x, const FT* __restrict__ f,
     const MT* __restrict__ M, YT* __restrict__ y, double alpha, double beta, const int* __restrict__ skip,
-    int* __restrict__ fault)
+    int* __restrict__ fault, unsigned long long wait_ns, int drop_first)
 {
     if (skip && *skip) return;
     using C = StageCfg<VT, IT>;
@@ -170,13 +181,15 @@ __global__ void __launch_bounds__(kStageThreads) k_rowop_staged(int n, int R, co
         // producer: one thread issues the copies of every tile of this block, NS tiles ahead
         if (l32 != 0) return;
         const unsigned long long pol = l2_evict_first();
+        const int dropped = (drop_first && blockIdx.x == 0) ? 0 : -1;   // tile index with no copy
         int it = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
             const int st = it % NS;
-            if (it >= NS && !mbar_wait(&empty[st], ((unsigned)(it / NS) & 1u) ^ 1u)) {
+            if (it >= NS && !mbar_wait(&empty[st], ((unsigned)(it / NS) & 1u) ^ 1u, wait_ns)) {
                 *(volatile int*)fault = 1;
                 break;
             }
+            if (it == dropped) continue;
             const int t0 = t * R, t1 = min(t0 + R, n);
             const int a0 = __ldg(row + t0) & ~7, a1 = (__ldg(row + t1) + 7) & ~7;
             const int cnt = a1 - a0, nrp = (t1 - t0 + 4) & ~3;
@@ -194,7 +207,7 @@ __global__ void __launch_bounds__(kStageThreads) k_rowop_staged(int n, int R, co
         }
         // the copies still in flight land before the block's shared memory is released
         for (int k = max(0, it - NS); k < it; k++)
-            if (!mbar_wait(&full[k % NS], (unsigned)(k / NS) & 1u)) *(volatile int*)fault = 4;
+            if (k != dropped && !mbar_wait(&full[k % NS], (unsigned)(k / NS) & 1u)) *(volatile int*)fault = 4;
         return;
     }
     const int lane = l32 & (S - 1), wsub = l32 / S;
@@ -207,8 +220,10 @@ __global__ void __launch_bounds__(kStageThreads) k_rowop_staged(int n, int R, co
         const int i1 = warp * SPW + wsub;
         AT p1 = 0, p2 = 0, p3 = 0;
         if (i1 < nr && lane == 0) row_operands<OP>(t0 + i1, x, f, M, y, beta, p1, p2, p3);
-        if (!mbar_wait(&full[st], (unsigned)(it / NS) & 1u)) {
-            *(volatile int*)fault = 2;
+        // every lane waits (each needs the barrier's acquire for its reads of the stage), and the
+        // warp gives up only as a whole
+        if (!__all_sync(0xffffffffu, mbar_wait(&full[st], (unsigned)(it / NS) & 1u, wait_ns))) {
+            if (l32 == 0) *(volatile int*)fault = 2;
             break;
         }
         const unsigned char* base = stage_smem + st * C::STAGE;

@@ -1,7 +1,7 @@
 """Regenerate tests/golden/reference_fixtures.npz from the reference's own test data.
 
-Run in a container where the BootCMatchGX sources are mounted (default path below); the
-GPU box never runs this. It packs, without modification:
+Run where the BootCMatchGX sources are available, with their root as the argument; the GPU box
+never runs this. It packs, without modification:
   * BCMGX/src/test/data/cmp/lap3d_{7p,27p}_10x10x10_{1x1x1,2x1x1,2x2x1,2x2x2}_sol.txt
     (FCG+BCMG solutions of A x = 1, rtol 1e-6, checked by compareSolutions at 1e-5,
     BCMGX/launchAndCompare.mk:320-330), in the reference's rank-block-major row order;
@@ -13,16 +13,15 @@ GPU box never runs this. It packs, without modification:
     of A x = 1, BCMGX/launchAndCompare.mk:136,207). The bcsstk13 / bcsstk24 solution files are all
     zeros (their _aux.txt: FLAG = 1, ITER = 0) and pin nothing, so they are not packed.
 
-Usage: python tests/golden/make_golden.py [REFERENCE_ROOT]
+Usage: python tests/golden/make_golden.py REFERENCE_ROOT
 """
 import os
 import sys
 
 import numpy as np
 
-ROOT = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-DATA = os.path.join(ROOT, "BCMGX", "src", "test", "data")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_fixtures.npz")
+DATA = None
 
 
 def read_mtx(path):
@@ -34,6 +33,10 @@ def read_mtx(path):
 
 
 def main():
+    global DATA
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py REFERENCE_ROOT (the BootCMatchGX source tree)")
+    DATA = os.path.join(sys.argv[1], "BCMGX", "src", "test", "data")
     out = {}
     for st in ("7p", "27p"):
         for grid in ("1x1x1", "2x1x1", "2x2x1", "2x2x2"):

@@ -232,3 +232,88 @@ def test_replica_timing_over_gloo_ranks():
     assert res[0] == (0, 15.0, "rank0") and res[1] == (1, 15.0, None)
     import bench
     assert bench.max_over_ranks(3.5, 1) == 3.5
+
+
+def _shard_rank(rank, world, port, out):
+    """One gloo rank of test_replica_sharding_over_gloo_ranks: solves its share of independent
+    systems and of right-hand-side columns with a stand-in solver (a dense solve on the CPU)."""
+    import datetime
+    import torch.distributed as dist
+    from bootcmatchgx_b200 import replicas
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        rng = np.random.default_rng(11)
+        mats = []
+        for k in range(9):   # uneven systems, the same on every rank
+            m = 3 + k
+            B = rng.uniform(-1, 1, (m, m))
+            mats.append((B @ B.T + m * np.eye(m), rng.uniform(-1, 1, m)))
+        mine = replicas.systems_of_rank(len(mats), rank, world)
+        xs = [np.linalg.solve(*mats[k]) for k in mine]
+        allx = replicas.gather_in_order(xs, mine, len(mats), world)
+        A, _ = mats[-1]
+        Bk = rng.uniform(-1, 1, (A.shape[0], 32))
+        cols = replicas.columns_of_rank(32, rank, world)
+        Xk = np.linalg.solve(A, Bk[:, cols.start:cols.stop])
+        allc = replicas.gather_in_order([Xk[:, j] for j in range(Xk.shape[1])], list(cols), 32, world)
+        out.put((rank, mine, list(cols), [x.tolist() for x in allx], np.stack(allc, axis=1).tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_replica_sharding_over_gloo_ranks():
+    """The batched forms at N > 1: systems go round robin and right-hand-side columns in
+    contiguous slices; every system and column is solved on exactly one rank, and the gathered
+    results equal the single-rank results in the single-rank order (two gloo ranks on CPU)."""
+    import multiprocessing as mp
+    import socket
+    from bootcmatchgx_b200 import replicas
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    world = 2
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    procs = [ctx.Process(target=_shard_rank, args=(r, world, port, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted(out.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert sorted(res[0][1] + res[1][1]) == list(range(9)) and not set(res[0][1]) & set(res[1][1])
+    assert res[0][2] + res[1][2] == list(range(32))
+    rng = np.random.default_rng(11)
+    mats = []
+    for k in range(9):
+        m = 3 + k
+        B = rng.uniform(-1, 1, (m, m))
+        mats.append((B @ B.T + m * np.eye(m), rng.uniform(-1, 1, m)))
+    single = [np.linalg.solve(*mk) for mk in mats]
+    Bk = rng.uniform(-1, 1, (mats[-1][0].shape[0], 32))
+    Xs = np.linalg.solve(mats[-1][0], Bk)
+    for r in res:
+        assert all(np.allclose(a, b, rtol=0, atol=1e-12) for a, b in zip(r[3], single))
+        assert np.allclose(np.array(r[4]), Xs, rtol=0, atol=1e-12)
+    # the split functions on their own: 33 columns over 4 ranks, 10 systems over 3 ranks
+    assert [len(replicas.columns_of_rank(33, r, 4)) for r in range(4)] == [9, 8, 8, 8]
+    assert replicas.systems_of_rank(10, 1, 3) == [1, 4, 7]
+
+
+def test_reference_arm_builds_the_same_problems(bx):
+    """bench.py's reference arm builds its matrices without the product library: the diffusion
+    matrix assembled in numpy equals bcmgx_diffusion_7p bit for bit, and the oracle's Laplacian
+    generator equals the library's."""
+    import bench
+    from oracle import pyoracle as O
+    rng = np.random.default_rng(3)
+    for g in [(5, 4, 3), (7, 7, 7), (1, 2, 9)]:
+        kappa = np.exp(rng.normal(size=int(np.prod(g))))
+        r1, c1, v1 = bx.diffusion_7p(*g, kappa)
+        r2, c2, v2 = bench.diffusion_csr_numpy(*g, kappa)
+        assert np.array_equal(r1, r2) and np.array_equal(c1, c2) and np.array_equal(v1, v2)
+    for st in (7, 27):
+        r1, c1, v1 = bx.laplacian_3d(st, 6, 5, 4)
+        r2, c2, v2 = O.Matrix.lap3d(st, 6, 5, 4).csr()
+        assert np.array_equal(r1, r2) and np.array_equal(c1, c2) and np.array_equal(v1, v2)

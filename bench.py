@@ -19,18 +19,24 @@ slice of the 32 right-hand-side columns (--multi).
 from __future__ import annotations
 
 import os
+import sys
 
-# OpenMP threads of the CPU legs (the oracle) pinned one per core; set before any OpenMP runtime
-# is loaded, since libgomp reads them once.
-os.environ.setdefault("OMP_PROC_BIND", "close")
-os.environ.setdefault("OMP_PLACES", "cores")
+# The host cores this process may run on, read before any OpenMP runtime loads: with thread
+# binding on, libgomp pins the calling thread to one core when it starts.
+HOST_CPUS = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+# The CPU legs (the reference arm, and the CPU baseline, which runs in a child process) pin their
+# OpenMP threads one per core; the GPU arm leaves its host threads unpinned.
+PIN_ENV = {"OMP_PROC_BIND": "close", "OMP_PLACES": "cores"}
+if "--impl=reference" in sys.argv or "--cpu-leg" in sys.argv or (
+        "--impl" in sys.argv and sys.argv[sys.argv.index("--impl") + 1:][:1] == ["reference"]):
+    for _k, _v in PIN_ENV.items():
+        os.environ.setdefault(_k, _v)
 
 import argparse
 import datetime
 import json
 import statistics
 import subprocess
-import sys
 import tempfile
 import threading
 import time
@@ -149,11 +155,7 @@ def host_info():
                     break
     except OSError:
         pass
-    try:
-        avail = len(os.sched_getaffinity(0))
-    except Exception:
-        avail = os.cpu_count() or 1
-    return {"cpu_model": model, "logical_cpus": os.cpu_count(), "cpus_available": avail,
+    return {"cpu_model": model, "logical_cpus": os.cpu_count(), "cpus_available": HOST_CPUS,
             "omp_proc_bind": os.environ.get("OMP_PROC_BIND"), "omp_places": os.environ.get("OMP_PLACES")}
 
 
@@ -215,7 +217,7 @@ def oracle_solve(O, A, b, rtol=RTOL):
     return t1 - t0, t2 - t1, x, info, H.level_sizes()
 
 
-def cpu_baseline(wl, runs=5):
+def cpu_baseline_leg(wl, runs=5):
     """The oracle (OpenMP C++ restatement of the same FCG+BCMG method) on this host's cores,
     threads pinned one per core: `runs` full set-up + solve runs of the same workload, the
     median reported. Also returns the oracle's solution and level sizes for the parity check."""
@@ -234,6 +236,19 @@ def cpu_baseline(wl, runs=5):
             "runs_s": tot, "setup_s": ts, "solve_s": tv, "niter": info["niter"], "host": hi,
             "err_vs_xstar": None if xs is None else float(np.linalg.norm(x - xs) / np.linalg.norm(xs))}
     return line, {"x": x, "niter": info["niter"], "levels": levels}
+
+
+def cpu_baseline(workload, runs=5):
+    """cpu_baseline_leg in a child process (python bench.py --cpu-leg), so that its OpenMP threads
+    are pinned without pinning the GPU arm's host threads; its results come back through a file."""
+    with tempfile.TemporaryDirectory() as td:
+        out = os.path.join(td, "leg.npz")
+        env = dict(os.environ, **PIN_ENV)
+        subprocess.run([sys.executable, os.path.abspath(__file__), "--cpu-leg", out, "--workload", workload,
+                        "--steps", str(runs)], check=True, env=env)
+        z = np.load(out, allow_pickle=False)
+        line = json.loads(str(z["line"]))
+        return line, {"x": z["x"], "niter": int(z["niter"]), "levels": [tuple(t) for t in z["levels"].tolist()]}
 
 
 def reference_arm(a, wl, rank, world):
@@ -937,6 +952,7 @@ def main():
     ap.add_argument("--adjoint", action="store_true", help="run the differentiated-solve configuration instead")
     ap.add_argument("--batch", action="store_true", help="run the batched-systems configuration instead")
     ap.add_argument("--multi", action="store_true", help="run the 32-right-hand-side configuration instead")
+    ap.add_argument("--cpu-leg", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--profile-step", action="store_true",
                     help="only W warm-up steps and one FP32 step (for ncu launch lists); prints the launch counts")
     a = ap.parse_args()
@@ -944,6 +960,10 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     wl = WORKLOADS[a.workload]
+    if a.cpu_leg:   # the CPU baseline's child process (cpu_baseline)
+        line, ora = cpu_baseline_leg(wl, runs=a.steps)
+        np.savez(a.cpu_leg, line=json.dumps(line), x=ora["x"], niter=ora["niter"], levels=np.array(ora["levels"]))
+        return
     if a.impl == "reference":
         line = reference_arm(a, wl, rank, world)
         if line is not None:
@@ -975,7 +995,7 @@ def main():
                 if line is not None:
                     line["secondary"] = sec
             if rank == 0 and world == 1 and not a.no_cpu_baseline:
-                cb, ora = cpu_baseline(wl)
+                cb, ora = cpu_baseline(a.workload)
                 line["cpu_baseline"] = cb
                 x64 = extra["x64"]
                 gl = list(zip(line["breakdown"]["levels"], line["breakdown"]["level_nnz"]))

@@ -108,6 +108,17 @@ SIGNATURES = {
     "bcmgx_last_error_string": (C.c_char_p, []),
     "bcmgx_version": (C.c_char_p, []),
     "bcmgx_launch_count": (C.c_int64, []),
+    "bcmgx_dist_setup_local": (C.c_int, [C.POINTER(Csr), C.c_int, _vp, C.POINTER(Params), C.POINTER(C.c_void_p)]),
+    "bcmgx_dist_setup_nccl": (C.c_int, [C.POINTER(Csr), C.c_int64, C.c_int64, _vp, C.POINTER(Params),
+                                        C.POINTER(C.c_void_p)]),
+    "bcmgx_dist_solve": (C.c_int, [_vp, _vp, _vp, C.c_int, C.POINTER(SolveInfo)]),
+    "bcmgx_dist_get_info": (C.c_int, [_vp, C.POINTER(HierarchyInfo)]),
+    "bcmgx_dist_get_level": (C.c_int, [_vp, C.c_int, _ip, _i64p, _vp, _vp, _vp, _vp]),
+    "bcmgx_dist_get_prolongator": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),
+    "bcmgx_dist_free": (C.c_int, [_vp]),
+    "bcmgx_nccl_unique_id": (C.c_int, [_vp]),
+    "bcmgx_nccl_comm_init": (C.c_int, [C.c_int, C.c_int, _vp, C.POINTER(C.c_void_p)]),
+    "bcmgx_nccl_comm_destroy": (C.c_int, [_vp]),
 }
 
 _lib = None

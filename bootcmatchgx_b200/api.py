@@ -389,6 +389,122 @@ class Batch:
             pass
 
 
+class Dist:
+    """The row-partitioned (multi-rank) set-up and solve: the reference's prec_setup / solve at
+    np > 1, FP64 V-cycle (bcmgx_dist_*).
+
+    Dist.local(row, col, val, offsets, params): all ranks' row blocks in this process on one device
+    (offsets: the ranks' first rows, ending with n). Dist.nccl(row, col, val, row_offset, n_global,
+    comm, nranks, params): this rank's rows (global column ids) on its own GPU, comm from
+    nccl_comm()."""
+
+    def __init__(self, h, params, nrows, nranks):
+        self.h = h
+        self.params = params
+        self.n = nrows
+        self.nranks = nranks
+
+    @classmethod
+    def local(cls, row, col, val, offsets, params):
+        dev = _is_device(row)
+        if not dev:
+            row = np.ascontiguousarray(row, dtype=np.int32)
+            col = np.ascontiguousarray(col, dtype=np.int32)
+            val = np.ascontiguousarray(val, dtype=np.float64)
+        n = int(row.shape[0]) - 1
+        A = L.Csr(n, n, int(col.shape[0]), _ptr(row), _ptr(col), _ptr(val), 1 if dev else 0)
+        off = np.ascontiguousarray(offsets, dtype=np.int64)
+        h = C.c_void_p()
+        check(lib().bcmgx_dist_setup_local(C.byref(A), off.size - 1, _ptr(off), C.byref(params), C.byref(h)),
+              "dist_setup_local")
+        return cls(h, params, n, off.size - 1)
+
+    @classmethod
+    def nccl(cls, row, col, val, row_offset, n_global, comm, nranks, params):
+        dev = _is_device(row)
+        if not dev:
+            row = np.ascontiguousarray(row, dtype=np.int32)
+            col = np.ascontiguousarray(col, dtype=np.int32)
+            val = np.ascontiguousarray(val, dtype=np.float64)
+        n = int(row.shape[0]) - 1
+        A = L.Csr(n, int(n_global), int(col.shape[0]), _ptr(row), _ptr(col), _ptr(val), 1 if dev else 0)
+        h = C.c_void_p()
+        check(lib().bcmgx_dist_setup_nccl(C.byref(A), int(row_offset), int(n_global), comm, C.byref(params),
+                                          C.byref(h)), "dist_setup_nccl")
+        return cls(h, params, n, nranks)
+
+    def solve(self, b, x0=None, raise_on_no_convergence=False):
+        info = L.SolveInfo()
+        if _is_device(b):
+            import torch
+            x = torch.zeros_like(b) if x0 is None else x0
+            rc = lib().bcmgx_dist_solve(self.h, _ptr(b), _ptr(x), 1, C.byref(info))
+        else:
+            b = np.ascontiguousarray(b, dtype=np.float64)
+            x = np.zeros(self.n) if x0 is None else np.array(x0, dtype=np.float64)
+            rc = lib().bcmgx_dist_solve(self.h, _ptr(b), _ptr(x), 0, C.byref(info))
+        if rc != L.OK and (rc != L.ERR_NO_CONVERGENCE or raise_on_no_convergence):
+            raise BcmgxError(rc, "dist solve", L.last_error())
+        return x, {"retv": info.retv, "niter": info.niter, "delta0": info.delta0, "exit_res": info.exit_res,
+                   "solve_ms": info.solve_ms, "status": rc}
+
+    def info(self):
+        inf = L.HierarchyInfo()
+        check(lib().bcmgx_dist_get_info(self.h, C.byref(inf)), "dist_get_info")
+        k = inf.num_levels
+        return {"num_levels": k, "n": list(inf.n[:k]), "nnz": list(inf.nnz[:k]), "op_cmplx": inf.op_cmplx,
+                "maxcoarsesize": inf.maxcoarsesize, "ftcoarse": inf.ftcoarse, "setup_ms": inf.setup_ms}
+
+    def level(self, l):
+        """This process's rows of level l with global column ids, and the level's rank offsets."""
+        rows, nnz = C.c_int(), C.c_int64()
+        check(lib().bcmgx_dist_get_level(self.h, l, C.byref(rows), C.byref(nnz), None, None, None, None),
+              "dist_get_level")
+        row = np.empty(rows.value + 1, np.int32)
+        col = np.empty(nnz.value, np.int32)
+        val = np.empty(nnz.value, np.float64)
+        off = np.empty(self.nranks + 1, np.int64)
+        check(lib().bcmgx_dist_get_level(self.h, l, C.byref(rows), C.byref(nnz), _ptr(row), _ptr(col), _ptr(val),
+                                         _ptr(off)), "dist_get_level")
+        return row, col, val, off
+
+    def prolongator(self, l, rows):
+        agg = np.empty(rows, np.int32)
+        p = np.empty(rows)
+        M = np.empty(rows)
+        check(lib().bcmgx_dist_get_prolongator(self.h, l, _ptr(agg), _ptr(p), _ptr(M)), "dist_get_prolongator")
+        return agg, p, M
+
+    def free(self):
+        if getattr(self, "h", None):
+            check(lib().bcmgx_dist_free(self.h), "dist_free")
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def nccl_unique_id() -> bytes:
+    buf = (C.c_ubyte * 128)()
+    check(lib().bcmgx_nccl_unique_id(buf), "nccl_unique_id")
+    return bytes(buf)
+
+
+def nccl_comm(nranks, rank, uid: bytes):
+    """An NCCL communicator for bcmgx_dist_setup_nccl on the current device."""
+    buf = (C.c_ubyte * 128).from_buffer_copy(uid)
+    c = C.c_void_p()
+    check(lib().bcmgx_nccl_comm_init(nranks, rank, buf, C.byref(c)), "nccl_comm_init")
+    return c
+
+
+def nccl_comm_destroy(comm):
+    check(lib().bcmgx_nccl_comm_destroy(comm), "nccl_comm_destroy")
+
+
 def prec_setup(row, col, val, params) -> Hierarchy:
     return Hierarchy(row, col, val, params)
 

@@ -248,6 +248,32 @@ const char* boot_name(int v);
 
 // ---- set-up (setup.cu) ----
 void build_hierarchy(bcmgx_hierarchy* H, const bcmgx_csr* A);
+// One sweep's matching + pairwise prolongator on a square matrix (see setup.cu).
+struct SweepAgg {
+    DBuf<int> agg, fine0, fine1;
+    DBuf<double> p, wc;
+    int nc = 0;
+};
+void sweep_aggregate(bcmgx_hierarchy* H, const DevCsr& A, const double* w, SweepAgg& out, int level, int sweep,
+    double min_cap);
+// C = P^T A P for the pairwise P given by agg / p over A's columns (coarse ids < ncols) and the fine
+// rows fine0 / fine1 of the nc coarse rows.
+void galerkin_dev(bcmgx_hierarchy* H, const DevCsr& A, const int* agg, const double* p, const int* fine0,
+    const int* fine1, int nc, int ncols, DevCsr& C);
+// Level finishing steps of build_hierarchy: int16 column offsets, divisor M (and the FP32 copies).
+void finish_level_matrix(Level& V, bool want_f32, cudaStream_t s);
+// R = P^T of a level's composite prolongator (agg with nc coarse rows).
+void build_restriction(Level& V, int nc, bool want_f32, cudaStream_t s);
+// P <- P * P_sweep on one-entry-per-row prolongators (first: P = P_sweep).
+void compose_prolongator(int n, int* agg, double* p, const int* agg_s, const double* p_s, bool first, cudaStream_t s);
+// Largest row length of a CSR (device arrays).
+int row_max_dev(int n, const int* row, cudaStream_t s);
+// Exclusive prefix sum on the device; out[n] = total (must fit int32). No host synchronisation.
+void scan_exclusive_dev(const int* in, int* out, long n, cudaStream_t s);
+// The same, returning the 64-bit total (synchronises the stream).
+long long scan_exclusive(const int* in, int* out, long n, bool with_total, cudaStream_t s);
+// Per-row lanes of the setup kernels and a grid-stride grid.
+int setup_grid(long n, int threads = 256);
 
 // ---- solve (solve.cu) ----
 void ensure_solve_workspace(bcmgx_hierarchy* H);
@@ -270,6 +296,17 @@ int multi_solve(bcmgx_hierarchy* H, int K, const double* B, double* X, bcmgx_sol
 // Y = alpha A X + beta Y for row-major n x K blocks on device memory (K <= 32).
 void launch_spmm(int n, int m, int K, const int* row, const int* col, const double* val, const double* X, double* Y,
     double alpha, double beta, cudaStream_t s);
+// FP64 cycle steps of one level on caller-chosen vectors (x may hold halo entries after the
+// level's own rows): one l1-Jacobi sweep, the residual, a sweep from zero, the restriction
+// R res, the prolongation y = x + P xc, and plain copies / zeroing.
+void step_jacobi64(const Level& V, const double* x, const double* f, double* y, cudaStream_t s);
+void step_resid64(const Level& V, const double* x, const double* f, double* y, cudaStream_t s);
+void step_first64(const Level& V, const double* f, double* u, cudaStream_t s);
+void step_restrict64(const Level& V, int nc, const double* res, double* out, cudaStream_t s);
+void step_prolong64(const Level& V, const double* xc, const double* x, double* y, cudaStream_t s);
+void step_copy64(int n, const double* a, double* b, cudaStream_t s);
+void step_zero64(int n, double* a, cudaStream_t s);
+int num_sms();
 void time_level_kernels(bcmgx_hierarchy* H, int l, int reps, double* out);
 void time_block_kernels(bcmgx_hierarchy* H, int K, int reps, double* out);
 double time_block_dots(bcmgx_hierarchy* H, int K, int reps);

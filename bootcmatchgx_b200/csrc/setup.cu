@@ -813,7 +813,7 @@ __global__ void k_galerkin(int nc, const int* __restrict__ rows, const int* __re
     const int* __restrict__ agg, const double* __restrict__ p, const int* __restrict__ Arow, const int* __restrict__ Acol,
     const double* __restrict__ Aval, const int* __restrict__ off, long long out_cap, int* __restrict__ Crow,
     int* __restrict__ Ccol, double* __restrict__ Cval, int cap, int* __restrict__ long_rows, int* __restrict__ nlong,
-    int* __restrict__ long_max, int* err)
+    int* __restrict__ long_max, int* err, int ncols)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int wpb = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -826,7 +826,7 @@ __global__ void k_galerkin(int nc, const int* __restrict__ rows, const int* __re
     unsigned* key32 = (unsigned*)key;
     unsigned* skey32 = key32 + cap;
     double* sval = (double*)(smem + (size_t)wpb * cap * 20) + (size_t)wid * cap;
-    const bool narrow = nc < (1 << 25);
+    const bool narrow = ncols < (1 << 25);   // every J = agg(c) < ncols fits the 32-bit key
     for (long k = (long)blockIdx.x * wpb + wid; k < nc; k += (long)gridDim.x * wpb) {
         const int I = rows ? rows[k] : (int)k;
         const int f0 = fine0[I], f1 = fine1[I];
@@ -1181,8 +1181,10 @@ static int row_max(const DevCsr& A, cudaStream_t s) { return row_max_raw(A.n, A.
 // The inputs of the edge weights: C_r (into C, n doubles), the transposed positions and the
 // substitute log argument SUITOR_EPS / (0.999 min |a_hat|) for a_hat == 0; returns it and, when
 // min_out_host is set, the minimum.
+// min_cap: an upper bound of the minimum (a rank of a row-partitioned set-up that has entries
+// outside its own columns takes 99999, makeAH's value for them, into its minimum).
 static double edge_prep_dev(int n, int64_t nnz, const int* row, const int* col, const double* val, const double* w,
-    double* C, int* tpos, double* min_out_host, cudaStream_t s)
+    double* C, int* tpos, double* min_out_host, cudaStream_t s, double min_cap = DBL_MAX)
 {
     DBuf<unsigned long long> mn;
     DBuf<int> err;
@@ -1200,6 +1202,7 @@ static double edge_prep_dev(int n, int64_t nnz, const int* row, const int* col, 
     BCMGX_CUDA(cudaMemcpyAsync(&m, mn.p, sizeof(double), cudaMemcpyDeviceToHost, s));
     int e = read_err(err.p, s);
     if (e) throw Error(BCMGX_ERR_INVALID_INPUT, "edge weights: " + err_text(e));
+    m = std::min(m, min_cap);
     if (std::fabs(m) < DBL_EPSILON) m = DBL_EPSILON;   // toMaximumProductMatrix, matching.cu:243-245
     if (min_out_host) *min_out_host = m;
     return kSuitorEps / (0.999 * m);
@@ -1306,7 +1309,12 @@ struct SweepOut {
     int nc = 0;
 };
 
-static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w, SweepOut& out, int level, int sweep)
+// The matching and the pairwise prolongator of one sweep on the square matrix A with weights w:
+// agg/p per row of A (aggregate ids 0..nc-1, pairs by master then singletons), the fine rows of
+// every aggregate (fine0, fine1; -1 for a singleton) and the coarse weights wc = R w. min_cap
+// bounds the edge weights' minimum (edge_prep_dev).
+void sweep_aggregate(bcmgx_hierarchy* H, const DevCsr& A, const double* w, SweepAgg& out, int level, int sweep,
+    double min_cap)
 {
     cudaStream_t s = H->stream;
     const int n = A.n;
@@ -1325,7 +1333,7 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
         FusedWeights fw;
         {
             PhaseTimer pt(H, "weights");
-            fw.zero_sub = edge_prep_dev(n, nnz, A.row.p, A.col.p, A.val.p, w, Cd.p, tpos.p, nullptr, s);
+            fw.zero_sub = edge_prep_dev(n, nnz, A.row.p, A.col.p, A.val.p, w, Cd.p, tpos.p, nullptr, s, min_cap);
         }
         fw.val = A.val.p;
         fw.w = w;
@@ -1336,12 +1344,17 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
         W.alloc(std::max<int64_t>(nnz, 1), s);
         {
             PhaseTimer pt(H, "weights");
-            edge_weights_dev(n, nnz, A.row.p, A.col.p, A.val.p, w, W.p, tpos.p, nullptr, s);
+            DBuf<double> C;
+            C.alloc(n, s);
+            const double zero_sub = edge_prep_dev(n, nnz, A.row.p, A.col.p, A.val.p, w, C.p, tpos.p, nullptr, s, min_cap);
+            BCMGX_SUBWARP_LAUNCH(k_logw, setup_subwarp(n, nnz), n, s, n, A.row.p, A.col.p, A.val.p, w, C.p, tpos.p,
+                zero_sub, W.p);
+            BCMGX_CHECK_LAUNCH();
         }
         PhaseTimer pt(H, "suitor");
         suitor_dev(n, nnz, A.row.p, A.col.p, W.p, tpos.p, M.p, amax0, s, nullptr, err.p);
     }
-    PhaseTimer pt_p(H, "makeP+galerkin");
+    PhaseTimer pt_p(H, "makeP");
     W.release();
     Cd.release();
     tpos.release();
@@ -1365,13 +1378,12 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
     const long long npairs = th[0], nsing = th[1];
     const int nc = (int)(npairs + nsing);
     out.nc = nc;
-    DBuf<int> fine0, fine1;
     out.agg.alloc(n, s);
     out.p.alloc(n, s);
     out.wc.alloc(nc, s);
-    fine0.alloc(nc, s);
-    fine1.alloc(nc, s);
-    note_launch(); k_make_p<<<gs_grid(n), 256, 0, s>>>(n, M.p, w, fm.p, pofs.p, sofs.p, (int)npairs, out.agg.p, out.p.p, fine0.p, fine1.p, out.wc.p);
+    out.fine0.alloc(nc, s);
+    out.fine1.alloc(nc, s);
+    note_launch(); k_make_p<<<gs_grid(n), 256, 0, s>>>(n, M.p, w, fm.p, pofs.p, sofs.p, (int)npairs, out.agg.p, out.p.p, out.fine0.p, out.fine1.p, out.wc.p);
     BCMGX_CHECK_LAUNCH();
     if (H->prm.record_sweeps) {
         SweepRecord r;
@@ -1390,32 +1402,40 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
         BCMGX_CUDA(cudaStreamSynchronize(s));
         H->rec.push_back(std::move(r));
     }
-    M.release();
-    fm.release();
-    fs.release();
-    pofs.release();
-    sofs.release();
-    // Galerkin: each coarse row's candidate count (the entries of its fine rows) and their prefix
-    // sum, which places the row's output (the counts add up to nnz(A), so the scratch is nnz(A)
-    // entries whatever the row lengths); the product of the rows that fit kGalCap candidates per
-    // warp, then of the longer ones (listed by the first launch) with one warp per block and shared
+}
+
+// The Galerkin product C = P^T A P of one sweep: A's rows (columns < A.m), agg/p indexed by A's
+// columns with coarse ids < ncols, fine0/fine1 the fine rows of the nc coarse rows of C (rows of
+// A). C has nc rows whose columns are agg ids, sorted, and ncols columns.
+void galerkin_dev(bcmgx_hierarchy* H, const DevCsr& A, const int* agg, const double* p, const int* fine0,
+    const int* fine1, int nc, int ncols, DevCsr& C)
+{
+    cudaStream_t s = H->stream;
+    PhaseTimer pt_g(H, "galerkin");
+    DBuf<int> err;
+    err.alloc(1, s);
+    BCMGX_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), s));
+    // each coarse row's candidate count (the entries of its fine rows) and their prefix sum, which
+    // places the row's output (the counts add up to nnz(A), so the scratch is nnz(A) entries
+    // whatever the row lengths); the product of the rows that fit kGalCap candidates per warp,
+    // then of the longer ones (listed by the first launch) with one warp per block and shared
     // memory for the longest; then compaction.
     const int amax = A.max_row > 0 ? A.max_row : row_max(A, s);
     constexpr int kGalCap = 512;
     constexpr size_t kGalBytes = 28;   // shared-memory bytes per candidate (keys, products, sort)
     const size_t smem_limit = 200 * 1024;
     const int cap1 = std::min(std::max(2 * amax, 32), kGalCap);
-    DevCsr& C = out.C;
-    C.n = C.m = nc;
+    C.n = nc;
+    C.m = ncols;
     C.row.alloc((size_t)nc + 1, s);
     DBuf<int> cand, off, counts, pcol, longr, lstat;
     DBuf<double> pval;
     cand.alloc(std::max(nc, 1), s);
     off.alloc((size_t)nc + 1, s);
-    note_launch(); k_galerkin_counts<<<gs_grid(nc), 256, 0, s>>>(nc, fine0.p, fine1.p, A.row.p, cand.p);
+    note_launch(); k_galerkin_counts<<<gs_grid(nc), 256, 0, s>>>(nc, fine0, fine1, A.row.p, cand.p);
     BCMGX_CHECK_LAUNCH();
-    // the candidates of all coarse rows are the entries of A (every fine row is in one aggregate);
-    // k_galerkin checks each row's range against that before writing
+    // the candidates of all coarse rows are entries of A (every row of A is in at most one
+    // aggregate); k_galerkin checks each row's range against that before writing
     scan_exclusive_dev(cand.p, off.p, nc, s);
     const long long total = A.nnz;
     cand.release();
@@ -1437,8 +1457,9 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
         ensure_smem_limit(k_galerkin, smem);
         const int g = (int)std::max<long>(1, std::min<long>(((long)nrows + wpb - 1) / wpb, (long)num_sms() * 32));
         note_launch();
-        k_galerkin<<<g, wpb * 32, smem, s>>>(nrows, rows, fine0.p, fine1.p, out.agg.p, out.p.p, A.row.p, A.col.p,
-            A.val.p, off.p, (long long)total, counts.p, pcol.p, pval.p, cap, list, stat, stat ? stat + 1 : nullptr, err.p);
+        k_galerkin<<<g, wpb * 32, smem, s>>>(nrows, rows, fine0, fine1, agg, p, A.row.p, A.col.p,
+            A.val.p, off.p, (long long)total, counts.p, pcol.p, pval.p, cap, list, stat, stat ? stat + 1 : nullptr, err.p,
+            ncols);
         BCMGX_CHECK_LAUNCH();
     };
     auto read2 = [&](const int* d, int (&h)[2]) {
@@ -1470,7 +1491,7 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
                 cnt3.alloc(n3, s);
                 seg.alloc((size_t)n3 + 1, s);
                 note_launch();
-                k_galerkin_list_counts<<<gs_grid(n3), 256, 0, s>>>(n3, longr2.p, fine0.p, fine1.p, A.row.p, cnt3.p);
+                k_galerkin_list_counts<<<gs_grid(n3), 256, 0, s>>>(n3, longr2.p, fine0, fine1, A.row.p, cnt3.p);
                 BCMGX_CHECK_LAUNCH();
                 const long long total3 = scan_exclusive(cnt3.p, seg.p, n3, true, s);
                 DBuf<unsigned long long> k_in, k_out;
@@ -1481,7 +1502,7 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
                 v_out.alloc((size_t)total3, s);
                 const int g3 = std::min(n3, num_sms() * 4);
                 note_launch();
-                k_galerkin_long_fill<<<g3, 256, 0, s>>>(n3, longr2.p, fine0.p, fine1.p, out.agg.p, out.p.p, A.row.p,
+                k_galerkin_long_fill<<<g3, 256, 0, s>>>(n3, longr2.p, fine0, fine1, agg, p, A.row.p,
                     A.col.p, A.val.p, seg.p, k_in.p, v_in.p);
                 BCMGX_CHECK_LAUNCH();
                 size_t tmp_bytes = 0;
@@ -1492,8 +1513,8 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
                 BCMGX_CUDA(cub::DeviceSegmentedSort::SortPairs(tmp.p, tmp_bytes, k_in.p, k_out.p, v_in.p, v_out.p,
                     (int)total3, n3, seg.p, seg.p + 1, s));
                 note_launch();
-                k_galerkin_long_rows<<<std::min(n3, num_sms() * 2), 1024, 0, s>>>(n3, longr2.p, fine0.p, fine1.p,
-                    out.p.p, seg.p, k_out.p, v_out.p, off.p, counts.p, pcol.p, pval.p);
+                k_galerkin_long_rows<<<std::min(n3, num_sms() * 2), 1024, 0, s>>>(n3, longr2.p, fine0, fine1,
+                    p, seg.p, k_out.p, v_out.p, off.p, counts.p, pcol.p, pval.p);
                 BCMGX_CHECK_LAUNCH();
             }
         }
@@ -1510,7 +1531,7 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
         BCMGX_CHECK_LAUNCH();
     }
     long long cnnz = 0;
-    int cmax = 0;
+    int cmax = 0, e = 0;
     BCMGX_CUDA(cudaMemcpyAsync(&cnnz, ctot.p, sizeof(long long), cudaMemcpyDeviceToHost, s));
     BCMGX_CUDA(cudaMemcpyAsync(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     BCMGX_CUDA(cudaMemcpyAsync(&cmax, cmx.p, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1523,6 +1544,18 @@ static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w,
     note_launch(); k_compact_rows<<<warp_grid(nc), 256, 0, s>>>(nc, off.p, C.row.p, pcol.p, pval.p, C.col.p, C.val.p);
     BCMGX_CHECK_LAUNCH();
     C.max_row = cmax;
+}
+
+static void pairwise_sweep(bcmgx_hierarchy* H, const DevCsr& A, const double* w, SweepOut& out, int level, int sweep)
+{
+    SweepAgg ag;
+    sweep_aggregate(H, A, w, ag, level, sweep, DBL_MAX);
+    galerkin_dev(H, A, ag.agg.p, ag.p.p, ag.fine0.p, ag.fine1.p, ag.nc, ag.nc, out.C);
+    out.C.m = out.C.n;
+    out.nc = ag.nc;
+    out.agg = std::move(ag.agg);
+    out.p = std::move(ag.p);
+    out.wc = std::move(ag.wc);
 }
 
 // Largest |col - row| of the matrix (atomicMax of per-thread maxima).
@@ -1560,7 +1593,7 @@ static void build_offsets(DevCsr& A, cudaStream_t s)
     BCMGX_CHECK_LAUNCH();
 }
 
-static void finish_level_matrix(Level& V, bool want_f32, cudaStream_t s)
+void finish_level_matrix(Level& V, bool want_f32, cudaStream_t s)
 {
     const int n = V.A.n;
     build_offsets(V.A, s);
@@ -1574,7 +1607,7 @@ static void finish_level_matrix(Level& V, bool want_f32, cudaStream_t s)
     BCMGX_CHECK_LAUNCH();
 }
 
-static void build_restriction(Level& V, int nc, bool want_f32, cudaStream_t s)
+void build_restriction(Level& V, int nc, bool want_f32, cudaStream_t s)
 {
     const int n = V.A.n;
     DBuf<int> cnt, fillpos;
@@ -1597,6 +1630,17 @@ static void build_restriction(Level& V, int nc, bool want_f32, cudaStream_t s)
     note_launch(); k_sort_rrows<<<gs_grid(nc), 256, 0, s>>>(nc, V.rptr.p, V.ridx.p, V.p.p, V.rval.p, want_f32 ? V.rval32.p : nullptr);
     BCMGX_CHECK_LAUNCH();
 }
+
+void compose_prolongator(int n, int* agg, double* p, const int* agg_s, const double* p_s, bool first, cudaStream_t s)
+{
+    note_launch();
+    k_compose<<<gs_grid(n), 256, 0, s>>>(n, agg, p, agg_s, p_s, first ? 1 : 0);
+    BCMGX_CHECK_LAUNCH();
+}
+
+int row_max_dev(int n, const int* row, cudaStream_t s) { return row_max_raw(n, row, s); }
+
+int setup_grid(long n, int threads) { return gs_grid(n, threads); }
 
 // AMG::ApplyData::setGridSweeps (AMG.cu:306-331).
 static std::vector<int> grid_sweeps(int cycle_type, int max_levels)
@@ -1685,8 +1729,7 @@ void build_hierarchy(bcmgx_hierarchy* H, const bcmgx_csr* Ain)
             const double size_precoarse = Ai_->n, size_coarse = cur.nc;
             const double coarse_ratio = size_precoarse / size_coarse;
             if (coarse_ratio <= kCoarseRatioThreshold) H->ftcoarse = kFtcoarseInc;
-            note_launch(); k_compose<<<gs_grid(nfine), 256, 0, s>>>(nfine, Pagg.p, Pval.p, cur.agg.p, cur.p.p, i == 0 ? 1 : 0);
-            BCMGX_CHECK_LAUNCH();
+            compose_prolongator(nfine, Pagg.p, Pval.p, cur.agg.p, cur.p.p, i == 0, s);
             if (size_coarse <= (double)H->ftcoarse * H->maxcoarsesize || i + 1 == sweepnumber) break;
             prev = std::move(cur);
             cur = SweepOut();

@@ -811,6 +811,60 @@ void prec_apply_dev(bcmgx_hierarchy* H, const double* r, double* v)
 }
 
 // ------------------------------------------------------------------------------------------
+// FP64 cycle steps on caller-chosen vectors (the row-partitioned cycle, dist.cu)
+// ------------------------------------------------------------------------------------------
+void step_jacobi64(const Level& V, const double* x, const double* f, double* y, cudaStream_t s)
+{
+    launch_rowop_A<OP_JACOBI>(V.A.tpr, V.A, V.A.val.p, x, f, V.M.p, y, 1.0, 0.0, nullptr, s);
+}
+
+void step_resid64(const Level& V, const double* x, const double* f, double* y, cudaStream_t s)
+{
+    launch_rowop_A<OP_RESID>(V.A.tpr, V.A, V.A.val.p, x, f, (const double*)nullptr, y, 1.0, 0.0, nullptr, s);
+}
+
+void step_first64(const Level& V, const double* f, double* u, cudaStream_t s)
+{
+    const int n = V.A.n;
+    if (n <= 0) return;
+    auto k = k_first_sweep<double, double, double, double>;
+    note_launch();
+    k<<<ew_grid(k, n), 256, 0, s>>>(n, f, V.M.p, u, (double*)nullptr, nullptr);
+    BCMGX_CHECK_LAUNCH();
+}
+
+void step_restrict64(const Level& V, int nc, const double* res, double* out, cudaStream_t s)
+{
+    if (nc <= 0) return;
+    auto k = k_restrict<double, double, double>;
+    note_launch();
+    k<<<ew_grid(k, nc), 256, 0, s>>>(nc, V.rptr.p, V.ridx.p, V.rval.p, res, out, nullptr);
+    BCMGX_CHECK_LAUNCH();
+}
+
+void step_prolong64(const Level& V, const double* xc, const double* x, double* y, cudaStream_t s)
+{
+    const int n = V.A.n;
+    if (n <= 0) return;
+    auto k = k_prolong<double, double, double, double>;
+    note_launch();
+    k<<<ew_grid(k, n), 256, 0, s>>>(n, V.agg.p, V.p.p, xc, x, y, nullptr);
+    BCMGX_CHECK_LAUNCH();
+}
+
+void step_copy64(int n, const double* a, double* b, cudaStream_t s)
+{
+    if (n <= 0 || a == b) return;
+    BCMGX_CUDA(cudaMemcpyAsync(b, a, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+}
+
+void step_zero64(int n, double* a, cudaStream_t s)
+{
+    if (n <= 0) return;
+    BCMGX_CUDA(cudaMemsetAsync(a, 0, sizeof(double) * n, s));
+}
+
+// ------------------------------------------------------------------------------------------
 // FCG kernels
 // ------------------------------------------------------------------------------------------
 constexpr int kRedBlocksPerSM = 8;

@@ -213,6 +213,53 @@ int bcmgx_batch_get_hierarchy(bcmgx_batch* B, int k, bcmgx_hierarchy** h);
 int bcmgx_batch_solve(bcmgx_batch* B, const double* const* b, double* const* x, bcmgx_solve_info* infos);
 int bcmgx_batch_free(bcmgx_batch* B);
 
+/* ---- row-partitioned multi-rank set-up and solve ------------------------------------------ */
+/* The reference's np > 1 path: prec_setup / solve with the matrix split by rows over nranks ranks
+ * (rank r holds rows offs[r] .. offs[r+1]-1 with global column ids; BCMGX/src/utility/
+ * distribuite.cu, row_shift in CSR.h:173-176). Matching and aggregation are rank-local
+ * (suitor.cu:95-100 skips other ranks' columns; makeAH writes 99999 for them, matching.cu:82-85;
+ * each rank numbers its own aggregates after the lower ranks', matchingPairAggregation.cu:188-222);
+ * every SpMV and l1-Jacobi sweep first brings the other ranks' entries of x that the local rows
+ * use (the halo exchange, halo_communication/halo_communication.cu, CSR.cu:829-985,
+ * l1jacobi.cu:94-342); the Galerkin product brings the prolongator rows of those columns
+ * (spspmpi.cu:770-1120); FCG sums its dot products over ranks (triple_inner_product.cu:80-91).
+ * The V-cycle runs in FP64 (the reference's arithmetic).
+ * Two transports:
+ *  - bcmgx_dist_setup_local: all nranks row blocks in this process on one device, the exchanges
+ *    as device copies between the blocks' buffers and the sums over ranks as one small kernel;
+ *  - bcmgx_dist_setup_nccl: one row block per process (one GPU each), exchanges as grouped
+ *    ncclSend / ncclRecv and sums as ncclAllReduce on the hierarchy's stream; the communicator
+ *    comes from bcmgx_nccl_comm_init. NCCL (libnccl.so.2) is loaded when first needed. */
+typedef struct bcmgx_dist bcmgx_dist;
+/* A: the whole matrix (host or device arrays); offs: nranks + 1 row offsets, offs[0] = 0,
+ * offs[nranks] = A->n, every block non-empty. */
+int bcmgx_dist_setup_local(const bcmgx_csr* A, int nranks, const int64_t* offs, const bcmgx_params* p,
+    bcmgx_dist** out);
+/* A_rows: this rank's rows (A_rows->n rows, A_rows->m = n_global columns, global column ids);
+ * row_offset: the global id of its first row; ranks hold consecutive blocks in rank order. */
+int bcmgx_dist_setup_nccl(const bcmgx_csr* A_rows, int64_t row_offset, int64_t n_global, void* nccl_comm,
+    const bcmgx_params* p, bcmgx_dist** out);
+/* FCG + the partitioned V-cycle. b, x: the rows this process holds (all rows in the local form,
+ * this rank's block with NCCL); x holds x0 on entry and the solution on return. */
+int bcmgx_dist_solve(bcmgx_dist* D, const double* b, double* x, int on_device, bcmgx_solve_info* info);
+/* Global level sizes (n, nnz summed over ranks) and the hierarchy statistics. */
+int bcmgx_dist_get_info(const bcmgx_dist* D, bcmgx_hierarchy_info* info);
+/* The rows of level l that this process holds (all of them in the local form), with global
+ * column ids: *rows and *nnz are set, and the arrays that are not NULL are filled (row: rows + 1
+ * offsets). offs (nranks + 1 entries, may be NULL) receives the level's row partition. */
+int bcmgx_dist_get_level(const bcmgx_dist* D, int l, int* rows, int64_t* nnz, int* row, int* col, double* val,
+    int64_t* offs);
+/* The composite prolongator of level l on this process's rows: global aggregate ids, values,
+ * and the l1-Jacobi divisor M. */
+int bcmgx_dist_get_prolongator(const bcmgx_dist* D, int l, int* agg, double* p, double* M);
+int bcmgx_dist_free(bcmgx_dist* D);
+/* NCCL plumbing for bcmgx_dist_setup_nccl: a unique id (128 bytes) made on one rank and shared
+ * with the others by the caller, the communicator of nranks ranks on the current device, and its
+ * release. */
+int bcmgx_nccl_unique_id(unsigned char* id128);
+int bcmgx_nccl_comm_init(int nranks, int rank, const unsigned char* id128, void** comm);
+int bcmgx_nccl_comm_destroy(void* comm);
+
 /* ---- kernels on caller-owned device memory ------------------------------------------------ */
 /* y = alpha * A x + beta * y on device pointers (driverSpMV, driverSpMV.cu:219-235; kernel
  * CSRm::CSRVector_product_adaptive_miniwarp_witho, CSR.cu:829-846). threads_per_row = 0 picks

@@ -75,6 +75,7 @@ struct Params {
 
 struct Level {
     Csr A;
+    std::vector<int> part;    // row partition over ranks: part[r] .. part[r+1]-1 (np = P set-ups)
     std::vector<double> M;    // absolute row sums (l1-Jacobi divisor)
     std::vector<int> agg;     // composite prolongator to the next level: column of row i
     std::vector<double> p;    // composite prolongator value of row i
@@ -417,6 +418,144 @@ int make_pairwise_p(const std::vector<int>& M, const std::vector<double>& w, std
     return nc;
 }
 
+// ---- the row-partitioned (np = P) set-up --------------------------------------------------
+// At np > 1 every rank holds a block of consecutive rows with global column ids; the matching
+// sees only the rank's own columns. The restatement below runs the P ranks' set-ups together on
+// the global matrix:
+//  * makeAH (matching.cu:66-111) writes 99999 for an entry whose column lies outside the rank's
+//    rows, and toMaximumProductMatrix (matching.cu:231-251) takes the absolute minimum over the
+//    rank's AH without any reduction over ranks: every block has its own minimum, over its
+//    within-block |a_hat| and the 99999 of its cross-block entries;
+//  * _write_T_warp (matching.cu:29-64) and find_Candidate (suitor.cu:95-100) skip columns outside
+//    the rank's rows: cross-block entries get weight 0 here, which the matching never proposes;
+//  * makeP_GPU (matchingPairAggregation.cu:109-170) numbers each rank's aggregates locally (pairs
+//    by master, then singletons) and matchingPairAggregation shifts them by the ranks' coarse
+//    offsets (matchingPairAggregation.cu:188-222): block b's aggregates follow block b-1's.
+// Everything else of the set-up and the whole solve is the same arithmetic as at np = 1 (halo
+// exchanges bring remote values; sizes and coarsening tests use the global counts, full_n).
+
+// block of every row of a partition (offsets part[0] = 0 < ... < part[P] = n)
+std::vector<int> block_of_rows(const std::vector<int>& part)
+{
+    std::vector<int> b(part.back());
+    for (size_t k = 0; k + 1 < part.size(); k++)
+        for (int r = part[k]; r < part[k + 1]; r++) b[r] = (int)k;
+    return b;
+}
+
+void edge_weights_parts(const Csr& A, const std::vector<double>& w, const std::vector<int>& part, std::vector<double>& W)
+{
+    const int n = A.n;
+    const int P = (int)part.size() - 1;
+    const std::vector<int> blk = block_of_rows(part);
+    std::vector<double> C(n, 0.0);
+    for (int r = 0; r < n; r++)
+        for (int j = A.row[r]; j < A.row[r + 1]; j++)
+            if (A.col[j] == r) {
+                C[r] = A.val[j] * w[r] * w[r];
+                break;
+            }
+    W.assign(A.nnz(), 0.0);
+    std::vector<double> mn(P, DBL_MAX);
+    for (int r = 0; r < n; r++) {
+        const int b = blk[r];
+        for (int j = A.row[r]; j < A.row[r + 1]; j++) {
+            int c = A.col[j];
+            if (c == r) continue;
+            if (blk[c] != b) {
+                mn[b] = std::min(mn[b], 99999.0);
+                continue;
+            }
+            double a = A.val[j];
+            double norm = C[r] + C[c];
+            double ah;
+            if (norm > DBL_EPSILON) {
+                double wt = w[r] * w[c];
+                ah = 1.0 - ((2.0 * a * wt) / norm);
+            } else {
+                ah = DBL_EPSILON;
+            }
+            W[j] = ah;
+            mn[b] = std::min(mn[b], std::fabs(ah));
+        }
+    }
+    for (int b = 0; b < P; b++)
+        if (std::fabs(mn[b]) < DBL_EPSILON) mn[b] = DBL_EPSILON;
+    for (int r = 0; r < n; r++) {
+        const double zero_sub = kSuitorEps / (0.999 * mn[blk[r]]);
+        for (int j = A.row[r]; j < A.row[r + 1]; j++) {
+            const int c = A.col[j];
+            if (c == r || blk[c] != blk[r]) continue;
+            double s = std::fabs(W[j]);
+            W[j] = std::log(s != 0.0 ? s : zero_sub);
+        }
+    }
+    std::vector<double> Wu(W);
+    for (int r = 0; r < n; r++) {
+        for (int j = A.row[r]; j < A.row[r + 1]; j++) {
+            int c = A.col[j];
+            if (c >= r) break;
+            if (blk[c] != blk[r]) continue;
+            const int* b = A.col.data() + A.row[c];
+            const int* e = A.col.data() + A.row[c + 1];
+            const int* f = std::lower_bound(b, e, r);
+            if (f != e && *f == r) W[j] = Wu[A.row[c] + (f - b)];
+        }
+    }
+}
+
+// make_pairwise_p block by block: block b's pairs (by master), then its singletons, numbered from
+// the sum of the earlier blocks' aggregate counts; coarse_part receives the coarse partition.
+int make_pairwise_p_parts(const std::vector<int>& M, const std::vector<double>& w, const std::vector<int>& part,
+    std::vector<int>& agg, std::vector<double>& p, std::vector<int>& fine0, std::vector<int>& fine1,
+    std::vector<int>& coarse_part)
+{
+    const int n = (int)M.size();
+    agg.assign(n, -1);
+    p.assign(n, 0.0);
+    coarse_part.assign(1, 0);
+    int nc = 0;
+    for (size_t b = 0; b + 1 < part.size(); b++) {
+        const int r0 = part[b], r1 = part[b + 1];
+        for (int v = r0; v < r1; v++) {
+            int u = M[v];
+            if (u >= 0 && v < u) {
+                double wv = w[v], wu = w[u];
+                double nrm = std::sqrt(wv * wv + wu * wu);
+                if (nrm > DBL_EPSILON) {
+                    agg[v] = agg[u] = nc++;
+                    p[v] = wv / nrm;
+                    p[u] = wu / nrm;
+                }
+            }
+        }
+        std::vector<int> bad;
+        for (int v = r0; v < r1; v++) {
+            if (agg[v] >= 0) continue;
+            if (std::fabs(w[v]) > DBL_EPSILON) {
+                agg[v] = nc++;
+                p[v] = w[v] / std::fabs(w[v]);
+            } else {
+                bad.push_back(v);
+            }
+        }
+        for (int v : bad) {
+            agg[v] = nc > coarse_part.back() ? nc - 1 : nc;
+            p[v] = 0.0;
+        }
+        if (nc == coarse_part.back() && !bad.empty()) nc++;
+        coarse_part.push_back(nc);
+    }
+    fine0.assign(nc, -1);
+    fine1.assign(nc, -1);
+    for (int v = 0; v < n; v++) {
+        int c = agg[v];
+        if (fine0[c] < 0) fine0[c] = v;
+        else if (fine1[c] < 0) fine1[c] = v;
+    }
+    return nc;
+}
+
 // Galerkin product C = P^T A P for a pairwise P. Restates the two nsparse products of
 // matchingAggregation.cu:128-131 (AP = A*P, then R*AP) as nsparse evaluates them: every
 // product a*b is rounded, then accumulated into a zero-initialised slot
@@ -739,7 +878,8 @@ Csr transpose(const Csr& G)
 // matchingAggregation (matchingAggregation.cu:106-269), with the parameters of
 // AMG::BootBuildData::initByParams (AMG.cu:366-388): sweepnumber = aggrsweeps+1, w = 1,
 // maxcoarsesize = (int)(40 * n^(1/3)) (AMG.cu:238-241).
-Hierarchy* build(const Csr& A0, const Params& prm, bool record)
+// part0: the row partition of A0 over P ranks (offsets, P + 1 entries), or empty for np = 1.
+Hierarchy* build(const Csr& A0, const Params& prm, bool record, const std::vector<int>& part0 = {})
 {
     Hierarchy* H = new Hierarchy();
     H->prm = prm;
@@ -747,6 +887,8 @@ Hierarchy* build(const Csr& A0, const Params& prm, bool record)
     H->grid_sweeps = grid_sweeps(prm.cycle_type, prm.max_levels);
     H->lv.emplace_back();
     H->lv[0].A = A0;
+    const bool parts = part0.size() > 2;
+    H->lv[0].part = part0.empty() ? std::vector<int> { 0, A0.n } : part0;
     H->lv[0].M = abs_row_sum(A0);
     if (prm.preconditioner == 1) {
         // set_l1j (l1jacobi.cu:484-493): mydiag + addAbsoluteRowSumNoDiag
@@ -777,13 +919,21 @@ Hierarchy* build(const Csr& A0, const Params& prm, bool record)
         std::vector<int> Pagg;
         std::vector<double> Pval;
         Csr Ai;
+        std::vector<int> part_i = H->lv[level - 1].part, part_c;
         for (int i = 0; i < sweepnumber; i++) {
             std::vector<double> W;
-            edge_weights(*Ai_, wi_, W, nullptr);
+            if (parts) edge_weights_parts(*Ai_, wi_, part_i, W);
+            else edge_weights(*Ai_, wi_, W, nullptr);
             std::vector<int> M = match_suitor(*Ai_, W);
             std::vector<int> agg, f0, f1;
             std::vector<double> p;
-            int nc = make_pairwise_p(M, wi_, agg, p, f0, f1);
+            int nc;
+            if (parts) {
+                nc = make_pairwise_p_parts(M, wi_, part_i, agg, p, f0, f1, part_c);
+            } else {
+                nc = make_pairwise_p(M, wi_, agg, p, f0, f1);
+                part_c = { 0, nc };
+            }
             if (record) H->rec.push_back({ level - 1, i, nc, M, agg, p, wi_ });
             Ai = galerkin_pairwise(*Ai_, agg, p, f0, f1, nc);
             wi = restrict_weights(wi_, p, f0, f1);
@@ -804,6 +954,7 @@ Hierarchy* build(const Csr& A0, const Params& prm, bool record)
             Ai_own = std::move(Ai);
             Ai_ = &Ai_own;
             wi_ = wi;
+            part_i = part_c;
         }
         w = wi;
         Level& prev = H->lv[level - 1];
@@ -813,6 +964,7 @@ Hierarchy* build(const Csr& A0, const Params& prm, bool record)
         build_restriction(prev, nc);
         Level nl;
         nl.A = std::move(Ai);
+        nl.part = part_c;
         nl.M = abs_row_sum(nl.A);
         H->lv.push_back(std::move(nl));
         double size_coarse = H->lv[level].A.n;
@@ -1434,6 +1586,20 @@ void orc_match(void* h, const double* W, int method, int* M)
 void* orc_setup(void* h, const orc_params* p, int record)
 {
     return build(*(Csr*)h, to_params(p), record != 0);
+}
+
+// The set-up of the reference run on nparts ranks, rank k holding rows part[k] .. part[k+1]-1.
+void* orc_setup_parts(void* h, const orc_params* p, int record, int nparts, const int* part)
+{
+    return build(*(Csr*)h, to_params(p), record != 0, std::vector<int>(part, part + nparts + 1));
+}
+
+// Row partition of level l (nparts + 1 offsets).
+int orc_hier_level_parts(void* h, int l, int* part)
+{
+    const std::vector<int>& pt = ((Hierarchy*)h)->lv[l].part;
+    if (part) std::copy(pt.begin(), pt.end(), part);
+    return (int)pt.size() - 1;
 }
 
 void orc_hier_free(void* h) { delete (Hierarchy*)h; }

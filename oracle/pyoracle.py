@@ -60,6 +60,10 @@ def lib():
         L.orc_match.argtypes = [vp, vp, C.c_int, vp]
         L.orc_setup.restype = vp
         L.orc_setup.argtypes = [vp, C.POINTER(OrcParams), C.c_int]
+        L.orc_setup_parts.restype = vp
+        L.orc_setup_parts.argtypes = [vp, C.POINTER(OrcParams), C.c_int, C.c_int, vp]
+        L.orc_hier_level_parts.restype = C.c_int
+        L.orc_hier_level_parts.argtypes = [vp, C.c_int, vp]
         L.orc_hier_free.argtypes = [vp]
         L.orc_hier_levels.argtypes = [vp]
         L.orc_hier_stats.argtypes = [vp, vp]
@@ -173,9 +177,22 @@ class Matrix:
 
 
 class Hierarchy:
-    def __init__(self, A: Matrix, prm: OrcParams, record=False):
+    """The oracle's set-up. parts: row offsets of the ranks (P + 1 entries, from 0 to n) for the
+    reference's np = P set-up (rank-local matching and aggregate numbering), or None for np = 1."""
+
+    def __init__(self, A: Matrix, prm: OrcParams, record=False, parts=None):
         self.A = A
-        self.h = lib().orc_setup(A.h, C.byref(prm), 1 if record else 0)
+        if parts is None:
+            self.h = lib().orc_setup(A.h, C.byref(prm), 1 if record else 0)
+        else:
+            pt = np.ascontiguousarray(parts, dtype=np.int32)
+            self.h = lib().orc_setup_parts(A.h, C.byref(prm), 1 if record else 0, pt.size - 1, _p(pt))
+
+    def level_parts(self, l):
+        k = lib().orc_hier_level_parts(self.h, l, None)
+        pt = np.empty(k + 1, np.int32)
+        lib().orc_hier_level_parts(self.h, l, _p(pt))
+        return pt
 
     def levels(self):
         return lib().orc_hier_levels(self.h)

@@ -134,3 +134,60 @@ def test_bcsstk09_golden(oracle, golden, bx, tmp_path):
     g = golden["sol__bcsstk09_sol"]
     assert info["retv"] == 0
     assert np.linalg.norm(x - g) / np.linalg.norm(g) < 1e-5
+
+
+def rank_offsets(nx, ny, nz, P, Q, R):
+    """Row offsets of the P*Q*R ranks of the reference's rank-block-major Laplacian."""
+    per = nx * ny * nz
+    return [k * per for k in range(P * Q * R + 1)]
+
+
+@pytest.mark.parametrize("st", [7, 27])
+@pytest.mark.parametrize("PQR", GRIDS[1:])
+def test_partitioned_golden_solutions(oracle, golden, st, PQR):
+    """The np = P restatement (rank-local matching and aggregate numbering) on the grids that the
+    reference's multi-rank runs produced: each rank holds its 10^3 block, and the solution matches
+    BCMGX/src/test/data/cmp/lap3d_{st}p_10x10x10_{PxQxR}_sol.txt within compareSolutions' 1e-5."""
+    P, Q, R = PQR
+    A = oracle.Matrix.lap3d(st, 10, 10, 10, P, Q, R)
+    parts = rank_offsets(10, 10, 10, P, Q, R)
+    H = oracle.Hierarchy(A, oracle.params(), parts=parts)
+    x, info = H.solve(np.ones(A.info()[0]))
+    g = golden[f"sol__lap3d_{st}p_10x10x10_{P}x{Q}x{R}_sol"]
+    assert info["retv"] == 0
+    assert np.linalg.norm(x - g) / np.linalg.norm(g) < 1e-5
+    assert list(H.level_parts(0)) == parts
+
+
+def test_partitioned_matching_stays_inside_blocks(oracle):
+    """Rank-local matching: no aggregate of any sweep crosses a block boundary, each block's
+    aggregates are numbered after the previous block's, and one block gives the np = 1 set-up."""
+    A = oracle.Matrix.lap3d(27, 9, 8, 7)
+    n = A.info()[0]
+    one = oracle.Hierarchy(A, oracle.params(), record=True)
+    same = oracle.Hierarchy(A, oracle.params(), record=True, parts=[0, n])
+    assert one.level_sizes() == same.level_sizes()
+    for a, b in zip(one.records(), same.records()):
+        assert np.array_equal(a["agg"], b["agg"]) and np.array_equal(a["p"], b["p"])
+    parts = [0, 150, 311, n]
+    H = oracle.Hierarchy(A, oracle.params(), record=True, parts=parts)
+    recs = H.records()
+    pt = np.array(parts)
+    crossed_somewhere = False
+    for r in recs:
+        m = r["match"]
+        if r["level"] == 0 and r["sweep"] == 0:
+            blk = np.searchsorted(pt, np.arange(n), side="right") - 1
+            ok = m >= 0
+            assert np.all(blk[m[ok]] == blk[ok])
+            crossed_somewhere = np.any(one.records()[0]["match"][ok] != m[ok])
+            # aggregates of block b are numbered after those of blocks < b
+            agg = r["agg"]
+            for b in range(3):
+                lo, hi = agg[pt[b]:pt[b + 1]].min(), agg[pt[b]:pt[b + 1]].max()
+                if b:
+                    assert lo == prev_hi + 1
+                prev_hi = hi
+    assert crossed_somewhere
+    lv0 = H.level_parts(1)
+    assert lv0[0] == 0 and lv0[-1] == H.level_sizes()[1][0] and len(lv0) == 4

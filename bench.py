@@ -510,7 +510,11 @@ def run_ours(a, wl, rank, world, local_rank):
         "kernels_level0": {"index_bytes": ib32, "fp32_jacobi_ms": k32["jacobi"], "fp32_jacobi_gbs": gbs_jac32,
                            "fp32_jacobi_int32_equivalent_gbs": bytes_jac32_int32 / (k32["jacobi"] * 1e-3) / 1e9,
                            "fp32_residual_ms": k32["residual"], "fp64_jacobi_ms": k64f["jacobi"],
-                           "fp64_jacobi_gbs": gbs_jac64, "fcg_spmv_dots_ms": k64f["fcg_spmv_dots"]},
+                           "fp64_jacobi_gbs": gbs_jac64, "fcg_spmv_dots_ms": k64f["fcg_spmv_dots"],
+                           "fcg_spmv_dots_gbs": ((ib64 + 8) * nnz + 4 * (n + 1) + 40 * n) / (k64f["fcg_spmv_dots"] * 1e-3) / 1e9,
+                           "fp32_jacobi_fp64_out_ms": k32["jacobi_fp64_out"],
+                           "fcg_update_ms": k32["fcg_update"],
+                           "fcg_update_gbs": 80 * n / (k32["fcg_update"] * 1e-3) / 1e9},
         "kernels_coarse_levels_fp32_jacobi_ms": [round(k["jacobi"], 4) for k in lvl],
         "vcycle": vcycle_roofline(vc_ms, inf32, params("FP32"), peak, peak_kind),
         "roofline": {"kernel": (f"k_rowop_staged<{-tpr0},OP_JACOBI,float>" if tpr0 < 0 else f"k_rowop<{tpr0},OP_JACOBI,float>")
@@ -870,6 +874,74 @@ def profile_step(a, wl):
     print(json.dumps({"warmup_launches": c1 - c0, "step_launches": c2 - c1, "niter": info["niter"]}), flush=True)
 
 
+def run_dist(a, wl, rank=0, world=1, local_rank=0, parts=2):
+    """The row-partitioned path (the reference's multi-rank solve): set-up + FCG solve to 1e-8 with
+    the FP64 V-cycle, rows split into equal blocks. With one process (world 1) all `parts` blocks
+    run on one GPU (the local form: exchanges as device copies); under torchrun every rank holds
+    one block on its own GPU and exchanges over NCCL (the communicator made from a unique id that
+    rank 0 shares through torch.distributed). Times: CUDA events, the slowest rank's."""
+    import torch
+    import bootcmatchgx_b200 as bx
+    dev = torch.device("cuda", local_rank)
+    row, col, val, xs, b = build_problem(wl)
+    n = row.size - 1
+    nparts = world if world > 1 else parts
+    offs = [n * k // nparts for k in range(nparts + 1)]
+    p = bx.params_default(solver="FCG", preconditioner="BCMG", rtol=RTOL, dispnorm=0, vcycle_precision="FP64")
+    comm = None
+    if world > 1:
+        import torch.distributed as dist
+        uid = [bx.nccl_unique_id() if rank == 0 else None]
+        dist.broadcast_object_list(uid, src=0)
+        comm = bx.nccl_comm(world, rank, uid[0])
+        r0, r1 = offs[rank], offs[rank + 1]
+        e0_, e1_ = row[r0], row[r1]
+        d = [torch.from_numpy(np.ascontiguousarray(row[r0:r1 + 1] - e0_)).to(dev),
+             torch.from_numpy(np.ascontiguousarray(col[e0_:e1_])).to(dev),
+             torch.from_numpy(np.ascontiguousarray(val[e0_:e1_])).to(dev)]
+        bd = torch.from_numpy(np.ascontiguousarray(b[r0:r1])).to(dev)
+    else:
+        d = [torch.from_numpy(x_).to(dev) for x_ in (row, col, val)]
+        bd = torch.from_numpy(b).to(dev)
+    x = torch.zeros_like(bd)
+
+    def step():
+        D = (bx.Dist.nccl(d[0], d[1], d[2], offs[rank], n, comm, world, p) if world > 1
+             else bx.Dist.local(d[0], d[1], d[2], offs, p))
+        x.zero_()
+        _, info = D.solve(bd, x)
+        inf = D.info()
+        D.free()
+        return info, inf
+    try:
+        for _ in range(max(1, a.warmup)):
+            step()
+        torch.cuda.synchronize()
+        steps = max(1, min(a.steps, 5))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res = [step() for _ in range(steps)]
+        e1.record()
+        torch.cuda.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1) / steps, world, dev)
+        xh = x.cpu().numpy()
+        err = None
+        if xs is not None:
+            xs_mine = xs[offs[rank]:offs[rank + 1]] if world > 1 else xs
+            err = max_over_ranks(float(np.linalg.norm(xh - xs_mine) / np.linalg.norm(xs_mine)), world, dev)
+    finally:
+        if comm is not None:
+            bx.nccl_comm_destroy(comm)
+    info, inf = res[-1]
+    return {"metric": "row-partitioned set-up + solve s to rel-res 1e-8 (FP64 V-cycle)", "value": ms / 1e3,
+            "unit": "s", "higher_is_better": False, "workload": a.workload, "n_gpus": world, "ranks": nparts,
+            "transport": "nccl (one block per GPU)" if world > 1 else "local (all blocks on one GPU, device copies)",
+            "setup_ms": float(np.mean([r[1]["setup_ms"] for r in res])),
+            "solve_ms": float(np.mean([r[0]["solve_ms"] for r in res])), "niter": info["niter"],
+            "levels": inf["n"], "level_nnz": inf["nnz"], "err_vs_xstar": err, "steps": steps,
+            "config": {"rows": int(n), "nnz": int(col.size), "blocks": "equal consecutive row blocks", "rtol": RTOL}}
+
+
 def run_small(a, name, rank=0, world=1, local_rank=0, steps=10, warmup=3):
     """A small workload (the 7-point 50^3 Poisson system by default: 125,000 rows, L2-resident)
     through the same step as the headline: set-up + FCG solve to 1e-8, FP32 and FP64 V-cycles,
@@ -929,6 +1001,11 @@ def secondary_configs(a, rank, world, local_rank):
             ("adjoint_diffusion7_96", lambda: run_adjoint(a, rank, world, local_rank, steps=3, warmup=1)),
             ("batch256_poisson7", lambda: run_batch(a, rank, world, local_rank, steps=3, warmup=2)),
             ("poisson27_100_x32", lambda: run_multi(a, rank, world, local_rank, steps=3, warmup=1, kernels=False))]
+    if world == 1:
+        # the row-partitioned path on the headline workload, two row blocks on this GPU
+        short = argparse.Namespace(**dict(vars(a), steps=2, warmup=1))
+        jobs.append(("partitioned_2blocks_" + a.workload,
+                     lambda: run_dist(short, WORKLOADS[a.workload], 0, 1, local_rank, parts=2)))
     out = {}
     for name, fn in jobs:
         t0 = time.perf_counter()
@@ -952,6 +1029,9 @@ def main():
     ap.add_argument("--adjoint", action="store_true", help="run the differentiated-solve configuration instead")
     ap.add_argument("--batch", action="store_true", help="run the batched-systems configuration instead")
     ap.add_argument("--multi", action="store_true", help="run the 32-right-hand-side configuration instead")
+    ap.add_argument("--dist", type=int, default=0, metavar="P",
+                    help="run the row-partitioned path instead: P blocks on one GPU, or one block per rank under "
+                         "torchrun (P is then the world size)")
     ap.add_argument("--cpu-leg", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--profile-step", action="store_true",
                     help="only W warm-up steps and one FP32 step (for ncu launch lists); prints the launch counts")
@@ -988,6 +1068,8 @@ def main():
             line = run_batch(a, rank, world, local_rank)
         elif a.multi:
             line = run_multi(a, rank, world, local_rank)
+        elif a.dist:
+            line = run_dist(a, wl, rank, world, local_rank, parts=a.dist)
         else:
             line, extra = run_ours(a, wl, rank, world, local_rank)
             if not a.no_secondary:

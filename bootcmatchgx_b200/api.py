@@ -297,10 +297,12 @@ class Hierarchy:
         return out
 
     def time_kernels(self, level=0, reps=20):
-        """Average ms per launch of the level's Jacobi sweep, residual, FP64 SpMV, FCG SpMV+dots."""
-        out = np.zeros(4)
+        """Average ms per launch of the level's Jacobi sweep, residual, FP64 SpMV, and on level 0
+        the FCG SpMV+dots, the FP32 cycle's sweep with FP64 output and the FCG update."""
+        out = np.zeros(6)
         check(lib().bcmgx_time_kernels(self.h, level, reps, _ptr(out)), "bcmgx_time_kernels")
-        return {"jacobi": out[0], "residual": out[1], "spmv": out[2], "fcg_spmv_dots": out[3]}
+        return {"jacobi": out[0], "residual": out[1], "spmv": out[2], "fcg_spmv_dots": out[3],
+                "jacobi_fp64_out": out[4], "fcg_update": out[5]}
 
     def time_block_kernels(self, nrhs=32, reps=20):
         """Average ms per launch of the level-0 block Jacobi sweep, block residual, FP64 block SpMM

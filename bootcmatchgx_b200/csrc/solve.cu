@@ -1117,7 +1117,8 @@ void ensure_solve_workspace(bcmgx_hierarchy* H)
 // Average device time of one launch of each solve-phase kernel of level l, timed with CUDA
 // events on the hierarchy's stream over `reps` back-to-back launches after one warm-up:
 // out[0] l1-Jacobi sweep (in the cycle's precision), out[1] residual, out[2] FP64 y = A x,
-// out[3] the FCG SpMV + dot products (level 0 only, else 0).
+// out[3] the FCG SpMV + dot products, out[4] the FP32 cycle's sweep that writes an FP64 result,
+// out[5] the FCG update (two merged axpys and the norm) (out[3..5] on level 0 only, else 0).
 void time_level_kernels(bcmgx_hierarchy* H, int l, int reps, double* out)
 {
     ensure_solve_workspace(H);
@@ -1163,11 +1164,34 @@ void time_level_kernels(bcmgx_hierarchy* H, int l, int reps, double* out)
     }
     out[2] = timeit([&] { launch_spmv(n, A.row.p, A.col.p, A.val.p, a.p, b.p, 1.0, 0.0, A.tpr, s); });
     out[3] = 0;
+    out[4] = 0;
+    out[5] = 0;
     if (l == 0) {
         FcgState init {};
         init.delta = 1.0;
         BCMGX_CUDA(cudaMemcpyAsync(H->st.p, &init, sizeof(FcgState), cudaMemcpyHostToDevice, s));
         out[3] = timeit([&] { fcg_dots<1>(A, a.p, b.p, c.p, c.p, H->st.p, H->partials.p, nullptr, s); });
+        // the cycle's last level-0 sweep writes the FP64 preconditioned vector
+        if (f32)
+            out[4] = timeit([&] { launch_rowop_A<OP_JACOBI>(A.tpr, A, A.val32.p, (const float*)a32.p, (const float*)c32.p,
+                                      V.M32.p, b.p, 1.0, 0.0, nullptr, s); });
+        DBuf<double> d4, d5, d6;
+        d4.alloc(n, s);
+        d5.alloc(n, s);
+        d6.alloc(n, s);
+        fill_probe(d4.p, n, 3u, s);
+        fill_probe(d5.p, n, 4u, s);
+        fill_probe(d6.p, n, 5u, s);
+        init.theta = 1e-3;
+        init.theta2 = 1e-3;
+        init.tol = 0.0;
+        init.itnlim = 1 << 30;
+        BCMGX_CUDA(cudaMemcpyAsync(H->st.p, &init, sizeof(FcgState), cudaMemcpyHostToDevice, s));
+        out[5] = timeit([&] {
+            note_launch();
+            k_fcg_update<<<red_grid(k_fcg_update, n), kRedThreads, 0, s>>>(n, a.p, c.p, b.p, d4.p, d5.p, d6.p, H->st.p,
+                H->partials.p, nullptr, nullptr);
+        });
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -187,11 +187,13 @@ int bcmgx_hierarchy_get_sweep(const bcmgx_hierarchy* h, int k, int* level, int* 
 int bcmgx_prec_apply(bcmgx_hierarchy* h, const double* r, double* v, int on_device);
 
 /* Average device time (ms, CUDA events on the hierarchy's stream, `reps` launches after one
- * warm-up) of level `level`'s solve kernels: out[0] one l1-Jacobi sweep in the cycle's
- * precision, out[1] the residual, out[2] the FP64 SpMV, out[3] the fused FCG SpMV + dots
- * (level 0 only). The kernels run on fixed non-constant vectors (values in [0.5, 1.5)), as in a
- * solve: on zero vectors every sweep divides zero residuals, which times slower. No counterpart
- * in the reference: the measurement hook of the benchmarks. */
+ * warm-up) of level `level`'s solve kernels into out[0..5]: out[0] one l1-Jacobi sweep in the
+ * cycle's precision, out[1] the residual, out[2] the FP64 SpMV, and on level 0 only (else 0):
+ * out[3] the fused FCG SpMV + dots, out[4] the FP32 cycle's sweep that writes the FP64
+ * preconditioned vector (0 for the FP64 cycle), out[5] the FCG update (two merged axpys and the
+ * norm). The kernels run on fixed non-constant vectors (values in [0.5, 1.5)), as in a solve: on
+ * zero vectors every sweep divides zero residuals, which times slower. No counterpart in the
+ * reference: the measurement hook of the benchmarks. */
 int bcmgx_time_kernels(bcmgx_hierarchy* h, int level, int reps, double* out_ms);
 /* The same for the level-0 block kernels of a solve with nrhs (1..32) right-hand sides (blocks of
  * nrhs rounded up to a power of two columns): out[0] one block l1-Jacobi sweep in the cycle's

@@ -290,9 +290,13 @@ int bcmgx_suitor_matching(int n, int64_t nnz, const int* row, const int* col, co
  * 8.5 MiB (per-row values and per-entry positions) that every GPU loading the library holds until
  * exit; matrices beyond 65536 rows or 2097152 non-zeros are rejected with
  * BCMGX_ERR_INVALID_INPUT. The first call on a device looks up that device's address of the
- * array (cudaGetSymbolAddress), so make that first call before any stream capture. All calls
- * share the array: calls that overlap on the GPU (other streams, other host threads) race on it
- * and must be serialised by the caller. */
+ * array (cudaGetSymbolAddress), so make that first call before any stream capture. With CUDA's
+ * lazy module loading (the default since CUDA 12.2) the array's device memory is committed only
+ * when the library's set-up module first loads on a device -- at that first call, or at the first
+ * set-up call -- so a caller whose allocator will later take nearly all of the GPU's memory makes
+ * one call (any size) before that, or runs with CUDA_MODULE_LOADING=EAGER. All calls share the
+ * array: calls that overlap on the GPU (other streams, other host threads) race on it and must be
+ * serialised by the caller. */
 int bcmgx_edge_weights_noalloc(int n, int64_t nnz, const int* row, const int* col, const double* val,
     const double* w, double* W, double* min_abs_out, void* stream);
 

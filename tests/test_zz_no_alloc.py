@@ -62,3 +62,39 @@ def test_noalloc_rejects_oversized_input(bx, cuda):
                                           C.byref(mn), C.c_void_p(stream.cuda_stream))
         assert rc == -1
         assert "too large for the allocation-free entry point" in bx._lib.last_error()
+
+
+def test_noalloc_takes_no_device_memory(bx, cuda):
+    """After the first call (which commits the static scratch), repeated calls leave the device's
+    free memory and the default memory pool's usage unchanged: nothing is allocated."""
+    import torch
+    from cuda.bindings import runtime as rt
+    stream = torch.cuda.current_stream(cuda)
+    row, col, val = bx.laplacian_3d(27, 20, 20, 20)
+    n = row.size - 1
+    d = [torch.from_numpy(a).to(cuda) for a in (row, col, val)]
+    w = torch.ones(n, dtype=torch.float64, device=cuda)
+    W = torch.empty_like(d[2])
+    mn = C.c_double()
+    L = bx.lib()
+
+    def call():
+        rc = L.bcmgx_edge_weights_noalloc(n, int(d[1].numel()), _ptr(d[0]), _ptr(d[1]), _ptr(d[2]), _ptr(w), _ptr(W),
+                                          C.byref(mn), C.c_void_p(stream.cuda_stream))
+        assert rc == 0, bx._lib.last_error()
+
+    def pool_used():
+        err, pool = rt.cudaDeviceGetDefaultMemPool(torch.cuda.current_device())
+        assert err == rt.cudaError_t.cudaSuccess
+        err, v = rt.cudaMemPoolGetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemCurrent)
+        assert err == rt.cudaError_t.cudaSuccess
+        return int(v)
+
+    call()
+    torch.cuda.synchronize()
+    free0, used0 = torch.cuda.mem_get_info(cuda)[0], pool_used()
+    for _ in range(5):
+        call()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(cuda)[0] == free0
+    assert pool_used() == used0

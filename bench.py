@@ -511,7 +511,8 @@ def run_ours(a, wl, rank, world, local_rank):
                            "fp32_jacobi_int32_equivalent_gbs": bytes_jac32_int32 / (k32["jacobi"] * 1e-3) / 1e9,
                            "fp32_residual_ms": k32["residual"], "fp64_jacobi_ms": k64f["jacobi"],
                            "fp64_jacobi_gbs": gbs_jac64, "fcg_spmv_dots_ms": k64f["fcg_spmv_dots"],
-                           "fcg_spmv_dots_gbs": ((ib64 + 8) * nnz + 4 * (n + 1) + 40 * n) / (k64f["fcg_spmv_dots"] * 1e-3) / 1e9,
+                           # pw = A pv (row kernel) then the three dots (r, pw, oq against pv)
+                           "fcg_spmv_dots_gbs": ((ib64 + 8) * nnz + 4 * (n + 1) + 48 * n) / (k64f["fcg_spmv_dots"] * 1e-3) / 1e9,
                            "fp32_jacobi_fp64_out_ms": k32["jacobi_fp64_out"],
                            "fcg_update_ms": k32["fcg_update"],
                            "fcg_update_gbs": 80 * n / (k32["fcg_update"] * 1e-3) / 1e9},

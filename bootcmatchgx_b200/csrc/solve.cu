@@ -178,6 +178,7 @@ void stage_fault_check()
 }
 
 static bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
+static bool al16(const void* p) { return aligned16(p); }
 
 // Fault-path test hook of the staged kernels: BCMGX_TEST_STAGE_FAULT=<ns> in the environment makes
 // the launches that follow (the variable is read at every launch; a captured graph keeps the value
@@ -909,33 +910,47 @@ __global__ void __launch_bounds__(kRedThreads) k_fcg_resid0(int n, const int* __
     }
 }
 
-// pw = A pv with the dots of the step: start-up (mode 0): alpha = r.pv, beta = pw.pv,
-// delta = beta, theta = alpha / delta (FCG.cu:59-86); loop (mode 1): alpha = r.pv, beta = pw.pv,
-// gamma = oq.pv (triple_innerproduct, triple_inner_product.cu:7-101) followed by the scalar
-// recurrence theta = gamma/delta, delta = beta - gamma^2/delta, theta2 = alpha/delta
-// (FCG.cu:132-136).
-template <int S, int MODE, typename IT>
-__global__ void __launch_bounds__(kRedThreads) k_fcg_spmv_dots(int n, const int* __restrict__ row, const IT* __restrict__ col,
-    const double* __restrict__ val, const double* __restrict__ pv, double* __restrict__ pw, const double* __restrict__ r,
-    const double* __restrict__ oq, FcgState* st, double* partials, const int* __restrict__ skip)
+// The dots of the step after pw = A pv (the level-0 FP64 row kernel, launched before): start-up
+// (mode 0): alpha = r.pv, beta = pw.pv, delta = beta, theta = alpha / delta (FCG.cu:59-86); loop
+// (mode 1): alpha = r.pv, beta = pw.pv, gamma = oq.pv (triple_innerproduct,
+// triple_inner_product.cu:7-101) followed by the scalar recurrence theta = gamma/delta, delta =
+// beta - gamma^2/delta, theta2 = alpha/delta (FCG.cu:132-136). The sums run in a fixed order
+// whichever row kernel formed pw (so staged and plain solves agree bit for bit); VEC: 16-byte
+// loads on aligned vectors.
+template <int MODE, bool VEC>
+__global__ void __launch_bounds__(kRedThreads, 4) k_fcg_dots(int n, const double* __restrict__ pv,
+    const double* __restrict__ pw, const double* __restrict__ r, const double* __restrict__ oq, FcgState* st,
+    double* partials, const int* __restrict__ skip)
 {
     if (skip && *skip) return;
-    const int lane = threadIdx.x & (S - 1);
-    const int sub = (threadIdx.x & 31) / S;
-    const long stride = (long)gridDim.x * blockDim.x / S;
     double acc[3] = { 0.0, 0.0, 0.0 };
-    for (long base = ((long)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) / S; base < n; base += stride) {
-        const long r0 = base + sub;
-        double s = 0;
-        if (r0 < n) s = row_partial<S, double>(row[r0], row[r0 + 1], lane, (int)r0, col, val, pv);
-        s = subwarp_sum<S>(s);
-        if (r0 < n && lane == 0) {
-            pw[r0] = s;
-            const double vi = pv[r0];
-            acc[0] += r[r0] * vi;
-            acc[1] += s * vi;
-            if (MODE == 1) acc[2] += oq[r0] * vi;
+    auto one = [&](long i) {
+        const double vi = pv[i];
+        acc[0] += r[i] * vi;
+        acc[1] += pw[i] * vi;
+        if (MODE == 1) acc[2] += oq[i] * vi;
+    };
+    if (VEC) {
+        const long n2 = n >> 1;
+        const double2* pv2 = reinterpret_cast<const double2*>(pv);
+        const double2* pw2 = reinterpret_cast<const double2*>(pw);
+        const double2* r2 = reinterpret_cast<const double2*>(r);
+        const double2* oq2 = reinterpret_cast<const double2*>(oq);
+        for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += (long)gridDim.x * blockDim.x) {
+            const double2 v = pv2[i], w = pw2[i], rr = r2[i];
+            acc[0] += rr.x * v.x;
+            acc[0] += rr.y * v.y;
+            acc[1] += w.x * v.x;
+            acc[1] += w.y * v.y;
+            if (MODE == 1) {
+                const double2 q = oq2[i];
+                acc[2] += q.x * v.x;
+                acc[2] += q.y * v.y;
+            }
         }
+        if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) one(n - 1);
+    } else {
+        for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) one(i);
     }
     double out[3];
     if (grid_sum<3>(acc, partials, &st->ticket[1], out) && threadIdx.x == 0) {
@@ -982,7 +997,11 @@ __global__ void __launch_bounds__(kRedThreads) k_fcg_update0(int n, const double
 
 // Loop update: pv = -theta od + pv; x += theta2 pv; pw = -theta oq + pw; r -= theta2 pw
 // (double_merged_axpy x2, FCG.cu:138-144), ||r|| and the stopping test (FCG.cu:146-156).
-__global__ void __launch_bounds__(kRedThreads) k_fcg_update(int n, double* __restrict__ pv, const double* __restrict__ od,
+// VEC: all six vectors 16-byte aligned; each thread then moves two entries per 16-byte load and
+// store (a streaming kernel wants bytes in flight), the odd last entry going to thread 0. At most
+// 64 registers, so that four blocks of 256 threads stay resident per SM.
+template <bool VEC>
+__global__ void __launch_bounds__(kRedThreads, 4) k_fcg_update(int n, double* __restrict__ pv, const double* __restrict__ od,
     double* __restrict__ x, double* __restrict__ pw, const double* __restrict__ oq, double* __restrict__ r, FcgState* st,
     double* partials, double* hist, const int* __restrict__ skip)
 {
@@ -994,7 +1013,7 @@ __global__ void __launch_bounds__(kRedThreads) k_fcg_update(int n, double* __res
     }
     const double th = st->theta, th2 = st->theta2;
     double acc[1] = { 0.0 };
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    auto one = [&](long i) {
         const double nv = -th * od[i] + pv[i];
         pv[i] = nv;
         x[i] = th2 * nv + x[i];
@@ -1003,6 +1022,36 @@ __global__ void __launch_bounds__(kRedThreads) k_fcg_update(int n, double* __res
         const double ri = -th2 * nw + r[i];
         r[i] = ri;
         acc[0] += ri * ri;
+    };
+    if (VEC) {
+        const long n2 = n >> 1;
+        double2* pv2 = reinterpret_cast<double2*>(pv);
+        const double2* od2 = reinterpret_cast<const double2*>(od);
+        double2* x2 = reinterpret_cast<double2*>(x);
+        double2* pw2 = reinterpret_cast<double2*>(pw);
+        const double2* oq2 = reinterpret_cast<const double2*>(oq);
+        double2* r2 = reinterpret_cast<double2*>(r);
+        for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += (long)gridDim.x * blockDim.x) {
+            const double2 a = od2[i], b = pv2[i], c = oq2[i], d = pw2[i], e = x2[i], f = r2[i];
+            double2 nv, nw, nx, nr;
+            nv.x = -th * a.x + b.x;
+            nv.y = -th * a.y + b.y;
+            nx.x = th2 * nv.x + e.x;
+            nx.y = th2 * nv.y + e.y;
+            nw.x = -th * c.x + d.x;
+            nw.y = -th * c.y + d.y;
+            nr.x = -th2 * nw.x + f.x;
+            nr.y = -th2 * nw.y + f.y;
+            pv2[i] = nv;
+            x2[i] = nx;
+            pw2[i] = nw;
+            r2[i] = nr;
+            acc[0] += nr.x * nr.x;
+            acc[0] += nr.y * nr.y;
+        }
+        if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) one(n - 1);
+    } else {
+        for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) one(i);
     }
     double out[1];
     if (grid_sum<1>(acc, partials, &st->ticket[3], out) && threadIdx.x == 0) {
@@ -1013,6 +1062,21 @@ __global__ void __launch_bounds__(kRedThreads) k_fcg_update(int n, double* __res
         if (!isfinite(l2)) st->bad = 1;
         st->done = (!(l2 > st->tol) || st->iter >= st->itnlim || st->bad) ? 1 : 0;
     }
+}
+
+// The loop update on the hierarchy's stream (the vector form when every vector allows it).
+static void fcg_update(int n, double* pv, const double* od, double* x, double* pw, const double* oq, double* r,
+    FcgState* st, double* part, double* hist, const int* skip, cudaStream_t s)
+{
+    note_launch();
+    if (al16(pv) && al16(od) && al16(x) && al16(pw) && al16(oq) && al16(r)) {
+        auto k = k_fcg_update<true>;
+        k<<<red_grid(k, ((long)n + 1) / 2), kRedThreads, 0, s>>>(n, pv, od, x, pw, oq, r, st, part, hist, skip);
+    } else {
+        auto k = k_fcg_update<false>;
+        k<<<red_grid(k, n), kRedThreads, 0, s>>>(n, pv, od, x, pw, oq, r, st, part, hist, skip);
+    }
+    BCMGX_CHECK_LAUNCH();
 }
 
 template <int S>
@@ -1027,20 +1091,6 @@ static void launch_resid0(const DevCsr& A, const double* x, const double* b, dou
         k<<<red_grid(k, (long)A.n * S), kRedThreads, 0, s>>>(A.n, A.row.p, A.col.p, A.val.p, x, b, r, st, part);
     }
 }
-template <int S, int MODE>
-static void launch_dots(const DevCsr& A, const double* pv, double* pw, const double* r, const double* oq, FcgState* st,
-    double* part, const int* skip, cudaStream_t s)
-{
-    note_launch();
-    if (A.dcol.p) {
-        auto k = k_fcg_spmv_dots<S, MODE, short>;
-        k<<<red_grid(k, (long)A.n * S), kRedThreads, 0, s>>>(A.n, A.row.p, A.dcol.p, A.val.p, pv, pw, r, oq, st, part, skip);
-    } else {
-        auto k = k_fcg_spmv_dots<S, MODE, int>;
-        k<<<red_grid(k, (long)A.n * S), kRedThreads, 0, s>>>(A.n, A.row.p, A.col.p, A.val.p, pv, pw, r, oq, st, part, skip);
-    }
-}
-
 static void fcg_resid0(const DevCsr& A, const double* x, const double* b, double* r, FcgState* st, double* part, cudaStream_t s)
 {
     switch (A.tpr) {
@@ -1054,17 +1104,21 @@ static void fcg_resid0(const DevCsr& A, const double* x, const double* b, double
     BCMGX_CHECK_LAUNCH();
 }
 
+// pw = A pv (the level's row kernel in FP64: the staged one when the tuning chose it) and the
+// step's dots and scalars (k_fcg_dots).
 template <int MODE>
 static void fcg_dots(const DevCsr& A, const double* pv, double* pw, const double* r, const double* oq, FcgState* st,
     double* part, const int* skip, cudaStream_t s)
 {
-    switch (A.tpr) {
-    case 1: launch_dots<1, MODE>(A, pv, pw, r, oq, st, part, skip, s); break;
-    case 2: launch_dots<2, MODE>(A, pv, pw, r, oq, st, part, skip, s); break;
-    case 4: launch_dots<4, MODE>(A, pv, pw, r, oq, st, part, skip, s); break;
-    case 8: launch_dots<8, MODE>(A, pv, pw, r, oq, st, part, skip, s); break;
-    case 16: launch_dots<16, MODE>(A, pv, pw, r, oq, st, part, skip, s); break;
-    default: launch_dots<32, MODE>(A, pv, pw, r, oq, st, part, skip, s); break;
+    launch_rowop_A<OP_AXPBY>(A.tpr, A, A.val.p, pv, (const double*)nullptr, (const double*)nullptr, pw, 1.0, 0.0, skip, s);
+    const int n = A.n;
+    note_launch();
+    if (al16(pv) && al16(pw) && al16(r) && (MODE == 0 || al16(oq))) {
+        auto k = k_fcg_dots<MODE, true>;
+        k<<<red_grid(k, ((long)n + 1) / 2), kRedThreads, 0, s>>>(n, pv, pw, r, oq, st, part, skip);
+    } else {
+        auto k = k_fcg_dots<MODE, false>;
+        k<<<red_grid(k, n), kRedThreads, 0, s>>>(n, pv, pw, r, oq, st, part, skip);
     }
     BCMGX_CHECK_LAUNCH();
 }
@@ -1187,11 +1241,7 @@ void time_level_kernels(bcmgx_hierarchy* H, int l, int reps, double* out)
         init.tol = 0.0;
         init.itnlim = 1 << 30;
         BCMGX_CUDA(cudaMemcpyAsync(H->st.p, &init, sizeof(FcgState), cudaMemcpyHostToDevice, s));
-        out[5] = timeit([&] {
-            note_launch();
-            k_fcg_update<<<red_grid(k_fcg_update, n), kRedThreads, 0, s>>>(n, a.p, c.p, b.p, d4.p, d5.p, d6.p, H->st.p,
-                H->partials.p, nullptr, nullptr);
-        });
+        out[5] = timeit([&] { fcg_update(n, a.p, c.p, b.p, d4.p, d5.p, d6.p, H->st.p, H->partials.p, nullptr, nullptr, s); });
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -1431,9 +1481,7 @@ static void fcg_iteration(bcmgx_hierarchy* H, bool even, double* x, double* hist
     const double* oq = even ? q : w;
     prec_apply_impl(H, r, pv, skip);
     fcg_dots<1>(A, pv, pw, r, oq, st, part, skip, s);
-    note_launch();
-    k_fcg_update<<<red_grid(k_fcg_update, n), kRedThreads, 0, s>>>(n, pv, od, x, pw, oq, r, st, part, hist, skip);
-    BCMGX_CHECK_LAUNCH();
+    fcg_update(n, pv, od, x, pw, oq, r, st, part, hist, skip, s);
 }
 
 // Adds the whole solve of hierarchy H to graph g as an independent branch: the start-up, then a

@@ -63,7 +63,8 @@ class HierarchyInfo(C.Structure):
                 ("op_wcmplx", C.c_double), ("avg_cratio", C.c_double),
                 ("maxcoarsesize", C.c_int), ("ftcoarse", C.c_int),
                 ("num_sweep_records", C.c_int), ("setup_ms", C.c_double),
-                ("tpr", C.c_int * MAX_LEVELS), ("index_bytes", C.c_int * MAX_LEVELS)]
+                ("tpr", C.c_int * MAX_LEVELS), ("index_bytes", C.c_int * MAX_LEVELS),
+                ("value_codes", C.c_int * MAX_LEVELS)]
 
 
 # name -> (restype, argtypes); every symbol include/bcmgx.h declares

@@ -250,7 +250,8 @@ class Hierarchy:
                 "op_cmplx": hi.op_cmplx, "op_wcmplx": hi.op_wcmplx, "avg_cratio": hi.avg_cratio,
                 "maxcoarsesize": hi.maxcoarsesize, "ftcoarse": hi.ftcoarse,
                 "num_sweep_records": hi.num_sweep_records, "setup_ms": hi.setup_ms,
-                "tpr": list(hi.tpr[:nl]), "index_bytes": list(hi.index_bytes[:nl])}
+                "tpr": list(hi.tpr[:nl]), "index_bytes": list(hi.index_bytes[:nl]),
+                "value_codes": list(hi.value_codes[:nl])}
 
     def afsai_factor(self):
         """The AFSAI factor G (CSR row, col, val) of an AFSAI hierarchy."""

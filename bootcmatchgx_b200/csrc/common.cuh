@@ -7,6 +7,8 @@
 namespace bcmgx {
 
 constexpr int kWarp = 32;
+// largest value table of a value-indexed (coded) matrix: one-byte codes
+constexpr int kValueCodes = 256;
 
 // Streaming loads for matrix data (read once per pass; evict-first so the vectors stay in L2).
 __device__ __forceinline__ int ld_stream(const int* p) { return __ldcs(p); }

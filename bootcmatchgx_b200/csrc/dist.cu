@@ -1380,6 +1380,7 @@ int bcmgx_dist_get_info(const bcmgx_dist* D, bcmgx_hierarchy_info* info)
             info->nnz[l] = D->level_nnz[l];
             info->tpr[l] = D->parts[0].H->lv[l].A.tpr;
             info->index_bytes[l] = D->parts[0].H->lv[l].A.dcol.p ? 2 : 4;
+            info->value_codes[l] = D->parts[0].H->lv[l].A.vcode.p ? D->parts[0].H->lv[l].A.nvalues : 0;
         }
         info->op_cmplx = D->op_cmplx;
         info->op_wcmplx = D->op_wcmplx;

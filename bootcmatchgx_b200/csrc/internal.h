@@ -117,6 +117,12 @@ struct DevCsr {
     DBuf<double> val;
     DBuf<float> val32;
     DBuf<short> dcol; // col - row as int16 when every entry is within 32767 of the diagonal, else empty
+    // value codes (value-indexed CSR, rowops.cuh Coded): when the matrix has at most 256 distinct
+    // values, entry j's value is vtab64[vcode[j]] (and its FP32 copy vtab32[vcode[j]]); else empty
+    DBuf<unsigned char> vcode;
+    DBuf<double> vtab64;
+    DBuf<float> vtab32;
+    int nvalues = 0;  // distinct values in the table (0: not coded)
     int tpr = 0;      // threads per row for SpMV / smoother (autotuned)
     bool staged = false;  // row kernels stream the entries through shared-memory stages (staged.cuh)
 };

@@ -1593,6 +1593,149 @@ static void build_offsets(DevCsr& A, cudaStream_t s)
     BCMGX_CHECK_LAUNCH();
 }
 
+// ---- value codes (value-indexed CSR) -------------------------------------------------------
+// A level whose values take at most kValueCodes distinct FP64 bit patterns (constant-coefficient
+// stencils take a handful) stores one byte per entry: the index of its value in a table of them.
+// The FP32 table holds the same entries rounded to FP32, so vtab32[vcode[j]] equals the stored
+// val32[j]: the coded and the stored forms give the same results bit for bit. Distinct values
+// are collected in a hash set of kVcSlots bit patterns (each block first in shared memory, then
+// merged into the global set); a block stops as soon as its set passes kValueCodes.
+constexpr int kVcSlots = 1024;
+constexpr unsigned long long kVcEmpty = ~0ull;   // a NaN pattern; a matrix holding it is not coded
+constexpr int64_t kVcMinNnz = 1 << 20;             // smaller levels are launch-bound: no codes
+
+__device__ __forceinline__ unsigned vc_hash(unsigned long long b)
+{
+    b ^= b >> 33;
+    b *= 0xff51afd7ed558ccdULL;
+    b ^= b >> 33;
+    return (unsigned)b & (kVcSlots - 1);
+}
+
+// Inserts bit pattern b into a kVcSlots-slot set (linear probing): 1 when it was new, 0 when it was
+// there, -1 when the set is full.
+__device__ __forceinline__ int vc_insert(unsigned long long* keys, unsigned long long b)
+{
+    unsigned h = vc_hash(b);
+    for (int probe = 0; probe < kVcSlots; probe++) {
+        const unsigned long long k = *(volatile unsigned long long*)(keys + h);
+        if (k == b) return 0;
+        if (k == kVcEmpty) {
+            const unsigned long long old = atomicCAS(keys + h, kVcEmpty, b);
+            if (old == kVcEmpty) return 1;
+            if (old == b) return 0;
+        }
+        h = (h + 1) & (kVcSlots - 1);
+    }
+    return -1;
+}
+
+__global__ void k_vc_collect(long nnz, const double* __restrict__ val, unsigned long long* gkeys, int* gcount, int* over)
+{
+    __shared__ unsigned long long keys[kVcSlots];
+    __shared__ int cnt, full;
+    for (int i = threadIdx.x; i < kVcSlots; i += blockDim.x) keys[i] = kVcEmpty;
+    if (threadIdx.x == 0) {
+        cnt = 0;
+        full = *(volatile int*)over;
+    }
+    __syncthreads();
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += (long)gridDim.x * blockDim.x) {
+        if (*(volatile int*)&full) break;
+        const unsigned long long b = (unsigned long long)__double_as_longlong(__ldcs(val + i));
+        const int r = b == kVcEmpty ? -1 : vc_insert(keys, b);
+        if (r < 0 || (r > 0 && atomicAdd(&cnt, 1) >= kValueCodes)) *(volatile int*)&full = 1;
+    }
+    __syncthreads();
+    if (full) {
+        if (threadIdx.x == 0) atomicExch(over, 1);
+        return;
+    }
+    for (int i = threadIdx.x; i < kVcSlots; i += blockDim.x) {
+        const unsigned long long b = keys[i];
+        if (b == kVcEmpty) continue;
+        const int r = vc_insert(gkeys, b);
+        if (r < 0 || (r > 0 && atomicAdd(gcount, 1) >= kValueCodes)) atomicExch(over, 1);
+    }
+}
+
+// code[i] = the table index of val[i] (every value is in the set)
+__global__ void k_vc_encode(long nnz, const double* __restrict__ val, const unsigned long long* __restrict__ gkeys,
+    const int* __restrict__ slot_code, unsigned char* __restrict__ code)
+{
+    __shared__ unsigned long long keys[kVcSlots];
+    __shared__ unsigned char sc[kVcSlots];
+    for (int i = threadIdx.x; i < kVcSlots; i += blockDim.x) {
+        keys[i] = gkeys[i];
+        sc[i] = (unsigned char)slot_code[i];
+    }
+    __syncthreads();
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += (long)gridDim.x * blockDim.x) {
+        const unsigned long long b = (unsigned long long)__double_as_longlong(__ldcs(val + i));
+        unsigned h = vc_hash(b);
+        for (int probe = 0; probe < kVcSlots && keys[h] != b; probe++) h = (h + 1) & (kVcSlots - 1);
+        code[i] = sc[h];
+    }
+}
+
+// Builds A's value codes when its values take at most kValueCodes distinct bit patterns (and the
+// level is large enough to be bandwidth-bound); BCMGX_VALUE_CODES=0 in the environment turns this
+// off. One host round trip for the distinct values.
+static void build_value_codes(DevCsr& A, cudaStream_t s)
+{
+    A.vcode.release();
+    A.vtab64.release();
+    A.vtab32.release();
+    A.nvalues = 0;
+    const char* env = std::getenv("BCMGX_VALUE_CODES");
+    if (env && env[0] == '0') return;
+    if (A.nnz < kVcMinNnz) return;
+    DBuf<unsigned long long> keys;
+    DBuf<int> cnt;
+    keys.alloc(kVcSlots, s);
+    cnt.alloc(2, s);
+    BCMGX_CUDA(cudaMemsetAsync(keys.p, 0xff, sizeof(unsigned long long) * kVcSlots, s));
+    BCMGX_CUDA(cudaMemsetAsync(cnt.p, 0, 2 * sizeof(int), s));
+    note_launch();
+    k_vc_collect<<<gs_grid(A.nnz), 256, 0, s>>>(A.nnz, A.val.p, keys.p, cnt.p, cnt.p + 1);
+    BCMGX_CHECK_LAUNCH();
+    std::vector<unsigned long long> hk(kVcSlots);
+    int hc[2] = { 0, 0 };
+    BCMGX_CUDA(cudaMemcpyAsync(hk.data(), keys.p, sizeof(unsigned long long) * kVcSlots, cudaMemcpyDeviceToHost, s));
+    BCMGX_CUDA(cudaMemcpyAsync(hc, cnt.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    BCMGX_CUDA(cudaStreamSynchronize(s));
+    if (hc[1] || hc[0] <= 0 || hc[0] > kValueCodes) return;
+    // the table in bit-pattern order (deterministic), the code of every occupied slot
+    std::vector<unsigned long long> vals;
+    for (unsigned long long k : hk)
+        if (k != kVcEmpty) vals.push_back(k);
+    std::sort(vals.begin(), vals.end());
+    std::vector<double> t64(kValueCodes, 0.0);
+    std::vector<float> t32(kValueCodes, 0.0f);
+    for (size_t i = 0; i < vals.size(); i++) {
+        std::memcpy(&t64[i], &vals[i], sizeof(double));
+        t32[i] = (float)t64[i];
+    }
+    std::vector<int> slot_code(kVcSlots, 0);
+    for (int h = 0; h < kVcSlots; h++)
+        if (hk[h] != kVcEmpty)
+            slot_code[h] = (int)(std::lower_bound(vals.begin(), vals.end(), hk[h]) - vals.begin());
+    DBuf<int> sc;
+    sc.alloc(kVcSlots, s);
+    BCMGX_CUDA(cudaMemcpyAsync(sc.p, slot_code.data(), sizeof(int) * kVcSlots, cudaMemcpyHostToDevice, s));
+    A.vtab64.alloc(kValueCodes, s);
+    A.vtab32.alloc(kValueCodes, s);
+    BCMGX_CUDA(cudaMemcpyAsync(A.vtab64.p, t64.data(), sizeof(double) * kValueCodes, cudaMemcpyHostToDevice, s));
+    BCMGX_CUDA(cudaMemcpyAsync(A.vtab32.p, t32.data(), sizeof(float) * kValueCodes, cudaMemcpyHostToDevice, s));
+    A.vcode.alloc(A.nnz, s);
+    note_launch();
+    k_vc_encode<<<gs_grid(A.nnz), 256, 0, s>>>(A.nnz, A.val.p, keys.p, sc.p, A.vcode.p);
+    BCMGX_CHECK_LAUNCH();
+    // the host vectors above are read by the copies before this returns
+    BCMGX_CUDA(cudaStreamSynchronize(s));
+    A.nvalues = (int)vals.size();
+}
+
 void finish_level_matrix(Level& V, bool want_f32, cudaStream_t s)
 {
     const int n = V.A.n;
@@ -1605,6 +1748,7 @@ void finish_level_matrix(Level& V, bool want_f32, cudaStream_t s)
         note_launch(); k_to_f32<<<gs_grid(V.A.nnz), 256, 0, s>>>(V.A.nnz, V.A.val.p, V.A.val32.p);
     }
     BCMGX_CHECK_LAUNCH();
+    build_value_codes(V.A, s);
 }
 
 void build_restriction(Level& V, int nc, bool want_f32, cudaStream_t s)

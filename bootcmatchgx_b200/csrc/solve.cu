@@ -104,8 +104,9 @@ int fit_grid(const void* kernel, int threads, long need_blocks)
     return (int)std::max<long>(1, std::min<long>(need_blocks, (long)num_sms() * b));
 }
 
-template <int OP, typename VT, typename XT, typename FT, typename MT, typename YT, typename IT>
-static void launch_rowop(int tpr, int n, const int* row, const IT* col, const VT* val, const XT* x, const FT* f,
+// VS: the matrix values (ValSrc: a `const T*`, or Coded<T> for a value-indexed matrix).
+template <int OP, typename VS, typename XT, typename FT, typename MT, typename YT, typename IT>
+static void launch_rowop(int tpr, int n, const int* row, const IT* col, VS val, const XT* x, const FT* f,
     const MT* M, YT* y, double alpha, double beta, const int* skip, cudaStream_t s)
 {
     if (n <= 0) return;
@@ -115,12 +116,12 @@ static void launch_rowop(int tpr, int n, const int* row, const IT* col, const VT
         kern<<<fit_grid(kern, 256, need), 256, 0, s>>>(n, row, col, val, x, f, M, y, alpha, beta, skip);
     };
     switch (tpr) {
-    case 1: go(k_rowop<1, OP, VT, XT, FT, MT, YT, IT>); break;
-    case 2: go(k_rowop<2, OP, VT, XT, FT, MT, YT, IT>); break;
-    case 4: go(k_rowop<4, OP, VT, XT, FT, MT, YT, IT>); break;
-    case 8: go(k_rowop<8, OP, VT, XT, FT, MT, YT, IT>); break;
-    case 16: go(k_rowop<16, OP, VT, XT, FT, MT, YT, IT>); break;
-    default: go(k_rowop<32, OP, VT, XT, FT, MT, YT, IT>); break;
+    case 1: go(k_rowop<1, OP, VS, XT, FT, MT, YT, IT>); break;
+    case 2: go(k_rowop<2, OP, VS, XT, FT, MT, YT, IT>); break;
+    case 4: go(k_rowop<4, OP, VS, XT, FT, MT, YT, IT>); break;
+    case 8: go(k_rowop<8, OP, VS, XT, FT, MT, YT, IT>); break;
+    case 16: go(k_rowop<16, OP, VS, XT, FT, MT, YT, IT>); break;
+    default: go(k_rowop<32, OP, VS, XT, FT, MT, YT, IT>); break;
     }
     BCMGX_CHECK_LAUNCH();
 }
@@ -193,16 +194,16 @@ static unsigned long long stage_test_wait_ns()
 }
 
 // The staged form of launch_rowop (staged.cuh): one resident wave of blocks over tiles of R rows.
-template <int S, int OP, typename VT, typename XT, typename FT, typename MT, typename YT, typename IT>
-static void launch_staged(int n, int64_t nnz, const int* row, const IT* col, const VT* val, const XT* x, const FT* f,
+template <int S, int OP, typename VS, typename XT, typename FT, typename MT, typename YT, typename IT>
+static void launch_staged(int n, int64_t nnz, const int* row, const IT* col, VS val, const XT* x, const FT* f,
     const MT* M, YT* y, double alpha, double beta, const int* skip, cudaStream_t s)
 {
-    using C = StageCfg<VT, IT>;
-    auto kern = k_rowop_staged<S, OP, VT, XT, FT, MT, YT, IT>;
+    using C = StageCfg<VS, IT>;
+    auto kern = k_rowop_staged<S, OP, VS, XT, FT, MT, YT, IT>;
     ensure_smem_limit(kern, C::SMEM);
     const int per_sm = blocks_per_sm((const void*)kern, kStageThreads, C::SMEM);
     stage_fault_init();
-    const int R = stage_tile_rows<VT, IT>(n, nnz, S);
+    const int R = stage_tile_rows<VS, IT>(n, nnz, S);
     const long ntiles = ((long)n + R - 1) / R;
     const int grid = (int)std::min<long>(ntiles, (long)per_sm * num_sms());
     const unsigned long long test_ns = stage_test_wait_ns();
@@ -212,16 +213,17 @@ static void launch_staged(int n, int64_t nnz, const int* row, const IT* col, con
     BCMGX_CHECK_LAUNCH();
 }
 
-// The row operation on a level matrix, through its int16 column offsets when it has them, and
-// through the staged kernel when the level's tuning chose it (stage: -1 follows A.staged, 0 / 1
-// force it off / on). The staged kernel exists for 1, 2, 4 and 8 threads per row.
-template <int OP, typename VT, typename XT, typename FT, typename MT, typename YT>
-static void launch_rowop_A(int tpr, const DevCsr& A, const VT* val, const XT* x, const FT* f, const MT* M, YT* y,
-    double alpha, double beta, const int* skip, cudaStream_t s, int stage = -1)
+// The row operation on a level matrix, through its int16 column offsets when it has them, through
+// its value codes when it has them and `val` is the level's own FP64 or FP32 value array (the
+// codes index a table of those same values), and through the staged kernel when the level's
+// tuning chose it (stage: -1 follows A.staged, 0 / 1 force it off / on). The staged kernel exists
+// for 1, 2, 4 and 8 threads per row.
+template <int OP, typename VS, typename XT, typename FT, typename MT, typename YT>
+static void launch_rowop_vs(int tpr, const DevCsr& A, VS val, const void* val_ptr, const XT* x, const FT* f, const MT* M,
+    YT* y, double alpha, double beta, const int* skip, cudaStream_t s, int stage)
 {
-    if (A.n <= 0) return;
     const bool staged = (stage < 0 ? A.staged : stage > 0) && (tpr == 1 || tpr == 2 || tpr == 4 || tpr == 8) &&
-        aligned16(A.row.p) && aligned16(val) && aligned16(A.dcol.p ? (const void*)A.dcol.p : (const void*)A.col.p);
+        aligned16(A.row.p) && aligned16(val_ptr) && aligned16(A.dcol.p ? (const void*)A.dcol.p : (const void*)A.col.p);
     if (staged) {
         auto go = [&](auto* colp) {
             switch (tpr) {
@@ -239,6 +241,28 @@ static void launch_rowop_A(int tpr, const DevCsr& A, const VT* val, const XT* x,
     else launch_rowop<OP>(tpr, A.n, A.row.p, (const int*)A.col.p, val, x, f, M, y, alpha, beta, skip, s);
 }
 
+template <int OP, typename VT, typename XT, typename FT, typename MT, typename YT>
+static void launch_rowop_A(int tpr, const DevCsr& A, const VT* val, const XT* x, const FT* f, const MT* M, YT* y,
+    double alpha, double beta, const int* skip, cudaStream_t s, int stage = -1)
+{
+    if (A.n <= 0) return;
+    const VT* own = nullptr;
+    const VT* tab = nullptr;
+    if constexpr (std::is_same<VT, float>::value) {
+        own = A.val32.p;
+        tab = A.vtab32.p;
+    } else {
+        own = A.val.p;
+        tab = A.vtab64.p;
+    }
+    if (A.vcode.p && tab && val == own) {
+        launch_rowop_vs<OP>(tpr, A, Coded<VT> { A.vcode.p, tab }, (const void*)A.vcode.p, x, f, M, y, alpha, beta,
+            skip, s, stage);
+        return;
+    }
+    launch_rowop_vs<OP>(tpr, A, val, (const void*)val, x, f, M, y, alpha, beta, skip, s, stage);
+}
+
 // About 6-8 entries per lane: 27-point rows -> 4 lanes, 7-point rows -> 2 lanes.
 int default_tpr(int n, int64_t nnz)
 {
@@ -254,8 +278,8 @@ int default_tpr(int n, int64_t nnz)
 void launch_spmv(int n, const int* row, const int* col, const double* val, const double* x, double* y,
     double alpha, double beta, int tpr, cudaStream_t s)
 {
-    launch_rowop<OP_AXPBY, double, double, double, double, double>(tpr, n, row, col, val, x,
-        (const double*)nullptr, (const double*)nullptr, y, alpha, beta, nullptr, s);
+    launch_rowop<OP_AXPBY>(tpr, n, row, col, val, x, (const double*)nullptr, (const double*)nullptr, y, alpha, beta,
+        nullptr, s);
 }
 
 void rowop_spmv(const DevCsr& A, const double* x, double* y, const int* skip, cudaStream_t s)

@@ -33,32 +33,42 @@ constexpr int kStageThreads = (kStageWarps + 1) * 32;
 constexpr int kStageMaxRows = kStageWarps * 32;  // rows per tile at most: one per lane (S = 1)
 constexpr int kStageRowSlots = kStageMaxRows + 8;
 
-// Shared-memory budget per value / index type: 4 stages of 18 KB for 6-byte entries (3 blocks
-// per SM), 3 stages of 30 KB for wider entries (2 blocks per SM).
-template <typename VT, typename IT>
+// Shared-memory budget per value source / index type: 4 stages of 18 KB for entries of at most 6
+// bytes (3 blocks per SM), 3 stages of 30 KB for wider entries (2 blocks per SM). A coded matrix
+// (ValSrc: one byte per entry) also keeps its value table after the stages.
+template <typename VS, typename IT>
 struct StageCfg {
-    static constexpr int kEntry = (int)(sizeof(VT) + sizeof(IT));
+    using VT = typename ValSrc<VS>::type;
+    static constexpr bool kCoded = ValSrc<VS>::coded;
+    static constexpr int kVal = ValSrc<VS>::bytes;                 // value bytes streamed per entry
+    static constexpr int kEntry = (int)sizeof(IT) + kVal;
+    // entries per copy granule: both streams of a tile move whole 16-byte granules
+    static constexpr int G = std::max(8, 16 / std::min((int)sizeof(IT), kVal));
     static constexpr int kBytes = kEntry <= 6 ? 18432 : 30720;
     static constexpr int NS = kEntry <= 6 ? 4 : 3;
-    static constexpr int CAP = ((kBytes - kStageRowSlots * 4) / kEntry) & ~7;   // entries per stage
-    static constexpr int COLS = kStageRowSlots * 4;                             // byte offsets in a stage
+    static constexpr int CAP = ((kBytes - kStageRowSlots * 4) / kEntry) & ~(G - 1);   // entries per stage
+    static constexpr int COLS = kStageRowSlots * 4;                                  // byte offsets in a stage
     static constexpr int VALS = COLS + CAP * (int)sizeof(IT);
-    static constexpr int STAGE = VALS + CAP * (int)sizeof(VT);
-    static constexpr int SMEM = NS * STAGE;
+    static constexpr int STAGE = VALS + CAP * kVal;
+    static constexpr int TAB = NS * STAGE;                                          // the value table (coded)
+    static constexpr int SMEM = TAB + (kCoded ? kValueCodes * (int)sizeof(VT) : 0);
     static_assert(COLS % 16 == 0 && VALS % 16 == 0 && STAGE % 16 == 0, "stage layout must keep 16-byte granules");
+    static_assert((G * (int)sizeof(IT)) % 16 == 0 && (G * kVal) % 16 == 0, "a granule must be whole 16-byte units");
     static_assert(SMEM <= 227 * 1024, "the stage ring must fit a block's shared memory");
     static_assert(CAP >= 64 * 8, "a stage must hold a useful tile");
     static_assert((kStageMaxRows + 4) <= kStageRowSlots, "a tile's widened row offsets must fit their slots");
 };
 
 // Rows per tile for a matrix of n rows and nnz entries and S threads per row: the largest multiple
-// of 4 whose entries (average row length plus 4 %) fit a stage, at most one row per consumer
-// sub-warp (kStageWarps * 32 / S), so that every sub-warp owns at most one row of a tile.
-template <typename VT, typename IT>
+// of 4 whose entries (average row length plus 4 %, plus the widening to whole granules) fit a
+// stage, at most one row per consumer sub-warp (kStageWarps * 32 / S), so that every sub-warp owns
+// at most one row of a tile.
+template <typename VS, typename IT>
 inline int stage_tile_rows(int n, int64_t nnz, int S)
 {
+    using C = StageCfg<VS, IT>;
     const double avg = n > 0 ? std::max(1.0, (double)nnz / n) : 1.0;
-    int r = (int)((StageCfg<VT, IT>::CAP - 16) / (avg * 1.04));
+    int r = (int)((C::CAP - 2 * C::G) / (avg * 1.04));
     r = std::min(r, kStageWarps * 32 / S) & ~3;
     return std::max(r, 4);
 }
@@ -149,26 +159,32 @@ __device__ __forceinline__ void row_operands(int r, const XT* __restrict__ x, co
 
 // The operations of k_rowop (y = alpha A x + beta y, y = f - A x, or one l1-Jacobi sweep) over
 // tiles of R rows, tile t on block t mod gridDim.x, row i of a tile on consumer sub-warp i.
-// Launch with kStageThreads threads and StageCfg<VT, IT>::SMEM bytes of dynamic shared memory;
-// R = stage_tile_rows<VT, IT>(n, nnz, S): a multiple of 4, at most kStageWarps * 32 / S.
+// Launch with kStageThreads threads and StageCfg<VS, IT>::SMEM bytes of dynamic shared memory;
+// R = stage_tile_rows<VS, IT>(n, nnz, S): a multiple of 4, at most kStageWarps * 32 / S. VS: the
+// values, stored or coded (the codes are staged, the table sits in shared memory).
 // wait_ns: limit of the producer's and the consumers' stage waits (kStageWaitNs in production).
 // drop_first: a fault-path test hook; when set, block 0's producer issues no copy for its first
 // tile, so that the consumers' wait for that stage runs out (the drain skips that stage, which
 // has no copy in flight).
-template <int S, int OP, typename VT, typename XT, typename FT, typename MT, typename YT, typename IT>
+template <int S, int OP, typename VS, typename XT, typename FT, typename MT, typename YT, typename IT>
 __global__ void __launch_bounds__(kStageThreads) k_rowop_staged(int n, int R, const int* __restrict__ row,
-    const IT* __restrict__ col, const VT* __restrict__ val, const XT* __restrict__ x, const FT* __restrict__ f,
+    const IT* __restrict__ col, VS val, const XT* __restrict__ x, const FT* __restrict__ f,
     const MT* __restrict__ M, YT* __restrict__ y, double alpha, double beta, const int* __restrict__ skip,
     int* __restrict__ fault, unsigned long long wait_ns, int drop_first)
 {
     if (skip && *skip) return;
-    using C = StageCfg<VT, IT>;
+    using C = StageCfg<VS, IT>;
+    using VT = typename C::VT;
     using AT = typename Acc<VT>::type;
-    constexpr int NS = C::NS, CAP = C::CAP, K = 8, SPW = 32 / S;
+    constexpr int NS = C::NS, CAP = C::CAP, K = 8, SPW = 32 / S, G = C::G;
     __shared__ unsigned long long full[NS], empty[NS];
     __shared__ int meta[NS][2];   // widened first entry of the stage; 1 when its entries are staged
     const int warp = threadIdx.x >> 5, l32 = threadIdx.x & 31;
     const int ntiles = (int)(((long)n + R - 1) / R);
+    VT* tab_s = (VT*)(stage_smem + C::TAB);
+    if constexpr (C::kCoded) {
+        for (int i = threadIdx.x; i < kValueCodes; i += blockDim.x) tab_s[i] = __ldg(val.tab + i);
+    }
     if (threadIdx.x == 0) {
         for (int k = 0; k < NS; k++) {
             mbar_init(&full[k], 1);
@@ -191,7 +207,7 @@ __global__ void __launch_bounds__(kStageThreads) k_rowop_staged(int n, int R, co
             }
             if (it == dropped) continue;
             const int t0 = t * R, t1 = min(t0 + R, n);
-            const int a0 = __ldg(row + t0) & ~7, a1 = (__ldg(row + t1) + 7) & ~7;
+            const int a0 = __ldg(row + t0) & ~(G - 1), a1 = (__ldg(row + t1) + G - 1) & ~(G - 1);
             const int cnt = a1 - a0, nrp = (t1 - t0 + 4) & ~3;
             const bool fits = cnt <= CAP;
             unsigned char* base = stage_smem + st * C::STAGE;
@@ -202,7 +218,10 @@ __global__ void __launch_bounds__(kStageThreads) k_rowop_staged(int n, int R, co
             bulk_to_smem(base, row + t0, (unsigned)nrp * 4u, &full[st], pol);
             if (fits && cnt > 0) {
                 bulk_to_smem(base + C::COLS, col + a0, (unsigned)cnt * (unsigned)sizeof(IT), &full[st], pol);
-                bulk_to_smem(base + C::VALS, val + a0, (unsigned)cnt * (unsigned)sizeof(VT), &full[st], pol);
+                if constexpr (C::kCoded)
+                    bulk_to_smem(base + C::VALS, val.code + a0, (unsigned)cnt, &full[st], pol);
+                else
+                    bulk_to_smem(base + C::VALS, val + a0, (unsigned)cnt * (unsigned)sizeof(VT), &full[st], pol);
             }
         }
         // the copies still in flight land before the block's shared memory is released
@@ -232,6 +251,7 @@ __global__ void __launch_bounds__(kStageThreads) k_rowop_staged(int n, int R, co
         const int* rp = (const int*)base;
         const IT* cs = (const IT*)(base + C::COLS) - a0;
         const VT* vs = (const VT*)(base + C::VALS) - a0;
+        const unsigned char* vc = (const unsigned char*)(base + C::VALS) - a0;   // codes (coded values)
         // partial sum of row i of the tile over this lane's entries (reads the stage)
         auto row_sum = [&](int i) {
             AT s = 0;
@@ -247,7 +267,8 @@ __global__ void __launch_bounds__(kStageThreads) k_rowop_staged(int n, int R, co
                         for (int k = 0; k < K; k++) {
                             const int j = j0 + k * S;
                             c[k] = j < e ? col_of(cs[j], r) : -1;
-                            v[k] = j < e ? vs[j] : VT(0);
+                            if constexpr (C::kCoded) v[k] = j < e ? tab_s[vc[j]] : VT(0);
+                            else v[k] = j < e ? vs[j] : VT(0);
                         }
 #pragma unroll
                         for (int k = 0; k < K; k++) xv[k] = c[k] >= 0 ? ld_ro(x + c[k]) : XT(0);

@@ -127,6 +127,8 @@ typedef struct bcmgx_hierarchy_info {
                                     staged kernel (matrix entries through shared memory) with -tpr */
     int index_bytes[BCMGX_MAX_LEVELS]; /* column index bytes the solve kernels stream per entry
                                           (2: int16 offsets from the diagonal, 4: int32) */
+    int value_codes[BCMGX_MAX_LEVELS]; /* distinct values of a level whose solve kernels stream
+                                          one-byte value codes (value-indexed CSR), else 0 */
 } bcmgx_hierarchy_info;
 
 typedef struct bcmgx_hierarchy bcmgx_hierarchy;

@@ -106,3 +106,68 @@ def test_autotuned_codes_are_reported(bx, cuda):
     for t in h.info()["tpr"]:
         assert t in (1, 2, 4, 8, 16, 32, -1, -2, -4, -8)
     h.free()
+
+
+# matrices of at least 2^20 entries with few distinct values: their row kernels stream one-byte
+# value codes (value-indexed CSR) on the large levels
+CODED = [("lap27", (40, 40, 40)), ("lap7", (110, 100, 100)), ("shift", (100, 100, 100))]
+
+
+def coded_matrix(bx, case):
+    kind, arg = case
+    if kind == "shift":   # 7-point Laplacian with a per-row diagonal shift taking 7 values
+        A = as_csr(bx, ("lap7", arg)).tocsr()
+        d = A.diagonal() + 0.125 * (np.arange(A.shape[0]) % 7)
+        A.setdiag(d)
+        A.sort_indices()
+        return A
+    return as_csr(bx, case)
+
+
+def solve_with_codes(bx, monkeypatch, A, b, codes, tpr, **kw):
+    monkeypatch.setenv("BCMGX_VALUE_CODES", "1" if codes else "0")
+    if tpr:
+        monkeypatch.setenv("BCMGX_TPR", str(tpr))
+    try:
+        h = bx.prec_setup(A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data, fcg(bx, **kw))
+    finally:
+        monkeypatch.delenv("BCMGX_VALUE_CODES")
+        if tpr:
+            monkeypatch.delenv("BCMGX_TPR")
+    x, info = h.solve(b.copy())
+    hi = h.info()
+    h.free()
+    return x, info, hi
+
+
+@pytest.mark.parametrize("prec", ["FP64", "FP32"])
+@pytest.mark.parametrize("tpr", [0, -4, 4, -1])
+@pytest.mark.parametrize("case", CODED)
+def test_value_codes_bit_identical(bx, cuda, monkeypatch, case, tpr, prec):
+    """Level matrices with at most 256 distinct values stream one-byte codes into a table of those
+    values (value-indexed CSR); the set-up and the solve give the same iterations and solution
+    bit for bit as with the stored values, on the staged and the plain row kernels (tpr 0: the
+    autotuner's choice)."""
+    A = coded_matrix(bx, case)
+    b = A @ np.random.default_rng(9).uniform(-1, 1, A.shape[0])
+    xc, ic, hc = solve_with_codes(bx, monkeypatch, A, b, True, tpr, rtol=1e-8, vcycle_precision=prec)
+    xs, is_, hs = solve_with_codes(bx, monkeypatch, A, b, False, tpr, rtol=1e-8, vcycle_precision=prec)
+    assert hc["value_codes"][0] > 0 and all(v == 0 for v in hs["value_codes"])
+    assert ic["status"] == 0 and is_["status"] == 0
+    if tpr or hc["tpr"] == hs["tpr"]:
+        assert ic["niter"] == is_["niter"]
+        assert np.array_equal(xc, xs)
+    else:   # the autotuner chose other lanes per row on some level: another summation order
+        assert abs(ic["niter"] - is_["niter"]) <= 1
+        assert np.linalg.norm(xc - xs) / np.linalg.norm(xs) < 1e-9
+
+
+def test_value_codes_need_few_values(bx, cuda):
+    """A level with more than 256 distinct values keeps its stored values."""
+    A = coded_matrix(bx, ("lap7", (110, 100, 100))).tocsr()
+    A.data = A.data * (1.0 + 1e-3 * np.random.default_rng(1).random(A.nnz))
+    A = ((A + A.T) * 0.5).tocsr()
+    A.sort_indices()
+    h = bx.prec_setup(A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data, fcg(bx))
+    assert h.info()["value_codes"][0] == 0
+    h.free()

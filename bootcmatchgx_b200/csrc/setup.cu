@@ -241,6 +241,62 @@ __global__ void k_validate(int n, int m, long long nnz, const int* __restrict__ 
     if (lane == 0 && mx > 0) atomicMax(max_row, mx);
 }
 
+// The input checks of k_validate with 8 lanes per row (4 rows of a warp in flight, the previous
+// column passed by shuffles), plus the largest |col - row| and, when dcol is given, every column
+// as an int16 offset from its row (clamped; the caller keeps them only when the largest offset
+// fits): one pass over the input instead of three.
+__global__ void k_validate_offsets(int n, int m, long long nnz, const int* __restrict__ row, const int* __restrict__ col,
+    int* err, int* max_row, int* max_off, short* __restrict__ dcol, int need_diag)
+{
+    constexpr int S = 8;
+    const int lane = threadIdx.x & (S - 1);
+    const int sub = (threadIdx.x & 31) / S;
+    const unsigned mask = 0xffu << (sub * S);
+    const long stride = (long)gridDim.x * blockDim.x / S;
+    int mx = 0, mo = 0;
+    for (long base = ((long)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) / S; base < n; base += stride) {
+        const long r = base + sub;
+        int bad = 0;
+        if (r < n) {
+            const int b = row[r], e = row[r + 1];
+            if (r == 0 && b != 0) bad |= ERR_ROW0;
+            if (r == n - 1 && (long long)e != nnz) bad |= ERR_ROWN;
+            if (e < b || b < 0 || (long long)e > nnz) {
+                bad |= ERR_ROWORDER;
+            } else {
+                bool diag = false;
+                int carry = 0;
+                for (int j0 = b; j0 < e; j0 += S) {
+                    const int j = j0 + lane;
+                    const int c = j < e ? __ldcs(col + j) : 0x7fffffff;
+                    int prev = __shfl_up_sync(mask, c, 1, S);
+                    if (lane == 0) prev = carry;
+                    if (j < e) {
+                        if (c < 0 || c >= m) bad |= ERR_COLRANGE;
+                        if (j > b && prev >= c) bad |= ERR_COLSORT;
+                        if (c == (int)r) diag = true;
+                        const int off = c - (int)r;
+                        mo = max(mo, off < 0 ? -off : off);
+                        if (dcol) dcol[j] = (short)max(-32768, min(32767, off));
+                    }
+                    carry = __shfl_sync(mask, c, S - 1, S);
+                }
+                diag = (__ballot_sync(mask, diag) & mask) != 0;
+                if (need_diag && !diag) bad |= ERR_NODIAG;
+                mx = max(mx, e - b);
+            }
+        }
+        bad = __reduce_or_sync(0xffffffffu, bad);
+        if ((threadIdx.x & 31) == 0 && bad) atomicOr(err, bad);
+    }
+    mx = __reduce_max_sync(0xffffffffu, mx);
+    mo = __reduce_max_sync(0xffffffffu, mo);
+    if ((threadIdx.x & 31) == 0) {
+        if (mx > 0) atomicMax(max_row, mx);
+        if (mo > 0) atomicMax(max_off, mo);
+    }
+}
+
 __global__ void k_row_max(int n, const int* __restrict__ row, int* max_row)
 {
     int mx = 0;
@@ -255,8 +311,17 @@ __global__ void k_abs_row_sum(int n, const int* __restrict__ row, const double* 
     float* __restrict__ M32)
 {
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        // the row's values are loaded 8 at a time (independent loads), then added in column order
         double s = 0.0;
-        for (int j = row[i]; j < row[i + 1]; j++) s = __dadd_rn(s, fabs(val[j]));
+        const int b = row[i], e = row[i + 1];
+        for (int j0 = b; j0 < e; j0 += 8) {
+            double v[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) v[k] = j0 + k < e ? __ldcs(val + j0 + k) : 0.0;
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+                if (j0 + k < e) s = __dadd_rn(s, fabs(v[k]));
+        }
         M[i] = s;
         if (M32) M32[i] = (float)s;
     }
@@ -295,17 +360,28 @@ __global__ void k_fill(long n, double* a, double v)
 __global__ void k_diag_c(int n, const int* __restrict__ row, const int* __restrict__ col, const double* __restrict__ val,
     const double* __restrict__ w, double* __restrict__ C, int* err)
 {
-    for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long)gridDim.x * blockDim.x) {
-        double c = 0.0;
-        bool found = false;
-        for (int j = row[r]; j < row[r + 1]; j++)
-            if (col[j] == r) {
-                c = __dmul_rn(__dmul_rn(val[j], w[r]), w[r]);
-                found = true;
-                break;
-            }
-        C[r] = c;
-        if (!found) atomicOr(err, ERR_NODIAG);
+    // 8 lanes per row look for the row's first diagonal entry together (4 rows of a warp in flight)
+    constexpr int S = 8;
+    const int lane = threadIdx.x & (S - 1);
+    const int sub = (threadIdx.x & 31) / S;
+    const unsigned mask = 0xffu << (sub * S);
+    const long stride = (long)gridDim.x * blockDim.x / S;
+    for (long base = ((long)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) / S; base < n; base += stride) {
+        const long r = base + sub;
+        if (r >= n) continue;
+        const int b = row[r], e = row[r + 1];
+        int found = -1;
+        for (int j0 = b; j0 < e && found < 0; j0 += S) {
+            const int j = j0 + lane;
+            const unsigned hit = __ballot_sync(mask, j < e && col[j] == (int)r) & mask;
+            if (hit) found = j0 + (__ffs(hit >> (sub * S)) - 1);
+        }
+        if (lane == 0) {
+            double c = 0.0;
+            if (found >= 0) c = __dmul_rn(__dmul_rn(val[found], w[r]), w[r]);
+            else atomicOr(err, ERR_NODIAG);
+            C[r] = c;
+        }
     }
 }
 
@@ -1581,7 +1657,7 @@ static void build_offsets(DevCsr& A, cudaStream_t s)
 {
     const char* env = std::getenv("BCMGX_INDEX16");
     if (env && env[0] == '0') return;
-    if (A.n <= 0 || A.nnz <= 0) return;
+    if (A.n <= 0 || A.nnz <= 0 || A.dcol.p) return;
     DBuf<int> mx;
     mx.alloc(1, s);
     BCMGX_CUDA(cudaMemsetAsync(mx.p, 0, sizeof(int), s));
@@ -1820,17 +1896,23 @@ void build_hierarchy(bcmgx_hierarchy* H, const bcmgx_csr* Ain)
     BCMGX_CUDA(cudaMemcpyAsync(A.col.p, Ain->col, sizeof(int) * A.nnz, kind, s));
     BCMGX_CUDA(cudaMemcpyAsync(A.val.p, Ain->val, sizeof(double) * A.nnz, kind, s));
     {
-        DBuf<int> err, mx;
-        err.alloc(1, s);
-        mx.alloc(1, s);
-        BCMGX_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), s));
-        BCMGX_CUDA(cudaMemsetAsync(mx.p, 0, sizeof(int), s));
-        note_launch(); k_validate<<<warp_grid(A.n), 256, 0, s>>>(A.n, A.m, A.nnz, A.row.p, A.col.p, err.p, mx.p,
-            P.preconditioner == BCMGX_PREC_BCMG ? 1 : 0);
+        // checks, longest row, largest column offset and the int16 offsets in one pass and one
+        // round trip; the offsets are kept when they all fit (build_offsets then has nothing to do)
+        DBuf<int> st;
+        st.alloc(3, s);
+        BCMGX_CUDA(cudaMemsetAsync(st.p, 0, 3 * sizeof(int), s));
+        const char* env16 = std::getenv("BCMGX_INDEX16");
+        const bool want16 = !(env16 && env16[0] == '0');
+        if (want16) A.dcol.alloc(A.nnz, s);
+        note_launch(); k_validate_offsets<<<gs_grid((long)A.n * 8), 256, 0, s>>>(A.n, A.m, A.nnz, A.row.p, A.col.p,
+            st.p, st.p + 1, st.p + 2, want16 ? A.dcol.p : nullptr, P.preconditioner == BCMGX_PREC_BCMG ? 1 : 0);
         BCMGX_CHECK_LAUNCH();
-        int e = read_err(err.p, s);
-        if (e) throw Error(BCMGX_ERR_INVALID_INPUT, "input matrix: " + err_text(e));
-        A.max_row = read_err(mx.p, s);
+        int h[3] = { 0, 0, 0 };
+        BCMGX_CUDA(cudaMemcpyAsync(h, st.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, s));
+        BCMGX_CUDA(cudaStreamSynchronize(s));
+        if (h[0]) throw Error(BCMGX_ERR_INVALID_INPUT, "input matrix: " + err_text(h[0]));
+        A.max_row = h[1];
+        if (h[2] > 32767) A.dcol.release();
     }
     const int L0n = A.n;
     H->grid_sweeps = grid_sweeps(P.cycle_type, P.max_levels);

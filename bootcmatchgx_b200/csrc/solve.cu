@@ -1240,7 +1240,8 @@ void time_level_kernels(bcmgx_hierarchy* H, int l, int reps, double* out)
         out[0] = timeit([&] { launch_rowop_A<OP_JACOBI>(A.tpr, A, A.val.p, (const double*)a.p, (const double*)c.p, V.M.p, b.p, 1.0, 0.0, nullptr, s); });
         out[1] = timeit([&] { launch_rowop_A<OP_RESID>(A.tpr, A, A.val.p, (const double*)a.p, (const double*)c.p, (const double*)nullptr, b.p, 1.0, 0.0, nullptr, s); });
     }
-    out[2] = timeit([&] { launch_spmv(n, A.row.p, A.col.p, A.val.p, a.p, b.p, 1.0, 0.0, A.tpr, s); });
+    // the public SpMV (bcmgx_spmv) on the stored CSR arrays, with its default threads per row
+    out[2] = timeit([&] { launch_spmv(n, A.row.p, A.col.p, A.val.p, a.p, b.p, 1.0, 0.0, default_tpr(n, A.nnz), s); });
     out[3] = 0;
     out[4] = 0;
     out[5] = 0;

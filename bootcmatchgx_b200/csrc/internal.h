@@ -150,6 +150,15 @@ struct SweepRecord {
 };
 
 // Typed view of a device vector (or block of vectors) used by the V-cycle.
+// A recorded persistent cycle program (persist.cuh) of one set of cycle arguments.
+struct PStep;
+struct PersistProgram {
+    int level = -1;
+    bool has_x = false;   // the call starts from the level's iterate (else from zero)
+    DBuf<PStep> steps;
+    int nsteps = 0;
+};
+
 struct Vec {
     void* p = nullptr;
     bool f32 = false;
@@ -213,6 +222,10 @@ struct bcmgx_hierarchy {
     bcmgx::DBuf<double> gb, gx;
     long long graph_startup_kernels = 0, graph_body_kernels = 0;
     bcmgx::CycleBufs cyc;                 // single-vector cycle buffers (views of lv[l] and res)
+    // the persistent coarse cycle: first level it covers (-1: none), its barrier words, programs
+    int persist_level = -1;
+    bcmgx::DBuf<unsigned> persist_bar;
+    std::vector<std::unique_ptr<bcmgx::PersistProgram>> persist;
     // multi-right-hand-side solve: its scratch and its captured graph (for multi_k columns)
     bcmgx::MultiWork* multi = nullptr;
     bcmgx::KrylovWork* krylov = nullptr;   // solvers other than FCG
@@ -285,6 +298,8 @@ int setup_grid(long n, int threads = 256);
 void ensure_solve_workspace(bcmgx_hierarchy* H);
 int fcg_solve(bcmgx_hierarchy* H, const double* b_dev, double* x_dev, bcmgx_solve_info* info);
 void prec_apply_dev(bcmgx_hierarchy* H, const double* r, double* v);
+// resets the persistent cycle's barrier state (start of a solve of another driver)
+void persist_reset_ext(bcmgx_hierarchy* H, cudaStream_t s);
 void prec_apply_impl(bcmgx_hierarchy* H, const double* r, double* v, const int* skip);
 // AFSAI preconditioner (afsai.cu): set-up of G and G^T, application v = G^T G r.
 void afsai_build_dev(bcmgx_hierarchy* H);

@@ -387,6 +387,7 @@ void startup_common(bcmgx_hierarchy* H, KrylovWork& wk, const double* b, const d
 {
     cudaStream_t s = H->stream;
     const DevCsr& A = H->lv[0].A;
+    persist_reset_ext(H, s);
     note_launch();
     k_kry_init<<<1, 1, 0, s>>>(wk.st.p, H->prm.itnlim);
     rowop_resid(A, x, b, H->r.p, nullptr, s);   // r = b - A x0

@@ -16,6 +16,7 @@
 #include "rowops.cuh"
 #include "staged.cuh"
 #include "blockops.cuh"
+#include "persist.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -151,8 +152,8 @@ static void fill_probe(T* a, long n, unsigned salt, cudaStream_t s)
     BCMGX_CHECK_LAUNCH();
 }
 
-// Fault word of the staged row kernels, in mapped pinned host memory: nonzero when one of their
-// waits on a shared-memory stage gave up. The entry points read it after their final stream
+// Fault word of the staged row kernels and the persistent cycle, in mapped pinned host memory:
+// nonzero when one of their waits (on a shared-memory stage, at a grid barrier: code 8) gave up. The entry points read it after their final stream
 // synchronisation (stage_fault_check), so the check costs no copy. It is one word for the
 // process: with solves on several threads, the entry point that reads it first reports it.
 static int* g_stage_fault = nullptr;
@@ -173,6 +174,8 @@ void stage_fault_check()
     if (g_stage_fault && *(volatile int*)g_stage_fault) {
         const int code = *(volatile int*)g_stage_fault;
         *(volatile int*)g_stage_fault = 0;
+        if (code == 8)
+            throw Error(BCMGX_ERR_TIMEOUT, "persistent cycle: a wait at a grid barrier gave up (code 8)");
         throw Error(BCMGX_ERR_TIMEOUT, "staged row kernel: a wait on a shared-memory stage gave up (code " +
             std::to_string(code) + ")");
     }
@@ -444,6 +447,63 @@ static void launch_blk_rowop(int n, int m, int ld, int K, const int* row, const 
 // the cycle: one code path for a single vector (lk < 0: the sub-warp row kernels above) and for
 // blocks of 2^lk right-hand sides (the block kernels of blockops.cuh)
 // ------------------------------------------------------------------------------------------
+template <typename T> static int tcode() { return std::is_same<T, float>::value ? 1 : 0; }
+
+// Launches k_persist cooperatively (every block resident) with up to two blocks per SM; af, ax,
+// ay: the vectors of the program's argument slots.
+static void launch_persist(bcmgx_hierarchy* H, const PStep* steps, int nsteps, const int* skip, cudaStream_t s,
+    const void* af, const void* ax, void* ay)
+{
+    stage_fault_init();
+    const int per_sm = std::min(2, blocks_per_sm((const void*)k_persist, kPersistThreads, 0));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(num_sms() * std::max(per_sm, 1)));
+    cfg.blockDim = dim3(kPersistThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    // fault-path test hook: BCMGX_TEST_PERSIST_FAULT=<ns> (read at every launch; a captured graph
+    // keeps the value of its capture) shortens the barrier wait and drops block 0
+    unsigned long long wait_ns = kPersistWaitNs;
+    int drop = 0;
+    if (const char* e = std::getenv("BCMGX_TEST_PERSIST_FAULT"))
+        if (std::atoll(e) > 0) {
+            wait_ns = (unsigned long long)std::atoll(e);
+            drop = 1;
+        }
+    note_launch();
+    BCMGX_CUDA(cudaLaunchKernelEx(&cfg, k_persist, steps, nsteps, H->persist_bar.p, g_stage_fault, skip, af, ax, ay,
+        wait_ns, drop));
+}
+
+// Resets the persistent cycle's barrier words (and a poisoned state left by a timeout); once at
+// the start of every solve or preconditioner application.
+static void persist_reset(bcmgx_hierarchy* H, cudaStream_t s)
+{
+    if (H->persist_level >= 0) BCMGX_CUDA(cudaMemsetAsync(H->persist_bar.p, 0, 4 * sizeof(unsigned), s));
+}
+
+// Entries of the largest level that the persistent cycle takes (BCMGX_PERSIST_NNZ overrides it;
+// 0 turns the persistent cycle off).
+constexpr int64_t kPersistMaxNnz = 2 << 20;
+
+static int choose_persist_level(const bcmgx_hierarchy* H)
+{
+    int64_t limit = kPersistMaxNnz;
+    if (const char* e = std::getenv("BCMGX_PERSIST_NNZ")) limit = std::atoll(e);
+    if (limit <= 0 || H->prm.preconditioner != BCMGX_PREC_BCMG) return -1;
+    int lc = -1;
+    for (int l = (int)H->lv.size() - 1; l >= 0; l--) {
+        if (H->lv[l].A.nnz > limit) break;
+        lc = l;
+    }
+    return lc;
+}
+
 struct Cycle {
     bcmgx_hierarchy* H;
     const CycleBufs& B;
@@ -452,6 +512,8 @@ struct Cycle {
     bool fp32;
     int L;
     int lk;   // -1: single vector; else the block has 2^lk columns (leading dimension 2^lk)
+    // recording mode (persist.cuh): the steps are appended here instead of launched
+    std::vector<PStep>* rec = nullptr;
 
     bool lf32(int l) const { return fp32 && l < L - 1; }
     Level& lv(int l) const { return H->lv[l]; }
@@ -462,12 +524,53 @@ struct Cycle {
     template <int OP, typename VT, typename XT, typename FT, typename MT, typename YT>
     void rowop(const DevCsr& A, const VT* val, const XT* x, const FT* f, const MT* M, YT* y) const
     {
+        if (rec) {
+            PStep p {};
+            p.op = OP == OP_JACOBI ? P_JACOBI : P_RESID;
+            p.n = A.n;
+            p.S = A.tpr;
+            p.vt = tcode<VT>();
+            const VT* own = std::is_same<VT, float>::value ? (const VT*)A.val32.p : (const VT*)A.val.p;
+            const void* tab = std::is_same<VT, float>::value ? (const void*)A.vtab32.p : (const void*)A.vtab64.p;
+            p.coded = (A.vcode.p && tab && val == own) ? 1 : 0;
+            p.val = p.coded ? tab : (const void*)val;
+            p.code = p.coded ? A.vcode.p : nullptr;
+            p.col16 = A.dcol.p ? 1 : 0;
+            p.col = A.dcol.p ? (const void*)A.dcol.p : (const void*)A.col.p;
+            p.row = A.row.p;
+            p.x = x;
+            p.xt = tcode<XT>();
+            p.f = f;
+            p.ft = tcode<FT>();
+            p.M = M;
+            p.mt = tcode<MT>();
+            p.y = y;
+            p.yt = tcode<YT>();
+            BCMGX_REQUIRE(OP != OP_AXPBY && p.xt == p.vt, BCMGX_ERR_INTERNAL, "cycle step without a persistent form");
+            rec->push_back(p);
+            return;
+        }
         if (lk < 0) launch_rowop_A<OP>(A.tpr, A, val, x, f, M, y, 1.0, 0.0, skip, s);
         else launch_blk_rowop<OP>(A.n, A.m, 1 << lk, 1 << lk, A.row.p, A.col.p, val, x, f, M, y, 1.0, 0.0, skip, s);
     }
     template <typename FT, typename MT, typename YT, typename CT>
     void first(int n, const FT* f, const MT* M, YT* u, CT* fcopy) const
     {
+        if (rec) {
+            PStep p {};
+            p.op = P_FIRST;
+            p.n = n;
+            p.f = f;
+            p.ft = tcode<FT>();
+            p.M = M;
+            p.mt = tcode<MT>();
+            p.y = u;
+            p.yt = tcode<YT>();
+            p.extra = fcopy;
+            p.ct = tcode<CT>();
+            rec->push_back(p);
+            return;
+        }
         note_launch();
         if (lk >= 0) {
             auto k = k_blk_first_sweep<FT, MT, YT, CT>;
@@ -481,6 +584,17 @@ struct Cycle {
     template <typename ST, typename DT>
     void convert(int n, const ST* a, DT* b) const
     {
+        if (rec) {
+            PStep p {};
+            p.op = P_CONVERT;
+            p.n = n;
+            p.x = a;
+            p.xt = tcode<ST>();
+            p.y = b;
+            p.yt = tcode<DT>();
+            rec->push_back(p);
+            return;
+        }
         note_launch();
         if (lk >= 0) {
             auto k = k_blk_convert<ST, DT>;
@@ -494,6 +608,15 @@ struct Cycle {
     template <typename T>
     void zero_n(int n, T* a) const
     {
+        if (rec) {
+            PStep p {};
+            p.op = P_ZERO;
+            p.n = n;
+            p.y = a;
+            p.yt = tcode<T>();
+            rec->push_back(p);
+            return;
+        }
         note_launch();
         if (lk >= 0) {
             auto k = k_blk_zero<T>;
@@ -508,6 +631,21 @@ struct Cycle {
     template <typename RT, typename WT, typename OT>
     void restrict_to(int nc, const Level& V, const WT* rval, const RT* res, OT* out) const
     {
+        if (rec) {
+            PStep p {};
+            p.op = P_RESTRICT;
+            p.n = nc;
+            p.idx = V.rptr.p;
+            p.idx2 = V.ridx.p;
+            p.M = rval;
+            p.mt = tcode<WT>();
+            p.f = res;
+            p.ft = tcode<RT>();
+            p.y = out;
+            p.yt = tcode<OT>();
+            rec->push_back(p);
+            return;
+        }
         if (lk >= 0) {
             launch_blk_rowop<OP_AXPBY>(nc, V.A.n, 1 << lk, 1 << lk, V.rptr.p, V.ridx.p, rval, res, (const OT*)nullptr,
                 (const OT*)nullptr, out, 1.0, 0.0, skip, s);
@@ -521,6 +659,22 @@ struct Cycle {
     template <typename PT, typename CT, typename XT, typename YT>
     void prolong(int n, const Level& V, const PT* p, const CT* xc, const XT* x, YT* y) const
     {
+        if (rec) {
+            PStep q {};
+            q.op = P_PROLONG;
+            q.n = n;
+            q.idx = V.agg.p;
+            q.M = p;
+            q.mt = tcode<PT>();
+            q.xc = xc;
+            q.ct = tcode<CT>();
+            q.x = x;
+            q.xt = tcode<XT>();
+            q.y = y;
+            q.yt = tcode<YT>();
+            rec->push_back(q);
+            return;
+        }
         note_launch();
         if (lk >= 0) {
             auto k = k_blk_prolong<PT, CT, XT, YT>;
@@ -616,7 +770,7 @@ struct Cycle {
         const Level& V = lv(l);
         const DevCsr& Am = V.A;
         const bool f32 = lf32(l);
-        if (!H->chain_in_block || lk >= 0 || k < 2 || fcopy.p || Am.nnz > kChainMaxNnz) return false;
+        if (rec || !H->chain_in_block || lk >= 0 || k < 2 || fcopy.p || Am.nnz > kChainMaxNnz) return false;
         for (const Vec& v : { f, dst, A, Bf })
             if (v.f32 != f32) return false;
         if (src.p && src.f32 != f32) return false;
@@ -652,8 +806,23 @@ struct Cycle {
 
     // One cycle on level l for right-hand side f, starting from x_cur (nullptr: zero),
     // leaving the result in dst.
+    // The cycle on the levels from l down as one persistent launch (persist.cuh), with the program
+    // recorded for this form of the call (ensure_solve_workspace).
+    void run_persistent(int l, Vec f, Vec x_cur, Vec dst) const
+    {
+        const PersistProgram* prog = nullptr;
+        for (auto& pp : H->persist)
+            if (pp->level == l && pp->has_x == (x_cur.p != nullptr)) prog = pp.get();
+        BCMGX_REQUIRE(prog != nullptr, BCMGX_ERR_INTERNAL, "no recorded persistent cycle for this call");
+        launch_persist(H, prog->steps.p, prog->nsteps, skip, s, f.p, x_cur.p, dst.p);
+    }
+
     void run(int l, Vec f, Vec x_cur, Vec dst) const
     {
+        if (!rec && lk < 0 && !H->chain_in_block && H->persist_level >= 0 && l == H->persist_level) {
+            run_persistent(l, f, x_cur, dst);
+            return;
+        }
         Level& V = lv(l);
         const int n = V.A.n;
         const bool f32 = lf32(l);
@@ -832,8 +1001,11 @@ void launch_spmm(int n, int m, int K, const int* row, const int* col, const doub
 void prec_apply_dev(bcmgx_hierarchy* H, const double* r, double* v)
 {
     ensure_solve_workspace(H);
+    persist_reset(H, H->stream);
     prec_apply_impl(H, r, v, nullptr);
 }
+
+void persist_reset_ext(bcmgx_hierarchy* H, cudaStream_t s) { persist_reset(H, s); }
 
 // ------------------------------------------------------------------------------------------
 // FP64 cycle steps on caller-chosen vectors (the row-partitioned cycle, dist.cu)
@@ -1147,6 +1319,65 @@ static void fcg_dots(const DevCsr& A, const double* pv, double* pw, const double
     BCMGX_CHECK_LAUNCH();
 }
 
+// Records the persistent programs of the hierarchy's cycle: the call on its first persistent level
+// from a zero iterate and, for cycles that visit a level more than once, from the level's iterate.
+// A program of the whole cycle (level 0) takes its right-hand side, iterate and output as argument
+// slots (placeholders while recording, replaced by the launch's vectors).
+static void record_persist_programs(bcmgx_hierarchy* H)
+{
+    cudaStream_t s = H->stream;
+    const int lc = H->persist_level;
+    const bool f32 = H->prm.vcycle_precision == BCMGX_VCYCLE_FP32;
+    const int L = (int)H->lv.size();
+    static char placeholders[3][16];
+    void* const PF = placeholders[0];
+    void* const PX = placeholders[1];
+    void* const PD = placeholders[2];
+    const bool multi_visit = lc > 0 && lc - 1 < (int)H->grid_sweeps.size() && H->grid_sweeps[lc - 1] > 1;
+    for (int has_x = 0; has_x <= (multi_visit ? 1 : 0); has_x++) {
+        Vec f, x, dst;
+        if (lc == 0) {
+            f = Vec { PF, false };
+            dst = Vec { PD, false };
+            if (has_x) x = Vec { PX, false };
+        } else {
+            f = H->cyc.lv[lc].rhs;
+            dst = H->cyc.lv[lc].x;
+            if (has_x) x = dst;
+        }
+        std::vector<PStep> steps;
+        Cycle c { H, H->cyc, s, nullptr, f32, L, -1 };
+        c.rec = &steps;
+        c.run(lc, f, x, dst);
+        auto slot = [&](const void*& ptr, unsigned char& sl) {
+            sl = 0;
+            if (ptr == PF) sl = 1;
+            else if (ptr == PX) sl = 2;
+            else if (ptr == PD) sl = 3;
+            if (sl) ptr = nullptr;
+        };
+        for (PStep& p : steps) {
+            slot(p.x, p.sx);
+            slot(p.f, p.sf);
+            const void* y = p.y;
+            slot(y, p.sy);
+            p.y = (void*)y;
+            const void* e = p.extra;
+            slot(e, p.se);
+            p.extra = (void*)e;
+            slot(p.xc, p.sc);
+        }
+        std::unique_ptr<PersistProgram> pp(new PersistProgram());
+        pp->level = lc;
+        pp->has_x = has_x != 0;
+        pp->nsteps = (int)steps.size();
+        pp->steps.alloc(steps.size(), s);
+        BCMGX_CUDA(cudaMemcpyAsync(pp->steps.p, steps.data(), sizeof(PStep) * steps.size(), cudaMemcpyHostToDevice, s));
+        BCMGX_CUDA(cudaStreamSynchronize(s));
+        H->persist.push_back(std::move(pp));
+    }
+}
+
 void ensure_solve_workspace(bcmgx_hierarchy* H)
 {
     const int n0 = H->lv[0].A.n;
@@ -1189,6 +1420,13 @@ void ensure_solve_workspace(bcmgx_hierarchy* H)
     }
     H->cyc.res = f32 ? Vec { H->res32.p, true } : Vec { H->res.p, false };
     if (H->prm.preconditioner == BCMGX_PREC_L1_JACOBI) H->l1tmp.alloc(n0, s);
+    H->persist.clear();
+    H->persist_level = choose_persist_level(H);
+    if (H->persist_level >= 0) {
+        H->persist_bar.alloc(4, s);
+        BCMGX_CUDA(cudaMemsetAsync(H->persist_bar.p, 0, 4 * sizeof(unsigned), s));
+        record_persist_programs(H);
+    }
     H->ws_n = n0;
 }
 
@@ -1480,6 +1718,7 @@ static void fcg_startup(bcmgx_hierarchy* H, const double* b, double* x, double* 
     FcgState* st = H->st.p;
     double* part = H->partials.p;
     double *r = H->r.p, *v = H->v.p, *w = H->w.p, *d = H->d.p, *q = H->q.p;
+    persist_reset(H, s);
     note_launch();
     k_fcg_init<<<1, 1, 0, s>>>(st, H->prm.rtol, H->prm.itnlim);
     fcg_resid0(A, x, b, r, st, part, s);

@@ -33,10 +33,10 @@ constexpr int kStageThreads = (kStageWarps + 1) * 32;
 constexpr int kStageMaxRows = kStageWarps * 32;  // rows per tile at most: one per lane (S = 1)
 constexpr int kStageRowSlots = kStageMaxRows + 8;
 
-// Shared-memory budget per value source / index type: 4 stages of 10 KB for coded entries with
-// int16 offsets (3 bytes), of 18 KB for entries of at most 6 bytes (3 blocks per SM), 3 stages of
-// 30 KB for wider entries (2 blocks per SM). A coded matrix (ValSrc: one byte per entry) also
-// keeps its value table after the stages.
+// Shared-memory budget per value source / index type: 4 stages of 18 KB for entries of at most 6
+// bytes (3 blocks per SM), 3 stages of 30 KB for wider entries (2 blocks per SM). A coded matrix
+// (ValSrc: one byte per entry) also keeps its value table after the stages. (Stages of 10 KB for
+// coded entries cut the tiles from 192 to 100 rows and made the sweep slower, 0.133 -> 0.163 ms.)
 template <typename VS, typename IT>
 struct StageCfg {
     using VT = typename ValSrc<VS>::type;
@@ -45,9 +45,7 @@ struct StageCfg {
     static constexpr int kEntry = (int)sizeof(IT) + kVal;
     // entries per copy granule: both streams of a tile move whole 16-byte granules
     static constexpr int G = std::max(8, 16 / std::min((int)sizeof(IT), kVal));
-    // coded entries (3 bytes) need a third of the room: smaller stages leave more of the SM's
-    // L1 to the gathers of x
-    static constexpr int kBytes = kEntry <= 3 ? 10240 : kEntry <= 6 ? 18432 : 30720;
+    static constexpr int kBytes = kEntry <= 6 ? 18432 : 30720;
     static constexpr int NS = kEntry <= 6 ? 4 : 3;
     static constexpr int CAP = ((kBytes - kStageRowSlots * 4) / kEntry) & ~(G - 1);   // entries per stage
     static constexpr int COLS = kStageRowSlots * 4;                                  // byte offsets in a stage
@@ -59,7 +57,6 @@ struct StageCfg {
     static_assert((G * (int)sizeof(IT)) % 16 == 0 && (G * kVal) % 16 == 0, "a granule must be whole 16-byte units");
     static_assert(SMEM <= 227 * 1024, "the stage ring must fit a block's shared memory");
     static_assert(CAP >= 64 * 8, "a stage must hold a useful tile");
-    static_assert(kEntry > 3 || CAP >= 96 * 27 + 2 * G, "a coded stage must hold 96 rows of 27 entries");
     static_assert((kStageMaxRows + 4) <= kStageRowSlots, "a tile's widened row offsets must fit their slots");
 };
 

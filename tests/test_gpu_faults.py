@@ -20,6 +20,12 @@ import scipy.sparse as sp
 
 pytestmark = pytest.mark.gpu
 
+
+@pytest.fixture(autouse=True)
+def multi_launch_cycle(monkeypatch):
+    """These tests exercise the cycle's own kernels: the persistent coarse cycle stays off."""
+    monkeypatch.setenv("BCMGX_PERSIST_NNZ", "0")
+
 OOM, TIMEOUT, NOT_SPD = -6, -5, -7
 
 

@@ -12,6 +12,12 @@ from test_gpu_parity import as_csr, fcg
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(autouse=True)
+def multi_launch_cycle(monkeypatch):
+    """These tests exercise the cycle's own kernels: the persistent coarse cycle stays off."""
+    monkeypatch.setenv("BCMGX_PERSIST_NNZ", "0")
+
+
 def far_columns(n, seed):
     """SPD, each row coupled to its neighbours and to the row n/2 away: column offsets beyond
     int16, so level 0 keeps int32 columns."""

@@ -283,6 +283,10 @@ bcmgx_hierarchy::~bcmgx_hierarchy()
     hist.release();
     gb.release();
     gx.release();
+    // every stream-ordered buffer goes before the stream does (members left to their own
+    // destructors would free on a destroyed stream)
+    persist.clear();
+    persist_bar.release();
     if (stream) cudaStreamSynchronize(stream);
     bcmgx::pinned_free(st_host);
     if (ev0) cudaEventDestroy(ev0);

@@ -30,6 +30,11 @@ template <> struct Acc<float> { using type = float; };
 template <typename T> struct Wider { using type = double; };
 template <> struct Wider<float> { using type = float; };
 
+// a * b + c with one rounding (an explicit fused multiply-add, so that kernels which must agree
+// bit for bit do not depend on the compiler's contraction choices)
+__device__ __forceinline__ double mad_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float mad_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+
 template <int S, typename T>
 __device__ __forceinline__ T subwarp_sum(T v)
 {

@@ -147,13 +147,13 @@ __device__ void pelem_step(const PStep& p)
             for (int t = __ldg(p.idx + i); t < t1; t++) {
                 const int k = __ldg(p.idx2 + t);
                 const AT rv = p.mt ? (AT)__ldg((const float*)p.M + t) : (AT)__ldg((const double*)p.M + t);
-                s += rv * ldv<AT>(p.f, p.ft, k);
+                s = mad_rn(rv, ldv<AT>(p.f, p.ft, k), s);
             }
             stv(p.y, p.yt, i, s);
         } else {   // P_PROLONG
             const int c = __ldg(p.idx + i);
             const AT pv = p.mt ? (AT)__ldg((const float*)p.M + i) : (AT)__ldg((const double*)p.M + i);
-            stv(p.y, p.yt, i, (AT)(pv * ldv<AT>(p.xc, p.ct, c) + ldv<AT>(p.x, p.xt, i)));
+            stv(p.y, p.yt, i, mad_rn(pv, ldv<AT>(p.xc, p.ct, c), ldv<AT>(p.x, p.xt, i)));
         }
     }
 }

@@ -375,7 +375,7 @@ __global__ void k_restrict(int nc, const int* __restrict__ rptr, const int* __re
     using AT = typename Wider<OT>::type;
     for (long c = (long)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (long)gridDim.x * blockDim.x) {
         AT s = 0;
-        for (int t = rptr[c]; t < rptr[c + 1]; t++) s += (AT)rval[t] * (AT)res[ridx[t]];
+        for (int t = rptr[c]; t < rptr[c + 1]; t++) s = mad_rn((AT)rval[t], (AT)res[ridx[t]], s);
         out[c] = (OT)s;
     }
 }
@@ -388,7 +388,7 @@ __global__ void k_prolong(int n, const int* __restrict__ agg, const PT* __restri
     if (skip && *skip) return;
     using AT = typename Wider<YT>::type;
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-        y[i] = (YT)((AT)p[i] * (AT)xc[agg[i]] + (AT)x[i]);
+        y[i] = (YT)mad_rn((AT)p[i], (AT)xc[agg[i]], (AT)x[i]);
 }
 
 // grid for an element-wise kernel over n elements

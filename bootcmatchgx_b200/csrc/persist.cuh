@@ -165,23 +165,40 @@ __device__ __forceinline__ unsigned long long pglobal_ns()
     return t;
 }
 
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned atom_add_acq_rel_gpu(unsigned* p, unsigned v)
+{
+    unsigned old;
+    asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 // Grid-wide barrier on bar[0] (arrivals) and bar[1] (generation); bar[2] != 0: poisoned by an
-// earlier timeout. Returns false after a bounded wait of wait_ns (fault code 8).
+// earlier timeout. The block's writes are ordered before its arrival by the block barrier and the
+// arrival's release; the waiters' acquire of the new generation orders the next step's loads
+// after every block's writes. Returns false after a bounded wait of wait_ns (fault code 8).
 __device__ __forceinline__ bool pgrid_sync(unsigned* bar, int* fault, unsigned long long wait_ns)
 {
     __shared__ int ok_s;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
-        const unsigned g = *(volatile unsigned*)(bar + 1);
-        __threadfence();
-        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
-            *(volatile unsigned*)bar = 0u;
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
+        const unsigned g = ld_acquire_gpu(bar + 1);
+        if (atom_add_acq_rel_gpu(bar, 1u) == gridDim.x - 1) {
+            bar[0] = 0u;
+            st_release_gpu(bar + 1, g + 1u);
         } else {
             const unsigned long long t0 = pglobal_ns();
-            while (*(volatile unsigned*)(bar + 1) == g) {
+            while (ld_acquire_gpu(bar + 1) == g) {
                 if (*(volatile unsigned*)(bar + 2) != 0u || pglobal_ns() - t0 > wait_ns) {
                     ok = 0;
                     *(volatile unsigned*)(bar + 2) = 1u;
@@ -190,7 +207,6 @@ __device__ __forceinline__ bool pgrid_sync(unsigned* bar, int* fault, unsigned l
                 }
             }
         }
-        __threadfence();
         ok_s = ok;
     }
     __syncthreads();

@@ -455,7 +455,9 @@ static void launch_persist(bcmgx_hierarchy* H, const PStep* steps, int nsteps, c
     const void* af, const void* ax, void* ay)
 {
     stage_fault_init();
-    const int per_sm = std::min(2, blocks_per_sm((const void*)k_persist, kPersistThreads, 0));
+    int want = 2;
+    if (const char* e = std::getenv("BCMGX_PERSIST_BLOCKS")) want = std::max(1, std::atoi(e));
+    const int per_sm = std::min(want, blocks_per_sm((const void*)k_persist, kPersistThreads, 0));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(num_sms() * std::max(per_sm, 1)));
     cfg.blockDim = dim3(kPersistThreads);

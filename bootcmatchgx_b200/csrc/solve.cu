@@ -489,9 +489,12 @@ static void persist_reset(bcmgx_hierarchy* H, cudaStream_t s)
     if (H->persist_level >= 0) BCMGX_CUDA(cudaMemsetAsync(H->persist_bar.p, 0, 4 * sizeof(unsigned), s));
 }
 
-// Entries of the largest level that the persistent cycle takes (BCMGX_PERSIST_NNZ overrides it;
-// 0 turns the persistent cycle off).
-constexpr int64_t kPersistMaxNnz = 2 << 20;
+// Entries of the largest level that the persistent cycle takes; 0, the default, leaves it off:
+// measured on one B200 it was slower than the graph-launched kernels it replaces (a grid barrier
+// costs about what a graph kernel node does, and the cooperative launch inside the solve graph
+// costs more: the 7-point 50^3 solve went from 2.6 to 4.9 ms, the 27-point 160^3 solve from 58.9
+// to 64.8 ms). BCMGX_PERSIST_NNZ=<entries> turns it on.
+constexpr int64_t kPersistMaxNnz = 0;
 
 static int choose_persist_level(const bcmgx_hierarchy* H)
 {

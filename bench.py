@@ -316,21 +316,23 @@ def vcycle_bytes(inf, pre, post, coarse):
     reads no matrix), the residual, the restriction R r (one entry per fine row) and the
     prolongation x += p x_c[agg]; the coarsest level runs `coarse` FP64 sweeps (the first from
     zero). Matrix entries
-    count index_bytes + value bytes, vectors 4 bytes (8 on the coarsest level); level 0 also reads
+    count index_bytes + value bytes (1 where the level streams 1-byte value codes, else 4; 8 for the
+    coarsest level's FP64 values), vectors 4 bytes (8 on the coarsest level); level 0 also reads
     the FP64 residual and writes the FP64 output."""
     n, z, ib = inf["n"], inf["nnz"], inf["index_bytes"]
+    vb = [1 if c else 4 for c in inf["value_codes"]]
     total = 0
     for l in range(len(n) - 1):
         nl, zl, nc = n[l], z[l], n[l + 1]
-        sweep = (ib[l] + 4) * zl + 4 * (nl + 1) + 16 * nl
+        sweep = (ib[l] + vb[l]) * zl + 4 * (nl + 1) + 16 * nl
         total += (pre + post - 1) * sweep + 12 * nl
-        total += (ib[l] + 4) * zl + 4 * (nl + 1) + 12 * nl
+        total += (ib[l] + vb[l]) * zl + 4 * (nl + 1) + 12 * nl
         total += 4 * (nc + 1) + 8 * nl + 4 * nl + 4 * nc
         total += 8 * nl + 4 * nc + 8 * nl
         if l == 0:
             total += 8 * nl + 4 * nl
     nL, zL = n[-1], z[-1]
-    total += (coarse - 1) * ((ib[-1] + 8) * zL + 4 * (nL + 1) + 32 * nL) + 24 * nL
+    total += (coarse - 1) * ((ib[-1] + (1 if inf["value_codes"][-1] else 8)) * zL + 4 * (nL + 1) + 32 * nL) + 24 * nL
     return int(total)
 
 
@@ -436,12 +438,15 @@ def run_ours(a, wl, rank, world, local_rank):
     h64.free()
     peak, peak_kind = read_peaks()
     # algorithmic bytes of the format the kernels stream: int16 column offsets (2 B) where the
-    # level has them, else int32 (4 B); bcmgx_spmv on raw CSR arrays always streams int32
+    # level has them, else int32 (4 B); 1-byte value codes where the level has them, else the
+    # 4- or 8-byte values; bcmgx_spmv on raw CSR arrays always streams int32 + FP64
     ib32, ib64 = inf32["index_bytes"][0], inf64["index_bytes"][0]
+    vb32 = 1 if inf32["value_codes"][0] else 4
+    vb64 = 1 if inf64["value_codes"][0] else 8
     bytes_spmv = 12 * nnz + 4 * (n + 1) + 16 * n
-    bytes_jac32 = (ib32 + 4) * nnz + 4 * (n + 1) + 16 * n
-    bytes_jac64 = (ib64 + 8) * nnz + 4 * (n + 1) + 32 * n
-    bytes_jac32_int32 = 8 * nnz + 4 * (n + 1) + 16 * n
+    bytes_jac32 = (ib32 + vb32) * nnz + 4 * (n + 1) + 16 * n
+    bytes_jac64 = (ib64 + vb64) * nnz + 4 * (n + 1) + 32 * n
+    bytes_jac32_csr = 8 * nnz + 4 * (n + 1) + 16 * n   # the same sweep on int32 columns + FP32 values
     gbs_spmv = bytes_spmv / (spmv_ms * 1e-3) / 1e9
     gbs_jac32 = bytes_jac32 / (k32["jacobi"] * 1e-3) / 1e9
     gbs_jac64 = bytes_jac64 / (k64f["jacobi"] * 1e-3) / 1e9
@@ -494,7 +499,8 @@ def run_ours(a, wl, rank, world, local_rank):
                    "l2": "inputs larger than L2 (CSR 1.39 GB)" if nnz > 5e7 else "inputs fit in L2",
                    "parallelism": f"replicas x{world} (one independent system per GPU)"},
         "breakdown": {"setup_ms": setup32, "solve_ms": solve32, "niter": infos32[-1][0]["niter"],
-                      "threads_per_row": inf32["tpr"],
+                      "threads_per_row": inf32["tpr"], "index_bytes": inf32["index_bytes"],
+                      "value_codes": inf32["value_codes"],
                       "levels": inf32["n"], "level_nnz": inf32["nnz"], "op_cmplx": inf32["op_cmplx"]},
         "fp64": {"value": ms64 / 1e3, "setup_ms": setup64, "solve_ms": solve64,
                  "niter": infos64[-1][0]["niter"]},
@@ -507,24 +513,28 @@ def run_ours(a, wl, rank, world, local_rank):
                    "fp32_rel_residual": float(nrm(b - _spmv(row, col, val, x32)) / nrm(b))},
         "spmv": {"gbs": gbs_spmv, "ms": spmv_ms, "bytes": bytes_spmv, "frac_of_peak": gbs_spmv / peak,
                  "frac_of_8TBs_nominal": gbs_spmv / 8000.0},
-        "kernels_level0": {"index_bytes": ib32, "fp32_jacobi_ms": k32["jacobi"], "fp32_jacobi_gbs": gbs_jac32,
-                           "fp32_jacobi_int32_equivalent_gbs": bytes_jac32_int32 / (k32["jacobi"] * 1e-3) / 1e9,
+        "kernels_level0": {"index_bytes": ib32, "value_bytes_fp32": vb32, "value_bytes_fp64": vb64,
+                           "fp32_jacobi_ms": k32["jacobi"], "fp32_jacobi_gbs": gbs_jac32,
+                           "fp32_jacobi_csr_equivalent_gbs": bytes_jac32_csr / (k32["jacobi"] * 1e-3) / 1e9,
                            "fp32_residual_ms": k32["residual"], "fp64_jacobi_ms": k64f["jacobi"],
                            "fp64_jacobi_gbs": gbs_jac64, "fcg_spmv_dots_ms": k64f["fcg_spmv_dots"],
                            # pw = A pv (row kernel) then the three dots (r, pw, oq against pv)
-                           "fcg_spmv_dots_gbs": ((ib64 + 8) * nnz + 4 * (n + 1) + 48 * n) / (k64f["fcg_spmv_dots"] * 1e-3) / 1e9,
+                           "fcg_spmv_dots_gbs": ((ib64 + vb64) * nnz + 4 * (n + 1) + 48 * n) / (k64f["fcg_spmv_dots"] * 1e-3) / 1e9,
                            "fp32_jacobi_fp64_out_ms": k32["jacobi_fp64_out"],
                            "fcg_update_ms": k32["fcg_update"],
                            "fcg_update_gbs": 80 * n / (k32["fcg_update"] * 1e-3) / 1e9},
         "kernels_coarse_levels_fp32_jacobi_ms": [round(k["jacobi"], 4) for k in lvl],
         "vcycle": vcycle_roofline(vc_ms, inf32, params("FP32"), peak, peak_kind),
-        "roofline": {"kernel": (f"k_rowop_staged<{-tpr0},OP_JACOBI,float>" if tpr0 < 0 else f"k_rowop<{tpr0},OP_JACOBI,float>")
-                     + " (FP32 l1-Jacobi sweep, level 0)",
+        "roofline": {"kernel": ((f"k_rowop_staged<{-tpr0}" if tpr0 < 0 else f"k_rowop<{tpr0}")
+                                + (",OP_JACOBI,Coded<float>>" if vb32 == 1 else ",OP_JACOBI,float>")
+                                + " (FP32 l1-Jacobi sweep, level 0)"),
+                     "format": f"int{8 * ib32} columns, " + ("1-byte value codes" if vb32 == 1 else "FP32 values"),
                      "bound": "hbm", "achieved": gbs_jac32, "peak": peak, "unit": "GB/s",
                      "frac": gbs_jac32 / peak, "peak_kind": f"{peak_kind} hbm_gbs (copy)",
                      "bytes_per_launch": bytes_jac32,
-                     "traffic": (int(TRAFFIC_RATIO[(ib32, tpr0 < 0)] * bytes_jac32)
-                                 if a.workload.startswith("poisson27") and (ib32, tpr0 < 0) in TRAFFIC_RATIO else None)},
+                     "traffic": (int(TRAFFIC_RATIO[(ib32, vb32, tpr0 < 0)] * bytes_jac32)
+                                 if a.workload.startswith("poisson27") and (ib32, vb32, tpr0 < 0) in TRAFFIC_RATIO
+                                 else None)},
         "cold_first_call": dict(cold, what="the first set-up + solve of each form in the process (threads-per-row "
                                 "autotuner running, kernels loading); the timed steps reuse the tuned choices"),
         "gpu_launches": int(round(launches32)),
@@ -537,11 +547,11 @@ def run_ours(a, wl, rank, world, local_rank):
 
 
 # DRAM bytes (read + write) of one level-0 FP32 Jacobi launch as a multiple of its algorithmic
-# bytes, per (index bytes, staged kernel): measured by ncu (dram__bytes_read.sum +
+# bytes, per (index bytes, value bytes, staged kernel): measured by ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum of single launches) on the 27-point 100^3 case, plain kernel with int32
-# columns, plain with int16 offsets, staged with int16 offsets; scaled by the algorithmic bytes to
-# the other 27-point workloads.
-TRAFFIC_RATIO = {(4, False): 0.99983, (2, False): 1.00115, (2, True): 1.01173}
+# columns, plain with int16 offsets, staged with int16 offsets (FP32 values); scaled by the
+# algorithmic bytes to the other 27-point workloads.
+TRAFFIC_RATIO = {(4, 4, False): 0.99983, (2, 4, False): 1.00115, (2, 4, True): 1.01173}
 
 
 def _spmv(row, col, val, x):

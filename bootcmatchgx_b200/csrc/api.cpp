@@ -197,13 +197,25 @@ static bcmgx_hierarchy* setup_one(const bcmgx_csr* A, const bcmgx_params* p, int
     BCMGX_CUDA(cudaEventRecord(t0.e, H->stream));
     stage_fault_init();
     build_hierarchy(H.get(), A);
-    const char* force = std::getenv("BCMGX_TPR");
+    // BCMGX_TPR forces the threads-per-row codes: one code for every level ("-2"), or one per level
+    // ("-2,-2,4"; levels past the list take its last code)
+    std::vector<int> force;
+    if (const char* env = std::getenv("BCMGX_TPR")) {
+        for (const char* q = env; *q;) {
+            char* end = nullptr;
+            const long v = std::strtol(q, &end, 10);
+            BCMGX_REQUIRE(end != q, BCMGX_ERR_INVALID_INPUT, "BCMGX_TPR: expected comma-separated integers");
+            force.push_back((int)v);
+            q = *end == ',' ? end + 1 : end;
+            BCMGX_REQUIRE(*q == 0 || *end == ',', BCMGX_ERR_INVALID_INPUT, "BCMGX_TPR: expected comma-separated integers");
+        }
+    }
     const int L = (int)H->lv.size();
     for (int l = 0; l < L; l++) {
         Level& V = H->lv[l];
         const bool f32 = p->vcycle_precision == BCMGX_VCYCLE_FP32 && l < L - 1;
         int code;
-        if (force) code = std::atoi(force);
+        if (!force.empty()) code = force[std::min(l, (int)force.size() - 1)];
         else if (p->autotune) code = autotune_tpr(V, f32, H->stream);
         else code = default_tpr(V.A.n, V.A.nnz);
         // negative: the staged kernel with -code threads per row (1, 2, 4 or 8)

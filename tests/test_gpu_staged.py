@@ -114,6 +114,30 @@ def test_autotuned_codes_are_reported(bx, cuda):
     h.free()
 
 
+def test_forced_codes_per_level(bx, cuda, monkeypatch):
+    """BCMGX_TPR takes one code per level; levels past the list take its last code, so the list
+    spelled out to every level gives the same codes and the same solution bit for bit; a malformed
+    list is an invalid input."""
+    A = as_csr(bx, ("lap27", (40, 40, 40)))
+    b = np.random.default_rng(5).uniform(-1, 1, A.shape[0])
+    monkeypatch.setenv("BCMGX_TPR", "-2,4")
+    h = bx.prec_setup(A.indptr, A.indices, A.data, fcg(bx, vcycle_precision="FP32"))
+    tpr = h.info()["tpr"]
+    assert len(tpr) >= 3 and tpr[:2] == [-2, 4] and all(t == 4 for t in tpr[2:])
+    x1, i1 = h.solve(b)
+    h.free()
+    monkeypatch.setenv("BCMGX_TPR", "-2," + ",".join(["4"] * (len(tpr) - 1)))
+    h = bx.prec_setup(A.indptr, A.indices, A.data, fcg(bx, vcycle_precision="FP32"))
+    assert h.info()["tpr"] == tpr
+    x2, i2 = h.solve(b)
+    h.free()
+    assert i1["niter"] == i2["niter"] and np.array_equal(x1, x2)
+    monkeypatch.setenv("BCMGX_TPR", "-2,x")
+    with pytest.raises(bx.BcmgxError) as e:
+        bx.prec_setup(A.indptr, A.indices, A.data, fcg(bx))
+    assert e.value.code == -1 and "BCMGX_TPR" in str(e.value)
+
+
 # matrices of at least 2^20 entries with few distinct values: their row kernels stream one-byte
 # value codes (value-indexed CSR) on the large levels
 CODED = [("lap27", (40, 40, 40)), ("lap7", (110, 100, 100)), ("shift", (100, 100, 100))]

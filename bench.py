@@ -486,7 +486,9 @@ def run_ours(a, wl, rank, world, local_rank):
     setup64 = float(np.mean([i[1]["setup_ms"] for i in infos64]))
     solve64 = float(np.mean([i[0]["solve_ms"] for i in infos64]))
     nrm = np.linalg.norm
-    tpr0 = inf32["tpr"][0]   # level 0's threads-per-row code: negative for the staged kernel
+    tpr0 = inf32["tpr"][0]   # level 0's kernel code: threads per row, negative staged, 64 sliced
+    form0 = "sliced" if tpr0 == 64 else "staged" if tpr0 < 0 else "plain"
+    kname0 = {"sliced": "k_rowop_sliced<", "staged": f"k_rowop_staged<{-tpr0},", "plain": f"k_rowop<{tpr0},"}[form0]
     line = {
         "metric": METRIC, "value": ms32 / 1e3, "unit": "s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms32, "higher_is_better": False, "scaling": "weak",
@@ -525,15 +527,14 @@ def run_ours(a, wl, rank, world, local_rank):
                            "fcg_update_gbs": 80 * n / (k32["fcg_update"] * 1e-3) / 1e9},
         "kernels_coarse_levels_fp32_jacobi_ms": [round(k["jacobi"], 4) for k in lvl],
         "vcycle": vcycle_roofline(vc_ms, inf32, params("FP32"), peak, peak_kind),
-        "roofline": {"kernel": ((f"k_rowop_staged<{-tpr0}" if tpr0 < 0 else f"k_rowop<{tpr0}")
-                                + (",OP_JACOBI,Coded<float>>" if vb32 == 1 else ",OP_JACOBI,float>")
+        "roofline": {"kernel": (kname0 + ("OP_JACOBI,Coded<float>>" if vb32 == 1 else "OP_JACOBI,float>")
                                 + " (FP32 l1-Jacobi sweep, level 0)"),
                      "format": f"int{8 * ib32} columns, " + ("1-byte value codes" if vb32 == 1 else "FP32 values"),
                      "bound": "hbm", "achieved": gbs_jac32, "peak": peak, "unit": "GB/s",
                      "frac": gbs_jac32 / peak, "peak_kind": f"{peak_kind} hbm_gbs (copy)",
                      "bytes_per_launch": bytes_jac32,
-                     "traffic": (int(TRAFFIC_RATIO[(ib32, vb32, tpr0 < 0)] * bytes_jac32)
-                                 if a.workload.startswith("poisson27") and (ib32, vb32, tpr0 < 0) in TRAFFIC_RATIO
+                     "traffic": (int(TRAFFIC_RATIO[(ib32, vb32, form0)] * bytes_jac32)
+                                 if a.workload.startswith("poisson27") and (ib32, vb32, form0) in TRAFFIC_RATIO
                                  else None)},
         "cold_first_call": dict(cold, what="the first set-up + solve of each form in the process (threads-per-row "
                                 "autotuner running, kernels loading); the timed steps reuse the tuned choices"),
@@ -547,11 +548,13 @@ def run_ours(a, wl, rank, world, local_rank):
 
 
 # DRAM bytes (read + write) of one level-0 FP32 Jacobi launch as a multiple of its algorithmic
-# bytes, per (index bytes, value bytes, staged kernel): measured by ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum of single launches) on the 27-point 100^3 case, plain kernel with int32
-# columns, plain with int16 offsets, staged with int16 offsets (FP32 values); scaled by the
-# algorithmic bytes to the other 27-point workloads.
-TRAFFIC_RATIO = {(4, 4, False): 0.99983, (2, 4, False): 1.00115, (2, 4, True): 1.01173}
+# bytes, per (index bytes, value bytes, kernel form): measured by ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum of single launches) on the 27-point 100^3 case: the plain kernel with int32
+# columns and with int16 offsets, the staged kernel with int16 offsets (FP32 values, and one-byte
+# value codes), the sliced kernel with int16 offsets and codes (its padding included, its row
+# offsets not read); scaled by the algorithmic bytes to the other 27-point workloads.
+TRAFFIC_RATIO = {(4, 4, "plain"): 0.99983, (2, 4, "plain"): 1.00115, (2, 4, "staged"): 1.01173,
+                 (2, 1, "staged"): 0.99886, (2, 1, "sliced"): 0.99216}
 
 
 def _spmv(row, col, val, x):

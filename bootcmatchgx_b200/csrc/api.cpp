@@ -218,7 +218,16 @@ static bcmgx_hierarchy* setup_one(const bcmgx_csr* A, const bcmgx_params* p, int
         if (!force.empty()) code = force[std::min(l, (int)force.size() - 1)];
         else if (p->autotune) code = autotune_tpr(V, f32, H->stream);
         else code = default_tpr(V.A.n, V.A.nnz);
-        // negative: the staged kernel with -code threads per row (1, 2, 4 or 8)
+        // negative: the staged kernel with -code threads per row (1, 2, 4 or 8); kSlicedCode: the
+        // sliced kernel (one lane per row: the CSR kernels stand in for it with 1 thread per row)
+        if (code == kSlicedCode) {
+            build_sliced(V.A, H->stream);
+            V.A.sliced = V.A.sl_ptr.p != nullptr;
+            V.A.staged = false;
+            V.A.tpr = 1;
+            continue;
+        }
+        release_sliced(V.A);
         V.A.staged = code < 0;
         V.A.tpr = code < 0 ? -code : code;
         if (V.A.tpr < 1) V.A.tpr = default_tpr(V.A.n, V.A.nnz);
@@ -563,7 +572,7 @@ int bcmgx_hierarchy_get_info(const bcmgx_hierarchy* h, bcmgx_hierarchy_info* inf
         for (int l = 0; l < info->num_levels && l < BCMGX_MAX_LEVELS; l++) {
             info->n[l] = h->lv[l].A.n;
             info->nnz[l] = h->lv[l].A.nnz;
-            info->tpr[l] = h->lv[l].A.staged ? -h->lv[l].A.tpr : h->lv[l].A.tpr;
+            info->tpr[l] = h->lv[l].A.sliced ? kSlicedCode : h->lv[l].A.staged ? -h->lv[l].A.tpr : h->lv[l].A.tpr;
             info->index_bytes[l] = h->lv[l].A.dcol.p ? 2 : 4;
             info->value_codes[l] = h->lv[l].A.vcode.p ? h->lv[l].A.nvalues : 0;
         }

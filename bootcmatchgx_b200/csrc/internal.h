@@ -125,7 +125,25 @@ struct DevCsr {
     int nvalues = 0;  // distinct values in the table (0: not coded)
     int tpr = 0;      // threads per row for SpMV / smoother (autotuned)
     bool staged = false;  // row kernels stream the entries through shared-memory stages (staged.cuh)
+    // sliced copy (sliced.cuh), built when the level's tuning picks the sliced kernels (tpr is then
+    // 1: the CSR kernels that stand in for it, in a batch graph or a persistent cycle, sum each
+    // row in the same order): slices of 32 rows, blocks of 4 entries per lane; int16 offsets when
+    // dcol exists, else int32 columns; the value codes when the level is coded, else its FP32
+    // (when val32 exists) and FP64 values
+    bool sliced = false;
+    DBuf<int> sl_ptr;
+    DBuf<short> sl_off;
+    DBuf<int> sl_col;
+    DBuf<unsigned char> sl_code;
+    DBuf<float> sl_val32;
+    DBuf<double> sl_val64;
 };
+
+// tuning code of the sliced kernels (hierarchy info, BCMGX_TPR, the tuning cache); the staged
+// kernels are coded as minus their threads per row
+constexpr int kSlicedCode = 64;
+void build_sliced(DevCsr& A, cudaStream_t s);
+void release_sliced(DevCsr& A);
 
 struct Level {
     DevCsr A;

@@ -15,6 +15,7 @@
 #include <type_traits>
 #include "rowops.cuh"
 #include "staged.cuh"
+#include "sliced.cuh"
 #include "blockops.cuh"
 #include "persist.cuh"
 
@@ -216,6 +217,76 @@ static void launch_staged(int n, int64_t nnz, const int* row, const IT* col, VS 
     BCMGX_CHECK_LAUNCH();
 }
 
+// ------------------------------------------------------------------------------------------
+// sliced form (sliced.cuh)
+// ------------------------------------------------------------------------------------------
+void release_sliced(DevCsr& A)
+{
+    A.sliced = false;
+    A.sl_ptr.release();
+    A.sl_off.release();
+    A.sl_col.release();
+    A.sl_code.release();
+    A.sl_val32.release();
+    A.sl_val64.release();
+}
+
+// Builds A's sliced copy from its CSR arrays (one host round trip for the total). The codes are
+// used when the level is coded and its table has a free (zero) slot for the padding.
+void build_sliced(DevCsr& A, cudaStream_t s)
+{
+    if (A.sl_ptr.p || A.n <= 0) return;
+    const long nsl = ((long)A.n + kSliceRows - 1) / kSliceRows;
+    DBuf<int> cnt;
+    cnt.alloc(nsl, s);
+    auto kw = k_sl_width;
+    note_launch();
+    kw<<<fit_grid(kw, 256, ceil_div(nsl * 32, 256)), 256, 0, s>>>(A.n, A.row.p, cnt.p);
+    BCMGX_CHECK_LAUNCH();
+    A.sl_ptr.alloc(nsl + 1, s);
+    const long long total = scan_exclusive(cnt.p, A.sl_ptr.p, nsl, true, s);
+    const bool coded = A.vcode.p && A.nvalues > 0 && A.nvalues < kValueCodes;
+    if (coded) A.sl_code.alloc(std::max<long long>(total, 1), s);
+    else {
+        A.sl_val64.alloc(std::max<long long>(total, 1), s);
+        if (A.val32.p) A.sl_val32.alloc(std::max<long long>(total, 1), s);
+    }
+    auto fill = [&](auto kern, auto* cidx, auto* sidx) {
+        note_launch();
+        kern<<<fit_grid(kern, 256, ceil_div(nsl * 32, 256)), 256, 0, s>>>(A.n, A.row.p, cidx, A.sl_ptr.p, sidx,
+            A.vcode.p, coded ? A.sl_code.p : nullptr, A.nvalues, A.val32.p, coded ? nullptr : A.sl_val32.p,
+            A.val.p, coded ? nullptr : A.sl_val64.p);
+        BCMGX_CHECK_LAUNCH();
+    };
+    if (A.dcol.p) {
+        A.sl_off.alloc(std::max<long long>(total, 1), s);
+        fill(k_sl_fill<short>, (const short*)A.dcol.p, A.sl_off.p);
+    } else {
+        A.sl_col.alloc(std::max<long long>(total, 1), s);
+        fill(k_sl_fill<int>, (const int*)A.col.p, A.sl_col.p);
+    }
+}
+
+template <int OP, typename VS, typename XT, typename FT, typename MT, typename YT>
+static void launch_sliced(const DevCsr& A, SlSrc<VS> sv, const XT* x, const FT* f, const MT* M, YT* y, double alpha,
+    double beta, const int* skip, cudaStream_t s)
+{
+    const long nsl = ((long)A.n + kSliceRows - 1) / kSliceRows;
+    auto go = [&](auto* idx) {
+        using IT = std::remove_const_t<std::remove_pointer_t<decltype(idx)>>;
+        using C = SlStage<IT, VS>;
+        auto kern = k_rowop_sliced<OP, VS, XT, FT, MT, YT, IT>;
+        ensure_smem_limit((const void*)kern, C::SMEM);
+        const int per_sm = blocks_per_sm((const void*)kern, kSlWarps * 32, C::SMEM);
+        const int grid = (int)std::max<long>(1, std::min<long>(ceil_div(nsl, kSlWarps), (long)per_sm * num_sms()));
+        note_launch();
+        kern<<<grid, kSlWarps * 32, C::SMEM, s>>>(A.n, A.sl_ptr.p, idx, sv, x, f, M, y, alpha, beta, skip);
+    };
+    if (A.sl_off.p) go((const short*)A.sl_off.p);
+    else go((const int*)A.sl_col.p);
+    BCMGX_CHECK_LAUNCH();
+}
+
 // The row operation on a level matrix, through its int16 column offsets when it has them, through
 // its value codes when it has them and `val` is the level's own FP64 or FP32 value array (the
 // codes index a table of those same values), and through the staged kernel when the level's
@@ -225,7 +296,7 @@ template <int OP, typename VS, typename XT, typename FT, typename MT, typename Y
 static void launch_rowop_vs(int tpr, const DevCsr& A, VS val, const void* val_ptr, const XT* x, const FT* f, const MT* M,
     YT* y, double alpha, double beta, const int* skip, cudaStream_t s, int stage)
 {
-    const bool staged = (stage < 0 ? A.staged : stage > 0) && (tpr == 1 || tpr == 2 || tpr == 4 || tpr == 8) &&
+    const bool staged = (stage < 0 ? A.staged : stage == 1) && (tpr == 1 || tpr == 2 || tpr == 4 || tpr == 8) &&
         aligned16(A.row.p) && aligned16(val_ptr) && aligned16(A.dcol.p ? (const void*)A.dcol.p : (const void*)A.col.p);
     if (staged) {
         auto go = [&](auto* colp) {
@@ -244,6 +315,9 @@ static void launch_rowop_vs(int tpr, const DevCsr& A, VS val, const void* val_pt
     else launch_rowop<OP>(tpr, A.n, A.row.p, (const int*)A.col.p, val, x, f, M, y, alpha, beta, skip, s);
 }
 
+// form (stage): -1 the level's tuned kernel (sliced, staged or plain), 0 the plain CSR kernel, 1 the
+// staged kernel, 2 the sliced kernel. The sliced kernel runs when the level has its sliced copy
+// and `val` is one of the level's own value arrays (else the CSR kernels do, with tpr).
 template <int OP, typename VT, typename XT, typename FT, typename MT, typename YT>
 static void launch_rowop_A(int tpr, const DevCsr& A, const VT* val, const XT* x, const FT* f, const MT* M, YT* y,
     double alpha, double beta, const int* skip, cudaStream_t s, int stage = -1)
@@ -251,12 +325,25 @@ static void launch_rowop_A(int tpr, const DevCsr& A, const VT* val, const XT* x,
     if (A.n <= 0) return;
     const VT* own = nullptr;
     const VT* tab = nullptr;
+    const VT* slv = nullptr;
     if constexpr (std::is_same<VT, float>::value) {
         own = A.val32.p;
         tab = A.vtab32.p;
+        slv = A.sl_val32.p;
     } else {
         own = A.val.p;
         tab = A.vtab64.p;
+        slv = A.sl_val64.p;
+    }
+    if ((stage == 2 || (stage < 0 && A.sliced)) && A.sl_ptr.p && val == own) {
+        if (A.sl_code.p && tab) {
+            launch_sliced<OP>(A, SlSrc<Coded<VT>> { A.sl_code.p, tab }, x, f, M, y, alpha, beta, skip, s);
+            return;
+        }
+        if (slv) {
+            launch_sliced<OP>(A, SlSrc<const VT*> { slv }, x, f, M, y, alpha, beta, skip, s);
+            return;
+        }
     }
     if (A.vcode.p && tab && val == own) {
         launch_rowop_vs<OP>(tpr, A, Coded<VT> { A.vcode.p, tab }, (const void*)A.vcode.p, x, f, M, y, alpha, beta,
@@ -1600,7 +1687,8 @@ static void tune_cache_load()
     long long z;
     int n, prec, t;
     while (std::fscanf(f, "%d %lld %d %d", &n, &z, &prec, &t) == 4)
-        if (t == 1 || t == 2 || t == 4 || t == 8 || t == 16 || t == 32 || t == -1 || t == -2 || t == -4 || t == -8)
+        if (t == 1 || t == 2 || t == 4 || t == 8 || t == 16 || t == 32 || t == -1 || t == -2 || t == -4 || t == -8 ||
+            t == kSlicedCode)
             g_tune_cache[std::make_tuple(n, (int64_t)z, prec)] = t;
     std::fclose(f);
 }
@@ -1617,7 +1705,7 @@ static void tune_cache_store(const std::tuple<int, int64_t, int>& key, int t)
 
 int autotune_tpr(Level& V, bool f32, cudaStream_t s)
 {
-    const DevCsr& A = V.A;
+    DevCsr& A = V.A;
     const int n = A.n;
     if (n < kTuneMinRows) return default_tpr(n, A.nnz);
     const auto key = std::make_tuple(n, A.nnz, f32 ? 1 : 0);
@@ -1647,9 +1735,12 @@ int autotune_tpr(Level& V, bool f32, cudaStream_t s)
     BCMGX_CUDA(cudaEventCreate(&e1));
     int best = default_tpr(n, A.nnz);
     float best_ms = 1e30f;
-    // candidates: 1..16 threads per row, then the staged kernel with 1, 2, 4 and 8 (coded negative)
-    for (int t : {1, 2, 4, 8, 16, -1, -2, -4, -8}) {
-        const int tp = t < 0 ? -t : t, stage = t < 0 ? 1 : 0;
+    // candidates: 1..16 threads per row, the staged kernel with 1, 2, 4 and 8 (coded negative),
+    // and the sliced kernel (its copy of the matrix is built for the trial and kept if it wins)
+    build_sliced(A, s);
+    for (int t : {1, 2, 4, 8, 16, -1, -2, -4, -8, kSlicedCode}) {
+        if (t == kSlicedCode && !A.sl_ptr.p) continue;
+        const int tp = t == kSlicedCode ? 1 : t < 0 ? -t : t, stage = t == kSlicedCode ? 2 : t < 0 ? 1 : 0;
         auto launch = [&] {
             if (f32)
                 launch_rowop_A<OP_JACOBI>(tp, A, A.val32.p, (const float*)a32.p, (const float*)c32.p, V.M32.p, b32.p, 1.0, 0.0, nullptr, s, stage);
@@ -1670,6 +1761,7 @@ int autotune_tpr(Level& V, bool f32, cudaStream_t s)
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    if (best != kSlicedCode) release_sliced(A);
     std::lock_guard<std::mutex> g(g_tune_mu);
     g_tune_cache[key] = best;
     tune_cache_store(key, best);
@@ -1851,14 +1943,18 @@ struct BatchCaptureMode {
     {
         H->chain_in_block = true;
         for (Level& V : H->lv) {
-            staged.push_back(V.A.staged ? 1 : 0);
+            staged.push_back((V.A.staged ? 1 : 0) | (V.A.sliced ? 2 : 0));
             V.A.staged = false;
+            V.A.sliced = false;
         }
     }
     ~BatchCaptureMode()
     {
         H->chain_in_block = false;
-        for (size_t l = 0; l < staged.size(); l++) H->lv[l].A.staged = staged[l] != 0;
+        for (size_t l = 0; l < staged.size(); l++) {
+            H->lv[l].A.staged = (staged[l] & 1) != 0;
+            H->lv[l].A.sliced = (staged[l] & 2) != 0;
+        }
     }
 };
 

@@ -124,7 +124,8 @@ typedef struct bcmgx_hierarchy_info {
     int maxcoarsesize, ftcoarse, num_sweep_records;
     double setup_ms;         /* device time of the set-up (CUDA events) */
     int tpr[BCMGX_MAX_LEVELS];   /* threads per row the solve kernels use on each level; negative: the
-                                    staged kernel (matrix entries through shared memory) with -tpr */
+                                    staged kernel (matrix entries through shared memory) with -tpr;
+                                    64: the sliced kernel (32-row slices, one thread per row) */
     int index_bytes[BCMGX_MAX_LEVELS]; /* column index bytes the solve kernels stream per entry
                                           (2: int16 offsets from the diagonal, 4: int32) */
     int value_codes[BCMGX_MAX_LEVELS]; /* distinct values of a level whose solve kernels stream

@@ -106,11 +106,11 @@ def test_staged_hierarchies_in_batch_graph(bx, cuda, monkeypatch):
 
 def test_autotuned_codes_are_reported(bx, cuda):
     """With the autotuner on (the default), every level reports a threads-per-row code of the
-    plain (1..32) or the staged (-1, -2, -4, -8) kernel."""
+    plain (1..32), the staged (-1, -2, -4, -8) or the sliced (64) kernel."""
     A = as_csr(bx, ("lap27", (40, 40, 40)))
     h = bx.prec_setup(A.indptr, A.indices, A.data, fcg(bx, vcycle_precision="FP32"))
     for t in h.info()["tpr"]:
-        assert t in (1, 2, 4, 8, 16, 32, -1, -2, -4, -8)
+        assert t in (1, 2, 4, 8, 16, 32, -1, -2, -4, -8, 64)
     h.free()
 
 

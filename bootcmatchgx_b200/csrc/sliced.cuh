@@ -132,7 +132,9 @@ extern __shared__ __align__(128) unsigned char sl_smem[];
 // so that a slice's gathers start without a round trip to memory for its indices. Blocks are taken
 // in chunks of up to 8 (their words read first), then gathered GB blocks at a time. Launch with
 // kSlWarps * 32 threads and SlStage<IT, VS>::SMEM bytes of dynamic shared memory.
-template <int OP, typename VS, typename XT, typename FT, typename MT, typename YT, typename IT>
+// FIT: every slice fits a stage (the matrix's longest row has at most NBMAX blocks), so no slice
+// takes the global-memory path.
+template <int OP, typename VS, typename XT, typename FT, typename MT, typename YT, typename IT, bool FIT>
 __global__ void __launch_bounds__(kSlWarps * 32, 3) k_rowop_sliced(int n, const int* __restrict__ sptr,
     const IT* __restrict__ sidx, SlSrc<VS> sv, const XT* __restrict__ x, const FT* __restrict__ f,
     const MT* __restrict__ M, YT* __restrict__ y, double alpha, double beta, const int* __restrict__ skip)
@@ -173,7 +175,7 @@ __global__ void __launch_bounds__(kSlWarps * 32, 3) k_rowop_sliced(int n, const 
     // copies of a slice's words into stage st (nothing when it is empty or wider than a stage)
     auto issue = [&](int st, int b, int e) {
         const int nb = (e - b) / kSliceBlock;
-        if (nb > 0 && nb <= ST::NBMAX) {
+        if (nb > 0 && (FIT || nb <= ST::NBMAX)) {
             const unsigned dst = stage0_s + (unsigned)(st * kSlStageBytes);
             const unsigned char* gi = (const unsigned char*)(sidx + b);
             const unsigned char* gv = (const unsigned char*)sv.at(b);
@@ -203,7 +205,7 @@ __global__ void __launch_bounds__(kSlWarps * 32, 3) k_rowop_sliced(int n, const 
         const bool live = r < n;
         const int rr = live ? r : n - 1;
         const int nb = (e0 - b0) / kSliceBlock;
-        const bool staged = nb <= ST::NBMAX;
+        const bool staged = FIT || nb <= ST::NBMAX;
         const unsigned char* sbase = stage0 + st * kSlStageBytes;
         // epilogue operands first: their latency overlaps the row's gathers
         AT o1 = 0, o2 = 0, o3 = 0;

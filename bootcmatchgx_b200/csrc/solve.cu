@@ -275,12 +275,15 @@ static void launch_sliced(const DevCsr& A, SlSrc<VS> sv, const XT* x, const FT* 
     auto go = [&](auto* idx) {
         using IT = std::remove_const_t<std::remove_pointer_t<decltype(idx)>>;
         using C = SlStage<IT, VS>;
-        auto kern = k_rowop_sliced<OP, VS, XT, FT, MT, YT, IT>;
-        ensure_smem_limit((const void*)kern, C::SMEM);
-        const int per_sm = blocks_per_sm((const void*)kern, kSlWarps * 32, C::SMEM);
-        const int grid = (int)std::max<long>(1, std::min<long>(ceil_div(nsl, kSlWarps), (long)per_sm * num_sms()));
-        note_launch();
-        kern<<<grid, kSlWarps * 32, C::SMEM, s>>>(A.n, A.sl_ptr.p, idx, sv, x, f, M, y, alpha, beta, skip);
+        auto run = [&](auto kern) {
+            ensure_smem_limit((const void*)kern, C::SMEM);
+            const int per_sm = blocks_per_sm((const void*)kern, kSlWarps * 32, C::SMEM);
+            const int grid = (int)std::max<long>(1, std::min<long>(ceil_div(nsl, kSlWarps), (long)per_sm * num_sms()));
+            note_launch();
+            kern<<<grid, kSlWarps * 32, C::SMEM, s>>>(A.n, A.sl_ptr.p, idx, sv, x, f, M, y, alpha, beta, skip);
+        };
+        if (A.max_row > 0 && A.max_row <= C::NBMAX * kSliceG) run(k_rowop_sliced<OP, VS, XT, FT, MT, YT, IT, true>);
+        else run(k_rowop_sliced<OP, VS, XT, FT, MT, YT, IT, false>);
     };
     if (A.sl_off.p) go((const short*)A.sl_off.p);
     else go((const int*)A.sl_col.p);

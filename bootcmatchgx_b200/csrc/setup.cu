@@ -559,9 +559,17 @@ __global__ void k_logw(int n, const int* __restrict__ row, const int* __restrict
 // Per row: rank of every candidate (off-diagonal, W > 0) in the row's preference order,
 // (W, column) descending (find_Candidate, suitor.cu:80-147); ordj lists the entries by rank.
 // Ranks of a row of at most 32 entries held in registers (lane = entry t = b + lane, column ct
-// and weight wt; ct = -1 past the row): ranks by shuffles, no reloads.
+// and weight wt; ct = -1 past the row). When the weights differ, every lane compares its entry
+// with all of the row's: the row's (weight, column) keys go to the warp's slots in shared memory
+// (`keys`, 32 per warp) and are read back as broadcasts, one 16-byte load per compared entry
+// (three shuffles per entry made shuffle throughput the bound).
+struct alignas(16) RankKey {
+    double w;
+    int c;     // column, -1 for an entry that is not a candidate
+    int pad;
+};
 __device__ __forceinline__ void rank_row32(long r, int b, int e, int ct, double wt, int* __restrict__ rank,
-    int* __restrict__ ordj, int* __restrict__ degE)
+    int* __restrict__ ordj, int* __restrict__ degE, RankKey* keys)
 {
     const int lane = threadIdx.x & 31;
     const int t = b + lane;
@@ -575,10 +583,14 @@ __device__ __forceinline__ void rank_row32(long r, int b, int e, int ct, double 
         // lane), so the rank is the number of candidates in higher lanes
         rk = __popc(lane == 31 ? 0u : (elig >> (lane + 1)));
     } else {
-        for (int k = 0; k < e - b; k++) {
-            const int ck = __shfl_sync(0xffffffffu, ct, k);
-            const double wk = __shfl_sync(0xffffffffu, wt, k);
-            rk += (((elig >> k) & 1u) && (wk > wt || (wk == wt && ck > ct))) ? 1 : 0;
+        __syncwarp();   // the warp's previous row has been read
+        keys[lane].w = wt;
+        keys[lane].c = el ? ct : -1;
+        __syncwarp();
+        const int d = e - b;
+        for (int k = 0; k < d; k++) {
+            const RankKey q = keys[k];
+            rk += (q.c >= 0 && (q.w > wt || (q.w == wt && q.c > ct))) ? 1 : 0;
         }
     }
     if (in) {
@@ -591,11 +603,13 @@ __device__ __forceinline__ void rank_row32(long r, int b, int e, int ct, double 
 // k_rank for a matrix whose rows all have at most 32 entries, with every entry's weight formed
 // in registers by k_logw's expression (same operations, same rounding) instead of read from W:
 // the weights are never stored.
-__global__ void k_rank_w(int n, const int* __restrict__ row, const int* __restrict__ col, const double* __restrict__ val,
+__global__ void __launch_bounds__(256, 8) k_rank_w(int n, const int* __restrict__ row, const int* __restrict__ col, const double* __restrict__ val,
     const double* __restrict__ w, const double* __restrict__ C, const int* __restrict__ tpos, double zero_sub,
     int* __restrict__ rank, int* __restrict__ ordj, int* __restrict__ degE)
 {
     const int lane = threadIdx.x & 31;
+    __shared__ RankKey keys[8][32];   // 256-thread blocks
+    RankKey* wkeys = keys[(threadIdx.x >> 5) & 7];
     for (long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32; r < n; r += (long)gridDim.x * blockDim.x / 32) {
         const int b = __ldg(row + r), e = __ldg(row + r + 1);
         const int t = b + lane;
@@ -607,7 +621,7 @@ __global__ void k_rank_w(int n, const int* __restrict__ row, const int* __restri
             const double sa = fabs(ahat(__ldg(val + src), __ldg(C + r), __ldg(C + ct), __ldg(w + r), __ldg(w + ct)));
             wt = log(sa != 0.0 ? sa : zero_sub);
         }
-        rank_row32(r, b, e, ct, wt, rank, ordj, degE);
+        rank_row32(r, b, e, ct, wt, rank, ordj, degE, wkeys);
     }
 }
 
@@ -615,12 +629,14 @@ __global__ void k_rank(int n, const int* __restrict__ row, const int* __restrict
     int* __restrict__ rank, int* __restrict__ ordj, int* __restrict__ degE)
 {
     const int lane = threadIdx.x & 31;
+    __shared__ RankKey keys[8][32];   // 256-thread blocks
+    RankKey* wkeys = keys[(threadIdx.x >> 5) & 7];
     for (long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32; r < n; r += (long)gridDim.x * blockDim.x / 32) {
         const int b = row[r], e = row[r + 1];
         if (e - b <= 32) {
             const int t = b + lane;
             const bool in = t < e;
-            rank_row32(r, b, e, in ? col[t] : -1, in ? W[t] : 0.0, rank, ordj, degE);
+            rank_row32(r, b, e, in ? col[t] : -1, in ? W[t] : 0.0, rank, ordj, degE, wkeys);
             continue;
         }
         int cnt = 0;
@@ -885,6 +901,34 @@ __global__ void k_make_p(int n, const int* __restrict__ M, const double* __restr
 // compaction then forms the CSR matrix. cap is the candidates a warp's shared memory holds: a
 // row with more is appended to long_rows (for a second launch with room for it, over that list:
 // rows = long_rows, nc its length), or flagged as an error when long_rows is NULL.
+// Rank sort of a coarse row's distinct 32-bit keys (k_galerkin's narrow form): lane l ranks keys
+// l, l + 32, ... (NS of them) against all cnt keys in one pass of broadcast reads, and writes each
+// key and its product to its sorted slot.
+template <int NS>
+__device__ __forceinline__ void gal_rank_pass(const unsigned* key32, const double* tv, int cnt, int lane,
+    unsigned* skey32, double* sval)
+{
+    unsigned kt[NS];
+    int pos[NS];
+#pragma unroll
+    for (int i = 0; i < NS; i++) {
+        kt[i] = lane + 32 * i < cnt ? key32[lane + 32 * i] : 0xffffffffu;
+        pos[i] = 0;
+    }
+#pragma unroll 4
+    for (int u = 0; u < cnt; u++) {
+        const unsigned ku = key32[u];
+#pragma unroll
+        for (int i = 0; i < NS; i++) pos[i] += ku < kt[i] ? 1 : 0;
+    }
+#pragma unroll
+    for (int i = 0; i < NS; i++)
+        if (lane + 32 * i < cnt) {
+            skey32[pos[i]] = kt[i];
+            sval[pos[i]] = tv[lane + 32 * i];
+        }
+}
+
 __global__ void k_galerkin(int nc, const int* __restrict__ rows, const int* __restrict__ fine0, const int* __restrict__ fine1,
     const int* __restrict__ agg, const double* __restrict__ p, const int* __restrict__ Arow, const int* __restrict__ Acol,
     const double* __restrict__ Aval, const int* __restrict__ off, long long out_cap, int* __restrict__ Crow,
@@ -937,13 +981,33 @@ __global__ void k_galerkin(int nc, const int* __restrict__ rows, const int* __re
                 tv[t] = __dmul_rn(Aval[j], p[c]);
             }
             __syncwarp();
-            for (int t = lane; t < cnt; t += 32) {
-                const unsigned kt = key32[t];
-                int pos = 0;
-#pragma unroll 8
-                for (int u = 0; u < cnt; u++) pos += key32[u] < kt ? 1 : 0;
-                skey32[pos] = kt;
-                sval[pos] = tv[t];
+            // when both fine rows' aggregate ids ascend along the row (the first sweep of a level
+            // numbers pairs by master id), their key lists are sorted: a merge places every key
+            bool asc = true;
+            for (int t = lane; t + 1 < cnt; t += 32)
+                if (t + 1 != d0 && (key32[t] >> 7) > (key32[t + 1] >> 7)) asc = false;
+            if (__all_sync(0xffffffffu, asc)) {
+                for (int t = lane; t < cnt; t += 32) {
+                    const unsigned kt = key32[t];
+                    const unsigned* other = t < d0 ? key32 + d0 : key32;
+                    int lo = 0, hi = t < d0 ? cnt - d0 : d0;
+                    while (lo < hi) {
+                        const int mid = (lo + hi) >> 1;
+                        if (other[mid] < kt) lo = mid + 1;
+                        else hi = mid;
+                    }
+                    const int pos = (t < d0 ? t : t - d0) + lo;
+                    skey32[pos] = kt;
+                    sval[pos] = tv[t];
+                }
+            } else {
+            // rank sort: each lane ranks its (up to 4) keys in one pass over the row's keys
+            switch ((cnt + 31) >> 5) {
+            case 1: gal_rank_pass<1>(key32, tv, cnt, lane, skey32, sval); break;
+            case 2: gal_rank_pass<2>(key32, tv, cnt, lane, skey32, sval); break;
+            case 3: gal_rank_pass<3>(key32, tv, cnt, lane, skey32, sval); break;
+            default: gal_rank_pass<4>(key32, tv, cnt, lane, skey32, sval); break;
+            }
             }
             __syncwarp();
             const double p0 = p[f0], p1 = f1 >= 0 ? p[f1] : 0.0;

@@ -635,8 +635,9 @@ def run_adjoint(a, rank=0, world=1, local_rank=0, steps=None, warmup=None):
 
 def run_batch(a, rank=0, world=1, local_rank=0, steps=None, warmup=None):
     """256 independent 7-point Poisson systems, box sides uniform in 10..46 (seed 4), diagonal shift
-    uniform[0, 0.5], FP32 V-cycle, rhs uniform[-1,1]: one CUDA-graph launch for all solves vs a
-    sequential loop of single solves (same hierarchies, warm graphs). At N > 1 rank r takes
+    uniform[0, 0.5], FP32 V-cycle, rhs uniform[-1,1]: one CUDA-graph launch for all solves (the
+    lockstep form; the per-system-branch form beside it) vs a sequential loop of single solves
+    (same hierarchies, warm graphs). At N > 1 rank r takes
     systems r, r + N, ... (bootcmatchgx_b200.replicas) on its own GPU, with no communication; the
     time is the slowest rank's and the value counts all 256 systems."""
     import scipy.sparse as sp
@@ -667,7 +668,10 @@ def run_batch(a, rank=0, world=1, local_rank=0, steps=None, warmup=None):
     B = bx.Batch(sysm, p, nthreads=nthreads)
     torch.cuda.synchronize()
     t_setup = max_over_ranks(time.perf_counter() - t0, world, dev)
-    xs, infos = B.solve(bs)   # builds the graph
+    t0 = time.perf_counter()
+    xs, infos = B.solve(bs)   # sets up the lockstep groups (the systems' block-diagonal unions) and the graph
+    torch.cuda.synchronize()
+    t_first = max_over_ranks(time.perf_counter() - t0, world, dev)
     for _ in range(max(0, warmup - 1)):
         B.solve(bs)
     torch.cuda.synchronize()
@@ -676,6 +680,17 @@ def run_batch(a, rank=0, world=1, local_rank=0, steps=None, warmup=None):
         xs, infos = B.solve(bs)
     torch.cuda.synchronize()
     t_batch = max_over_ranks((time.perf_counter() - t0) / steps, world, dev)
+    # the per-system form of the same batch (one graph branch per system) for comparison
+    B.set_lockstep(False)
+    for _ in range(max(1, warmup)):
+        B.solve(bs)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        B.solve(bs)
+    torch.cuda.synchronize()
+    t_branch = max_over_ranks((time.perf_counter() - t0) / steps, world, dev)
+    B.set_lockstep(True)
     hs = [B.hierarchy(k) for k in range(len(sysm))]
     for k, h in enumerate(hs):   # warm each single-solve graph
         h.solve(bs[k])
@@ -697,8 +712,12 @@ def run_batch(a, rank=0, world=1, local_rank=0, steps=None, warmup=None):
     B.free()
     return {"metric": "batched solves/s (256 uneven 7-point systems, one graph launch)", "value": 256 / t_batch,
             "unit": "solves/s", "higher_is_better": True, "workload": "batch256_poisson7", "n_gpus": world,
+            "form": "lockstep: every step one kernel over the systems of a group (groups of at most 32 systems "
+                    "with the same level count, neighbouring sizes), one graph for all groups",
             "sequential_solves_per_s": 256 / t_seq, "speedup_vs_sequential": t_seq / t_batch,
+            "per_system_graph_solves_per_s": 256 / t_branch,
             "batch_solve_ms": t_batch * 1e3, "sequential_ms": t_seq * 1e3, "setup_ms": t_setup * 1e3,
+            "first_solve_ms": t_first * 1e3,
             "total_rows": rows, "iters_min_max": [int(it_lo), int(it_hi)],
             "max_rel_residual": worst, "steps": steps, "warmup": warmup,
             "config": {"systems": 256, "sides": "uniform 10..46 (numpy default_rng(4))", "shift": "uniform[0,0.5]",

@@ -83,6 +83,7 @@ SIGNATURES = {
     "bcmgx_batch_from_hierarchies": (C.c_int, [C.c_int, _vp, C.POINTER(C.c_void_p)]),
     "bcmgx_batch_get_hierarchy": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_void_p)]),
     "bcmgx_batch_solve": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "bcmgx_batch_set_lockstep": (C.c_int, [_vp, C.c_int]),
     "bcmgx_batch_free": (C.c_int, [_vp]),
     "bcmgx_hierarchy_get_info": (C.c_int, [_vp, C.POINTER(HierarchyInfo)]),
     "bcmgx_hierarchy_get_level": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),

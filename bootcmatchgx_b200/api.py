@@ -339,9 +339,12 @@ class _Borrowed(Hierarchy):
 
 class Batch:
     """Independent systems whose set-ups run concurrently and whose solves run as one CUDA graph
-    launch (bcmgx_setup_batch / bcmgx_batch_solve). systems: list of host (row, col, val)."""
+    launch (bcmgx_setup_batch / bcmgx_batch_solve). systems: list of host (row, col, val).
+    lockstep: True (the library's default) runs every step as one kernel over all systems of a
+    level-count group (results equal single solves to rounding); False gives every system its own
+    graph branch (results equal single solves bit for bit); None keeps the library's default."""
 
-    def __init__(self, systems, params, nthreads=0):
+    def __init__(self, systems, params, nthreads=0, lockstep=None):
         arrs = []
         descs = (L.Csr * len(systems))()
         for k, (row, col, val) in enumerate(systems):
@@ -356,6 +359,11 @@ class Batch:
         self.h = h
         self.params = params
         self.sizes = [(r.size - 1, c.size) for r, c, _ in arrs]
+        if lockstep is not None:
+            self.set_lockstep(lockstep)
+
+    def set_lockstep(self, on):
+        check(lib().bcmgx_batch_set_lockstep(self.h, 1 if on else 0), "batch_set_lockstep")
 
     def __len__(self):
         return len(self.sizes)
@@ -369,7 +377,9 @@ class Batch:
         """bs, xs: lists of CUDA float64 tensors (xs updated in place; zeros when None)."""
         import torch
         if xs is None:
-            xs = [torch.zeros_like(b) for b in bs]
+            # one zeroed block for all systems (one fill instead of one per system), split into views
+            flat = torch.zeros(sum(int(b.numel()) for b in bs), dtype=torch.float64, device=bs[0].device)
+            xs = list(flat.split([int(b.numel()) for b in bs]))
         m = len(bs)
         pb = (C.c_void_p * m)(*[b.data_ptr() for b in bs])
         px = (C.c_void_p * m)(*[x.data_ptr() for x in xs])

@@ -160,6 +160,47 @@ static void after_caller(cudaStream_t s, cudaEvent_t ev, bool own)
     BCMGX_CUDA(cudaStreamWaitEvent(s, ev, 0));
 }
 
+// The row kernel of every level: BCMGX_TPR forces the codes (one code for every level, "-2", or
+// one per level, "-2,-2,4"; levels past the list take its last code); else the autotuner times
+// them (levels of at least 20,000 rows) or the default threads per row apply.
+void choose_level_kernels(bcmgx_hierarchy* H)
+{
+    const bcmgx_params* p = &H->prm;
+    std::vector<int> force;
+    if (const char* env = std::getenv("BCMGX_TPR")) {
+        for (const char* q = env; *q;) {
+            char* end = nullptr;
+            const long v = std::strtol(q, &end, 10);
+            BCMGX_REQUIRE(end != q, BCMGX_ERR_INVALID_INPUT, "BCMGX_TPR: expected comma-separated integers");
+            force.push_back((int)v);
+            q = *end == ',' ? end + 1 : end;
+            BCMGX_REQUIRE(*q == 0 || *end == ',', BCMGX_ERR_INVALID_INPUT, "BCMGX_TPR: expected comma-separated integers");
+        }
+    }
+    const int L = (int)H->lv.size();
+    for (int l = 0; l < L; l++) {
+        Level& V = H->lv[l];
+        const bool f32 = p->vcycle_precision == BCMGX_VCYCLE_FP32 && l < L - 1;
+        int code;
+        if (!force.empty()) code = force[std::min(l, (int)force.size() - 1)];
+        else if (p->autotune) code = autotune_tpr(V, f32, H->stream);
+        else code = default_tpr(V.A.n, V.A.nnz);
+        // negative: the staged kernel with -code threads per row (1, 2, 4 or 8); kSlicedCode: the
+        // sliced kernel (one lane per row: the CSR kernels stand in for it with 1 thread per row)
+        if (code == kSlicedCode) {
+            build_sliced(V.A, H->stream);
+            V.A.sliced = V.A.sl_ptr.p != nullptr;
+            V.A.staged = false;
+            V.A.tpr = 1;
+            continue;
+        }
+        release_sliced(V.A);
+        V.A.staged = code < 0;
+        V.A.tpr = code < 0 ? -code : code;
+        if (V.A.tpr < 1) V.A.tpr = default_tpr(V.A.n, V.A.nnz);
+    }
+}
+
 static bcmgx_hierarchy* setup_one(const bcmgx_csr* A, const bcmgx_params* p, int device, bool own_stream)
 {
     check_params(p);
@@ -197,41 +238,7 @@ static bcmgx_hierarchy* setup_one(const bcmgx_csr* A, const bcmgx_params* p, int
     BCMGX_CUDA(cudaEventRecord(t0.e, H->stream));
     stage_fault_init();
     build_hierarchy(H.get(), A);
-    // BCMGX_TPR forces the threads-per-row codes: one code for every level ("-2"), or one per level
-    // ("-2,-2,4"; levels past the list take its last code)
-    std::vector<int> force;
-    if (const char* env = std::getenv("BCMGX_TPR")) {
-        for (const char* q = env; *q;) {
-            char* end = nullptr;
-            const long v = std::strtol(q, &end, 10);
-            BCMGX_REQUIRE(end != q, BCMGX_ERR_INVALID_INPUT, "BCMGX_TPR: expected comma-separated integers");
-            force.push_back((int)v);
-            q = *end == ',' ? end + 1 : end;
-            BCMGX_REQUIRE(*q == 0 || *end == ',', BCMGX_ERR_INVALID_INPUT, "BCMGX_TPR: expected comma-separated integers");
-        }
-    }
-    const int L = (int)H->lv.size();
-    for (int l = 0; l < L; l++) {
-        Level& V = H->lv[l];
-        const bool f32 = p->vcycle_precision == BCMGX_VCYCLE_FP32 && l < L - 1;
-        int code;
-        if (!force.empty()) code = force[std::min(l, (int)force.size() - 1)];
-        else if (p->autotune) code = autotune_tpr(V, f32, H->stream);
-        else code = default_tpr(V.A.n, V.A.nnz);
-        // negative: the staged kernel with -code threads per row (1, 2, 4 or 8); kSlicedCode: the
-        // sliced kernel (one lane per row: the CSR kernels stand in for it with 1 thread per row)
-        if (code == kSlicedCode) {
-            build_sliced(V.A, H->stream);
-            V.A.sliced = V.A.sl_ptr.p != nullptr;
-            V.A.staged = false;
-            V.A.tpr = 1;
-            continue;
-        }
-        release_sliced(V.A);
-        V.A.staged = code < 0;
-        V.A.tpr = code < 0 ? -code : code;
-        if (V.A.tpr < 1) V.A.tpr = default_tpr(V.A.n, V.A.nnz);
-    }
+    choose_level_kernels(H.get());
     BCMGX_CUDA(cudaEventRecord(t1.e, H->stream));
     BCMGX_CUDA(cudaEventSynchronize(t1.e));
     float ms = 0;
@@ -262,6 +269,9 @@ using namespace bcmgx;
 bcmgx_batch::~bcmgx_batch()
 {
     if (stream) cudaStreamSynchronize(stream);
+    bcmgx::lock_free(this);
+    bcmgx::pinned_free(lock_copies_host);
+    bcmgx::pinned_free(lock_states_host);
     if (exec) cudaGraphExecDestroy(exec);
     copies.release();
     states_ptr.release();
@@ -438,14 +448,28 @@ int bcmgx_batch_solve(bcmgx_batch* B, const double* const* b, double* const* x, 
     int rc = guarded([&] {
         BCMGX_REQUIRE(B && b && x, BCMGX_ERR_INVALID_INPUT, "NULL argument");
         DeviceScope ds(B->device);
-        if (!B->exec) batch_build(B);
-        after_caller(B->stream, B->ev_in, B->own_stream);
-        status = batch_solve(B, b, x, infos);
+        if (B->lockstep && lock_supported(B)) {
+            if (!B->lock_exec) lock_build(B);
+            after_caller(B->stream, B->ev_in, B->own_stream);
+            status = lock_solve(B, b, x, infos);
+        } else {
+            if (!B->exec) batch_build(B);
+            after_caller(B->stream, B->ev_in, B->own_stream);
+            status = batch_solve(B, b, x, infos);
+        }
         if (status == BCMGX_ERR_NO_CONVERGENCE) set_last_error("batch solve: a system reached itnlim");
         if (status == BCMGX_ERR_NOT_SPD) set_last_error("batch solve: FCG breakdown in a system");
         stage_fault_check();
     });
     return rc != BCMGX_OK ? rc : status;
+}
+
+int bcmgx_batch_set_lockstep(bcmgx_batch* B, int on)
+{
+    return guarded([&] {
+        BCMGX_REQUIRE(B, BCMGX_ERR_INVALID_INPUT, "NULL argument");
+        B->lockstep = on ? 1 : 0;
+    });
 }
 
 int bcmgx_batch_free(bcmgx_batch* B)

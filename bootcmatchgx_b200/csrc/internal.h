@@ -256,6 +256,16 @@ struct bcmgx_hierarchy {
 };
 
 // A set of hierarchies whose solves run together as one CUDA graph launch.
+namespace bcmgx {
+struct LockGroup;
+// one copy of a batch solve's vector list (lockstep.cu)
+struct LockCopy {
+    const double* src;
+    double* dst;
+    int n;
+};
+}  // namespace bcmgx
+
 struct bcmgx_batch {
     std::vector<bcmgx_hierarchy*> hs;
     bool own = false;              // created by bcmgx_setup_batch: frees the hierarchies too
@@ -268,6 +278,15 @@ struct bcmgx_batch {
     void* states_host = nullptr;
     void* copies_host = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_in = nullptr;
+    // lockstep form (lockstep.cu, the default where the members share their cycle settings): the
+    // members grouped by level count, each group one block-diagonal hierarchy, one graph for all
+    int lockstep = 1;
+    std::vector<bcmgx::LockGroup*> groups;   // owned; released by lock_free
+    cudaGraphExec_t lock_exec = nullptr;
+    bcmgx::DBuf<bcmgx::LockCopy> lock_copies;
+    bcmgx::DBuf<bcmgx::FcgState> lock_states;
+    void* lock_copies_host = nullptr;
+    void* lock_states_host = nullptr;
     ~bcmgx_batch();
 };
 
@@ -352,6 +371,10 @@ double time_block_dots(bcmgx_hierarchy* H, int K, int reps);
 void grad_pattern(const DevCsr& A, const double* lam, const double* x, double* dA, cudaStream_t s);
 void batch_build(bcmgx_batch* B);
 int batch_solve(bcmgx_batch* B, const double* const* b, double* const* x, bcmgx_solve_info* infos);
+bool lock_supported(const bcmgx_batch* B);
+void lock_build(bcmgx_batch* B);
+int lock_solve(bcmgx_batch* B, const double* const* b, double* const* x, bcmgx_solve_info* infos);
+void lock_free(bcmgx_batch* B);
 
 // Blocks of `kernel` resident per SM with `threads` threads and `smem` bytes of dynamic shared
 // memory on the current device (queried once per combination and device, then cached).
@@ -375,6 +398,7 @@ inline void ensure_smem_limit(void (*kernel)(A...), size_t bytes)
 
 // ---- kernels usable on raw device memory (kernels.cu) ----
 int autotune_tpr(Level& V, bool f32, cudaStream_t s);
+void choose_level_kernels(bcmgx_hierarchy* H);
 void stage_fault_init();
 void stage_fault_check();
 int default_tpr(int n, int64_t nnz);

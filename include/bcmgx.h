@@ -216,6 +216,14 @@ int bcmgx_batch_from_hierarchies(int nsys, bcmgx_hierarchy* const* hs, bcmgx_bat
 int bcmgx_batch_get_hierarchy(bcmgx_batch* B, int k, bcmgx_hierarchy** h);
 /* b[k], x[k]: device vectors of system k (x: x0 in, solution out). infos: nsys entries or NULL. */
 int bcmgx_batch_solve(bcmgx_batch* B, const double* const* b, double* const* x, bcmgx_solve_info* infos);
+/* Lockstep form of the batch solve (on = 1, the default, when every member is BCMG with the same
+ * cycle settings, rtol and itnlim): the members are grouped by their number of levels, each group's
+ * hierarchy is the block-diagonal union of its members' (set up on the first solve), and every
+ * V-cycle step and FCG step is one kernel over all members of a group; each member keeps its own
+ * FCG scalars and stopping test, and the solution agrees with the member's single solve to
+ * rounding. on = 0: one graph branch per member, whose iterates equal single solves bit for bit.
+ * No counterpart in the reference. */
+int bcmgx_batch_set_lockstep(bcmgx_batch* B, int on);
 int bcmgx_batch_free(bcmgx_batch* B);
 
 /* ---- row-partitioned multi-rank set-up and solve ------------------------------------------ */

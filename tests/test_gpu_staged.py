@@ -87,7 +87,7 @@ def test_staged_hierarchies_in_batch_graph(bx, cuda, monkeypatch):
     systems = _systems(bx, 4, 21, lo=20, hi=34)
     p = bx.params_default(solver="FCG", preconditioner="BCMG", rtol=1e-8, dispnorm=0, vcycle_precision="FP32")
     monkeypatch.setenv("BCMGX_TPR", "-4")
-    B = bx.Batch(systems, p, nthreads=2)
+    B = bx.Batch(systems, p, nthreads=2, lockstep=False)
     singles = [bx.prec_setup(r, c, v, p) for r, c, v in systems]
     monkeypatch.delenv("BCMGX_TPR")
     rng = np.random.default_rng(8)

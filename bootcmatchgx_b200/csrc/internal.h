@@ -415,6 +415,7 @@ struct FusedWeights {
     const double* w = nullptr;
     const double* C = nullptr;
     double zero_sub = 0.0;
+    const double* zero_sub_dev = nullptr;   // when set, the substitute is read from here
 };
 // err_out: when given, the matching's error bits go to that device word and are not read back
 // here (the caller reads them with its next round trip); otherwise they are checked on return.

@@ -512,8 +512,9 @@ __global__ void k_ahat_min(int n, const int* __restrict__ row, const int* __rest
 template <int S>
 __global__ void k_logw(int n, const int* __restrict__ row, const int* __restrict__ col, const double* __restrict__ val,
     const double* __restrict__ w, const double* __restrict__ C, const int* __restrict__ tpos, double zero_sub,
-    double* __restrict__ W)
+    double* __restrict__ W, const double* __restrict__ zero_sub_dev = nullptr)
 {
+    if (zero_sub_dev) zero_sub = *zero_sub_dev;
     constexpr int U = kSetupBatch;
     const int lane = threadIdx.x & (S - 1);
     BCMGX_SUBWARP_ROWS(r, n, S)
@@ -605,8 +606,9 @@ __device__ __forceinline__ void rank_row32(long r, int b, int e, int ct, double 
 // the weights are never stored.
 __global__ void __launch_bounds__(256, 8) k_rank_w(int n, const int* __restrict__ row, const int* __restrict__ col, const double* __restrict__ val,
     const double* __restrict__ w, const double* __restrict__ C, const int* __restrict__ tpos, double zero_sub,
-    int* __restrict__ rank, int* __restrict__ ordj, int* __restrict__ degE)
+    int* __restrict__ rank, int* __restrict__ ordj, int* __restrict__ degE, const double* __restrict__ zero_sub_dev)
 {
+    if (zero_sub_dev) zero_sub = *zero_sub_dev;
     const int lane = threadIdx.x & 31;
     __shared__ RankKey keys[8][32];   // 256-thread blocks
     RankKey* wkeys = keys[(threadIdx.x >> 5) & 7];
@@ -1318,6 +1320,19 @@ static int row_max_raw(int n, const int* row, cudaStream_t s)
 }
 static int row_max(const DevCsr& A, cudaStream_t s) { return row_max_raw(A.n, A.row.p, s); }
 
+__global__ void k_set_u64(unsigned long long* p, unsigned long long v) { *p = v; }
+
+// SUITOR_EPS / (0.999 min |a_hat|) on the device, with the host form's operations (edge_prep_dev):
+// the minimum capped by min_cap and raised to DBL_EPSILON (toMaximumProductMatrix,
+// matching.cu:243-245)
+__global__ void k_zero_sub(const unsigned long long* min_bits, double min_cap, double* out)
+{
+    double m = __longlong_as_double((long long)*min_bits);
+    m = fmin(m, min_cap);
+    if (fabs(m) < DBL_EPSILON) m = DBL_EPSILON;
+    *out = __ddiv_rn(kSuitorEps, __dmul_rn(0.999, m));
+}
+
 // The inputs of the edge weights: C_r (into C, n doubles), the transposed positions and the
 // substitute log argument SUITOR_EPS / (0.999 min |a_hat|) for a_hat == 0; returns it and, when
 // min_out_host is set, the minimum.
@@ -1406,7 +1421,8 @@ void suitor_dev(int n, int64_t nnz, const int* row, const int* col, const double
     }
     if (fw) {
         note_launch();
-        k_rank_w<<<warp_grid(n), 256, 0, s>>>(n, row, col, fw->val, fw->w, fw->C, tpos, fw->zero_sub, rank.p, ordj.p, degE.p);
+        k_rank_w<<<warp_grid(n), 256, 0, s>>>(n, row, col, fw->val, fw->w, fw->C, tpos, fw->zero_sub, rank.p, ordj.p, degE.p,
+            fw->zero_sub_dev);
     } else {
         note_launch(); k_rank<<<warp_grid(n), 256, 0, s>>>(n, row, col, W, rank.p, ordj.p, degE.p);
     }
@@ -1452,6 +1468,20 @@ struct SweepOut {
 // The matching and the pairwise prolongator of one sweep on the square matrix A with weights w:
 // agg/p per row of A (aggregate ids 0..nc-1, pairs by master then singletons), the fine rows of
 // every aggregate (fine0, fine1; -1 for a singleton) and the coarse weights wc = R w. min_cap
+// edge_prep_dev without a host round trip: the substitute goes to *zs_dev, the diagonal check's
+// error bits to the caller's error word (read with its next round trip).
+static void edge_prep_async(int n, int64_t nnz, const int* row, const int* col, const double* val, const double* w,
+    double* C, int* tpos, double* zs_dev, unsigned long long* mn, int* err, cudaStream_t s, double min_cap)
+{
+    const int S = setup_subwarp(n, nnz);
+    note_launch(); k_set_u64<<<1, 1, 0, s>>>(mn, (unsigned long long)__builtin_bit_cast(long long, DBL_MAX));
+    note_launch(); k_diag_c<<<gs_grid(n), 256, 0, s>>>(n, row, col, val, w, C, err);
+    BCMGX_SUBWARP_LAUNCH(k_tpos, S, n, s, n, row, col, tpos);
+    BCMGX_SUBWARP_LAUNCH(k_ahat_min, S, n, s, n, row, col, val, w, C, mn);
+    note_launch(); k_zero_sub<<<1, 1, 0, s>>>(mn, min_cap, zs_dev);
+    BCMGX_CHECK_LAUNCH();
+}
+
 // bounds the edge weights' minimum (edge_prep_dev).
 void sweep_aggregate(bcmgx_hierarchy* H, const DevCsr& A, const double* w, SweepAgg& out, int level, int sweep,
     double min_cap)
@@ -1467,17 +1497,23 @@ void sweep_aggregate(bcmgx_hierarchy* H, const DevCsr& A, const double* w, Sweep
     err.alloc(1, s);
     BCMGX_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), s));
     const int amax0 = A.max_row > 0 ? A.max_row : row_max(A, s);
+    // the substitute weight and the minimum it comes from stay on the device (no round trip)
+    DBuf<double> zs;
+    DBuf<unsigned long long> mn;
+    zs.alloc(1, s);
+    mn.alloc(1, s);
     if (amax0 <= 32) {
         // rows of at most 32 entries: the rank kernel forms the edge weights itself
         Cd.alloc(n, s);
         FusedWeights fw;
         {
             PhaseTimer pt(H, "weights");
-            fw.zero_sub = edge_prep_dev(n, nnz, A.row.p, A.col.p, A.val.p, w, Cd.p, tpos.p, nullptr, s, min_cap);
+            edge_prep_async(n, nnz, A.row.p, A.col.p, A.val.p, w, Cd.p, tpos.p, zs.p, mn.p, err.p, s, min_cap);
         }
         fw.val = A.val.p;
         fw.w = w;
         fw.C = Cd.p;
+        fw.zero_sub_dev = zs.p;
         PhaseTimer pt(H, "suitor");
         suitor_dev(n, nnz, A.row.p, A.col.p, nullptr, tpos.p, M.p, amax0, s, &fw, err.p);
     } else {
@@ -1486,9 +1522,9 @@ void sweep_aggregate(bcmgx_hierarchy* H, const DevCsr& A, const double* w, Sweep
             PhaseTimer pt(H, "weights");
             DBuf<double> C;
             C.alloc(n, s);
-            const double zero_sub = edge_prep_dev(n, nnz, A.row.p, A.col.p, A.val.p, w, C.p, tpos.p, nullptr, s, min_cap);
+            edge_prep_async(n, nnz, A.row.p, A.col.p, A.val.p, w, C.p, tpos.p, zs.p, mn.p, err.p, s, min_cap);
             BCMGX_SUBWARP_LAUNCH(k_logw, setup_subwarp(n, nnz), n, s, n, A.row.p, A.col.p, A.val.p, w, C.p, tpos.p,
-                zero_sub, W.p);
+                0.0, W.p, zs.p);
             BCMGX_CHECK_LAUNCH();
         }
         PhaseTimer pt(H, "suitor");
@@ -1514,6 +1550,7 @@ void sweep_aggregate(bcmgx_hierarchy* H, const DevCsr& A, const double* w, Sweep
     BCMGX_CUDA(cudaMemcpyAsync(th, tots.p, 2 * sizeof(long long), cudaMemcpyDeviceToHost, s));
     BCMGX_CUDA(cudaMemcpyAsync(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     BCMGX_CUDA(cudaStreamSynchronize(s));
+    if (e & ERR_NODIAG) throw Error(BCMGX_ERR_INVALID_INPUT, "edge weights: " + err_text(e));
     if (e) throw Error(e & ERR_SUITOR_BUDGET ? BCMGX_ERR_TIMEOUT : BCMGX_ERR_INTERNAL, "aggregation: " + err_text(e));
     const long long npairs = th[0], nsing = th[1];
     const int nc = (int)(npairs + nsing);

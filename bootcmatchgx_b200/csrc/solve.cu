@@ -1382,8 +1382,36 @@ static void launch_resid0(const DevCsr& A, const double* x, const double* b, dou
         k<<<red_grid(k, (long)A.n * S), kRedThreads, 0, s>>>(A.n, A.row.p, A.col.p, A.val.p, x, b, r, st, part);
     }
 }
+// ||r||^2 -> delta0 and the tolerance, as k_fcg_resid0 finishes, for an r formed by the level's
+// row kernel
+__global__ void __launch_bounds__(kRedThreads) k_fcg_norm0(int n, const double* __restrict__ r, FcgState* st,
+    double* partials)
+{
+    double acc[1] = { 0.0 };
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        acc[0] += r[i] * r[i];
+    double out[1];
+    if (grid_sum<1>(acc, partials, &st->ticket[0], out) && threadIdx.x == 0) {
+        st->delta0 = sqrt(out[0]);
+        st->tol = st->tol * st->delta0;   // tol holds rtol on entry
+        st->iter = 0;
+        st->done = 0;
+        st->bad = 0;
+    }
+}
+
 static void fcg_resid0(const DevCsr& A, const double* x, const double* b, double* r, FcgState* st, double* part, cudaStream_t s)
 {
+    if (A.sliced) {
+        // the sliced kernel forms r = b - A x with the one-thread-per-row kernel's row sums; the
+        // norm follows in a kernel of its own
+        rowop_resid(A, x, b, r, nullptr, s);
+        note_launch();
+        auto k = k_fcg_norm0;
+        k<<<red_grid(k, A.n), kRedThreads, 0, s>>>(A.n, r, st, part);
+        BCMGX_CHECK_LAUNCH();
+        return;
+    }
     switch (A.tpr) {
     case 1: launch_resid0<1>(A, x, b, r, st, part, s); break;
     case 2: launch_resid0<2>(A, x, b, r, st, part, s); break;

@@ -145,3 +145,28 @@ def test_cli_reproduces_every_golden(golden, cuda, tmp_path, st, PQR):
     g = golden[f"sol__lap3d_{st}p_10x10x10_{PQR[0]}x{PQR[1]}x{PQR[2]}_sol"]
     assert x.size == g.size
     assert np.linalg.norm(x - g) / np.linalg.norm(g) < 1e-5
+
+
+def test_config_diffusion7_256_hierarchy(bx, oracle, cuda):
+    """The heterogeneous-diffusion workload (7-point finite volume 256^3, 16,777,216 rows,
+    kappa = exp(theta), theta a Gaussian random field of length 8 and sigma 2 from seed 2): every
+    sweep and every level bit for bit against the oracle's set-up, and the GPU's FP64 and FP32
+    solves to 1e-8 reach the tolerance (b ~ U[0,1] from seed 3)."""
+    from bootcmatchgx_b200 import problems
+    g = (256, 256, 256)
+    theta = problems.gaussian_random_field(g, 8.0, 2.0, 2).reshape(-1, order="F")
+    row, col, val = bx.diffusion_7p(*g, np.exp(theta))
+    n = row.size - 1
+    A = sp.csr_matrix((val, col, row), shape=(n, n))
+    assert A.nnz == 117047296
+    oracle.num_threads(os.cpu_count() or 1)
+    Ao = oracle.Matrix.from_csr(A.indptr, A.indices, A.data)
+    Ho = check_hierarchy(bx, oracle, A, Ao)
+    del Ho
+    b = np.random.default_rng(3).uniform(0.0, 1.0, n)
+    for prec in ("FP64", "FP32"):
+        h = bx.prec_setup(A.indptr, A.indices, A.data, fcg(bx, rtol=1e-8, vcycle_precision=prec))
+        x, info = h.solve(b)
+        h.free()
+        assert info["status"] == 0
+        assert np.linalg.norm(b - A @ x) <= 1e-8 * np.linalg.norm(b) * 1.0001

@@ -26,6 +26,26 @@ constexpr int kSliceRows = 32;                       // rows per slice (one warp
 constexpr int kSliceG = 4;                           // entries per lane per block
 constexpr int kSliceBlock = kSliceRows * kSliceG;    // entries per block of a slice
 
+// loads from a shared-memory stage by 32-bit shared addresses
+__device__ __forceinline__ uint2 lds_v2(unsigned a)
+{
+    uint2 v;
+    asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ unsigned lds_v1(unsigned a)
+{
+    unsigned v;
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ uint4 lds_v4(unsigned a)
+{
+    uint4 v;
+    asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(a));
+    return v;
+}
+
 // raw index words of a block (decoded into columns only when the gathers are issued); load:
 // from the sliced arrays in global memory (streamed), lds: from a shared-memory stage
 template <typename IT> struct SlIdxRaw;
@@ -33,6 +53,7 @@ template <> struct SlIdxRaw<short> {
     uint2 u;
     __device__ __forceinline__ void load(const short* p) { u = __ldcs((const uint2*)p); }
     __device__ __forceinline__ void lds(const unsigned char* p) { u = *(const uint2*)p; }
+    __device__ __forceinline__ void ldsa(unsigned a) { u = lds_v2(a); }
     __device__ __forceinline__ int col(int i, int rr) const
     {
         const unsigned w = i < 2 ? u.x : u.y;
@@ -43,6 +64,11 @@ template <> struct SlIdxRaw<int> {
     int4 u;
     __device__ __forceinline__ void load(const int* p) { u = __ldcs((const int4*)p); }
     __device__ __forceinline__ void lds(const unsigned char* p) { u = *(const int4*)p; }
+    __device__ __forceinline__ void ldsa(unsigned a)
+    {
+        const uint4 v = lds_v4(a);
+        u = make_int4((int)v.x, (int)v.y, (int)v.z, (int)v.w);
+    }
     __device__ __forceinline__ int col(int i, int) const { return i == 0 ? u.x : i == 1 ? u.y : i == 2 ? u.z : u.w; }
 };
 
@@ -55,6 +81,7 @@ template <typename T> struct SlVal<Coded<T>> {
     unsigned u;
     __device__ __forceinline__ void load(const void* p) { u = __ldcs((const unsigned*)p); }
     __device__ __forceinline__ void lds(const unsigned char* p) { u = *(const unsigned*)p; }
+    __device__ __forceinline__ void ldsa(unsigned a) { u = lds_v1(a); }
     __device__ __forceinline__ T get(int i, const T* tab) const { return tab[__byte_perm(u, 0u, 0x4440u + i)]; }
 };
 template <> struct SlVal<const float*> {
@@ -124,6 +151,40 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 extern __shared__ __align__(128) unsigned char sl_smem[];
+
+// The row sum of a lane over a staged slice of exactly NBC blocks (known at compile time: every
+// loop unrolled, no per-block test), in the order of the general path: block by block, entry by
+// entry. sb: the stage's 32-bit shared address.
+template <int NBC, typename VS, typename XT, typename IT, typename AT, typename VT>
+__device__ __forceinline__ AT slice_sum_fixed(unsigned sb, int lane, int rr, const XT* __restrict__ x, const VT* tab_s)
+{
+    using V = SlVal<VS>;
+    using ST = SlStage<IT, VS>;
+    constexpr int GB = sizeof(XT) == 4 ? 4 : 2;
+    SlIdxRaw<IT> ix[NBC];
+    V vv[NBC];
+#pragma unroll
+    for (int u = 0; u < NBC; u++) {
+        ix[u].ldsa(sb + (unsigned)(u * ST::kIdxB + lane * kSliceG * (int)sizeof(IT)));
+        vv[u].ldsa(sb + (unsigned)(ST::VAL + u * ST::kValB + lane * kSliceG * V::kBytes));
+    }
+    AT s = 0;
+#pragma unroll
+    for (int g = 0; g < NBC; g += GB) {
+        XT xv[GB][kSliceG];
+#pragma unroll
+        for (int u = 0; u < GB; u++)
+            if (g + u < NBC)
+#pragma unroll
+                for (int i = 0; i < kSliceG; i++) xv[u][i] = ld_ro(x + ix[g + u].col(i, rr));
+#pragma unroll
+        for (int u = 0; u < GB; u++)
+            if (g + u < NBC)
+#pragma unroll
+                for (int i = 0; i < kSliceG; i++) s += (AT)vv[g + u].get(i, tab_s) * (AT)xv[u][i];
+    }
+    return s;
+}
 
 // y = alpha A x + beta y, y = f - A x, or one l1-Jacobi sweep (the operations of k_rowop) over the
 // sliced form: one warp per slice (grid-stride over slices), one lane per row. Each warp copies the
@@ -222,7 +283,25 @@ __global__ void __launch_bounds__(kSlWarps * 32, 3) k_rowop_sliced(int n, const 
         }
         AT s = 0;
         const long base = (long)b0 + lane * kSliceG;
-        for (int q0 = 0; q0 < nb; q0 += CB) {
+        bool fixed = false;
+        if constexpr (FIT && ValSrc<VS>::coded) {
+            // coded levels, whose kernels are bound by instruction issue: the slice's width as a
+            // compile-time count
+            const unsigned sb = stage0_s + (unsigned)(st * kSlStageBytes);
+            fixed = true;
+            switch (nb) {
+            case 1: s = slice_sum_fixed<1, VS, XT, IT, AT>(sb, lane, rr, x, tab_s); break;
+            case 2: s = slice_sum_fixed<2, VS, XT, IT, AT>(sb, lane, rr, x, tab_s); break;
+            case 3: if constexpr (ST::NBMAX >= 3) { s = slice_sum_fixed<3, VS, XT, IT, AT>(sb, lane, rr, x, tab_s); break; } [[fallthrough]];
+            case 4: if constexpr (ST::NBMAX >= 4) { s = slice_sum_fixed<4, VS, XT, IT, AT>(sb, lane, rr, x, tab_s); break; } [[fallthrough]];
+            case 5: if constexpr (ST::NBMAX >= 5) { s = slice_sum_fixed<5, VS, XT, IT, AT>(sb, lane, rr, x, tab_s); break; } [[fallthrough]];
+            case 6: if constexpr (ST::NBMAX >= 6) { s = slice_sum_fixed<6, VS, XT, IT, AT>(sb, lane, rr, x, tab_s); break; } [[fallthrough]];
+            case 7: if constexpr (ST::NBMAX >= 7) { s = slice_sum_fixed<7, VS, XT, IT, AT>(sb, lane, rr, x, tab_s); break; } [[fallthrough]];
+            case 8: if constexpr (ST::NBMAX >= 8) { s = slice_sum_fixed<8, VS, XT, IT, AT>(sb, lane, rr, x, tab_s); break; } [[fallthrough]];
+            default: fixed = nb == 0;
+            }
+        }
+        for (int q0 = 0; !fixed && q0 < nb; q0 += CB) {
             SlIdxRaw<IT> ix[CB];
             V vv[CB];
 #pragma unroll

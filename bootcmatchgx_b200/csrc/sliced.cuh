@@ -91,6 +91,11 @@ template <> struct SlVal<const float*> {
     float4 u;
     __device__ __forceinline__ void load(const void* p) { u = __ldcs((const float4*)p); }
     __device__ __forceinline__ void lds(const unsigned char* p) { u = *(const float4*)p; }
+    __device__ __forceinline__ void ldsa(unsigned a)
+    {
+        const uint4 v = lds_v4(a);
+        u = make_float4(__uint_as_float(v.x), __uint_as_float(v.y), __uint_as_float(v.z), __uint_as_float(v.w));
+    }
     __device__ __forceinline__ float get(int i, const float*) const { return i == 0 ? u.x : i == 1 ? u.y : i == 2 ? u.z : u.w; }
 };
 template <> struct SlVal<const double*> {
@@ -107,6 +112,12 @@ template <> struct SlVal<const double*> {
     {
         a = *(const double2*)p;
         b = *((const double2*)p + 1);
+    }
+    __device__ __forceinline__ void ldsa(unsigned addr)
+    {
+        const uint4 v = lds_v4(addr), w = lds_v4(addr + 16);
+        a = make_double2(__hiloint2double((int)v.y, (int)v.x), __hiloint2double((int)v.w, (int)v.z));
+        b = make_double2(__hiloint2double((int)w.y, (int)w.x), __hiloint2double((int)w.w, (int)w.z));
     }
     __device__ __forceinline__ double get(int i, const double*) const { return i == 0 ? a.x : i == 1 ? a.y : i == 2 ? b.x : b.y; }
 };
@@ -284,9 +295,8 @@ __global__ void __launch_bounds__(kSlWarps * 32, 3) k_rowop_sliced(int n, const 
         AT s = 0;
         const long base = (long)b0 + lane * kSliceG;
         bool fixed = false;
-        if constexpr (FIT && ValSrc<VS>::coded) {
-            // coded levels, whose kernels are bound by instruction issue: the slice's width as a
-            // compile-time count
+        if (staged) {
+            // the width of a staged slice as a compile-time count
             const unsigned sb = stage0_s + (unsigned)(st * kSlStageBytes);
             fixed = true;
             switch (nb) {

@@ -932,7 +932,7 @@ __device__ __forceinline__ void gal_rank_pass(const unsigned* key32, const doubl
 }
 
 __global__ void k_galerkin(int nc, const int* __restrict__ rows, const int* __restrict__ fine0, const int* __restrict__ fine1,
-    const int* __restrict__ agg, const double* __restrict__ p, const int* __restrict__ Arow, const int* __restrict__ Acol,
+    const int* __restrict__ agg, const double* __restrict__ p, const int4* __restrict__ span, const int* __restrict__ Acol,
     const double* __restrict__ Aval, const int* __restrict__ off, long long out_cap, int* __restrict__ Crow,
     int* __restrict__ Ccol, double* __restrict__ Cval, int cap, int* __restrict__ long_rows, int* __restrict__ nlong,
     int* __restrict__ long_max, int* err, int ncols)
@@ -952,9 +952,11 @@ __global__ void k_galerkin(int nc, const int* __restrict__ rows, const int* __re
     for (long k = (long)blockIdx.x * wpb + wid; k < nc; k += (long)gridDim.x * wpb) {
         const int I = rows ? rows[k] : (int)k;
         const int f0 = fine0[I], f1 = fine1[I];
-        const int b0 = Arow[f0], d0 = Arow[f0 + 1] - b0;
-        const int b1 = f1 >= 0 ? Arow[f1] : 0, d1 = f1 >= 0 ? Arow[f1 + 1] - b1 : 0;
+        const int4 sp = __ldg(span + I);
+        const int b0 = sp.x, d0 = sp.y, b1 = sp.z, d1 = sp.w;
         const int cnt = d0 + d1;
+        // the fine rows' prolongator values, requested before the row's entries and used last
+        const double p0 = p[f0], p1 = f1 >= 0 ? p[f1] : 0.0;
         if (off[I] < 0 || (long long)off[I] + cnt > out_cap) {
             if (lane == 0) {
                 atomicOr(err, ERR_GALERKIN_OFS);
@@ -1012,7 +1014,6 @@ __global__ void k_galerkin(int nc, const int* __restrict__ rows, const int* __re
             }
             }
             __syncwarp();
-            const double p0 = p[f0], p1 = f1 >= 0 ? p[f1] : 0.0;
             const long outbase = off[I];
             int nheads = 0;
             for (int base = 0; base < cnt; base += 32) {
@@ -1068,7 +1069,6 @@ __global__ void k_galerkin(int nc, const int* __restrict__ rows, const int* __re
             sidx[pos] = t;
         }
         __syncwarp();
-        const double p0 = p[f0], p1 = f1 >= 0 ? p[f1] : 0.0;
         const long outbase = off[I];
         int nheads = 0;
         for (int base = 0; base < cnt; base += 32) {
@@ -1208,12 +1208,18 @@ __global__ void k_galerkin_list_counts(int nrows, const int* __restrict__ rows, 
 }
 
 // Number of candidate entries of every coarse row: the entries of its fine rows.
+// cnt[I]: the candidate entries of coarse row I (its fine rows' entries); span[I]: the first entry
+// and the length of each fine row (b0, d0, b1, d1), so that the product kernel finds them with one
+// load instead of two dependent ones
 __global__ void k_galerkin_counts(int nc, const int* __restrict__ fine0, const int* __restrict__ fine1,
-    const int* __restrict__ Arow, int* __restrict__ cnt)
+    const int* __restrict__ Arow, int* __restrict__ cnt, int4* __restrict__ span)
 {
     for (long I = (long)blockIdx.x * blockDim.x + threadIdx.x; I < nc; I += (long)gridDim.x * blockDim.x) {
         const int f0 = fine0[I], f1 = fine1[I];
-        cnt[I] = (Arow[f0 + 1] - Arow[f0]) + (f1 >= 0 ? Arow[f1 + 1] - Arow[f1] : 0);
+        const int b0 = Arow[f0], d0 = Arow[f0 + 1] - b0;
+        const int b1 = f1 >= 0 ? Arow[f1] : 0, d1 = f1 >= 0 ? Arow[f1 + 1] - b1 : 0;
+        cnt[I] = d0 + d1;
+        span[I] = make_int4(b0, d0, b1, d1);
     }
 }
 
@@ -1609,7 +1615,9 @@ void galerkin_dev(bcmgx_hierarchy* H, const DevCsr& A, const int* agg, const dou
     DBuf<double> pval;
     cand.alloc(std::max(nc, 1), s);
     off.alloc((size_t)nc + 1, s);
-    note_launch(); k_galerkin_counts<<<gs_grid(nc), 256, 0, s>>>(nc, fine0, fine1, A.row.p, cand.p);
+    DBuf<int4> span;
+    span.alloc(std::max(nc, 1), s);
+    note_launch(); k_galerkin_counts<<<gs_grid(nc), 256, 0, s>>>(nc, fine0, fine1, A.row.p, cand.p, span.p);
     BCMGX_CHECK_LAUNCH();
     // the candidates of all coarse rows are entries of A (every row of A is in at most one
     // aggregate); k_galerkin checks each row's range against that before writing
@@ -1634,7 +1642,7 @@ void galerkin_dev(bcmgx_hierarchy* H, const DevCsr& A, const int* agg, const dou
         ensure_smem_limit(k_galerkin, smem);
         const int g = (int)std::max<long>(1, std::min<long>(((long)nrows + wpb - 1) / wpb, (long)num_sms() * 32));
         note_launch();
-        k_galerkin<<<g, wpb * 32, smem, s>>>(nrows, rows, fine0, fine1, agg, p, A.row.p, A.col.p,
+        k_galerkin<<<g, wpb * 32, smem, s>>>(nrows, rows, fine0, fine1, agg, p, span.p, A.col.p,
             A.val.p, off.p, (long long)total, counts.p, pcol.p, pval.p, cap, list, stat, stat ? stat + 1 : nullptr, err.p,
             ncols);
         BCMGX_CHECK_LAUNCH();

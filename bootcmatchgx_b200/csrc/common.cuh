@@ -18,6 +18,14 @@ __device__ __forceinline__ float ld_stream(const float* p) { return __ldcs(p); }
 template <typename T>
 __device__ __forceinline__ T ld_ro(const T* p) { return __ldg(p); }
 
+// Programmatic dependent launch (launch_dep): dep_wait() returns once the kernel before this one in
+// the stream has completed and its writes are visible (at once for an ordinary launch);
+// dep_release() lets the next kernel of the stream be scheduled while this one runs. A kernel that
+// launch_dep launches calls dep_wait() before it touches a vector an earlier kernel writes and
+// before it returns, so that its own completion implies its predecessors'.
+__device__ __forceinline__ void dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void dep_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // Loads / stores that bypass L1 (values written by other SMs during the same kernel).
 __device__ __forceinline__ int ld_cg(const int* p) { return __ldcg(p); }
 __device__ __forceinline__ unsigned ld_cg(const unsigned* p) { return __ldcg(p); }

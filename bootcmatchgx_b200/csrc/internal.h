@@ -48,6 +48,36 @@ extern thread_local long long t_fail_alloc_countdown;
 
 #define BCMGX_CHECK_LAUNCH() BCMGX_CUDA(cudaGetLastError())
 
+// Programmatic dependent launch of the solve path's kernels: a kernel launched through launch_dep
+// with the attribute set may be scheduled while the kernel before it in the stream is still
+// running, runs its prologue (reads of data that no kernel of a solve writes), then waits in
+// dep_wait() (common.cuh) for its predecessor. Only kernels that call dep_wait() before any other
+// global-memory access, and on every path, are launched this way. KIND: 0 = row kernels (plain,
+// staged, sliced), 1 = element-wise cycle kernels, 2 = FCG kernels; BCMGX_PDL is a bit mask of the
+// kinds that get the attribute, default 1 (row kernels only). Measured on one B200 (27-point 160^3,
+// FP32 cycle): row kernels only, solve 31.4 -> 30.1 ms and one stream-launched cycle 1.19 -> 1.06 ms;
+// adding the element-wise kernels made the graph solve slower (32.3 ms), adding the FCG kernels
+// slowed the SpMV + dots pair (0.130 -> 0.144 ms).
+bool dep_launch_enabled(int kind);
+#ifdef __CUDACC__
+template <int KIND = 1, typename... KA, typename... Args>
+inline void launch_dep(void (*kernel)(KA...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = dep_launch_enabled(KIND) ? 1 : 0;
+    note_launch();
+    BCMGX_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<KA>(args)...));
+}
+#endif
+
 #define BCMGX_REQUIRE(cond, code, text)                                   \
     do {                                                                  \
         if (!(cond)) throw ::bcmgx::Error((code), std::string(text));     \

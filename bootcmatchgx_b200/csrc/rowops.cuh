@@ -83,6 +83,8 @@ __global__ void __launch_bounds__(256) k_rowop(int n, const int* __restrict__ ro
     VS val, const XT* __restrict__ x, const FT* __restrict__ f, const MT* __restrict__ M,
     YT* __restrict__ y, double alpha, double beta, const int* __restrict__ skip)
 {
+    dep_wait();
+    dep_release();
     if (skip && *skip) return;
     using VT = typename ValSrc<VS>::type;
     using AT = typename Acc<VT>::type;

@@ -211,7 +211,6 @@ __global__ void __launch_bounds__(kSlWarps * 32, 3) k_rowop_sliced(int n, const 
     const IT* __restrict__ sidx, SlSrc<VS> sv, const XT* __restrict__ x, const FT* __restrict__ f,
     const MT* __restrict__ M, YT* __restrict__ y, double alpha, double beta, const int* __restrict__ skip)
 {
-    if (skip && *skip) return;
     using V = SlVal<VS>;
     using VT = typename V::VT;
     using AT = typename Acc<VT>::type;
@@ -264,6 +263,14 @@ __global__ void __launch_bounds__(kSlWarps * 32, 3) k_rowop_sliced(int n, const 
     ptrs(gw + 2 * nw, b2, e2);
     issue(0, b0, e0);
     issue(1, b1, e1);
+    // the prologue above reads only the sliced copy and its table, which no kernel of a solve
+    // writes (build_sliced returns after they are complete); vectors are read after the wait
+    dep_wait();
+    dep_release();
+    if (skip && *skip) {
+        cp_async_wait<0>();   // no copy into this block's shared memory outlives the block
+        return;
+    }
     int st = 0;
     for (long sl = gw; sl < nsl; sl += nw) {
         // the stage that the slice two ahead goes to was read by this warp one slice ago

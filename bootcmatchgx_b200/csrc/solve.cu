@@ -100,6 +100,15 @@ int blocks_per_sm(const void* kernel, int threads, size_t smem)
     return b;
 }
 
+bool dep_launch_enabled(int kind)
+{
+    static const int mask = [] {
+        const char* e = std::getenv("BCMGX_PDL");
+        return e && *e ? std::atoi(e) : 1;
+    }();
+    return (mask >> kind) & 1;
+}
+
 int fit_grid(const void* kernel, int threads, long need_blocks)
 {
     const int b = blocks_per_sm(kernel, threads, 0);
@@ -114,8 +123,7 @@ static void launch_rowop(int tpr, int n, const int* row, const IT* col, VS val, 
     if (n <= 0) return;
     const long need = ((long)n * tpr + 255) / 256;
     auto go = [&](auto kern) {
-        note_launch();
-        kern<<<fit_grid(kern, 256, need), 256, 0, s>>>(n, row, col, val, x, f, M, y, alpha, beta, skip);
+        launch_dep<0>(kern, fit_grid(kern, 256, need), 256, 0, s, n, row, col, val, x, f, M, y, alpha, beta, skip);
     };
     switch (tpr) {
     case 1: go(k_rowop<1, OP, VS, XT, FT, MT, YT, IT>); break;
@@ -211,8 +219,7 @@ static void launch_staged(int n, int64_t nnz, const int* row, const IT* col, VS 
     const long ntiles = ((long)n + R - 1) / R;
     const int grid = (int)std::min<long>(ntiles, (long)per_sm * num_sms());
     const unsigned long long test_ns = stage_test_wait_ns();
-    note_launch();
-    kern<<<grid, kStageThreads, C::SMEM, s>>>(n, R, row, col, val, x, f, M, y, alpha, beta, skip, g_stage_fault,
+    launch_dep<0>(kern, grid, kStageThreads, C::SMEM, s, n, R, row, col, val, x, f, M, y, alpha, beta, skip, g_stage_fault,
         test_ns ? test_ns : kStageWaitNs, test_ns ? 1 : 0);
     BCMGX_CHECK_LAUNCH();
 }
@@ -265,6 +272,9 @@ void build_sliced(DevCsr& A, cudaStream_t s)
         A.sl_col.alloc(std::max<long long>(total, 1), s);
         fill(k_sl_fill<int>, (const int*)A.col.p, A.sl_col.p);
     }
+    // the sliced kernels read the copy in their prologue, before their dependency wait (launch_dep),
+    // so it is complete before the first of them is launched
+    BCMGX_CUDA(cudaStreamSynchronize(s));
 }
 
 template <int OP, typename VS, typename XT, typename FT, typename MT, typename YT>
@@ -279,8 +289,7 @@ static void launch_sliced(const DevCsr& A, SlSrc<VS> sv, const XT* x, const FT* 
             ensure_smem_limit((const void*)kern, C::SMEM);
             const int per_sm = blocks_per_sm((const void*)kern, kSlWarps * 32, C::SMEM);
             const int grid = (int)std::max<long>(1, std::min<long>(ceil_div(nsl, kSlWarps), (long)per_sm * num_sms()));
-            note_launch();
-            kern<<<grid, kSlWarps * 32, C::SMEM, s>>>(A.n, A.sl_ptr.p, idx, sv, x, f, M, y, alpha, beta, skip);
+            launch_dep<0>(kern, grid, kSlWarps * 32, C::SMEM, s, A.n, A.sl_ptr.p, idx, sv, x, f, M, y, alpha, beta, skip);
         };
         if (A.max_row > 0 && A.max_row <= C::NBMAX * kSliceG) run(k_rowop_sliced<OP, VS, XT, FT, MT, YT, IT, true>);
         else run(k_rowop_sliced<OP, VS, XT, FT, MT, YT, IT, false>);
@@ -394,6 +403,8 @@ template <typename FT, typename MT, typename YT, typename CT>
 __global__ void k_first_sweep(int n, const FT* __restrict__ f, const MT* __restrict__ M, YT* __restrict__ u,
     CT* __restrict__ fcopy, const int* __restrict__ skip)
 {
+    dep_wait();
+    dep_release();
     if (skip && *skip) return;
     using AT = typename Wider<MT>::type;
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
@@ -417,6 +428,8 @@ __global__ void __launch_bounds__(kChainThreads) k_chain_block(int n, const int*
     const T* __restrict__ val, const T* __restrict__ f, const T* __restrict__ M, const T* src, T* dst, T* q0, T* q1, int k,
     const int* __restrict__ skip)
 {
+    dep_wait();
+    dep_release();
     if (skip && *skip) return;
     using AT = typename Acc<T>::type;
     using WT = typename Wider<T>::type;
@@ -445,6 +458,8 @@ __global__ void __launch_bounds__(kChainThreads) k_chain_block(int n, const int*
 template <typename T>
 __global__ void k_zero(int n, T* __restrict__ a, const int* __restrict__ skip)
 {
+    dep_wait();
+    dep_release();
     if (skip && *skip) return;
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) a[i] = T(0);
 }
@@ -452,6 +467,8 @@ __global__ void k_zero(int n, T* __restrict__ a, const int* __restrict__ skip)
 template <typename ST, typename DT>
 __global__ void k_convert(int n, const ST* __restrict__ a, DT* __restrict__ b, const int* __restrict__ skip)
 {
+    dep_wait();
+    dep_release();
     if (skip && *skip) return;
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) b[i] = (DT)a[i];
 }
@@ -461,6 +478,8 @@ template <typename RT, typename WT, typename OT>
 __global__ void k_restrict(int nc, const int* __restrict__ rptr, const int* __restrict__ ridx,
     const WT* __restrict__ rval, const RT* __restrict__ res, OT* __restrict__ out, const int* __restrict__ skip)
 {
+    dep_wait();
+    dep_release();
     if (skip && *skip) return;
     using AT = typename Wider<OT>::type;
     for (long c = (long)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (long)gridDim.x * blockDim.x) {
@@ -475,6 +494,8 @@ template <typename PT, typename CT, typename XT, typename YT>
 __global__ void k_prolong(int n, const int* __restrict__ agg, const PT* __restrict__ p, const CT* __restrict__ xc,
     const XT* x, YT* y, const int* __restrict__ skip)
 {
+    dep_wait();
+    dep_release();
     if (skip && *skip) return;
     using AT = typename Wider<YT>::type;
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
@@ -666,13 +687,13 @@ struct Cycle {
             rec->push_back(p);
             return;
         }
-        note_launch();
         if (lk >= 0) {
             auto k = k_blk_first_sweep<FT, MT, YT, CT>;
+            note_launch();
             k<<<grid(k, n), 256, 0, s>>>(n, lk, f, M, u, fcopy, skip);
         } else {
             auto k = k_first_sweep<FT, MT, YT, CT>;
-            k<<<grid(k, n), 256, 0, s>>>(n, f, M, u, fcopy, skip);
+            launch_dep(k, grid(k, n), 256, 0, s, n, f, M, u, fcopy, skip);
         }
         BCMGX_CHECK_LAUNCH();
     }
@@ -690,13 +711,13 @@ struct Cycle {
             rec->push_back(p);
             return;
         }
-        note_launch();
         if (lk >= 0) {
             auto k = k_blk_convert<ST, DT>;
+            note_launch();
             k<<<grid(k, n), 256, 0, s>>>(n, lk, a, b, skip);
         } else {
             auto k = k_convert<ST, DT>;
-            k<<<grid(k, n), 256, 0, s>>>(n, a, b, skip);
+            launch_dep(k, grid(k, n), 256, 0, s, n, a, b, skip);
         }
         BCMGX_CHECK_LAUNCH();
     }
@@ -712,13 +733,13 @@ struct Cycle {
             rec->push_back(p);
             return;
         }
-        note_launch();
         if (lk >= 0) {
             auto k = k_blk_zero<T>;
+            note_launch();
             k<<<grid(k, n), 256, 0, s>>>(n, lk, a, skip);
         } else {
             auto k = k_zero<T>;
-            k<<<grid(k, n), 256, 0, s>>>(n, a, skip);
+            launch_dep(k, grid(k, n), 256, 0, s, n, a, skip);
         }
         BCMGX_CHECK_LAUNCH();
     }
@@ -747,8 +768,7 @@ struct Cycle {
             return;
         }
         auto k = k_restrict<RT, WT, OT>;
-        note_launch();
-        k<<<grid(k, nc), 256, 0, s>>>(nc, V.rptr.p, V.ridx.p, rval, res, out, skip);
+        launch_dep(k, grid(k, nc), 256, 0, s, nc, V.rptr.p, V.ridx.p, rval, res, out, skip);
         BCMGX_CHECK_LAUNCH();
     }
     template <typename PT, typename CT, typename XT, typename YT>
@@ -770,13 +790,13 @@ struct Cycle {
             rec->push_back(q);
             return;
         }
-        note_launch();
         if (lk >= 0) {
             auto k = k_blk_prolong<PT, CT, XT, YT>;
+            note_launch();
             k<<<grid(k, n), 256, 0, s>>>(n, lk, V.agg.p, p, xc, x, y, skip);
         } else {
             auto k = k_prolong<PT, CT, XT, YT>;
-            k<<<grid(k, n), 256, 0, s>>>(n, V.agg.p, p, xc, x, y, skip);
+            launch_dep(k, grid(k, n), 256, 0, s, n, V.agg.p, p, xc, x, y, skip);
         }
         BCMGX_CHECK_LAUNCH();
     }
@@ -1011,8 +1031,7 @@ static void l1jacobi_apply(bcmgx_hierarchy* H, const double* r, double* v, const
     out[k - 1] = v;
     for (int i = k - 2; i >= 0; i--) out[i] = (out[i + 1] == v) ? H->l1tmp.p : v;
     auto first = k_first_sweep<double, double, double, double>;
-    note_launch();
-    first<<<ew_grid(first, n), 256, 0, s>>>(n, r, H->l1d.p, out[0], (double*)nullptr, skip);
+    launch_dep(first, ew_grid(first, n), 256, 0, s, n, r, H->l1d.p, out[0], (double*)nullptr, skip);
     BCMGX_CHECK_LAUNCH();
     for (int i = 1; i < k; i++)
         launch_rowop_A<OP_JACOBI>(A.tpr, A, A.val.p, (const double*)out[i - 1], r, (const double*)H->l1d.p,
@@ -1176,6 +1195,8 @@ __global__ void __launch_bounds__(kRedThreads) k_fcg_resid0(int n, const int* __
     const double* __restrict__ val, const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ r,
     FcgState* st, double* partials)
 {
+    dep_wait();
+    dep_release();
     const int lane = threadIdx.x & (S - 1);
     const int sub = (threadIdx.x & 31) / S;
     const long stride = (long)gridDim.x * blockDim.x / S;
@@ -1213,6 +1234,8 @@ __global__ void __launch_bounds__(kRedThreads, 4) k_fcg_dots(int n, const double
     const double* __restrict__ pw, const double* __restrict__ r, const double* __restrict__ oq, FcgState* st,
     double* partials, const int* __restrict__ skip)
 {
+    dep_wait();
+    dep_release();
     if (skip && *skip) return;
     double acc[3] = { 0.0, 0.0, 0.0 };
     auto one = [&](long i) {
@@ -1267,6 +1290,8 @@ __global__ void __launch_bounds__(kRedThreads) k_fcg_update0(int n, const double
     double* __restrict__ x, double* __restrict__ r, double* __restrict__ d, double* __restrict__ q, FcgState* st, double* partials,
     double* hist)
 {
+    dep_wait();
+    dep_release();
     if (st->bad) return;
     const double th = st->theta;
     double acc[1] = { 0.0 };
@@ -1296,6 +1321,8 @@ __global__ void __launch_bounds__(kRedThreads, 4) k_fcg_update(int n, double* __
     double* __restrict__ x, double* __restrict__ pw, const double* __restrict__ oq, double* __restrict__ r, FcgState* st,
     double* partials, double* hist, const int* __restrict__ skip)
 {
+    dep_wait();
+    dep_release();
     if (skip && *skip) return;
     // a breakdown found by the dots kernel leaves x at the last valid iterate
     if (st->bad) {
@@ -1359,13 +1386,12 @@ __global__ void __launch_bounds__(kRedThreads, 4) k_fcg_update(int n, double* __
 static void fcg_update(int n, double* pv, const double* od, double* x, double* pw, const double* oq, double* r,
     FcgState* st, double* part, double* hist, const int* skip, cudaStream_t s)
 {
-    note_launch();
     if (al16(pv) && al16(od) && al16(x) && al16(pw) && al16(oq) && al16(r)) {
         auto k = k_fcg_update<true>;
-        k<<<red_grid(k, ((long)n + 1) / 2), kRedThreads, 0, s>>>(n, pv, od, x, pw, oq, r, st, part, hist, skip);
+        launch_dep<2>(k, red_grid(k, ((long)n + 1) / 2), kRedThreads, 0, s, n, pv, od, x, pw, oq, r, st, part, hist, skip);
     } else {
         auto k = k_fcg_update<false>;
-        k<<<red_grid(k, n), kRedThreads, 0, s>>>(n, pv, od, x, pw, oq, r, st, part, hist, skip);
+        launch_dep<2>(k, red_grid(k, n), kRedThreads, 0, s, n, pv, od, x, pw, oq, r, st, part, hist, skip);
     }
     BCMGX_CHECK_LAUNCH();
 }
@@ -1373,13 +1399,12 @@ static void fcg_update(int n, double* pv, const double* od, double* x, double* p
 template <int S>
 static void launch_resid0(const DevCsr& A, const double* x, const double* b, double* r, FcgState* st, double* part, cudaStream_t s)
 {
-    note_launch();
     if (A.dcol.p) {
         auto k = k_fcg_resid0<S, short>;
-        k<<<red_grid(k, (long)A.n * S), kRedThreads, 0, s>>>(A.n, A.row.p, A.dcol.p, A.val.p, x, b, r, st, part);
+        launch_dep<2>(k, red_grid(k, (long)A.n * S), kRedThreads, 0, s, A.n, A.row.p, A.dcol.p, A.val.p, x, b, r, st, part);
     } else {
         auto k = k_fcg_resid0<S, int>;
-        k<<<red_grid(k, (long)A.n * S), kRedThreads, 0, s>>>(A.n, A.row.p, A.col.p, A.val.p, x, b, r, st, part);
+        launch_dep<2>(k, red_grid(k, (long)A.n * S), kRedThreads, 0, s, A.n, A.row.p, A.col.p, A.val.p, x, b, r, st, part);
     }
 }
 // ||r||^2 -> delta0 and the tolerance, as k_fcg_resid0 finishes, for an r formed by the level's
@@ -1387,6 +1412,8 @@ static void launch_resid0(const DevCsr& A, const double* x, const double* b, dou
 __global__ void __launch_bounds__(kRedThreads) k_fcg_norm0(int n, const double* __restrict__ r, FcgState* st,
     double* partials)
 {
+    dep_wait();
+    dep_release();
     double acc[1] = { 0.0 };
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
         acc[0] += r[i] * r[i];
@@ -1406,9 +1433,8 @@ static void fcg_resid0(const DevCsr& A, const double* x, const double* b, double
         // the sliced kernel forms r = b - A x with the one-thread-per-row kernel's row sums; the
         // norm follows in a kernel of its own
         rowop_resid(A, x, b, r, nullptr, s);
-        note_launch();
         auto k = k_fcg_norm0;
-        k<<<red_grid(k, A.n), kRedThreads, 0, s>>>(A.n, r, st, part);
+        launch_dep<2>(k, red_grid(k, A.n), kRedThreads, 0, s, A.n, r, st, part);
         BCMGX_CHECK_LAUNCH();
         return;
     }
@@ -1431,13 +1457,12 @@ static void fcg_dots(const DevCsr& A, const double* pv, double* pw, const double
 {
     launch_rowop_A<OP_AXPBY>(A.tpr, A, A.val.p, pv, (const double*)nullptr, (const double*)nullptr, pw, 1.0, 0.0, skip, s);
     const int n = A.n;
-    note_launch();
     if (al16(pv) && al16(pw) && al16(r) && (MODE == 0 || al16(oq))) {
         auto k = k_fcg_dots<MODE, true>;
-        k<<<red_grid(k, ((long)n + 1) / 2), kRedThreads, 0, s>>>(n, pv, pw, r, oq, st, part, skip);
+        launch_dep<2>(k, red_grid(k, ((long)n + 1) / 2), kRedThreads, 0, s, n, pv, pw, r, oq, st, part, skip);
     } else {
         auto k = k_fcg_dots<MODE, false>;
-        k<<<red_grid(k, n), kRedThreads, 0, s>>>(n, pv, pw, r, oq, st, part, skip);
+        launch_dep<2>(k, red_grid(k, n), kRedThreads, 0, s, n, pv, pw, r, oq, st, part, skip);
     }
     BCMGX_CHECK_LAUNCH();
 }
@@ -1825,6 +1850,8 @@ void grad_pattern(const DevCsr& A, const double* lam, const double* x, double* d
 // Initial FCG state (replaces a host copy so the start-up can be captured in a graph).
 __global__ void k_fcg_init(FcgState* st, double rtol, int itnlim)
 {
+    dep_wait();
+    dep_release();
     FcgState z {};
     z.tol = rtol;
     z.itnlim = itnlim;
@@ -1833,6 +1860,8 @@ __global__ void k_fcg_init(FcgState* st, double rtol, int itnlim)
 
 __global__ void k_set_while(cudaGraphConditionalHandle h, const FcgState* st)
 {
+    dep_wait();
+    dep_release();
     cudaGraphSetConditional(h, st->done ? 0u : 1u);
 }
 
@@ -1847,13 +1876,11 @@ static void fcg_startup(bcmgx_hierarchy* H, const double* b, double* x, double* 
     double* part = H->partials.p;
     double *r = H->r.p, *v = H->v.p, *w = H->w.p, *d = H->d.p, *q = H->q.p;
     persist_reset(H, s);
-    note_launch();
-    k_fcg_init<<<1, 1, 0, s>>>(st, H->prm.rtol, H->prm.itnlim);
+    launch_dep<2>(k_fcg_init, 1, 1, 0, s, st, H->prm.rtol, H->prm.itnlim);
     fcg_resid0(A, x, b, r, st, part, s);
     prec_apply_impl(H, r, v, nullptr);
     fcg_dots<0>(A, v, w, r, nullptr, st, part, nullptr, s);
-    note_launch();
-    k_fcg_update0<<<red_grid(k_fcg_update0, n), kRedThreads, 0, s>>>(n, v, w, x, r, d, q, st, part, hist);
+    launch_dep<2>(k_fcg_update0, red_grid(k_fcg_update0, n), kRedThreads, 0, s, n, v, w, x, r, d, q, st, part, hist);
     BCMGX_CHECK_LAUNCH();
 }
 
@@ -1914,8 +1941,7 @@ static void add_solve_to_graph(bcmgx_hierarchy* H, cudaGraph_t g)
     BCMGX_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     fcg_iteration(H, true, H->gx.p, H->hist.p, &H->st.p->done);
     fcg_iteration(H, false, H->gx.p, H->hist.p, &H->st.p->done);
-    note_launch();
-    k_set_while<<<1, 1, 0, s>>>(h, H->st.p);
+    launch_dep<2>(k_set_while, 1, 1, 0, s, h, (const FcgState*)H->st.p);
     BCMGX_CHECK_LAUNCH();
     BCMGX_CUDA(cudaStreamEndCapture(s, &body));
     const long long c2 = launch_count();

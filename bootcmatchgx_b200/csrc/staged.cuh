@@ -173,6 +173,8 @@ __global__ void __launch_bounds__(kStageThreads) k_rowop_staged(int n, int R, co
     const MT* __restrict__ M, YT* __restrict__ y, double alpha, double beta, const int* __restrict__ skip,
     int* __restrict__ fault, unsigned long long wait_ns, int drop_first)
 {
+    dep_wait();
+    dep_release();
     if (skip && *skip) return;
     using C = StageCfg<VS, IT>;
     using VT = typename C::VT;

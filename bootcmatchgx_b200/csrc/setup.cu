@@ -266,20 +266,32 @@ __global__ void k_validate_offsets(int n, int m, long long nnz, const int* __res
             } else {
                 bool diag = false;
                 int carry = 0;
-                for (int j0 = b; j0 < e; j0 += S) {
-                    const int j = j0 + lane;
-                    const int c = j < e ? __ldcs(col + j) : 0x7fffffff;
-                    int prev = __shfl_up_sync(mask, c, 1, S);
-                    if (lane == 0) prev = carry;
-                    if (j < e) {
-                        if (c < 0 || c >= m) bad |= ERR_COLRANGE;
-                        if (j > b && prev >= c) bad |= ERR_COLSORT;
-                        if (c == (int)r) diag = true;
-                        const int off = c - (int)r;
-                        mo = max(mo, off < 0 ? -off : off);
-                        if (dcol) dcol[j] = (short)max(-32768, min(32767, off));
+                constexpr int U = 4;   // chunks of S entries whose columns are requested together
+                for (int j00 = b; j00 < e; j00 += U * S) {
+                    int cv[U];
+#pragma unroll
+                    for (int u = 0; u < U; u++) {
+                        const int j = j00 + u * S + lane;
+                        cv[u] = j < e ? __ldcs(col + j) : 0x7fffffff;
                     }
-                    carry = __shfl_sync(mask, c, S - 1, S);
+#pragma unroll
+                    for (int u = 0; u < U; u++) {
+                        const int j0 = j00 + u * S;
+                        if (j0 >= e) break;   // uniform across the row's lanes
+                        const int j = j0 + lane;
+                        const int c = cv[u];
+                        int prev = __shfl_up_sync(mask, c, 1, S);
+                        if (lane == 0) prev = carry;
+                        if (j < e) {
+                            if (c < 0 || c >= m) bad |= ERR_COLRANGE;
+                            if (j > b && prev >= c) bad |= ERR_COLSORT;
+                            if (c == (int)r) diag = true;
+                            const int off = c - (int)r;
+                            mo = max(mo, off < 0 ? -off : off);
+                            if (dcol) dcol[j] = (short)max(-32768, min(32767, off));
+                        }
+                        carry = __shfl_sync(mask, c, S - 1, S);
+                    }
                 }
                 diag = (__ballot_sync(mask, diag) & mask) != 0;
                 if (need_diag && !diag) bad |= ERR_NODIAG;
@@ -401,27 +413,116 @@ static int setup_subwarp(long n, int64_t nnz)
     return avg <= 12 ? 4 : avg <= 40 ? 8 : avg <= 96 ? 16 : 32;
 }
 
-// Position of the transposed entry: tpos[j] for a_rc is the index of a_cr in row c (-1 if the
-// pattern has no a_cr); the diagonal maps to itself. The binary searches of a lane's batch run
-// in lock step, one round of independent loads per halving.
-template <int S>
-__global__ void k_tpos(int n, const int* __restrict__ row, const int* __restrict__ col, int* __restrict__ tpos)
+// launch of a matching kernel K<S> for the lanes-per-row choice S of setup_subwarp
+#define BCMGX_SUBWARP_LAUNCH(K, S, n, s, ...)                                                      \
+    do {                                                                                           \
+        note_launch();                                                                             \
+        switch (S) {                                                                               \
+        case 4: K<4><<<gs_grid((long)(n) * 4), 256, 0, s>>>(__VA_ARGS__); break;                   \
+        case 8: K<8><<<gs_grid((long)(n) * 8), 256, 0, s>>>(__VA_ARGS__); break;                   \
+        case 16: K<16><<<gs_grid((long)(n) * 16), 256, 0, s>>>(__VA_ARGS__); break;                \
+        default: K<32><<<gs_grid((long)(n) * 32), 256, 0, s>>>(__VA_ARGS__); break;                \
+        }                                                                                          \
+    } while (0)
+// the same for a kernel K<S, X> with a second template argument X
+#define BCMGX_SUBWARP_LAUNCH2(K, X, S, n, s, ...)                                                  \
+    do {                                                                                           \
+        note_launch();                                                                             \
+        switch (S) {                                                                               \
+        case 4: K<4, X><<<gs_grid((long)(n) * 4), 256, 0, s>>>(__VA_ARGS__); break;                \
+        case 8: K<8, X><<<gs_grid((long)(n) * 8), 256, 0, s>>>(__VA_ARGS__); break;                \
+        case 16: K<16, X><<<gs_grid((long)(n) * 16), 256, 0, s>>>(__VA_ARGS__); break;             \
+        default: K<32, X><<<gs_grid((long)(n) * 32), 256, 0, s>>>(__VA_ARGS__); break;             \
+        }                                                                                          \
+    } while (0)
+
+// a_hat = 1 - (2 a w_r w_c) / (C_r + C_c), or DBL_EPSILON if C_r + C_c <= DBL_EPSILON
+// (_makeAH_warp, matching.cu:66-111). Symmetric in (r, c) apart from a.
+__device__ __forceinline__ double ahat(double a, double Cr, double Cc, double wr, double wc)
 {
+    const double norm = __dadd_rn(Cr, Cc);
+    if (norm > DBL_EPSILON) {
+        const double wt = __dmul_rn(wr, wc);
+        return __dsub_rn(1.0, __ddiv_rn(__dmul_rn(__dmul_rn(2.0, a), wt), norm));
+    }
+    return DBL_EPSILON;
+}
+
+// Position of the transposed entry: tpos[j] for a_rc is the index of a_cr in row c (-1 if the
+// pattern has no a_cr); the diagonal maps to itself. The first probe is the mirror position:
+// entry k of row r (of d_r entries) is looked for at entry d_c - 1 - k of row c, where a
+// symmetric stencil puts it when both rows are full; a miss narrows the range and the binary
+// search goes on from there. The searches of a lane's batch run in lock step, one round of
+// independent loads per halving. MODE 0: the positions; 1: also the minimum over the off-diagonal
+// |a_hat| (find_Max_Min with AbsMin, matching.cu:188-217) into *min_bits (the bit pattern of a
+// non-negative double orders like its value, so atomicMin on it is exact), its loads going out
+// with the search's first round; 2: the minimum alone.
+template <int S, int MODE>
+__global__ void __launch_bounds__(256, 4) k_tpos(int n, const int* __restrict__ row, const int* __restrict__ col, int* __restrict__ tpos,
+    const double* __restrict__ val, const double* __restrict__ w, const double* __restrict__ C,
+    unsigned long long* min_bits)
+{
+    constexpr bool TP = MODE != 2, MIN = MODE != 0;
     constexpr int U = kSetupBatch;
     const int lane = threadIdx.x & (S - 1);
+    double mn = DBL_MAX;
     BCMGX_SUBWARP_ROWS(r, n, S)
     {
         const int b = __ldg(row + r), e = __ldg(row + r + 1);
+        double Cr = 0.0, wr = 0.0;
+        if (MIN) {
+            Cr = __ldg(C + r);
+            wr = __ldg(w + r);
+        }
         for (int j0 = b + lane; j0 < e; j0 += U * S) {
-            int c[U], lo[U], hi[U], end[U];
+            int c[U], lo[U], hi[U], end[U], fnd[U];
+            double a[U], Cc[U], wc[U];
 #pragma unroll
-            for (int u = 0; u < U; u++) c[u] = j0 + u * S < e ? __ldg(col + j0 + u * S) : -1;
+            for (int u = 0; u < U; u++) {
+                c[u] = j0 + u * S < e ? __ldg(col + j0 + u * S) : -1;
+                if (MIN) a[u] = j0 + u * S < e ? __ldg(val + j0 + u * S) : 0.0;
+            }
 #pragma unroll
             for (int u = 0; u < U; u++) {
                 const bool srch = c[u] >= 0 && c[u] != (int)r;
-                lo[u] = srch ? __ldg(row + c[u]) : 0;
-                end[u] = srch ? __ldg(row + c[u] + 1) : 0;
+                lo[u] = TP && srch ? __ldg(row + c[u]) : 0;
+                end[u] = TP && srch ? __ldg(row + c[u] + 1) : 0;
+                if (MIN) {
+                    Cc[u] = srch ? __ldg(C + c[u]) : 0.0;
+                    wc[u] = srch ? __ldg(w + c[u]) : 0.0;
+                }
                 hi[u] = end[u];
+                fnd[u] = -1;
+            }
+            if (MIN) {
+#pragma unroll
+                for (int u = 0; u < U; u++)
+                    if (c[u] >= 0 && c[u] != (int)r) mn = fmin(mn, fabs(ahat(a[u], Cr, Cc[u], wr, wc[u])));
+            }
+            if (!TP) continue;
+            {
+                int g[U], cm[U];
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    g[u] = -1;
+                    if (lo[u] < hi[u]) {
+                        const int k = j0 + u * S - b;
+                        g[u] = min(max(hi[u] - 1 - k, lo[u]), hi[u] - 1);
+                        cm[u] = __ldg(col + g[u]);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; u++)
+                    if (g[u] >= 0) {
+                        if (cm[u] == (int)r) {
+                            fnd[u] = g[u];
+                            hi[u] = lo[u];
+                        } else if (cm[u] < (int)r) {
+                            lo[u] = g[u] + 1;
+                        } else {
+                            hi[u] = g[u];
+                        }
+                    }
             }
             for (int step = 0; step < 32; step++) {
                 int cm[U];
@@ -443,67 +544,41 @@ __global__ void k_tpos(int n, const int* __restrict__ row, const int* __restrict
             }
             int hit[U];
 #pragma unroll
-            for (int u = 0; u < U; u++) hit[u] = c[u] >= 0 && c[u] != (int)r && lo[u] < end[u] ? __ldg(col + lo[u]) : -1;
+            for (int u = 0; u < U; u++)
+                hit[u] = fnd[u] >= 0 ? (int)r : (c[u] >= 0 && c[u] != (int)r && lo[u] < end[u] ? __ldg(col + lo[u]) : -1);
 #pragma unroll
             for (int u = 0; u < U; u++) {
                 const int j = j0 + u * S;
                 if (c[u] < 0) continue;
-                tpos[j] = c[u] == (int)r ? j : (hit[u] == (int)r ? lo[u] : -1);
+                tpos[j] = c[u] == (int)r ? j : (fnd[u] >= 0 ? fnd[u] : (hit[u] == (int)r ? lo[u] : -1));
             }
         }
     }
-}
-
-// a_hat = 1 - (2 a w_r w_c) / (C_r + C_c), or DBL_EPSILON if C_r + C_c <= DBL_EPSILON
-// (_makeAH_warp, matching.cu:66-111). Symmetric in (r, c) apart from a.
-__device__ __forceinline__ double ahat(double a, double Cr, double Cc, double wr, double wc)
-{
-    const double norm = __dadd_rn(Cr, Cc);
-    if (norm > DBL_EPSILON) {
-        const double wt = __dmul_rn(wr, wc);
-        return __dsub_rn(1.0, __ddiv_rn(__dmul_rn(__dmul_rn(2.0, a), wt), norm));
-    }
-    return DBL_EPSILON;
-}
-
-// min over all off-diagonal |a_hat| (find_Max_Min with AbsMin, matching.cu:188-217). The bit
-// pattern of a non-negative double orders like its value, so atomicMin on it is exact.
-template <int S>
-__global__ void k_ahat_min(int n, const int* __restrict__ row, const int* __restrict__ col, const double* __restrict__ val,
-    const double* __restrict__ w, const double* __restrict__ C, unsigned long long* min_bits)
-{
-    constexpr int U = kSetupBatch;
-    const int lane = threadIdx.x & (S - 1);
-    double mn = DBL_MAX;
-    BCMGX_SUBWARP_ROWS(r, n, S)
-    {
-        const int b = __ldg(row + r), e = __ldg(row + r + 1);
-        const double Cr = __ldg(C + r), wr = __ldg(w + r);
-        for (int j0 = b + lane; j0 < e; j0 += U * S) {
-            int c[U];
-            double a[U], Cc[U], wc[U];
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                const bool in = j0 + u * S < e;
-                c[u] = in ? __ldg(col + j0 + u * S) : (int)r;
-                a[u] = in ? __ldg(val + j0 + u * S) : 0.0;
-            }
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                Cc[u] = c[u] != (int)r ? __ldg(C + c[u]) : 0.0;
-                wc[u] = c[u] != (int)r ? __ldg(w + c[u]) : 0.0;
-            }
-#pragma unroll
-            for (int u = 0; u < U; u++)
-                if (c[u] != (int)r) mn = fmin(mn, fabs(ahat(a[u], Cr, Cc[u], wr, wc[u])));
+    if (MIN) {
+        unsigned long long bits = (unsigned long long)__double_as_longlong(mn);
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long other = __shfl_xor_sync(0xffffffffu, bits, o);
+            bits = other < bits ? other : bits;
         }
+        if ((threadIdx.x & 31) == 0) atomicMin(min_bits, bits);
     }
-    unsigned long long bits = (unsigned long long)__double_as_longlong(mn);
-    for (int o = 16; o > 0; o >>= 1) {
-        unsigned long long other = __shfl_xor_sync(0xffffffffu, bits, o);
-        bits = other < bits ? other : bits;
+}
+
+// The transposed positions and the |a_hat| minimum: one fused pass (k_tpos<S, 1>) or two
+// (BCMGX_TPOS_FUSE=0).
+static void tpos_min_launch(int S, int n, const int* row, const int* col, int* tpos, const double* val, const double* w,
+    const double* C, unsigned long long* min_bits, cudaStream_t s)
+{
+    static const bool fuse = [] {
+        const char* e = std::getenv("BCMGX_TPOS_FUSE");
+        return !(e && e[0] == '0');
+    }();
+    if (fuse) {
+        BCMGX_SUBWARP_LAUNCH2(k_tpos, 1, S, n, s, n, row, col, tpos, val, w, C, min_bits);
+    } else {
+        BCMGX_SUBWARP_LAUNCH2(k_tpos, 0, S, n, s, n, row, col, tpos, val, w, C, min_bits);
+        BCMGX_SUBWARP_LAUNCH2(k_tpos, 2, S, n, s, n, row, col, tpos, val, w, C, min_bits);
     }
-    if ((threadIdx.x & 31) == 0) atomicMin(min_bits, bits);
 }
 
 // W = log(|a_hat|), or log(SUITOR_EPS / (0.999 min)) where a_hat == 0 (_make_w,
@@ -603,7 +678,9 @@ __device__ __forceinline__ void rank_row32(long r, int b, int e, int ct, double 
 
 // k_rank for a matrix whose rows all have at most 32 entries, with every entry's weight formed
 // in registers by k_logw's expression (same operations, same rounding) instead of read from W:
-// the weights are never stored.
+// the weights are never stored. A warp's rows are pipelined two deep: while it ranks row r, the
+// columns and transposed positions of its next row and the bounds of the row after are in
+// flight, so a row costs one memory round trip instead of three dependent ones.
 __global__ void __launch_bounds__(256, 8) k_rank_w(int n, const int* __restrict__ row, const int* __restrict__ col, const double* __restrict__ val,
     const double* __restrict__ w, const double* __restrict__ C, const int* __restrict__ tpos, double zero_sub,
     int* __restrict__ rank, int* __restrict__ ordj, int* __restrict__ degE, const double* __restrict__ zero_sub_dev)
@@ -612,18 +689,47 @@ __global__ void __launch_bounds__(256, 8) k_rank_w(int n, const int* __restrict_
     const int lane = threadIdx.x & 31;
     __shared__ RankKey keys[8][32];   // 256-thread blocks
     RankKey* wkeys = keys[(threadIdx.x >> 5) & 7];
-    for (long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32; r < n; r += (long)gridDim.x * blockDim.x / 32) {
-        const int b = __ldg(row + r), e = __ldg(row + r + 1);
+    const long step = (long)gridDim.x * blockDim.x / 32;
+    long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32;   // uniform across the warp
+    if (r >= n) return;
+    int b = __ldg(row + r), e = __ldg(row + r + 1);
+    int ct = b + lane < e ? __ldg(col + b + lane) : -1;
+    int tp = b + lane < e ? __ldg(tpos + b + lane) : -1;
+    long r1 = r + step;
+    int b1 = 0, e1 = 0;
+    if (r1 < n) {
+        b1 = __ldg(row + r1);
+        e1 = __ldg(row + r1 + 1);
+    }
+    while (true) {
+        const long r2 = r1 + step;
+        int b2 = 0, e2 = 0;
+        if (r2 < n) {
+            b2 = __ldg(row + r2);
+            e2 = __ldg(row + r2 + 1);
+        }
+        int ct1 = -1, tp1 = -1;
+        if (b1 + lane < e1) {
+            ct1 = __ldg(col + b1 + lane);
+            tp1 = __ldg(tpos + b1 + lane);
+        }
         const int t = b + lane;
-        const int ct = t < e ? __ldg(col + t) : -1;
         double wt = 0.0;
         if (ct >= 0 && ct != (int)r) {
-            const int tp = __ldg(tpos + t);
             const int src = (ct < (int)r && tp >= 0) ? tp : t;
             const double sa = fabs(ahat(__ldg(val + src), __ldg(C + r), __ldg(C + ct), __ldg(w + r), __ldg(w + ct)));
             wt = log(sa != 0.0 ? sa : zero_sub);
         }
         rank_row32(r, b, e, ct, wt, rank, ordj, degE, wkeys);
+        if (r1 >= n) break;
+        r = r1;
+        b = b1;
+        e = e1;
+        ct = ct1;
+        tp = tp1;
+        r1 = r2;
+        b1 = b2;
+        e1 = e2;
     }
 }
 
@@ -670,11 +776,13 @@ __global__ void k_rank(int n, const int* __restrict__ row, const int* __restrict
 
 // Preference records: pref[row[v] + k] = {k-th candidate y of v, v's offer value at y}, where
 // the offer value is degE[y] - (rank of v in y's list), or 0 when y does not rank v (no
-// transposed entry: the pair is never proposed). rinfo[v] = {row[v], degE[v]}.
+// transposed entry: the pair is never proposed). rinfo[v] = {row[v], degE[v]}. With mark_last
+// (the wide suitor's form) the last record of each list also carries kPrefLast.
+constexpr int kPrefLast = 1 << 30;
 template <int S>
 __global__ void k_pref(int n, const int* __restrict__ row, const int* __restrict__ col, const int* __restrict__ ordj,
     const int* __restrict__ rank, const int* __restrict__ tpos, const int* __restrict__ degE, int2* __restrict__ pref,
-    int2* __restrict__ rinfo)
+    int2* __restrict__ rinfo, int mark_last)
 {
     constexpr int U = kSetupBatch;
     const int lane = threadIdx.x & (S - 1);
@@ -697,23 +805,16 @@ __global__ void k_pref(int n, const int* __restrict__ row, const int* __restrict
             }
 #pragma unroll
             for (int u = 0; u < U; u++)
-                if (j[u] >= 0) pref[b + k0 + u * S] = make_int2(y[u], ry[u] >= 0 ? dy[u] - ry[u] : 0);
+                if (j[u] >= 0) {
+                    const int k = k0 + u * S;
+                    const int last = (mark_last && k == dE - 1) ? kPrefLast : 0;
+                    pref[b + k] = make_int2(y[u], (ry[u] >= 0 ? dy[u] - ry[u] : 0) | last);
+                }
         }
         if (lane == 0) rinfo[r] = make_int2(b, dE);
     }
 }
 
-// launch of a matching kernel K<S> for the lanes-per-row choice S of setup_subwarp
-#define BCMGX_SUBWARP_LAUNCH(K, S, n, s, ...)                                                      \
-    do {                                                                                           \
-        note_launch();                                                                             \
-        switch (S) {                                                                               \
-        case 4: K<4><<<gs_grid((long)(n) * 4), 256, 0, s>>>(__VA_ARGS__); break;                   \
-        case 8: K<8><<<gs_grid((long)(n) * 8), 256, 0, s>>>(__VA_ARGS__); break;                   \
-        case 16: K<16><<<gs_grid((long)(n) * 16), 256, 0, s>>>(__VA_ARGS__); break;                \
-        default: K<32><<<gs_grid((long)(n) * 32), 256, 0, s>>>(__VA_ARGS__); break;                \
-        }                                                                                          \
-    } while (0)
 
 // Lock-free suitor. A vertex proposes to its candidates in preference order; y keeps the best
 // suitor by atomicMax on its offer word (set_suitor/find_Candidate, suitor.cu:51-147, with the
@@ -759,52 +860,62 @@ __global__ void k_suitor(int n, const int2* __restrict__ rinfo, const int2* __re
     }
 }
 
-// The same suitor with 64-bit offer words [offer value (16 bits) | proposer v (32) | index of y in
-// v's list (16)], for rows of fewer than 65536 entries. Offer values at y differ between
-// proposers, so atomicMax orders the words as it orders the offer values and the matching is
-// the same; but the word a proposal displaces names the old suitor d and its position at y, so
-// d resumes at once instead of after two dependent lookups, and the proposal needs no load of
-// the current offer first. Each step of a displacement chain is then three dependent memory
-// operations (row info, preference record, atomic) instead of seven.
+// The same suitor with 64-bit offer words [offer value (16 bits) | last (1) | position p (47)],
+// for rows of fewer than 65536 entries: p is the proposer's record in pref (row[v] + its list
+// index) and `last` marks the proposer's last candidate. Offer values at y differ between
+// proposers, so atomicMax orders the words as it orders the offer values and the matching is the
+// same; but the word a proposal displaces holds the old suitor's position, so the displaced
+// vertex resumes at record p + 1 with one load (no lookup of its row), and the proposal needs no
+// load of the current offer first. Each step of a displacement chain is then two dependent memory
+// operations (preference record, atomic); the record after the current one is requested before
+// the atomic, so a refused proposal costs the atomic's round trip alone.
 __global__ void k_suitor_w(int n, const int2* __restrict__ rinfo, const int2* __restrict__ pref,
     unsigned long long* offer, long long budget, int* err, int descending)
 {
+    constexpr unsigned long long kPosMask = (1ull << 47) - 1;
     for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
-        int cur = descending ? (int)(n - 1 - t) : (int)t;
-        int k = 0;
+        const int v = descending ? (int)(n - 1 - t) : (int)t;
+        const int2 vi = __ldg(rinfo + v);
+        if (vi.y <= 0) continue;
+        long long p = vi.x;
         long long steps = 0;
-        while (cur >= 0) {
-            const int2 ci = __ldg(rinfo + cur);
-            int next = -1, nextk = 0;
-            for (; k < ci.y; k++) {
-                if (++steps > budget) {
-                    atomicOr(err, ERR_SUITOR_BUDGET);
-                    return;
-                }
-                const int2 pr = __ldg(pref + ci.x + k);
-                if (pr.y == 0) continue;
-                const unsigned long long mine = ((unsigned long long)(unsigned)pr.y << 48) |
-                    ((unsigned long long)(unsigned)cur << 16) | (unsigned long long)(unsigned)k;
+        int2 nxt = __ldg(pref + p);
+        while (true) {
+            if (++steps > budget) {
+                atomicOr(err, ERR_SUITOR_BUDGET);
+                return;
+            }
+            const int2 pr = nxt;
+            const bool last = (pr.y & kPrefLast) != 0;
+            if (!last) nxt = __ldg(pref + p + 1);
+            const unsigned ov = (unsigned)pr.y & 0xffffu;
+            if (ov != 0u) {
+                const unsigned long long mine = ((unsigned long long)ov << 48) |
+                    (last ? (1ull << 47) : 0ull) | (unsigned long long)p;
                 const unsigned long long old = atomicMax(offer + pr.x, mine);
                 if (old < mine) {
-                    if (old != 0ull) {
-                        next = (int)((old >> 16) & 0xffffffffull);
-                        nextk = (int)(old & 0xffffull) + 1;
-                    }
-                    break;
+                    // accepted: the displaced suitor (if any, and if it has candidates left) walks on
+                    if (old == 0ull || ((old >> 47) & 1ull)) break;
+                    p = (long long)(old & kPosMask) + 1;
+                    nxt = __ldg(pref + p);
+                    continue;
                 }
             }
-            cur = next;
-            k = nextk;
+            if (last) break;
+            p++;
         }
     }
 }
 
-__global__ void k_suitor_result_w(int n, const unsigned long long* __restrict__ offer, int* __restrict__ M)
+// M[y] = the suitor v of y: its offer value degE[y] - (rank of v in y's list) names v's place in
+// y's own list, whose record holds v.
+__global__ void k_suitor_result_w(int n, const int2* __restrict__ rinfo, const int2* __restrict__ pref,
+    const unsigned long long* __restrict__ offer, int* __restrict__ M)
 {
     for (long y = (long)blockIdx.x * blockDim.x + threadIdx.x; y < n; y += (long)gridDim.x * blockDim.x) {
         const unsigned long long o = offer[y];
-        M[y] = o ? (int)((o >> 16) & 0xffffffffull) : -1;
+        const int2 yi = rinfo[y];
+        M[y] = o ? __ldg(pref + yi.x + yi.y - (int)(o >> 48)).x : -1;
     }
 }
 
@@ -1223,16 +1334,33 @@ __global__ void k_galerkin_counts(int nc, const int* __restrict__ fine0, const i
     }
 }
 
-// rows written from off[I] -> CSR; one warp per row
+// rows written from off[I] -> CSR; 8 lanes per row (4 rows of a warp in flight), each lane
+// moving up to 4 entries per round with all of their loads issued first
 __global__ void k_compact_rows(int nc, const int* __restrict__ off, const int* __restrict__ rowptr, const int* __restrict__ pcol,
     const double* __restrict__ pval, int* __restrict__ col, double* __restrict__ val)
 {
-    const int lane = threadIdx.x & 31;
-    for (long I = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32; I < nc; I += (long)gridDim.x * blockDim.x / 32) {
-        const int b = rowptr[I], len = rowptr[I + 1] - b;
-        for (int t = lane; t < len; t += 32) {
-            col[b + t] = pcol[(long)off[I] + t];
-            val[b + t] = pval[(long)off[I] + t];
+    constexpr int S = 8, U = 4;
+    const int lane = threadIdx.x & (S - 1);
+    for (long I = ((long)blockIdx.x * blockDim.x + threadIdx.x) / S; I < nc; I += (long)gridDim.x * blockDim.x / S) {
+        const int b = __ldg(rowptr + I), len = __ldg(rowptr + I + 1) - b;
+        const long o = __ldg(off + I);
+        for (int t0 = lane; t0 < len; t0 += U * S) {
+            int c[U];
+            double v[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int t = t0 + u * S;
+                c[u] = t < len ? __ldcs(pcol + o + t) : 0;
+                v[u] = t < len ? __ldcs(pval + o + t) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int t = t0 + u * S;
+                if (t < len) {
+                    col[b + t] = c[u];
+                    val[b + t] = v[u];
+                }
+            }
         }
     }
 }
@@ -1356,8 +1484,7 @@ static double edge_prep_dev(int n, int64_t nnz, const int* row, const int* col, 
     BCMGX_CUDA(cudaMemcpyAsync(mn.p, &dmax, sizeof(double), cudaMemcpyHostToDevice, s));
     const int S = setup_subwarp(n, nnz);
     note_launch(); k_diag_c<<<gs_grid(n), 256, 0, s>>>(n, row, col, val, w, C, err.p);
-    BCMGX_SUBWARP_LAUNCH(k_tpos, S, n, s, n, row, col, tpos);
-    BCMGX_SUBWARP_LAUNCH(k_ahat_min, S, n, s, n, row, col, val, w, C, mn.p);
+    tpos_min_launch(S, n, row, col, tpos, val, w, C, mn.p, s);
     BCMGX_CHECK_LAUNCH();
     double m = 0;
     BCMGX_CUDA(cudaMemcpyAsync(&m, mn.p, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -1395,7 +1522,8 @@ void validate_csr_dev(int n, int m, int64_t nnz, const int* row, const int* col,
 
 void tpos_dev(int n, int64_t nnz, const int* row, const int* col, int* tpos, cudaStream_t s)
 {
-    BCMGX_SUBWARP_LAUNCH(k_tpos, setup_subwarp(n, nnz), n, s, n, row, col, tpos);
+    BCMGX_SUBWARP_LAUNCH2(k_tpos, 0, setup_subwarp(n, nnz), n, s, n, row, col, tpos, nullptr, nullptr, nullptr,
+        nullptr);
     BCMGX_CHECK_LAUNCH();
 }
 
@@ -1434,7 +1562,8 @@ void suitor_dev(int n, int64_t nnz, const int* row, const int* col, const double
     }
     pref.alloc(z, s);
     rinfo.alloc(n, s);
-    BCMGX_SUBWARP_LAUNCH(k_pref, setup_subwarp(n, nnz), n, s, n, row, col, ordj.p, rank.p, tpos, degE.p, pref.p, rinfo.p);
+    BCMGX_SUBWARP_LAUNCH(k_pref, setup_subwarp(n, nnz), n, s, n, row, col, ordj.p, rank.p, tpos, degE.p, pref.p, rinfo.p,
+        wide ? 1 : 0);
     BCMGX_CHECK_LAUNCH();
     rank.release();
     ordj.release();
@@ -1451,7 +1580,7 @@ void suitor_dev(int n, int64_t nnz, const int* row, const int* col, const double
         if (*tb) budget = std::max(0LL, std::atoll(tb));
     if (wide) {
         note_launch(); k_suitor_w<<<ceil_div(n, 128), 128, 0, s>>>(n, rinfo.p, pref.p, offer_w.p, budget, errp, asc ? 0 : 1);
-        note_launch(); k_suitor_result_w<<<gs_grid(n), 256, 0, s>>>(n, offer_w.p, M);
+        note_launch(); k_suitor_result_w<<<gs_grid(n), 256, 0, s>>>(n, rinfo.p, pref.p, offer_w.p, M);
     } else {
         note_launch(); k_suitor<<<ceil_div(n, 128), 128, 0, s>>>(n, rinfo.p, pref.p, offer.p, budget, errp, asc ? 0 : 1);
         note_launch(); k_suitor_result<<<gs_grid(n), 256, 0, s>>>(n, rinfo.p, pref.p, offer.p, M);
@@ -1482,8 +1611,7 @@ static void edge_prep_async(int n, int64_t nnz, const int* row, const int* col, 
     const int S = setup_subwarp(n, nnz);
     note_launch(); k_set_u64<<<1, 1, 0, s>>>(mn, (unsigned long long)__builtin_bit_cast(long long, DBL_MAX));
     note_launch(); k_diag_c<<<gs_grid(n), 256, 0, s>>>(n, row, col, val, w, C, err);
-    BCMGX_SUBWARP_LAUNCH(k_tpos, S, n, s, n, row, col, tpos);
-    BCMGX_SUBWARP_LAUNCH(k_ahat_min, S, n, s, n, row, col, val, w, C, mn);
+    tpos_min_launch(S, n, row, col, tpos, val, w, C, mn, s);
     note_launch(); k_zero_sub<<<1, 1, 0, s>>>(mn, min_cap, zs_dev);
     BCMGX_CHECK_LAUNCH();
 }
@@ -1726,7 +1854,7 @@ void galerkin_dev(bcmgx_hierarchy* H, const DevCsr& A, const int* agg, const dou
     C.nnz = cnnz;
     C.col.alloc(std::max<int64_t>(C.nnz, 1), s);
     C.val.alloc(std::max<int64_t>(C.nnz, 1), s);
-    note_launch(); k_compact_rows<<<warp_grid(nc), 256, 0, s>>>(nc, off.p, C.row.p, pcol.p, pval.p, C.col.p, C.val.p);
+    note_launch(); k_compact_rows<<<gs_grid((long)nc * 8), 256, 0, s>>>(nc, off.p, C.row.p, pcol.p, pval.p, C.col.p, C.val.p);
     BCMGX_CHECK_LAUNCH();
     C.max_row = cmax;
 }
@@ -2188,8 +2316,7 @@ static void edge_weights_noalloc(int n, int64_t nnz, const int* row, const int* 
     note_launch();
     k_diag_c<<<gs_grid(n), 256, 0, s>>>(n, row, col, val, w, C, err);
     const int S = setup_subwarp(n, nnz);
-    BCMGX_SUBWARP_LAUNCH(k_tpos, S, n, s, n, row, col, tpos);
-    BCMGX_SUBWARP_LAUNCH(k_ahat_min, S, n, s, n, row, col, val, w, C, minb);
+    tpos_min_launch(S, n, row, col, tpos, val, w, C, minb, s);
     BCMGX_CHECK_LAUNCH();
     double m = 0;
     BCMGX_CUDA(cudaMemcpyAsync(&m, minb, sizeof(double), cudaMemcpyDeviceToHost, s));

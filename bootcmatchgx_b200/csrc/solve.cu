@@ -63,7 +63,9 @@ int num_sms()
 
 void ensure_smem_limit(const void* kernel, size_t bytes)
 {
-    if (bytes <= 48 * 1024) return;
+    // the default limit covers 48 KB of static and dynamic shared memory together, so a kernel
+    // with static shared memory needs the attribute already at 48 KB of dynamic memory
+    if (bytes < 32 * 1024) return;
     static std::mutex mu;
     static std::map<std::pair<int, const void*>, size_t> set;
     int dev = 0;

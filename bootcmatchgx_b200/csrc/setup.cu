@@ -633,7 +633,7 @@ __global__ void k_logw(int n, const int* __restrict__ row, const int* __restrict
 // ------------------------------------------------------------------------------------------
 
 // Per row: rank of every candidate (off-diagonal, W > 0) in the row's preference order,
-// (W, column) descending (find_Candidate, suitor.cu:80-147); ordj lists the entries by rank.
+// (W, column) descending (find_Candidate, suitor.cu:80-147).
 // Ranks of a row of at most 32 entries held in registers (lane = entry t = b + lane, column ct
 // and weight wt; ct = -1 past the row). When the weights differ, every lane compares its entry
 // with all of the row's: the row's (weight, column) keys go to the warp's slots in shared memory
@@ -645,7 +645,7 @@ struct alignas(16) RankKey {
     int pad;
 };
 __device__ __forceinline__ void rank_row32(long r, int b, int e, int ct, double wt, int* __restrict__ rank,
-    int* __restrict__ ordj, int* __restrict__ degE, RankKey* keys)
+    int* __restrict__ degE, RankKey* keys)
 {
     const int lane = threadIdx.x & 31;
     const int t = b + lane;
@@ -669,10 +669,7 @@ __device__ __forceinline__ void rank_row32(long r, int b, int e, int ct, double 
             rk += (q.c >= 0 && (q.w > wt || (q.w == wt && q.c > ct))) ? 1 : 0;
         }
     }
-    if (in) {
-        rank[t] = el ? rk : -1;
-        if (el) ordj[b + rk] = t;
-    }
+    if (in) rank[t] = el ? rk : -1;
     if (lane == 0) degE[r] = __popc(elig);
 }
 
@@ -683,7 +680,7 @@ __device__ __forceinline__ void rank_row32(long r, int b, int e, int ct, double 
 // flight, so a row costs one memory round trip instead of three dependent ones.
 __global__ void __launch_bounds__(256, 8) k_rank_w(int n, const int* __restrict__ row, const int* __restrict__ col, const double* __restrict__ val,
     const double* __restrict__ w, const double* __restrict__ C, const int* __restrict__ tpos, double zero_sub,
-    int* __restrict__ rank, int* __restrict__ ordj, int* __restrict__ degE, const double* __restrict__ zero_sub_dev)
+    int* __restrict__ rank, int* __restrict__ degE, const double* __restrict__ zero_sub_dev)
 {
     if (zero_sub_dev) zero_sub = *zero_sub_dev;
     const int lane = threadIdx.x & 31;
@@ -720,7 +717,7 @@ __global__ void __launch_bounds__(256, 8) k_rank_w(int n, const int* __restrict_
             const double sa = fabs(ahat(__ldg(val + src), __ldg(C + r), __ldg(C + ct), __ldg(w + r), __ldg(w + ct)));
             wt = log(sa != 0.0 ? sa : zero_sub);
         }
-        rank_row32(r, b, e, ct, wt, rank, ordj, degE, wkeys);
+        rank_row32(r, b, e, ct, wt, rank, degE, wkeys);
         if (r1 >= n) break;
         r = r1;
         b = b1;
@@ -734,7 +731,7 @@ __global__ void __launch_bounds__(256, 8) k_rank_w(int n, const int* __restrict_
 }
 
 __global__ void k_rank(int n, const int* __restrict__ row, const int* __restrict__ col, const double* __restrict__ W,
-    int* __restrict__ rank, int* __restrict__ ordj, int* __restrict__ degE)
+    int* __restrict__ rank, int* __restrict__ degE)
 {
     const int lane = threadIdx.x & 31;
     __shared__ RankKey keys[8][32];   // 256-thread blocks
@@ -744,7 +741,7 @@ __global__ void k_rank(int n, const int* __restrict__ row, const int* __restrict
         if (e - b <= 32) {
             const int t = b + lane;
             const bool in = t < e;
-            rank_row32(r, b, e, in ? col[t] : -1, in ? W[t] : 0.0, rank, ordj, degE, wkeys);
+            rank_row32(r, b, e, in ? col[t] : -1, in ? W[t] : 0.0, rank, degE, wkeys);
             continue;
         }
         int cnt = 0;
@@ -763,7 +760,6 @@ __global__ void k_rank(int n, const int* __restrict__ row, const int* __restrict
                         rk += (ck != r && wk > 0.0 && (wk > wt || (wk == wt && ck > ct))) ? 1 : 0;
                     }
                     rank[t] = rk;
-                    ordj[b + rk] = t;
                 } else {
                     rank[t] = -1;
                 }
@@ -777,38 +773,39 @@ __global__ void k_rank(int n, const int* __restrict__ row, const int* __restrict
 // Preference records: pref[row[v] + k] = {k-th candidate y of v, v's offer value at y}, where
 // the offer value is degE[y] - (rank of v in y's list), or 0 when y does not rank v (no
 // transposed entry: the pair is never proposed). rinfo[v] = {row[v], degE[v]}. With mark_last
-// (the wide suitor's form) the last record of each list also carries kPrefLast.
+// (the wide suitor's form) the last record of each list also carries kPrefLast. The row's
+// entries are taken in CSR order (their column, transposed position and rank read together) and
+// each record is stored at its rank.
 constexpr int kPrefLast = 1 << 30;
 template <int S>
-__global__ void k_pref(int n, const int* __restrict__ row, const int* __restrict__ col, const int* __restrict__ ordj,
-    const int* __restrict__ rank, const int* __restrict__ tpos, const int* __restrict__ degE, int2* __restrict__ pref,
-    int2* __restrict__ rinfo, int mark_last)
+__global__ void k_pref(int n, const int* __restrict__ row, const int* __restrict__ col, const int* __restrict__ rank,
+    const int* __restrict__ tpos, const int* __restrict__ degE, int2* __restrict__ pref, int2* __restrict__ rinfo,
+    int mark_last)
 {
     constexpr int U = kSetupBatch;
     const int lane = threadIdx.x & (S - 1);
     BCMGX_SUBWARP_ROWS(r, n, S)
     {
-        const int b = __ldg(row + r), dE = __ldg(degE + r);
-        for (int k0 = lane; k0 < dE; k0 += U * S) {
-            int j[U], y[U], tj[U], ry[U], dy[U];
-#pragma unroll
-            for (int u = 0; u < U; u++) j[u] = k0 + u * S < dE ? __ldg(ordj + b + k0 + u * S) : -1;
+        const int b = __ldg(row + r), e = __ldg(row + r + 1), dE = __ldg(degE + r);
+        for (int j0 = b + lane; j0 < e; j0 += U * S) {
+            int rk[U], y[U], tj[U], ry[U], dy[U];
 #pragma unroll
             for (int u = 0; u < U; u++) {
-                y[u] = j[u] >= 0 ? __ldg(col + j[u]) : 0;
-                tj[u] = j[u] >= 0 ? __ldg(tpos + j[u]) : -1;
+                const int j = j0 + u * S;
+                rk[u] = j < e ? __ldg(rank + j) : -1;
+                y[u] = j < e ? __ldg(col + j) : 0;
+                tj[u] = j < e ? __ldg(tpos + j) : -1;
             }
 #pragma unroll
             for (int u = 0; u < U; u++) {
-                ry[u] = tj[u] >= 0 ? __ldg(rank + tj[u]) : -1;
-                dy[u] = j[u] >= 0 ? __ldg(degE + y[u]) : 0;
+                ry[u] = (rk[u] >= 0 && tj[u] >= 0) ? __ldg(rank + tj[u]) : -1;
+                dy[u] = rk[u] >= 0 ? __ldg(degE + y[u]) : 0;
             }
 #pragma unroll
             for (int u = 0; u < U; u++)
-                if (j[u] >= 0) {
-                    const int k = k0 + u * S;
-                    const int last = (mark_last && k == dE - 1) ? kPrefLast : 0;
-                    pref[b + k] = make_int2(y[u], (ry[u] >= 0 ? dy[u] - ry[u] : 0) | last);
+                if (rk[u] >= 0) {
+                    const int last = (mark_last && rk[u] == dE - 1) ? kPrefLast : 0;
+                    pref[b + rk[u]] = make_int2(y[u], (ry[u] >= 0 ? dy[u] - ry[u] : 0) | last);
                 }
         }
         if (lane == 0) rinfo[r] = make_int2(b, dE);
@@ -1533,13 +1530,12 @@ void suitor_dev(int n, int64_t nnz, const int* row, const int* col, const double
     if (max_row <= 0) max_row = row_max_raw(n, row, s);
     if (fw && max_row > 32) throw Error(BCMGX_ERR_INTERNAL, "weights formed in the rank kernel need rows of <= 32 entries");
     const bool wide = max_row < 65536;
-    DBuf<int> rank, ordj, degE, err;
+    DBuf<int> rank, degE, err;
     DBuf<int2> pref, rinfo;
     DBuf<unsigned> offer;
     DBuf<unsigned long long> offer_w;
     const int64_t z = std::max<int64_t>(nnz, 1);
     rank.alloc(z, s);
-    ordj.alloc(z, s);
     degE.alloc(n, s);
     if (!err_out) {
         err.alloc(1, s);
@@ -1555,18 +1551,17 @@ void suitor_dev(int n, int64_t nnz, const int* row, const int* col, const double
     }
     if (fw) {
         note_launch();
-        k_rank_w<<<warp_grid(n), 256, 0, s>>>(n, row, col, fw->val, fw->w, fw->C, tpos, fw->zero_sub, rank.p, ordj.p, degE.p,
+        k_rank_w<<<warp_grid(n), 256, 0, s>>>(n, row, col, fw->val, fw->w, fw->C, tpos, fw->zero_sub, rank.p, degE.p,
             fw->zero_sub_dev);
     } else {
-        note_launch(); k_rank<<<warp_grid(n), 256, 0, s>>>(n, row, col, W, rank.p, ordj.p, degE.p);
+        note_launch(); k_rank<<<warp_grid(n), 256, 0, s>>>(n, row, col, W, rank.p, degE.p);
     }
     pref.alloc(z, s);
     rinfo.alloc(n, s);
-    BCMGX_SUBWARP_LAUNCH(k_pref, setup_subwarp(n, nnz), n, s, n, row, col, ordj.p, rank.p, tpos, degE.p, pref.p, rinfo.p,
+    BCMGX_SUBWARP_LAUNCH(k_pref, setup_subwarp(n, nnz), n, s, n, row, col, rank.p, tpos, degE.p, pref.p, rinfo.p,
         wide ? 1 : 0);
     BCMGX_CHECK_LAUNCH();
     rank.release();
-    ordj.release();
     static int asc = -1;
     if (asc < 0) {
         const char* e = std::getenv("BCMGX_SUITOR_ASC");

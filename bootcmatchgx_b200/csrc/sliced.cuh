@@ -137,10 +137,14 @@ template <typename T> struct SlSrc<const T*> {
 
 // Shared-memory stages of the sliced kernel: every warp keeps kSlStages stages of kSlStageBytes,
 // each holding one slice's index words (first) and value words (after NBMAX blocks of indices),
-// filled by the warp's own cp.async copies two slices ahead of the one it works on. A slice wider
-// than NBMAX blocks is read from global memory instead.
+// filled by the warp's own cp.async copies kSlStages - 1 slices ahead of the one it works on. A
+// slice wider than NBMAX blocks is read from global memory instead. The depth of the ring, not
+// the number of resident warps, sets the rate (at 27-point 160^3, level 0: 2 stages with 32
+// resident warps 0.131 ms a sweep, 3 with 24 warps 0.090 ms, 4 with 16 warps 0.085 ms; 5 with 12
+// warps in 6-warp blocks 0.100 ms, 5 with 8 warps 0.134 ms).
 constexpr int kSlWarps = 8;            // warps per block (256 threads)
-constexpr int kSlStages = 3;
+constexpr int kSlStages = 4;
+constexpr int kSlMinBlocks = 2;        // blocks per SM that the stages (96 KB a block) leave room for
 constexpr int kSlStageBytes = 3072;
 template <typename IT, typename VS>
 struct SlStage {
@@ -207,7 +211,7 @@ __device__ __forceinline__ AT slice_sum_fixed(unsigned sb, int lane, int rr, con
 // FIT: every slice fits a stage (the matrix's longest row has at most NBMAX blocks), so no slice
 // takes the global-memory path.
 template <int OP, typename VS, typename XT, typename FT, typename MT, typename YT, typename IT, bool FIT>
-__global__ void __launch_bounds__(kSlWarps * 32, 3) k_rowop_sliced(int n, const int* __restrict__ sptr,
+__global__ void __launch_bounds__(kSlWarps * 32, kSlMinBlocks) k_rowop_sliced(int n, const int* __restrict__ sptr,
     const IT* __restrict__ sidx, SlSrc<VS> sv, const XT* __restrict__ x, const FT* __restrict__ f,
     const MT* __restrict__ M, YT* __restrict__ y, double alpha, double beta, const int* __restrict__ skip)
 {
@@ -257,12 +261,11 @@ __global__ void __launch_bounds__(kSlWarps * 32, 3) k_rowop_sliced(int n, const 
         cp_async_commit();
     };
 
-    int b0, e0, b1, e1, b2, e2;
-    ptrs(gw, b0, e0);
-    ptrs(gw + nw, b1, e1);
-    ptrs(gw + 2 * nw, b2, e2);
-    issue(0, b0, e0);
-    issue(1, b1, e1);
+    int pb[kSlStages], pe[kSlStages];
+#pragma unroll
+    for (int k = 0; k < kSlStages; k++) ptrs(gw + k * nw, pb[k], pe[k]);
+#pragma unroll
+    for (int k = 0; k + 1 < kSlStages; k++) issue(k, pb[k], pe[k]);
     // the prologue above reads only the sliced copy and its table, which no kernel of a solve
     // writes (build_sliced returns after they are complete); vectors are read after the wait
     dep_wait();
@@ -273,12 +276,13 @@ __global__ void __launch_bounds__(kSlWarps * 32, 3) k_rowop_sliced(int n, const 
     }
     int st = 0;
     for (long sl = gw; sl < nsl; sl += nw) {
-        // the stage that the slice two ahead goes to was read by this warp one slice ago
+        // the stage that the slice kSlStages - 1 ahead goes to was read by this warp one slice ago
         __syncwarp();
-        issue(st == 0 ? 2 : st - 1, b2, e2);
+        issue(st == 0 ? kSlStages - 1 : st - 1, pb[kSlStages - 1], pe[kSlStages - 1]);
         int bn, en;
-        ptrs(sl + 3 * nw, bn, en);
-        cp_async_wait<2>();   // this slice's copies (the group before the last two) have landed
+        ptrs(sl + kSlStages * nw, bn, en);
+        cp_async_wait<kSlStages - 1>();   // this slice's copies (the group before the last ones) have landed
+        const int b0 = pb[0], e0 = pe[0];
         __syncwarp();         // ... including those of the other lanes
         const int r = (int)(sl * kSliceRows) + lane;
         const bool live = r < n;
@@ -359,12 +363,13 @@ __global__ void __launch_bounds__(kSlWarps * 32, 3) k_rowop_sliced(int n, const 
                 y[r] = (YT)(((-s + o1) / o2) + o3);
             }
         }
-        b0 = b1;
-        e0 = e1;
-        b1 = b2;
-        e1 = e2;
-        b2 = bn;
-        e2 = en;
+#pragma unroll
+        for (int k = 0; k + 1 < kSlStages; k++) {
+            pb[k] = pb[k + 1];
+            pe[k] = pe[k + 1];
+        }
+        pb[kSlStages - 1] = bn;
+        pe[kSlStages - 1] = en;
         st = st == kSlStages - 1 ? 0 : st + 1;
     }
     cp_async_wait<0>();

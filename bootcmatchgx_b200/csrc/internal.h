@@ -147,6 +147,7 @@ struct DevCsr {
     DBuf<double> val;
     DBuf<float> val32;
     DBuf<short> dcol; // col - row as int16 when every entry is within 32767 of the diagonal, else empty
+    DBuf<int> dpos;   // position of each row's diagonal entry (-1: none), where the producing kernel records it
     // value codes (value-indexed CSR, rowops.cuh Coded): when the matrix has at most 256 distinct
     // values, entry j's value is vtab64[vcode[j]] (and its FP32 copy vtab32[vcode[j]]); else empty
     DBuf<unsigned char> vcode;

@@ -246,7 +246,7 @@ __global__ void k_validate(int n, int m, long long nnz, const int* __restrict__ 
 // as an int16 offset from its row (clamped; the caller keeps them only when the largest offset
 // fits): one pass over the input instead of three.
 __global__ void k_validate_offsets(int n, int m, long long nnz, const int* __restrict__ row, const int* __restrict__ col,
-    int* err, int* max_row, int* max_off, short* __restrict__ dcol, int need_diag)
+    int* err, int* max_row, int* max_off, short* __restrict__ dcol, int need_diag, int* __restrict__ dpos)
 {
     constexpr int S = 8;
     const int lane = threadIdx.x & (S - 1);
@@ -285,7 +285,10 @@ __global__ void k_validate_offsets(int n, int m, long long nnz, const int* __res
                         if (j < e) {
                             if (c < 0 || c >= m) bad |= ERR_COLRANGE;
                             if (j > b && prev >= c) bad |= ERR_COLSORT;
-                            if (c == (int)r) diag = true;
+                            if (c == (int)r) {
+                                diag = true;
+                                if (dpos) dpos[r] = j;
+                            }
                             const int off = c - (int)r;
                             mo = max(mo, off < 0 ? -off : off);
                             if (dcol) dcol[j] = (short)max(-32768, min(32767, off));
@@ -295,6 +298,7 @@ __global__ void k_validate_offsets(int n, int m, long long nnz, const int* __res
                 }
                 diag = (__ballot_sync(mask, diag) & mask) != 0;
                 if (need_diag && !diag) bad |= ERR_NODIAG;
+                if (dpos && !diag && lane == 0) dpos[r] = -1;
                 mx = max(mx, e - b);
             }
         }
@@ -394,6 +398,24 @@ __global__ void k_diag_c(int n, const int* __restrict__ row, const int* __restri
             else atomicOr(err, ERR_NODIAG);
             C[r] = c;
         }
+    }
+}
+
+// k_diag_c for a matrix whose diagonal positions were recorded by the kernel that produced it
+// (k_validate_offsets, k_compact_rows): one gather per row, the same product.
+__global__ void k_diag_c_pos(int n, const int* __restrict__ dpos, const double* __restrict__ val,
+    const double* __restrict__ w, double* __restrict__ C, int* err)
+{
+    for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long)gridDim.x * blockDim.x) {
+        const int j = dpos[r];
+        double c = 0.0;
+        if (j >= 0) {
+            const double wr = w[r];
+            c = __dmul_rn(__dmul_rn(__ldg(val + j), wr), wr);
+        } else {
+            atomicOr(err, ERR_NODIAG);
+        }
+        C[r] = c;
     }
 }
 
@@ -1334,7 +1356,7 @@ __global__ void k_galerkin_counts(int nc, const int* __restrict__ fine0, const i
 // rows written from off[I] -> CSR; 8 lanes per row (4 rows of a warp in flight), each lane
 // moving up to 4 entries per round with all of their loads issued first
 __global__ void k_compact_rows(int nc, const int* __restrict__ off, const int* __restrict__ rowptr, const int* __restrict__ pcol,
-    const double* __restrict__ pval, int* __restrict__ col, double* __restrict__ val)
+    const double* __restrict__ pval, int* __restrict__ col, double* __restrict__ val, int* __restrict__ dpos)
 {
     constexpr int S = 8, U = 4;
     const int lane = threadIdx.x & (S - 1);
@@ -1356,6 +1378,7 @@ __global__ void k_compact_rows(int nc, const int* __restrict__ off, const int* _
                 if (t < len) {
                     col[b + t] = c[u];
                     val[b + t] = v[u];
+                    if (c[u] == (int)I) dpos[I] = b + t;
                 }
             }
         }
@@ -1601,11 +1624,16 @@ struct SweepOut {
 // edge_prep_dev without a host round trip: the substitute goes to *zs_dev, the diagonal check's
 // error bits to the caller's error word (read with its next round trip).
 static void edge_prep_async(int n, int64_t nnz, const int* row, const int* col, const double* val, const double* w,
-    double* C, int* tpos, double* zs_dev, unsigned long long* mn, int* err, cudaStream_t s, double min_cap)
+    double* C, int* tpos, double* zs_dev, unsigned long long* mn, int* err, cudaStream_t s, double min_cap,
+    const int* dpos = nullptr)
 {
     const int S = setup_subwarp(n, nnz);
     note_launch(); k_set_u64<<<1, 1, 0, s>>>(mn, (unsigned long long)__builtin_bit_cast(long long, DBL_MAX));
-    note_launch(); k_diag_c<<<gs_grid(n), 256, 0, s>>>(n, row, col, val, w, C, err);
+    if (dpos) {
+        note_launch(); k_diag_c_pos<<<gs_grid(n), 256, 0, s>>>(n, dpos, val, w, C, err);
+    } else {
+        note_launch(); k_diag_c<<<gs_grid(n), 256, 0, s>>>(n, row, col, val, w, C, err);
+    }
     tpos_min_launch(S, n, row, col, tpos, val, w, C, mn, s);
     note_launch(); k_zero_sub<<<1, 1, 0, s>>>(mn, min_cap, zs_dev);
     BCMGX_CHECK_LAUNCH();
@@ -1637,7 +1665,7 @@ void sweep_aggregate(bcmgx_hierarchy* H, const DevCsr& A, const double* w, Sweep
         FusedWeights fw;
         {
             PhaseTimer pt(H, "weights");
-            edge_prep_async(n, nnz, A.row.p, A.col.p, A.val.p, w, Cd.p, tpos.p, zs.p, mn.p, err.p, s, min_cap);
+            edge_prep_async(n, nnz, A.row.p, A.col.p, A.val.p, w, Cd.p, tpos.p, zs.p, mn.p, err.p, s, min_cap, A.dpos.p);
         }
         fw.val = A.val.p;
         fw.w = w;
@@ -1651,7 +1679,7 @@ void sweep_aggregate(bcmgx_hierarchy* H, const DevCsr& A, const double* w, Sweep
             PhaseTimer pt(H, "weights");
             DBuf<double> C;
             C.alloc(n, s);
-            edge_prep_async(n, nnz, A.row.p, A.col.p, A.val.p, w, C.p, tpos.p, zs.p, mn.p, err.p, s, min_cap);
+            edge_prep_async(n, nnz, A.row.p, A.col.p, A.val.p, w, C.p, tpos.p, zs.p, mn.p, err.p, s, min_cap, A.dpos.p);
             BCMGX_SUBWARP_LAUNCH(k_logw, setup_subwarp(n, nnz), n, s, n, A.row.p, A.col.p, A.val.p, w, C.p, tpos.p,
                 0.0, W.p, zs.p);
             BCMGX_CHECK_LAUNCH();
@@ -1849,7 +1877,10 @@ void galerkin_dev(bcmgx_hierarchy* H, const DevCsr& A, const int* agg, const dou
     C.nnz = cnnz;
     C.col.alloc(std::max<int64_t>(C.nnz, 1), s);
     C.val.alloc(std::max<int64_t>(C.nnz, 1), s);
-    note_launch(); k_compact_rows<<<gs_grid((long)nc * 8), 256, 0, s>>>(nc, off.p, C.row.p, pcol.p, pval.p, C.col.p, C.val.p);
+    C.dpos.alloc(std::max(nc, 1), s);
+    BCMGX_CUDA(cudaMemsetAsync(C.dpos.p, 0xff, sizeof(int) * (size_t)std::max(nc, 1), s));
+    note_launch(); k_compact_rows<<<gs_grid((long)nc * 8), 256, 0, s>>>(nc, off.p, C.row.p, pcol.p, pval.p, C.col.p, C.val.p,
+        C.dpos.p);
     BCMGX_CHECK_LAUNCH();
     C.max_row = cmax;
 }
@@ -2136,8 +2167,10 @@ void build_hierarchy(bcmgx_hierarchy* H, const bcmgx_csr* Ain)
         const char* env16 = std::getenv("BCMGX_INDEX16");
         const bool want16 = !(env16 && env16[0] == '0');
         if (want16) A.dcol.alloc(A.nnz, s);
+        const bool bcmg = P.preconditioner == BCMGX_PREC_BCMG;
+        if (bcmg) A.dpos.alloc(A.n, s);
         note_launch(); k_validate_offsets<<<gs_grid((long)A.n * 8), 256, 0, s>>>(A.n, A.m, A.nnz, A.row.p, A.col.p,
-            st.p, st.p + 1, st.p + 2, want16 ? A.dcol.p : nullptr, P.preconditioner == BCMGX_PREC_BCMG ? 1 : 0);
+            st.p, st.p + 1, st.p + 2, want16 ? A.dcol.p : nullptr, bcmg ? 1 : 0, bcmg ? A.dpos.p : nullptr);
         BCMGX_CHECK_LAUNCH();
         int h[3] = { 0, 0, 0 };
         BCMGX_CUDA(cudaMemcpyAsync(h, st.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, s));

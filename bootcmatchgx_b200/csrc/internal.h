@@ -168,12 +168,22 @@ struct DevCsr {
     DBuf<unsigned char> sl_code;
     DBuf<float> sl_val32;
     DBuf<double> sl_val64;
+    // pattern-indexed rows (build_patterns): when the rows' column-offset sequences take at most
+    // 255 distinct forms, sl_pid[r] is row r's form (rows past n take row n-1's) and sl_pat its
+    // offsets, npat forms of patw int16 offsets each (zero past a form's length); else empty
+    DBuf<unsigned char> sl_pid;
+    DBuf<short> sl_pat;
+    int npat = 0, patw = 0;
 };
 
 // tuning code of the sliced kernels (hierarchy info, BCMGX_TPR, the tuning cache); the staged
 // kernels are coded as minus their threads per row
 constexpr int kSlicedCode = 64;
 void build_sliced(DevCsr& A, cudaStream_t s);
+// Pattern-indexed rows of a coded level with int16 offsets and rows of at most 32 entries (one
+// host round trip for the distinct forms, one for the check); leaves A.sl_pid empty when the level
+// does not qualify. BCMGX_SLPAT=0 turns it off.
+void build_patterns(DevCsr& A, cudaStream_t s);
 void release_sliced(DevCsr& A);
 
 struct Level {

@@ -2075,6 +2075,125 @@ static void build_value_codes(DevCsr& A, cudaStream_t s)
     A.nvalues = (int)vals.size();
 }
 
+// ---- pattern-indexed rows ------------------------------------------------------------------
+// A stencil level's rows repeat a handful of column-offset sequences (a 27-point grid has 27
+// boundary types). Each row's sequence gets a 63-bit hash; the distinct hashes are collected and
+// numbered with the value codes' hash set (k_vc_collect / k_vc_encode on the hashes' bit patterns),
+// one row per number gives the form's offsets, and a check pass compares every row with its form,
+// so a hash collision only costs the pattern form, never a wrong column.
+__global__ void k_pat_hash(int n, const int* __restrict__ row, const short* __restrict__ dcol,
+    unsigned long long* __restrict__ h)
+{
+    for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long)gridDim.x * blockDim.x) {
+        const int b = row[r], e = row[r + 1];
+        unsigned long long v = 1469598103934665603ull ^ (unsigned long long)(e - b);
+        for (int j = b; j < e; j++) v = (v ^ (unsigned long long)(unsigned short)dcol[j]) * 1099511628211ull;
+        h[r] = v & 0x7fffffffffffffffull;   // never kVcEmpty
+    }
+}
+
+// rep[id] = some row of form id; len[id] its length. The claim is tried only while the form has
+// none (a plain load first): millions of rows share a few forms, and atomics on one word serialise.
+__global__ void k_pat_rep(int n, const int* __restrict__ row, const unsigned char* __restrict__ pid, int* rep,
+    int* len)
+{
+    for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long)gridDim.x * blockDim.x) {
+        const int id = pid[r];
+        if (ld_cg(rep + id) == -1 && atomicCAS(rep + id, -1, (int)r) == -1) len[id] = row[r + 1] - row[r];
+    }
+}
+
+// pat[id * W + k] = offset k of form id (0 past its length)
+__global__ void k_pat_table(int npat, int W, const int* __restrict__ row, const short* __restrict__ dcol,
+    const int* __restrict__ rep, const int* __restrict__ len, short* __restrict__ pat)
+{
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < (long)npat * W; t += (long)gridDim.x * blockDim.x) {
+        const int id = (int)(t / W), k = (int)(t % W);
+        const int r = rep[id];
+        pat[t] = (r >= 0 && k < len[id]) ? dcol[row[r] + k] : (short)0;
+    }
+}
+
+// every row against its form (length and offsets); rows n .. total-1 of the per-slice array take
+// row n-1's form
+__global__ void k_pat_check(int n, long total, int W, const int* __restrict__ row, const short* __restrict__ dcol,
+    unsigned char* __restrict__ pid, const short* __restrict__ pat, const int* __restrict__ len, int* bad)
+{
+    for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < total; r += (long)gridDim.x * blockDim.x) {
+        if (r >= n) {
+            pid[r] = pid[n - 1];
+            continue;
+        }
+        const int id = pid[r];
+        const int b = row[r], e = row[r + 1];
+        bool ok = e - b == len[id] && e - b <= W;
+        for (int j = b; ok && j < e; j++) ok = dcol[j] == pat[(long)id * W + (j - b)];
+        if (!ok) atomicOr(bad, 1);
+    }
+}
+
+void build_patterns(DevCsr& A, cudaStream_t s)
+{
+    A.sl_pid.release();
+    A.sl_pat.release();
+    A.npat = A.patw = 0;
+    const char* env = std::getenv("BCMGX_SLPAT");
+    if (env && env[0] == '0') return;
+    const int n = A.n;
+    if (n <= 0 || !A.dcol.p || !A.sl_code.p || A.max_row <= 0 || A.max_row > 32) return;
+    const long total = ((long)n + 31) / 32 * 32;   // whole 32-row slices
+    DBuf<unsigned long long> h, keys;
+    DBuf<int> cnt;
+    h.alloc(n, s);
+    keys.alloc(kVcSlots, s);
+    cnt.alloc(2, s);
+    note_launch(); k_pat_hash<<<gs_grid(n), 256, 0, s>>>(n, A.row.p, A.dcol.p, h.p);
+    BCMGX_CUDA(cudaMemsetAsync(keys.p, 0xff, sizeof(unsigned long long) * kVcSlots, s));
+    BCMGX_CUDA(cudaMemsetAsync(cnt.p, 0, 2 * sizeof(int), s));
+    note_launch(); k_vc_collect<<<gs_grid(n), 256, 0, s>>>(n, (const double*)h.p, keys.p, cnt.p, cnt.p + 1);
+    BCMGX_CHECK_LAUNCH();
+    std::vector<unsigned long long> hk(kVcSlots);
+    int hc[2] = { 0, 0 };
+    BCMGX_CUDA(cudaMemcpyAsync(hk.data(), keys.p, sizeof(unsigned long long) * kVcSlots, cudaMemcpyDeviceToHost, s));
+    BCMGX_CUDA(cudaMemcpyAsync(hc, cnt.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    BCMGX_CUDA(cudaStreamSynchronize(s));
+    if (hc[1] || hc[0] <= 0 || hc[0] > 255) return;
+    std::vector<unsigned long long> forms;
+    for (unsigned long long k : hk)
+        if (k != kVcEmpty) forms.push_back(k);
+    std::sort(forms.begin(), forms.end());
+    const int npat = (int)forms.size();
+    std::vector<int> slot_id(kVcSlots, 0);
+    for (int t = 0; t < kVcSlots; t++)
+        if (hk[t] != kVcEmpty) slot_id[t] = (int)(std::lower_bound(forms.begin(), forms.end(), hk[t]) - forms.begin());
+    const int W = ((A.max_row + 3) / 4) * 4;
+    DBuf<int> sid, rep, len, bad;
+    sid.alloc(kVcSlots, s);
+    rep.alloc(npat, s);
+    len.alloc(npat, s);
+    bad.alloc(1, s);
+    BCMGX_CUDA(cudaMemcpyAsync(sid.p, slot_id.data(), sizeof(int) * kVcSlots, cudaMemcpyHostToDevice, s));
+    BCMGX_CUDA(cudaMemsetAsync(rep.p, 0xff, sizeof(int) * npat, s));
+    BCMGX_CUDA(cudaMemsetAsync(len.p, 0, sizeof(int) * npat, s));
+    BCMGX_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
+    A.sl_pid.alloc(total, s);
+    A.sl_pat.alloc((size_t)npat * W, s);
+    note_launch(); k_vc_encode<<<gs_grid(n), 256, 0, s>>>(n, (const double*)h.p, keys.p, sid.p, A.sl_pid.p);
+    note_launch(); k_pat_rep<<<gs_grid(n), 256, 0, s>>>(n, A.row.p, A.sl_pid.p, rep.p, len.p);
+    note_launch(); k_pat_table<<<gs_grid((long)npat * W), 256, 0, s>>>(npat, W, A.row.p, A.dcol.p, rep.p, len.p, A.sl_pat.p);
+    note_launch(); k_pat_check<<<gs_grid(total), 256, 0, s>>>(n, total, W, A.row.p, A.dcol.p, A.sl_pid.p, A.sl_pat.p, len.p,
+        bad.p);
+    BCMGX_CHECK_LAUNCH();
+    // the host vector above is read by its copy before this returns
+    if (read_err(bad.p, s)) {
+        A.sl_pid.release();
+        A.sl_pat.release();
+        return;
+    }
+    A.npat = npat;
+    A.patw = W;
+}
+
 void finish_level_matrix(Level& V, bool want_f32, cudaStream_t s)
 {
     const int n = V.A.n;

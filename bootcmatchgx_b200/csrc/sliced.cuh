@@ -375,6 +375,168 @@ __global__ void __launch_bounds__(kSlWarps * 32, kSlMinBlocks) k_rowop_sliced(in
     cp_async_wait<0>();
 }
 
+// ---- pattern-indexed rows ----
+// A coded level whose rows' column-offset sequences take at most 255 forms (build_patterns) keeps,
+// besides its sliced codes, one byte per row naming its form and a table of the forms' int16
+// offsets (zero past a form's length). k_rowop_slpat streams the codes and the form bytes only (about
+// 1 byte per entry and 1 per row instead of 3 per entry) and reads the offsets from the table in
+// shared memory; it adds a row's entries in the order of k_rowop_sliced, so the results are the same
+// bit for bit. Stages hold a slice's 32 form bytes, then its code blocks.
+constexpr int kSpStages = 6;
+constexpr int kSpStageBytes = 32 + 8 * kSliceBlock;   // the form bytes and up to 8 blocks of codes
+
+// the row sum of a lane over a slice of exactly NBC blocks: offsets from the form's table row (pr, a
+// 32-bit shared address, 8-byte aligned), codes from the stage (sb)
+template <int NBC, typename T, typename XT, typename AT>
+__device__ __forceinline__ AT slpat_sum_fixed(unsigned sb, unsigned pr, int lane, int rr, const XT* __restrict__ x,
+    const T* tab_s)
+{
+    constexpr int GB = sizeof(XT) == 4 ? 4 : 2;
+    SlIdxRaw<short> ix[NBC];
+    SlVal<Coded<T>> vv[NBC];
+#pragma unroll
+    for (int u = 0; u < NBC; u++) {
+        ix[u].ldsa(pr + (unsigned)(u * kSliceG * (int)sizeof(short)));
+        vv[u].ldsa(sb + (unsigned)(32 + u * kSliceBlock + lane * kSliceG));
+    }
+    AT s = 0;
+#pragma unroll
+    for (int g = 0; g < NBC; g += GB) {
+        XT xv[GB][kSliceG];
+#pragma unroll
+        for (int u = 0; u < GB; u++)
+            if (g + u < NBC)
+#pragma unroll
+                for (int i = 0; i < kSliceG; i++) xv[u][i] = ld_ro(x + ix[g + u].col(i, rr));
+#pragma unroll
+        for (int u = 0; u < GB; u++)
+            if (g + u < NBC)
+#pragma unroll
+                for (int i = 0; i < kSliceG; i++) s += (AT)vv[g + u].get(i, tab_s) * (AT)xv[u][i];
+    }
+    return s;
+}
+
+// The operations of k_rowop_sliced (OP_AXPBY, OP_RESID, OP_JACOBI) on a pattern-indexed coded level
+// whose slices are all at most 8 blocks wide. Dynamic shared memory: the form table (npat * W int16,
+// rounded up to 16 bytes) and kSlWarps * kSpStages * kSpStageBytes of stages.
+template <int OP, typename T, typename XT, typename FT, typename MT, typename YT>
+__global__ void __launch_bounds__(kSlWarps * 32, 3) k_rowop_slpat(int n, const int* __restrict__ sptr,
+    const unsigned char* __restrict__ pid, const unsigned char* __restrict__ code, const T* __restrict__ tab,
+    const short* __restrict__ pat, int npat, int W, const XT* __restrict__ x, const FT* __restrict__ f,
+    const MT* __restrict__ M, YT* __restrict__ y, double alpha, double beta, const int* __restrict__ skip)
+{
+    using AT = typename Acc<T>::type;
+    __shared__ T tab_s[kValueCodes];
+    short* pat_s = (short*)sl_smem;
+    const int patb = ((npat * W * (int)sizeof(short)) + 15) & ~15;
+    for (int i = threadIdx.x; i < kValueCodes; i += blockDim.x) tab_s[i] = __ldg(tab + i);
+    for (int i = threadIdx.x; i < npat * W; i += blockDim.x) pat_s[i] = __ldg(pat + i);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const long nsl = ((long)n + kSliceRows - 1) / kSliceRows;
+    const long nw = (long)gridDim.x * (blockDim.x / 32);
+    const long gw = (long)blockIdx.x * (blockDim.x / 32) + wib;
+    unsigned char* stage0 = sl_smem + patb + (size_t)wib * kSpStages * kSpStageBytes;
+    const unsigned stage0_s = (unsigned)__cvta_generic_to_shared(stage0);
+    const unsigned pat_sa = (unsigned)__cvta_generic_to_shared(pat_s);
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    auto ptrs = [&](long sl, int& b, int& e) {
+        if (sl < nsl) {
+            b = __ldg(sptr + sl);
+            e = __ldg(sptr + sl + 1);
+        } else {
+            b = e = 0;
+        }
+    };
+    // a slice's 32 form bytes (two 16-byte copies) and its code blocks into stage st
+    auto issue = [&](int st, long sl, int b, int e) {
+        const int nb = (e - b) / kSliceBlock;
+        if (sl < nsl && nb > 0) {
+            const unsigned dst = stage0_s + (unsigned)(st * kSpStageBytes);
+            if (lane < 2) cp_async16(dst + lane * 16, pid + sl * kSliceRows + lane * 16, pol);
+            const int cv = nb * kSliceBlock / 16;
+            for (int c = lane; c < cv; c += 32) cp_async16(dst + 32 + c * 16, code + b + c * 16, pol);
+        }
+        cp_async_commit();
+    };
+    int pb[kSpStages], pe[kSpStages];
+#pragma unroll
+    for (int k = 0; k < kSpStages; k++) ptrs(gw + k * nw, pb[k], pe[k]);
+#pragma unroll
+    for (int k = 0; k + 1 < kSpStages; k++) issue(k, gw + k * nw, pb[k], pe[k]);
+    // the prologue reads only the sliced codes, the form bytes and the tables, which no kernel of a
+    // solve writes (build_sliced returns after they are complete); vectors are read after the wait
+    dep_wait();
+    dep_release();
+    if (skip && *skip) {
+        cp_async_wait<0>();
+        return;
+    }
+    int st = 0;
+    for (long sl = gw; sl < nsl; sl += nw) {
+        __syncwarp();
+        issue(st == 0 ? kSpStages - 1 : st - 1, sl + (kSpStages - 1) * nw, pb[kSpStages - 1], pe[kSpStages - 1]);
+        int bn, en;
+        ptrs(sl + kSpStages * nw, bn, en);
+        cp_async_wait<kSpStages - 1>();
+        const int b0 = pb[0], e0 = pe[0];
+        __syncwarp();
+        const int r = (int)(sl * kSliceRows) + lane;
+        const bool live = r < n;
+        const int rr = live ? r : n - 1;
+        const int nb = (e0 - b0) / kSliceBlock;
+        const unsigned char* sbase = stage0 + st * kSpStageBytes;
+        const unsigned sb = stage0_s + (unsigned)(st * kSpStageBytes);
+        AT o1 = 0, o2 = 0, o3 = 0;
+        if (live) {
+            if (OP == OP_AXPBY) {
+                if (beta != 0.0) o1 = (AT)y[r];
+            } else if (OP == OP_RESID) {
+                o1 = (AT)ld_stream(f + r);
+            } else {
+                o1 = (AT)ld_stream(f + r);
+                o2 = (AT)ld_stream(M + r);
+                o3 = (AT)ld_ro(x + r);
+            }
+        }
+        const unsigned pr = pat_sa + (unsigned)((int)sbase[lane] * W * (int)sizeof(short));
+        AT s = 0;
+        switch (nb) {
+        case 1: s = slpat_sum_fixed<1, T, XT, AT>(sb, pr, lane, rr, x, tab_s); break;
+        case 2: s = slpat_sum_fixed<2, T, XT, AT>(sb, pr, lane, rr, x, tab_s); break;
+        case 3: s = slpat_sum_fixed<3, T, XT, AT>(sb, pr, lane, rr, x, tab_s); break;
+        case 4: s = slpat_sum_fixed<4, T, XT, AT>(sb, pr, lane, rr, x, tab_s); break;
+        case 5: s = slpat_sum_fixed<5, T, XT, AT>(sb, pr, lane, rr, x, tab_s); break;
+        case 6: s = slpat_sum_fixed<6, T, XT, AT>(sb, pr, lane, rr, x, tab_s); break;
+        case 7: s = slpat_sum_fixed<7, T, XT, AT>(sb, pr, lane, rr, x, tab_s); break;
+        case 8: s = slpat_sum_fixed<8, T, XT, AT>(sb, pr, lane, rr, x, tab_s); break;
+        default: break;
+        }
+        if (live) {
+            if (OP == OP_AXPBY) {
+                AT o = (AT)alpha * s;
+                if (beta != 0.0) o += (AT)beta * o1;
+                y[r] = (YT)o;
+            } else if (OP == OP_RESID) {
+                y[r] = (YT)(o1 - s);
+            } else {
+                y[r] = (YT)(((-s + o1) / o2) + o3);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k + 1 < kSpStages; k++) {
+            pb[k] = pb[k + 1];
+            pe[k] = pe[k + 1];
+        }
+        pb[kSpStages - 1] = bn;
+        pe[kSpStages - 1] = en;
+        st = st == kSpStages - 1 ? 0 : st + 1;
+    }
+    cp_async_wait<0>();
+}
+
 // ---- building the sliced form from the CSR arrays ----
 
 // entries of slice s: 128 x the blocks of its longest row

@@ -242,6 +242,9 @@ static void launch_staged(int n, int64_t nnz, const int* row, const IT* col, VS 
 void release_sliced(DevCsr& A)
 {
     A.sliced = false;
+    A.sl_pid.release();
+    A.sl_pat.release();
+    A.npat = A.patw = 0;
     A.sl_ptr.release();
     A.sl_off.release();
     A.sl_col.release();
@@ -284,6 +287,7 @@ void build_sliced(DevCsr& A, cudaStream_t s)
         A.sl_col.alloc(std::max<long long>(total, 1), s);
         fill(k_sl_fill<int>, (const int*)A.col.p, A.sl_col.p);
     }
+    build_patterns(A, s);
     // the sliced kernels read the copy in their prologue, before their dependency wait (launch_dep),
     // so it is complete before the first of them is launched
     BCMGX_CUDA(cudaStreamSynchronize(s));
@@ -294,6 +298,23 @@ static void launch_sliced(const DevCsr& A, SlSrc<VS> sv, const XT* x, const FT* 
     double beta, const int* skip, cudaStream_t s)
 {
     const long nsl = ((long)A.n + kSliceRows - 1) / kSliceRows;
+    if constexpr (ValSrc<VS>::coded) {
+        if (A.sl_pid.p && A.npat > 0 && A.sl_code.p && sv.code == A.sl_code.p) {
+            // pattern-indexed rows: codes and form bytes streamed, offsets from the form table
+            using T = typename ValSrc<VS>::type;
+            auto kern = k_rowop_slpat<OP, T, XT, FT, MT, YT>;
+            const size_t smem = (((size_t)A.npat * A.patw * sizeof(short) + 15) & ~(size_t)15) +
+                (size_t)kSlWarps * kSpStages * kSpStageBytes;
+            ensure_smem_limit((const void*)kern, smem);
+            const int per_sm = blocks_per_sm((const void*)kern, kSlWarps * 32, smem);
+            const int grid = (int)std::max<long>(1, std::min<long>(ceil_div(nsl, kSlWarps), (long)per_sm * num_sms()));
+            launch_dep<0>(kern, grid, kSlWarps * 32, smem, s, A.n, A.sl_ptr.p, (const unsigned char*)A.sl_pid.p,
+                (const unsigned char*)sv.code, sv.tab, (const short*)A.sl_pat.p, A.npat, A.patw, x, f, M, y, alpha, beta,
+                skip);
+            BCMGX_CHECK_LAUNCH();
+            return;
+        }
+    }
     auto go = [&](auto* idx) {
         using IT = std::remove_const_t<std::remove_pointer_t<decltype(idx)>>;
         using C = SlStage<IT, VS>;

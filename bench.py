@@ -323,22 +323,25 @@ def vcycle_bytes(inf, pre, post, coarse):
     prolongation x += p x_c[agg]; the coarsest level runs `coarse` FP64 sweeps (the first from
     zero). Matrix entries
     count index_bytes + value bytes (1 where the level streams 1-byte value codes, else 4; 8 for the
-    coarsest level's FP64 values), vectors 4 bytes (8 on the coarsest level); level 0 also reads
-    the FP64 residual and writes the FP64 output."""
+    coarsest level's FP64 values; index_bytes 0, pattern-indexed rows, streams 1 byte per row instead),
+    vectors 4 bytes (8 on the coarsest level); level 0 also reads the FP64 residual and writes the FP64
+    output."""
     n, z, ib = inf["n"], inf["nnz"], inf["index_bytes"]
     vb = [1 if c else 4 for c in inf["value_codes"]]
     total = 0
     for l in range(len(n) - 1):
         nl, zl, nc = n[l], z[l], n[l + 1]
-        sweep = (ib[l] + vb[l]) * zl + 4 * (nl + 1) + 16 * nl
+        mat = (ib[l] + vb[l]) * zl + (nl if ib[l] == 0 else 0)
+        sweep = mat + 4 * (nl + 1) + 16 * nl
         total += (pre + post - 1) * sweep + 12 * nl
-        total += (ib[l] + vb[l]) * zl + 4 * (nl + 1) + 12 * nl
+        total += mat + 4 * (nl + 1) + 12 * nl
         total += 4 * (nc + 1) + 8 * nl + 4 * nl + 4 * nc
         total += 8 * nl + 4 * nc + 8 * nl
         if l == 0:
             total += 8 * nl + 4 * nl
     nL, zL = n[-1], z[-1]
-    total += (coarse - 1) * ((ib[-1] + (1 if inf["value_codes"][-1] else 8)) * zL + 4 * (nL + 1) + 32 * nL) + 24 * nL
+    total += (coarse - 1) * ((ib[-1] + (1 if inf["value_codes"][-1] else 8)) * zL + (nL if ib[-1] == 0 else 0)
+                             + 4 * (nL + 1) + 32 * nL) + 24 * nL
     return int(total)
 
 
@@ -444,14 +447,16 @@ def run_ours(a, wl, rank, world, local_rank):
     h64.free()
     peak, peak_kind = read_peaks()
     # algorithmic bytes of the format the kernels stream: int16 column offsets (2 B) where the
-    # level has them, else int32 (4 B); 1-byte value codes where the level has them, else the
-    # 4- or 8-byte values; bcmgx_spmv on raw CSR arrays always streams int32 + FP64
+    # level has them, else int32 (4 B), or with pattern-indexed rows (index bytes 0) one byte per
+    # row naming its offsets; 1-byte value codes where the level has them, else the 4- or 8-byte
+    # values; bcmgx_spmv on raw CSR arrays always streams int32 + FP64
     ib32, ib64 = inf32["index_bytes"][0], inf64["index_bytes"][0]
     vb32 = 1 if inf32["value_codes"][0] else 4
     vb64 = 1 if inf64["value_codes"][0] else 8
+    rb32, rb64 = (n if ib32 == 0 else 0), (n if ib64 == 0 else 0)
     bytes_spmv = 12 * nnz + 4 * (n + 1) + 16 * n
-    bytes_jac32 = (ib32 + vb32) * nnz + 4 * (n + 1) + 16 * n
-    bytes_jac64 = (ib64 + vb64) * nnz + 4 * (n + 1) + 32 * n
+    bytes_jac32 = (ib32 + vb32) * nnz + rb32 + 4 * (n + 1) + 16 * n
+    bytes_jac64 = (ib64 + vb64) * nnz + rb64 + 4 * (n + 1) + 32 * n
     bytes_jac32_csr = 8 * nnz + 4 * (n + 1) + 16 * n   # the same sweep on int32 columns + FP32 values
     gbs_spmv = bytes_spmv / (spmv_ms * 1e-3) / 1e9
     gbs_jac32 = bytes_jac32 / (k32["jacobi"] * 1e-3) / 1e9
@@ -527,15 +532,17 @@ def run_ours(a, wl, rank, world, local_rank):
                            "fp32_residual_ms": k32["residual"], "fp64_jacobi_ms": k64f["jacobi"],
                            "fp64_jacobi_gbs": gbs_jac64, "fcg_spmv_dots_ms": k64f["fcg_spmv_dots"],
                            # pw = A pv (row kernel) then the three dots (r, pw, oq against pv)
-                           "fcg_spmv_dots_gbs": ((ib64 + vb64) * nnz + 4 * (n + 1) + 48 * n) / (k64f["fcg_spmv_dots"] * 1e-3) / 1e9,
+                           "fcg_spmv_dots_gbs": ((ib64 + vb64) * nnz + rb64 + 4 * (n + 1) + 48 * n) / (k64f["fcg_spmv_dots"] * 1e-3) / 1e9,
                            "fp32_jacobi_fp64_out_ms": k32["jacobi_fp64_out"],
                            "fcg_update_ms": k32["fcg_update"],
                            "fcg_update_gbs": 80 * n / (k32["fcg_update"] * 1e-3) / 1e9},
         "kernels_coarse_levels_fp32_jacobi_ms": [round(k["jacobi"], 4) for k in lvl],
         "vcycle": vcycle_roofline(vc_ms, inf32, params("FP32"), peak, peak_kind),
-        "roofline": {"kernel": (kname0 + ("OP_JACOBI,Coded<float>>" if vb32 == 1 else "OP_JACOBI,float>")
+        "roofline": {"kernel": (("k_rowop_slpat<OP_JACOBI,float>" if (form0 == "sliced" and ib32 == 0) else
+                                 kname0 + ("OP_JACOBI,Coded<float>>" if vb32 == 1 else "OP_JACOBI,float>"))
                                 + " (FP32 l1-Jacobi sweep, level 0)"),
-                     "format": f"int{8 * ib32} columns, " + ("1-byte value codes" if vb32 == 1 else "FP32 values"),
+                     "format": ("pattern-indexed rows (1 byte per row)" if ib32 == 0 else f"int{8 * ib32} columns")
+                               + ", " + ("1-byte value codes" if vb32 == 1 else "FP32 values"),
                      "bound": "hbm", "achieved": gbs_jac32, "peak": peak, "unit": "GB/s",
                      "frac": gbs_jac32 / peak, "peak_kind": f"{peak_kind} hbm_gbs (copy)",
                      "bytes_per_launch": bytes_jac32,

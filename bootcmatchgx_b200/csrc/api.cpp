@@ -598,7 +598,7 @@ int bcmgx_hierarchy_get_info(const bcmgx_hierarchy* h, bcmgx_hierarchy_info* inf
             info->n[l] = h->lv[l].A.n;
             info->nnz[l] = h->lv[l].A.nnz;
             info->tpr[l] = h->lv[l].A.sliced ? kSlicedCode : h->lv[l].A.staged ? -h->lv[l].A.tpr : h->lv[l].A.tpr;
-            info->index_bytes[l] = h->lv[l].A.dcol.p ? 2 : 4;
+            info->index_bytes[l] = h->lv[l].A.sl_pid.p ? 0 : h->lv[l].A.dcol.p ? 2 : 4;
             info->value_codes[l] = h->lv[l].A.vcode.p ? h->lv[l].A.nvalues : 0;
         }
         info->op_cmplx = h->op_cmplx;

@@ -127,7 +127,8 @@ typedef struct bcmgx_hierarchy_info {
                                     staged kernel (matrix entries through shared memory) with -tpr;
                                     64: the sliced kernel (32-row slices, one thread per row) */
     int index_bytes[BCMGX_MAX_LEVELS]; /* column index bytes the solve kernels stream per entry
-                                          (2: int16 offsets from the diagonal, 4: int32) */
+                                          (2: int16 offsets from the diagonal, 4: int32; 0: pattern-
+                                          indexed rows, one byte per row naming the row's offsets) */
     int value_codes[BCMGX_MAX_LEVELS]; /* distinct values of a level whose solve kernels stream
                                           one-byte value codes (value-indexed CSR), else 0 */
 } bcmgx_hierarchy_info;

@@ -245,7 +245,6 @@ static bcmgx_hierarchy* setup_one(const bcmgx_csr* A, const bcmgx_params* p, int
     cudaEventElapsedTime(&ms, t0.e, t1.e);
     stage_fault_check();
     H->setup_ms = ms;
-    H->setup_done = true;
     return H.release();
 }
 

@@ -262,9 +262,6 @@ struct bcmgx_hierarchy {
     std::vector<bcmgx::SweepRecord> rec;
     int maxcoarsesize = 0, ftcoarse = 1;
     double op_cmplx = 0, op_wcmplx = 0, avg_cratio = 1, setup_ms = 0;
-    // set once bcmgx_setup has waited for its last kernel: from then on no kernel writes the level
-    // matrices, and the cycle's row kernels may read them before their dependency wait
-    bool setup_done = false;
     std::vector<int> grid_sweeps;
     std::vector<std::pair<std::string, double>> prof;   // set-up phase times (BCMGX_PROFILE=1)
     // solve workspace

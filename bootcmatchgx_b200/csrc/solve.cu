@@ -117,15 +117,6 @@ int fit_grid(const void* kernel, int threads, long need_blocks)
     return (int)std::max<long>(1, std::min<long>(need_blocks, (long)num_sms() * b));
 }
 
-// Set while Cycle::rowop launches the row kernels of a hierarchy whose set-up has finished: the
-// plain row kernel may then read its matrix before its dependency wait (k_rowop's `pre`).
-static thread_local bool t_rowop_pre = false;
-struct RowopPreScope {
-    bool old;
-    explicit RowopPreScope(bool on) : old(t_rowop_pre) { t_rowop_pre = on; }
-    ~RowopPreScope() { t_rowop_pre = old; }
-};
-
 // VS: the matrix values (ValSrc: a `const T*`, or Coded<T> for a value-indexed matrix).
 template <int OP, typename VS, typename XT, typename FT, typename MT, typename YT, typename IT>
 static void launch_rowop(int tpr, int n, const int* row, const IT* col, VS val, const XT* x, const FT* f,
@@ -134,8 +125,7 @@ static void launch_rowop(int tpr, int n, const int* row, const IT* col, VS val, 
     if (n <= 0) return;
     const long need = ((long)n * tpr + 255) / 256;
     auto go = [&](auto kern) {
-        launch_dep<0>(kern, fit_grid(kern, 256, need), 256, 0, s, n, row, col, val, x, f, M, y, alpha, beta, skip,
-            t_rowop_pre ? 1 : 0);
+        launch_dep<0>(kern, fit_grid(kern, 256, need), 256, 0, s, n, row, col, val, x, f, M, y, alpha, beta, skip);
     };
     switch (tpr) {
     case 1: go(k_rowop<1, OP, VS, XT, FT, MT, YT, IT>); break;
@@ -699,12 +689,8 @@ struct Cycle {
             rec->push_back(p);
             return;
         }
-        if (lk < 0) {
-            RowopPreScope pre(H->setup_done);
-            launch_rowop_A<OP>(A.tpr, A, val, x, f, M, y, 1.0, 0.0, skip, s);
-        } else {
-            launch_blk_rowop<OP>(A.n, A.m, 1 << lk, 1 << lk, A.row.p, A.col.p, val, x, f, M, y, 1.0, 0.0, skip, s);
-        }
+        if (lk < 0) launch_rowop_A<OP>(A.tpr, A, val, x, f, M, y, 1.0, 0.0, skip, s);
+        else launch_blk_rowop<OP>(A.n, A.m, 1 << lk, 1 << lk, A.row.p, A.col.p, val, x, f, M, y, 1.0, 0.0, skip, s);
     }
     template <typename FT, typename MT, typename YT, typename CT>
     void first(int n, const FT* f, const MT* M, YT* u, CT* fcopy) const

@@ -565,9 +565,11 @@ def run_ours(a, wl, rank, world, local_rank):
 # dram__bytes_write.sum of single launches) on the 27-point 100^3 case: the plain kernel with int32
 # columns and with int16 offsets, the staged kernel with int16 offsets (FP32 values, and one-byte
 # value codes), the sliced kernel with int16 offsets and codes (its padding included, its row
-# offsets not read); scaled by the algorithmic bytes to the other 27-point workloads.
+# offsets not read), the pattern-indexed sliced kernel (index bytes 0: its padding codes read, the
+# row offsets counted in the algorithmic bytes not read, part of x served by L2); scaled by the
+# algorithmic bytes to the other 27-point workloads.
 TRAFFIC_RATIO = {(4, 4, "plain"): 0.99983, (2, 4, "plain"): 1.00115, (2, 4, "staged"): 1.01173,
-                 (2, 1, "staged"): 0.99886, (2, 1, "sliced"): 0.99216}
+                 (2, 1, "staged"): 0.99886, (2, 1, "sliced"): 0.99216, (0, 1, "sliced"): 0.88800}
 
 
 def _spmv(row, col, val, x):
